@@ -1,0 +1,138 @@
+"""ctypes binding of ``libcpphf_b200.so`` (the C ABI declared in ``include/cpphf_b200.h``).
+
+Loading fails loudly: there is no CPU fallback anywhere in this package.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = Path(os.environ.get("CPPHF_B200_LIB", HERE / "libcpphf_b200.so"))
+
+CPPHF_OK = 0
+CPPHF_ERR_INVALID = -1
+CPPHF_ERR_CUDA = -2
+CPPHF_ERR_TIMEOUT = -3
+CPPHF_ERR_NONFINITE = -4
+CPPHF_ERR_UNSUPPORTED = -5
+
+i64 = C.c_int64
+i32 = C.c_int32
+f64 = C.c_double
+vp = C.c_void_p
+dp = C.POINTER(C.c_double)
+sz = C.c_size_t
+
+
+class Kernel(C.Structure):
+    """``cpphf_kernel`` (device pointers)."""
+
+    _fields_ = [
+        ("nk1", i64), ("nk2", i64), ("nb", i64), ("dv", i64),
+        ("include_hartree", i32), ("include_exchange", i32), ("exchange_hcp", i32),
+        ("has_refP", i32), ("has_contact", i32), ("n_contact", i32),
+        ("exchange_precision", i32), ("reserved0", i32),
+        ("T", f64), ("weight_sum", f64),
+        ("h", vp), ("VR", vp), ("refP", vp), ("w2d", vp), ("HH", vp),
+        ("contact_g", vp), ("contact_Oi", vp), ("contact_Oj", vp),
+    ]
+
+
+class DmConfig(C.Structure):
+    _fields_ = [
+        ("max_iter", i64), ("tol_E", f64), ("tol_grad", f64), ("plateau_window", i64),
+        ("denom_scale", f64), ("max_step", f64), ("cg_restart", i64), ("bt_shrink", f64),
+        ("bt_max", i64), ("mu_maxiter", i32), ("optimizer", i32),
+        ("block_sizes", C.POINTER(i64)), ("n_block_sizes", i64),
+    ]
+
+
+class DmResult(C.Structure):
+    _fields_ = [("mu", f64), ("energy", f64), ("n_iter", i64), ("converged", i32), ("reserved", i32)]
+
+
+class ScfConfig(C.Structure):
+    _fields_ = [
+        ("max_iter", i64), ("density_tol", f64), ("comm_tol", f64), ("mixing", f64),
+        ("level_shift", f64), ("acceleration", i32), ("reserved", i32),
+    ]
+
+
+class ScfResult(C.Structure):
+    _fields_ = [("energy", f64), ("mu", f64), ("iterations", i64), ("converged", i32), ("reserved", i32)]
+
+
+PROJECT_FN = C.CFUNCTYPE(C.c_int, vp, vp, i64, i64, i64, vp)
+
+# name -> (restype, argtypes)
+_SIGS = {
+    "cpphf_last_error": (C.c_char_p, []),
+    "cpphf_version": (C.c_int, []),
+    "cpphf_copy_d2h": (C.c_int, [vp, vp, sz, vp]),
+    "cpphf_copy_h2d": (C.c_int, [vp, vp, sz, vp]),
+    "cpphf_exchange_workspace_bytes": (sz, [i64, i64, i64, C.c_int, C.c_int]),
+    "cpphf_exchange": (C.c_int, [vp, vp, vp, vp, i64, i64, i64, i64, C.c_int, C.c_int, C.c_int,
+                                 vp, sz, vp]),
+    "cpphf_clear_fft_plan_cache": (C.c_int, []),
+    "cpphf_eigh_batched": (C.c_int, [vp, vp, vp, i64, i64, vp]),
+    "cpphf_eigh_block_sizes": (C.c_int, [vp, vp, vp, i64, i64, C.POINTER(i64), i64, C.c_int, vp]),
+    "cpphf_max_offblock_sizes": (C.c_int, [vp, i64, i64, C.POINTER(i64), i64, vp, vp]),
+    "cpphf_mu_workspace_bytes": (sz, [i64, i64]),
+    "cpphf_find_mu_bisection": (C.c_int, [vp, vp, i64, i64, f64, f64, C.c_int, vp, vp, sz, vp]),
+    "cpphf_solve_mu_inloop": (C.c_int, [vp, vp, i64, i64, f64, vp, f64, C.c_int, vp, vp, sz, vp]),
+    "cpphf_build_fock_workspace_bytes": (sz, [C.POINTER(Kernel)]),
+    "cpphf_build_fock": (C.c_int, [C.POINTER(Kernel), vp, vp, vp, vp, vp, vp, vp, sz, vp]),
+    "cpphf_cayley_spectral_setup": (C.c_int, [vp, vp, vp, i64, i64, vp]),
+    "cpphf_cayley_unitary": (C.c_int, [vp, vp, f64, vp, i64, i64, vp]),
+    "cpphf_diag_ufu": (C.c_int, [vp, vp, vp, f64, vp, i64, i64, vp]),
+    "cpphf_solve_dm_workspace_bytes": (sz, [C.POINTER(Kernel)]),
+    "cpphf_solve_dm": (C.c_int, [C.POINTER(Kernel), C.POINTER(DmConfig), vp, f64, PROJECT_FN, vp,
+                                 vp, vp, vp, vp, dp, dp, C.POINTER(DmResult), vp, sz, vp]),
+    "cpphf_solve_scf_workspace_bytes": (sz, [C.POINTER(Kernel)]),
+    "cpphf_solve_scf": (C.c_int, [C.POINTER(Kernel), C.POINTER(ScfConfig), vp, f64, PROJECT_FN, vp,
+                                  vp, vp, dp, dp, dp, C.POINTER(ScfResult), vp, sz, vp]),
+}
+
+_lib = None
+
+
+def load():
+    """Load the shared library once (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python -m cpp_hf_b200.build` "
+            "(this package has no CPU fallback)")
+    lib = C.CDLL(str(LIB_PATH))
+    for name, (res, args) in _SIGS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def exported_symbols():
+    """Names this binding expects the library to export."""
+    return sorted(_SIGS)
+
+
+class NativeError(RuntimeError):
+    pass
+
+
+def check(status: int, what: str = "") -> None:
+    """Map a C status to the reference's Python exception types."""
+    if status == CPPHF_OK:
+        return
+    msg = load().cpphf_last_error().decode(errors="replace")
+    if status == CPPHF_ERR_INVALID:
+        raise ValueError(msg)
+    if status == CPPHF_ERR_UNSUPPORTED:
+        raise NotImplementedError(msg)
+    raise NativeError(f"{what}: status {status}: {msg}")

@@ -1,0 +1,509 @@
+"""Drop-in ``cpp_hf._native`` backed by the B200 library (``libcpphf_b200.so``).
+
+Same 16 names, positional/keyword signatures, return tuples and error text as
+the pybind11 module of skilledwolf/cpp_hf (``cpp/cpp_hf_native.cpp:242-840``).
+NumPy inputs are copied to the current CUDA device once per call and results
+come back as NumPy arrays; ``torch`` CUDA tensors are used in place and results
+stay on the device as tensors.  Every computation runs in the CUDA library on
+``torch.cuda.current_stream()``; there is no CPU fallback.
+
+Outside the hot path and not built: the trust-region Newton optimiser
+(``optimizer=1``, ``_rtr_joint_hvp``, ``_deflation_bias``) and SCF DIIS / ODA
+acceleration raise ``NotImplementedError``.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check
+
+__all__ = [
+    "selfenergy_fft_full",
+    "clear_fft_plan_cache",
+    "eigh_batched",
+    "eigh_block_sizes",
+    "max_offblock_sizes",
+    "find_mu_bisection",
+    "build_fock_apply",
+    "solve_scf",
+    "solve_dm",
+    "_cayley_spectral_setup",
+    "_cayley_unitary_from_spectrum",
+    "_diag_UFU_from_spectrum",
+    "_rtr_joint_hvp",
+    "_deflation_bias",
+    "selfenergy_superlattice_streamed",
+    "resample_kgrid_2d",
+]
+
+# Exchange precision used by build_fock_apply / solve_* when the kernel_args
+# dict does not carry an "exchange_precision" entry (64 = complex128 FFT).
+DEFAULT_EXCHANGE_PRECISION = 64
+
+
+def _lib_handle():
+    if not torch.cuda.is_available():
+        raise RuntimeError("cpp_hf_b200 needs a CUDA device (no CPU fallback)")
+    return _lib.load()
+
+
+def _dev():
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+def _stream():
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else C.c_void_p(0)
+
+
+def _is_torch(x):
+    return isinstance(x, torch.Tensor)
+
+
+def _to_dev(x, kind):
+    """numpy/torch -> contiguous CUDA tensor ('c' complex128, 'f' float64, 'i' int64)."""
+    tdt = {"c": torch.complex128, "f": torch.float64, "i": torch.int64}[kind]
+    if _is_torch(x):
+        return x.to(device=_dev(), dtype=tdt).contiguous()
+    ndt = {"c": np.complex128, "f": np.float64, "i": np.int64}[kind]
+    a = np.ascontiguousarray(np.asarray(x), dtype=ndt)
+    return torch.from_numpy(a).to(_dev())
+
+
+def _out(t, as_numpy):
+    if t is None:
+        return None
+    return t.cpu().numpy() if as_numpy else t
+
+
+def _ws(nbytes):
+    return torch.empty(max(int(nbytes), 16), dtype=torch.uint8, device=_dev())
+
+
+def _sync():
+    torch.cuda.current_stream().synchronize()
+
+
+# ---------------------------------------------------------------------------
+# exchange
+# ---------------------------------------------------------------------------
+
+def _exchange(VR_t, P_t, apply_ifftshift, hcp, precision=64):
+    lib = _lib_handle()
+    nk1, nk2, nb = P_t.shape[0], P_t.shape[1], P_t.shape[2]
+    dv1, dv2 = VR_t.shape[2], VR_t.shape[3]
+    if hcp and (dv1 != 1 or dv2 != 1):
+        raise ValueError("hermitian_channel_packing requires VR with shape (...,1,1)")
+    if not ((dv1 == 1 and dv2 == 1) or (dv1 == nb and dv2 == nb)):
+        raise ValueError("VR shape must be (..., 1, 1) or (..., nb, nb).")
+    sigma = torch.empty_like(P_t)
+    need = lib.cpphf_exchange_workspace_bytes(nk1, nk2, nb, int(bool(hcp)), precision)
+    ws = _ws(need)
+    check(lib.cpphf_exchange(_ptr(P_t), None, _ptr(VR_t), _ptr(sigma), nk1, nk2, nb, dv1,
+                             int(bool(hcp)), int(bool(apply_ifftshift)), precision, _ptr(ws),
+                             ws.numel(), _stream()), "selfenergy_fft_full")
+    return sigma
+
+
+def selfenergy_fft_full(VR, P, apply_ifftshift=True, hermitian_channel_packing=False):
+    """cpp_hf_native.cpp:246-278."""
+    as_np = not _is_torch(P)
+    if np.ndim(P) != 4 if as_np else P.dim() != 4:
+        raise ValueError("P must be (nk1,nk2,nb,nb)")
+    if (np.ndim(VR) if not _is_torch(VR) else VR.dim()) != 4:
+        raise ValueError("VR must be (nk1,nk2,dv1,dv2)")
+    P_t = _to_dev(P, "c")
+    VR_t = _to_dev(VR, "c")
+    sigma = _exchange(VR_t, P_t, apply_ifftshift, hermitian_channel_packing)
+    return _out(sigma, as_np)
+
+
+def clear_fft_plan_cache():
+    """cpp_hf_native.cpp:280-284."""
+    check(_lib_handle().cpphf_clear_fft_plan_cache())
+
+
+# ---------------------------------------------------------------------------
+# eigh
+# ---------------------------------------------------------------------------
+
+def _check_square(M, name="M"):
+    if M.dim() < 2:
+        raise ValueError(f"{name} needs at least 2 dims")
+    if M.shape[-1] != M.shape[-2]:
+        raise ValueError(f"{name} last two dims must be square")
+
+
+def eigh_batched(M):
+    """cpp_hf_native.cpp:287-312."""
+    lib = _lib_handle()
+    as_np = not _is_torch(M)
+    M_t = _to_dev(M, "c")
+    _check_square(M_t)
+    nb = M_t.shape[-1]
+    batch = int(np.prod(M_t.shape[:-2])) if M_t.dim() > 2 else 1
+    w = torch.empty(M_t.shape[:-1], dtype=torch.float64, device=_dev())
+    V = torch.empty_like(M_t)
+    check(lib.cpphf_eigh_batched(_ptr(M_t), _ptr(w), _ptr(V), batch, nb, _stream()), "eigh_batched")
+    return _out(w, as_np), _out(V, as_np)
+
+
+def _sizes_arr(sizes):
+    s = [int(x) for x in sizes]
+    return (_lib.i64 * max(len(s), 1))(*s), len(s)
+
+
+def eigh_block_sizes(M, sizes, sort=True):
+    """cpp_hf_native.cpp:314-343."""
+    lib = _lib_handle()
+    as_np = not _is_torch(M)
+    M_t = _to_dev(M, "c")
+    if M_t.dim() < 2:
+        raise ValueError("M needs at least 2 dims")
+    nb = M_t.shape[-1]
+    if sum(int(x) for x in sizes) != nb:
+        raise ValueError("block sizes must sum to nb")
+    batch = int(np.prod(M_t.shape[:-2])) if M_t.dim() > 2 else 1
+    w = torch.empty(M_t.shape[:-1], dtype=torch.float64, device=_dev())
+    V = torch.empty_like(M_t)
+    arr, n = _sizes_arr(sizes)
+    check(lib.cpphf_eigh_block_sizes(_ptr(M_t), _ptr(w), _ptr(V), batch, nb, arr, n, int(bool(sort)),
+                                     _stream()), "eigh_block_sizes")
+    return _out(w, as_np), _out(V, as_np)
+
+
+def max_offblock_sizes(M, sizes):
+    """cpp_hf_native.cpp:345-358."""
+    lib = _lib_handle()
+    M_t = _to_dev(M, "c")
+    if M_t.dim() < 2:
+        raise ValueError("M needs at least 2 dims")
+    nb = M_t.shape[-1]
+    batch = int(np.prod(M_t.shape[:-2])) if M_t.dim() > 2 else 1
+    out = torch.zeros(1, dtype=torch.float64, device=_dev())
+    arr, n = _sizes_arr(sizes)
+    check(lib.cpphf_max_offblock_sizes(_ptr(M_t), batch, nb, arr, n, _ptr(out), _stream()),
+          "max_offblock_sizes")
+    return float(out.item())
+
+
+# ---------------------------------------------------------------------------
+# mu
+# ---------------------------------------------------------------------------
+
+def find_mu_bisection(bands, weights, n_e, T, maxiter=0):
+    """cpp_hf_native.cpp:361-377."""
+    lib = _lib_handle()
+    b = _to_dev(bands, "f")
+    w = _to_dev(weights, "f")
+    nb = b.shape[-1]
+    nk = int(np.prod(b.shape[:-1])) if b.dim() > 1 else 1
+    if w.numel() < nk:
+        raise ValueError("weights must have one entry per k-point of bands")
+    out = torch.zeros(1, dtype=torch.float64, device=_dev())
+    ws = _ws(lib.cpphf_mu_workspace_bytes(nk, nb))
+    check(lib.cpphf_find_mu_bisection(_ptr(b), _ptr(w), nk, nb, float(n_e), float(T), int(maxiter),
+                                      _ptr(out), _ptr(ws), ws.numel(), _stream()), "find_mu_bisection")
+    mu = float(out.item())
+    if not math.isfinite(mu):
+        raise _lib.NativeError("find_mu_bisection: device wait timed out or non-finite result")
+    return mu
+
+
+# ---------------------------------------------------------------------------
+# kernel view
+# ---------------------------------------------------------------------------
+
+class _DeviceKernel:
+    """Device copies of a kernel_args dict + the ``cpphf_kernel`` struct."""
+
+    def __init__(self, args, precision=None):
+        h = _to_dev(args["h"], "c")
+        if h.dim() != 4:
+            raise ValueError("h must be (nk1,nk2,nb,nb)")
+        nk1, nk2, nb = h.shape[0], h.shape[1], h.shape[2]
+        if h.shape[3] != nb:
+            raise ValueError("h last two axes must be square (nb,nb)")
+        VR = _to_dev(args["VR"], "c")
+        if VR.dim() != 4:
+            raise ValueError("VR must be (nk1,nk2,dv1,dv2)")
+        dv1, dv2 = VR.shape[2], VR.shape[3]
+        if not ((dv1 == 1 and dv2 == 1) or (dv1 == nb and dv2 == nb)):
+            raise ValueError("VR last two dims must be (1,1) or (nb,nb)")
+        has_refP = bool(args["has_refP"])
+        refP = None
+        if has_refP:
+            refP = _to_dev(args["refP"], "c")
+            if tuple(refP.shape) != (nk1, nk2, nb, nb):
+                raise ValueError("refP must match h shape when has_refP is true")
+        w2d = _to_dev(args["w2d"], "f").reshape(-1)
+        HH = _to_dev(args["HH"], "f").reshape(-1)
+        cg_host = np.asarray(args["contact_g"].cpu() if _is_torch(args["contact_g"]) else args["contact_g"],
+                             dtype=np.float64)
+        if cg_host.ndim != 1:
+            raise ValueError("contact_g must be 1-D")
+        n_contact = cg_host.shape[0]
+        has_contact = bool(np.any(cg_host != 0.0)) or n_contact > 1
+        cg = _to_dev(cg_host, "f")
+        cOi = _to_dev(args["contact_Oi"], "c")
+        cOj = _to_dev(args["contact_Oj"], "c")
+        if args.get("superlattice_fock_active", False) or args.get("superlattice_hartree_active", False):
+            raise NotImplementedError("superlattice kernel_args are not supported by this entry point yet")
+        prec = int(args.get("exchange_precision", precision or DEFAULT_EXCHANGE_PRECISION))
+        self._keep = [h, VR, refP, w2d, HH, cg, cOi, cOj]
+        self.shape = (nk1, nk2, nb)
+        K = _lib.Kernel()
+        K.nk1, K.nk2, K.nb, K.dv = nk1, nk2, nb, dv1
+        K.include_hartree = int(bool(args["include_hartree"]))
+        K.include_exchange = int(bool(args["include_exchange"]))
+        K.exchange_hcp = int(bool(args["exchange_hcp"]))
+        K.has_refP = int(has_refP)
+        K.has_contact = int(has_contact)
+        K.n_contact = n_contact
+        K.exchange_precision = prec
+        K.T = float(args["T"])
+        K.weight_sum = float(args["weight_sum"])
+        K.h, K.VR = h.data_ptr(), VR.data_ptr()
+        K.refP = refP.data_ptr() if refP is not None else None
+        K.w2d, K.HH = w2d.data_ptr(), HH.data_ptr()
+        K.contact_g, K.contact_Oi, K.contact_Oj = cg.data_ptr(), cOi.data_ptr(), cOj.data_ptr()
+        self.K = K
+
+    def ref(self):
+        return C.byref(self.K)
+
+
+def _host_project(project_fn, F):
+    """Apply a projector to a device field through the host (cpp_hf_native.cpp:215-238)."""
+    host = F.cpu().numpy()
+    out = np.ascontiguousarray(np.asarray(project_fn(host)), dtype=np.complex128)
+    if out.ndim != 4 or out.shape != host.shape:
+        raise RuntimeError("project_fn returned an array of wrong shape")
+    t = torch.from_numpy(out).to(F.device)
+    return 0.5 * (t + t.conj().transpose(-1, -2))
+
+
+def build_fock_apply(kernel_args, P, project_fn):
+    """cpp_hf_native.cpp:380-415 -> (Sigma, H, F, E)."""
+    lib = _lib_handle()
+    as_np = not _is_torch(P)
+    dk = _DeviceKernel(kernel_args)
+    P_t = _to_dev(P, "c")
+    nk1, nk2, nb = dk.shape
+    if tuple(P_t.shape) != (nk1, nk2, nb, nb):
+        raise ValueError("P must match h shape")
+    Sigma = torch.empty_like(P_t)
+    F = torch.empty_like(P_t)
+    H = torch.empty_like(P_t)
+    hd = torch.zeros(nb, dtype=torch.float64, device=_dev())
+    E = torch.zeros(1, dtype=torch.float64, device=_dev())
+    ws = _ws(lib.cpphf_build_fock_workspace_bytes(dk.ref()))
+    check(lib.cpphf_build_fock(dk.ref(), _ptr(P_t), _ptr(Sigma), _ptr(F), _ptr(hd), _ptr(E), _ptr(H),
+                               _ptr(ws), ws.numel(), _stream()), "build_fock_apply")
+    if project_fn is not None:
+        F = _host_project(project_fn, F)
+    return _out(Sigma, as_np), _out(H, as_np), _out(F, as_np), float(E.item())
+
+
+# ---------------------------------------------------------------------------
+# solvers
+# ---------------------------------------------------------------------------
+
+def _project_callback(project_fn, errors):
+    if project_fn is None:
+        return _lib.PROJECT_FN()
+    lib = _lib.load()
+
+    def cb(user, M, nk1, nk2, nb, stream):
+        try:
+            host = np.empty((nk1, nk2, nb, nb), dtype=np.complex128)
+            check(lib.cpphf_copy_d2h(host.ctypes.data, M, host.nbytes, stream), "project d2h")
+            out = np.ascontiguousarray(np.asarray(project_fn(host)), dtype=np.complex128)
+            if out.ndim != 4 or out.shape != host.shape:
+                raise RuntimeError("project_fn returned an array of wrong shape")
+            check(lib.cpphf_copy_h2d(M, out.ctypes.data, out.nbytes, stream), "project h2d")
+            return 0
+        except BaseException as exc:  # re-raised after the native call returns
+            errors.append(exc)
+            return 1
+
+    return _lib.PROJECT_FN(cb)
+
+
+def _raise_callback(errors):
+    if errors:
+        raise errors[0]
+
+
+def solve_dm(kernel_args, P0, n_e, max_iter, tol_E, tol_grad, max_step, bt_shrink, denom_scale, bt_max,
+             cg_restart, plateau_window, mu_maxiter, optimizer, tr_delta0, tr_cg_max, deflation_targets,
+             deflation_sigma, deflation_length, block_sizes, project_fn, return_Q, return_density,
+             return_fock):
+    """cpp_hf_native.cpp:488-582 (optimizer 0)."""
+    lib = _lib_handle()
+    if int(optimizer) == 1:
+        raise NotImplementedError("optimizer='newton' (trust-region Newton) is not built into cpp_hf_b200")
+    as_np = not _is_torch(P0)
+    dk = _DeviceKernel(kernel_args)
+    P0_t = _to_dev(P0, "c")
+    nk1, nk2, nb = dk.shape
+    max_iter = int(max_iter)
+    cfg = _lib.DmConfig()
+    cfg.max_iter = max_iter
+    cfg.tol_E, cfg.tol_grad = float(tol_E), float(tol_grad)
+    cfg.plateau_window = int(plateau_window)
+    cfg.denom_scale, cfg.max_step = float(denom_scale), float(max_step)
+    cfg.cg_restart, cfg.bt_shrink, cfg.bt_max = int(cg_restart), float(bt_shrink), int(bt_max)
+    cfg.mu_maxiter, cfg.optimizer = int(mu_maxiter), int(optimizer)
+    bs_arr, n_bs = _sizes_arr(block_sizes)
+    cfg.block_sizes = C.cast(bs_arr, C.POINTER(_lib.i64))
+    cfg.n_block_sizes = n_bs
+    Q = torch.empty_like(P0_t) if return_Q else None
+    D = torch.empty_like(P0_t) if return_density else None
+    F = torch.empty_like(P0_t) if return_fock else None
+    p = torch.empty((nk1, nk2, nb), dtype=torch.float64, device=_dev())
+    hE = np.zeros(max(max_iter, 1))
+    hG = np.zeros(max(max_iter, 1))
+    res = _lib.DmResult()
+    errors = []
+    cb = _project_callback(project_fn, errors)
+    ws = _ws(lib.cpphf_solve_dm_workspace_bytes(dk.ref()))
+    st = check(lib.cpphf_solve_dm(dk.ref(), C.byref(cfg), _ptr(P0_t), float(n_e), cb, None, _ptr(Q), _ptr(p),
+                                  _ptr(D), _ptr(F), hE.ctypes.data_as(_lib.dp), hG.ctypes.data_as(_lib.dp),
+                                  C.byref(res), _ptr(ws), ws.numel(), _stream()), "solve_dm")
+    _raise_callback(errors)
+    del st
+    _sync()
+    n = int(res.n_iter)
+    return (_out(Q, as_np), _out(p, as_np), _out(D, as_np), _out(F, as_np), float(res.mu),
+            float(res.energy), n, bool(res.converged), hE[:n].copy(), hG[:n].copy())
+
+
+def solve_scf(kernel_args, P0, n_e, max_iter, density_tol, comm_tol, mixing, level_shift, project_fn,
+              block_sizes, acceleration, diis_size, diis_start, diis_damping, trust_radius,
+              return_density, return_fock):
+    """cpp_hf_native.cpp:418-485 (linear mixing)."""
+    lib = _lib_handle()
+    acc = str(acceleration)
+    if acc not in ("linear", "diis", "oda"):
+        raise ValueError("SCFConfig.acceleration must be 'linear', 'diis', or 'oda'")
+    if acc != "linear":
+        raise NotImplementedError(f"SCF acceleration {acc!r} is not built into cpp_hf_b200")
+    if float(trust_radius) > 0.0:
+        raise NotImplementedError("SCF trust_radius is not built into cpp_hf_b200")
+    as_np = not _is_torch(P0)
+    dk = _DeviceKernel(kernel_args)
+    P0_t = _to_dev(P0, "c")
+    max_iter = int(max_iter)
+    cfg = _lib.ScfConfig()
+    cfg.max_iter = max_iter
+    cfg.density_tol, cfg.comm_tol = float(density_tol), float(comm_tol)
+    cfg.mixing, cfg.level_shift = float(mixing), float(level_shift)
+    cfg.acceleration = 0
+    D = torch.empty_like(P0_t) if return_density else None
+    F = torch.empty_like(P0_t) if return_fock else None
+    hE = np.zeros(max(max_iter, 1))
+    hD = np.zeros(max(max_iter, 1))
+    hC = np.zeros(max(max_iter, 1))
+    res = _lib.ScfResult()
+    errors = []
+    cb = _project_callback(project_fn, errors)
+    ws = _ws(lib.cpphf_solve_scf_workspace_bytes(dk.ref()))
+    check(lib.cpphf_solve_scf(dk.ref(), C.byref(cfg), _ptr(P0_t), float(n_e), cb, None, _ptr(D), _ptr(F),
+                              hE.ctypes.data_as(_lib.dp), hD.ctypes.data_as(_lib.dp),
+                              hC.ctypes.data_as(_lib.dp), C.byref(res), _ptr(ws), ws.numel(), _stream()),
+          "solve_scf")
+    _raise_callback(errors)
+    _sync()
+    n = int(res.iterations)
+    return (_out(D, as_np), _out(F, as_np), float(res.energy), float(res.mu), n, bool(res.converged),
+            hE[:n].copy(), hD[:n].copy(), hC[:n].copy())
+
+
+# ---------------------------------------------------------------------------
+# spectral Cayley hooks
+# ---------------------------------------------------------------------------
+
+def _cayley_spectral_setup(d):
+    """cpp_hf_native.cpp:585-609."""
+    lib = _lib_handle()
+    as_np = not _is_torch(d)
+    d_t = _to_dev(d, "c")
+    if d_t.dim() < 2:
+        raise ValueError("d needs at least 2 dims")
+    if d_t.shape[-1] != d_t.shape[-2]:
+        raise ValueError("d last two dims must match")
+    nb = d_t.shape[-1]
+    batch = int(np.prod(d_t.shape[:-2])) if d_t.dim() > 2 else 1
+    V = torch.empty_like(d_t)
+    lam = torch.empty(d_t.shape[:-1], dtype=torch.float64, device=_dev())
+    check(lib.cpphf_cayley_spectral_setup(_ptr(d_t), _ptr(V), _ptr(lam), batch, nb, _stream()),
+          "_cayley_spectral_setup")
+    return _out(V, as_np), _out(lam, as_np)
+
+
+def _cayley_unitary_from_spectrum(V, lam, tau):
+    """cpp_hf_native.cpp:611-630."""
+    lib = _lib_handle()
+    as_np = not _is_torch(V)
+    V_t = _to_dev(V, "c")
+    if V_t.dim() < 2:
+        raise ValueError("V needs at least 2 dims")
+    lam_t = _to_dev(lam, "f")
+    nb = V_t.shape[-1]
+    batch = int(np.prod(V_t.shape[:-2])) if V_t.dim() > 2 else 1
+    U = torch.empty_like(V_t)
+    check(lib.cpphf_cayley_unitary(_ptr(V_t), _ptr(lam_t), float(tau), _ptr(U), batch, nb, _stream()),
+          "_cayley_unitary_from_spectrum")
+    return _out(U, as_np)
+
+
+def _diag_UFU_from_spectrum(V, Ft_eig, lam, tau):
+    """cpp_hf_native.cpp:632-651."""
+    lib = _lib_handle()
+    as_np = not _is_torch(V)
+    V_t = _to_dev(V, "c")
+    if V_t.dim() < 2:
+        raise ValueError("V needs at least 2 dims")
+    Fe = _to_dev(Ft_eig, "c")
+    lam_t = _to_dev(lam, "f")
+    nb = V_t.shape[-1]
+    batch = int(np.prod(V_t.shape[:-2])) if V_t.dim() > 2 else 1
+    out = torch.empty(V_t.shape[:-1], dtype=torch.float64, device=_dev())
+    check(lib.cpphf_diag_ufu(_ptr(V_t), _ptr(Fe), _ptr(lam_t), float(tau), _ptr(out), batch, nb, _stream()),
+          "_diag_UFU_from_spectrum")
+    return _out(out, as_np)
+
+
+# ---------------------------------------------------------------------------
+# outside the hot path
+# ---------------------------------------------------------------------------
+
+def _rtr_joint_hvp(kernel_args, X, dp, Q, p, Ft):
+    """cpp_hf_native.cpp:654-694: trust-region Newton HVP (not built)."""
+    raise NotImplementedError("_rtr_joint_hvp (trust-region Newton) is not built into cpp_hf_b200")
+
+
+def _deflation_bias(P, targets, w2d, sigma, length):
+    """cpp_hf_native.cpp:697-716: deflation bias (not built)."""
+    raise NotImplementedError("_deflation_bias (trust-region Newton deflation) is not built into cpp_hf_b200")
+
+
+def selfenergy_superlattice_streamed(rho, VR_fft, g_a_off, pair_i, pair_j, pair_start, nkx, nky, n_G,
+                                     dim_orb, N_ext_x, N_ext_y, VR_fft_orbital=None, hermitian_rho=False):
+    """cpp_hf_native.cpp:719-816."""
+    raise NotImplementedError("selfenergy_superlattice_streamed is not built into cpp_hf_b200 yet")
+
+
+def resample_kgrid_2d(values, nk_new):
+    """cpp_hf_native.cpp:819-840."""
+    raise NotImplementedError("resample_kgrid_2d is not built into cpp_hf_b200 yet")

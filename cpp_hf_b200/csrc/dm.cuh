@@ -1,0 +1,46 @@
+// Internal interface of the direct-minimisation per-k kernels.
+#pragma once
+
+#include "common.cuh"
+
+namespace cpphf {
+
+constexpr int kDmMaxPartials = 1024;
+
+// Device-resident scalars of one DM iteration (written by last-block
+// reductions, read by later kernels of the same iteration).
+struct DmScalars {
+    double mu;         // current chemical potential
+    double mu_new;     // result of the in-loop mu solve
+    double energy;     // E of the current iteration
+    double grad_norm;
+    double lam_pc;
+    double beta;
+    double tau0, tau_cur, tau_final;
+    double omega0;
+    int accepted;
+    unsigned counter;  // last-block reduction counter (self-resetting)
+    double pad[2];
+    double part[3 * kDmMaxPartials];
+};
+
+int dm_check_nb(int64_t nb);
+int dm_density(const double2* Q, const double* p, double2* P, int64_t nk, int nb, cudaStream_t st);
+int dm_rotate(const double2* U, const double2* M, double2* Out, double* eps, int64_t nk, int nb, cudaStream_t st);
+int dm_q_times_u(double2* Q, const double2* U, int64_t nk, int nb, cudaStream_t st);
+int dm_occupations(const double* eps, const double* mu, double T_r, double* p, int64_t n, cudaStream_t st);
+int dm_gradient(const double2* Ft, const double* p, const double* eps, const double* w, double2* G, double* g_p,
+                int64_t nk, int nb, double T_r, double denom_scale, DmScalars* S, cudaStream_t st);
+int dm_pr_beta(const double2* G, const double2* Gp, const double* g_p, const double* g_pp, const double* eps,
+               const double* p, const double* w, int64_t nk, int nb, double T_r, int restart, int iter,
+               DmScalars* S, cudaStream_t st);
+int dm_direction(const double2* G, const double2* dQp, const double* g_p, const double* dpp, const double* eps,
+                 const double* p, const double* w, double2* dQ, double* d_p, int64_t nk, int nb, double T_r,
+                 double max_step, DmScalars* S, cudaStream_t st);
+int dm_trial(const double2* V, const double2* Fe, const double* lam, const double* p, const double* d_p,
+             const double* w, int64_t nk, int nb, double T_r, double shrink, int last_trial, double fallback,
+             DmScalars* S, cudaStream_t st);
+int dm_retract(double2* Q, const double2* V, const double2* Fe, const double* lam, double* ew, int64_t nk, int nb,
+               const DmScalars* S, cudaStream_t st);
+
+}  // namespace cpphf

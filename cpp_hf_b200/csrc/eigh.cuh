@@ -1,0 +1,24 @@
+// Internal interface of the batched Jacobi eigensolver.
+#pragma once
+
+#include "common.cuh"
+
+namespace cpphf {
+
+constexpr int kMaxEighNb = 80;
+
+// Optional block-diagonal structure (linalg.hpp:72-120): entries outside the
+// diagonal blocks are ignored; sort=0 orders eigenvalues block by block.
+struct BlockSpec {
+    int nblocks;
+    int sort;
+    short start[kMaxEighNb + 1];
+    unsigned char blk[kMaxEighNb];
+};
+
+// mode 0: eigh(herm(M)); mode 1: eigh(herm(i M)) (Cayley spectral setup).
+int eigh_batched(const double2* M, double* w, double2* V, int64_t batch, int64_t nb, int mode,
+                 const BlockSpec* bs, cudaStream_t st);
+int make_block_spec(int64_t nb, const int64_t* sizes, int64_t n_sizes, int sort, BlockSpec& bs);
+
+}  // namespace cpphf

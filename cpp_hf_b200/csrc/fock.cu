@@ -1,0 +1,324 @@
+// Fock assembly and Hartree-Fock energy (cpp_hf fock.hpp:34-383).
+//
+//   pre      (only with Hartree or contact terms): rho_bar = sum_k w_k (P - refP)
+//            by per-block partials + fixed-order final sum; then
+//            hartree_diag = HH n_vec (n_vec = Re diag rho_bar) and the contact
+//            self-energy SC = sum_t g_t [Oi tr(Oj rho_bar) - Oi rho_bar Oj].
+//   exchange Sigma = -IFFT2[FFT2(P - refP) VR] (exchange.cu), or zero.
+//   assemble one thread per (k, i<=j) pair: Sigma += SC,
+//            F = herm(h + Sigma + diag(hartree_diag)), energy partials
+//            w_k Re[h_ij P_ji + (Sigma_ij + H_ij)/2 (P - refP)_ji] (+ the
+//            mirrored term); optional dense H.
+//   energy   fixed-order sum of the block partials.
+#include "common.cuh"
+#include "exchange.cuh"
+#include "fock.cuh"
+
+#include <algorithm>
+#include <string>
+
+namespace cpphf {
+
+namespace {
+
+constexpr int kAsmThreads = 256;
+constexpr int kRedThreads = 256;
+constexpr int kMaxPartials = 2048;
+
+// rho_bar partials: grid (Gk, ceil(nb2 / CH)), CH channels per block, lanes =
+// blockDim / CH k-lanes.
+__global__ void k_rho_bar_partial(const double2* __restrict__ P, const double2* __restrict__ refP,
+                                  const double* __restrict__ w, int64_t nk, int nb2, int CH,
+                                  double2* __restrict__ part) {
+    __shared__ double2 acc_sh[kRedThreads];
+    const int lanes = blockDim.x / CH;
+    const int c_local = threadIdx.x % CH, lane = threadIdx.x / CH;
+    const int c = blockIdx.y * CH + c_local;
+    const int Gk = gridDim.x;
+    const int64_t per = (nk + Gk - 1) / Gk;
+    const int64_t k0 = (int64_t)blockIdx.x * per, k1 = min(nk, k0 + per);
+    double2 acc = mk(0.0, 0.0);
+    if (lane < lanes && c < nb2) {
+        for (int64_t k = k0 + lane; k < k1; k += lanes) {
+            double2 v = P[(size_t)k * nb2 + c];
+            if (refP) v = csub(v, refP[(size_t)k * nb2 + c]);
+            const double wk = w[k];
+            acc.x += wk * v.x;
+            acc.y += wk * v.y;
+        }
+    }
+    acc_sh[threadIdx.x] = acc;
+    __syncthreads();
+    if (lane == 0 && c < nb2) {
+        double2 s = acc;
+        for (int l = 1; l < lanes; ++l) s = cadd(s, acc_sh[l * CH + c_local]);
+        part[(size_t)blockIdx.x * nb2 + c] = s;
+    }
+}
+
+// Final: rho_bar, hartree_diag and the contact self-energy SC (single block).
+__global__ void k_hartree_contact(const double2* __restrict__ part, int Gk, int nb,
+                                  const double* __restrict__ HH, int include_hartree,
+                                  int has_contact, int n_contact, const double* __restrict__ cg,
+                                  const double2* __restrict__ Oi, const double2* __restrict__ Oj,
+                                  double2* __restrict__ rho_bar, double* __restrict__ hd,
+                                  double2* __restrict__ SC) {
+    const int nb2 = nb * nb;
+    for (int c = threadIdx.x; c < nb2; c += blockDim.x) {
+        double2 s = mk(0.0, 0.0);
+        for (int b = 0; b < Gk; ++b) s = cadd(s, part[(size_t)b * nb2 + c]);
+        rho_bar[c] = s;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+        double s = 0.0;
+        if (include_hartree)
+            for (int j = 0; j < nb; ++j) s += HH[i * nb + j] * rho_bar[j * nb + j].x;
+        hd[i] = s;
+    }
+    if (!has_contact) return;
+    // SC_ij = sum_t g [Oi_ij tr(Oj rho) - (Oi rho Oj)_ij]
+    __shared__ double2 tr_sh[64];
+    for (int c = threadIdx.x; c < nb2; c += blockDim.x) SC[c] = mk(0.0, 0.0);
+    __syncthreads();
+    for (int t = 0; t < n_contact; ++t) {
+        const double g = cg[t];
+        if (g == 0.0) continue;
+        const double2* oi = Oi + (size_t)t * nb2;
+        const double2* oj = Oj + (size_t)t * nb2;
+        if (threadIdx.x == 0) {
+            double2 tr = mk(0.0, 0.0);
+            for (int i = 0; i < nb; ++i)
+                for (int j = 0; j < nb; ++j) tr = cadd(tr, cmul(oj[i * nb + j], rho_bar[j * nb + i]));
+            tr_sh[0] = tr;
+        }
+        __syncthreads();
+        const double2 tr = tr_sh[0];
+        for (int c = threadIdx.x; c < nb2; c += blockDim.x) {
+            const int i = c / nb, j = c - i * nb;
+            // herm = Oi * tr * g ; fk = -g * (Oi rho Oj)
+            const double2 herm = cscale(cmul(oi[c], tr), g);
+            double2 orho_oj = mk(0.0, 0.0);
+            for (int l = 0; l < nb; ++l) {
+                double2 orho = mk(0.0, 0.0);
+                for (int m = 0; m < nb; ++m) orho = cadd(orho, cmul(oi[i * nb + m], rho_bar[m * nb + l]));
+                orho_oj = cadd(orho_oj, cmul(orho, oj[l * nb + j]));
+            }
+            const double2 fk = cscale(orho_oj, -g);
+            SC[c] = cadd(SC[c], cadd(herm, fk));
+        }
+        __syncthreads();
+    }
+}
+
+struct AsmArgs {
+    const double2* h;
+    double2* Sigma;
+    double2* F;
+    const double2* P;
+    const double2* refP;
+    const double* w;
+    const double* hd;     // may be null (no Hartree)
+    const double2* SC;    // may be null (no contact)
+    double2* Hdense;      // may be null
+    int64_t nk;
+    int nb;
+    double* part;         // energy partials [gridDim.x]
+};
+
+__global__ void __launch_bounds__(kAsmThreads) k_assemble(AsmArgs a) {
+    __shared__ double red[64];
+    const int nb = a.nb;
+    const int npair = nb * (nb + 1) / 2;
+    const int64_t total = a.nk * npair;
+    double e_acc[1] = {0.0};
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = t / npair;
+        int r = (int)(t - k * npair);
+        int i = 0;
+        while (r >= nb - i) {
+            r -= nb - i;
+            ++i;
+        }
+        const int j = i + r;
+        const size_t base = (size_t)k * nb * nb;
+        const size_t ij = base + (size_t)i * nb + j, ji = base + (size_t)j * nb + i;
+        double2 sij = a.Sigma[ij], sji = a.Sigma[ji];
+        if (a.SC) {
+            sij = cadd(sij, a.SC[i * nb + j]);
+            sji = cadd(sji, a.SC[j * nb + i]);
+            a.Sigma[ij] = sij;
+            if (i != j) a.Sigma[ji] = sji;
+        }
+        const double2 hij = a.h[ij], hji = a.h[ji];
+        double2 Aij = cadd(hij, sij), Aji = cadd(hji, sji);
+        const double hdi = a.hd ? a.hd[i] : 0.0;
+        if (i == j) {
+            Aij.x += hdi;
+            Aji = Aij;
+        }
+        const double2 f = mk(0.5 * (Aij.x + Aji.x), 0.5 * (Aij.y - Aji.y));
+        a.F[ij] = f;
+        if (i != j) a.F[ji] = cconj(f);
+        if (a.Hdense) {
+            a.Hdense[ij] = mk(i == j ? hdi : 0.0, 0.0);
+            if (i != j) a.Hdense[ji] = mk(0.0, 0.0);
+        }
+        // energy: w_k [Re(h_ij P_ji) + Re(inter_ij dP_ji)] (+ mirrored (j,i))
+        const double2 pji = a.P[ji], pij = a.P[ij];
+        double2 dji = pji, dij = pij;
+        if (a.refP) {
+            dji = csub(pji, a.refP[ji]);
+            dij = csub(pij, a.refP[ij]);
+        }
+        double2 iij = cscale(sij, 0.5);
+        if (i == j && a.hd) iij.x += 0.5 * hdi;
+        double s = (hij.x * pji.x - hij.y * pji.y) + (iij.x * dji.x - iij.y * dji.y);
+        if (i != j) {
+            const double2 iji = cscale(sji, 0.5);
+            s += (hji.x * pij.x - hji.y * pij.y) + (iji.x * dij.x - iji.y * dij.y);
+        }
+        e_acc[0] += a.w[k] * s;
+    }
+    block_sum<1>(e_acc, red);
+    if (threadIdx.x == 0) a.part[blockIdx.x] = e_acc[0];
+}
+
+__global__ void k_sum_partials(const double* __restrict__ part, int n, double* __restrict__ out) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double s = 0.0;
+        for (int b = 0; b < n; ++b) s += part[b];
+        *out = s;
+    }
+}
+
+struct FockWs {
+    size_t off_part, off_rho_part, off_rho_bar, off_sc, off_hd, off_exch, total;
+    int Gasm, Gk;
+};
+
+FockWs fock_ws_layout(const cpphf_kernel* K) {
+    FockWs L;
+    const int64_t nk = K->nk1 * K->nk2;
+    const int64_t nb = K->nb, nb2 = nb * nb;
+    const int64_t npair = nb * (nb + 1) / 2;
+    const int64_t need = (nk * npair + kAsmThreads - 1) / kAsmThreads;
+    L.Gasm = (int)std::max<int64_t>(1, std::min<int64_t>(need, std::min(kMaxPartials, 8 * num_sms())));
+    L.Gk = (int)std::max<int64_t>(1, std::min<int64_t>(nk, 2 * num_sms()));
+    size_t o = 0;
+    auto take = [&](size_t bytes) {
+        size_t at = o;
+        o += (bytes + 255) & ~(size_t)255;
+        return at;
+    };
+    L.off_part = take(sizeof(double) * kMaxPartials);
+    L.off_rho_part = take(sizeof(double2) * (size_t)L.Gk * nb2);
+    L.off_rho_bar = take(sizeof(double2) * nb2);
+    L.off_sc = take(sizeof(double2) * nb2);
+    L.off_hd = take(sizeof(double) * nb);
+    const int hcp = (K->exchange_hcp && K->dv == 1) ? 1 : 0;
+    L.off_exch = take(exchange_workspace_bytes(K->nk1, K->nk2, K->nb, hcp, K->exchange_precision));
+    L.total = o;
+    return L;
+}
+
+}  // namespace
+
+int validate_kernel(const cpphf_kernel* K) {
+    if (!K) return fail(CPPHF_ERR_INVALID, "kernel: null");
+    if (K->nk1 < 1 || K->nk2 < 1 || K->nb < 1) return fail(CPPHF_ERR_INVALID, "h must be (nk1,nk2,nb,nb)");
+    if (!(K->dv == 1 || K->dv == K->nb)) return fail(CPPHF_ERR_INVALID, "VR last two dims must be (1,1) or (nb,nb)");
+    if (!K->h || !K->w2d) return fail(CPPHF_ERR_INVALID, "kernel: null h or w2d");
+    if (K->include_exchange && !K->VR) return fail(CPPHF_ERR_INVALID, "kernel: null VR");
+    if (K->has_refP && !K->refP) return fail(CPPHF_ERR_INVALID, "refP must match h shape when has_refP is true");
+    if (K->include_hartree && !K->HH) return fail(CPPHF_ERR_INVALID, "kernel: null HH");
+    if (K->has_contact && (!K->contact_g || !K->contact_Oi || !K->contact_Oj || K->n_contact < 1))
+        return fail(CPPHF_ERR_INVALID, "kernel: contact arrays missing");
+    if (K->has_contact && K->nb > 64) return fail(CPPHF_ERR_UNSUPPORTED, "contact terms need nb <= 64");
+    if (K->exchange_precision != 32 && K->exchange_precision != 64)
+        return fail(CPPHF_ERR_INVALID, "kernel: exchange_precision must be 32 or 64");
+    return CPPHF_OK;
+}
+
+size_t build_fock_workspace_bytes(const cpphf_kernel* K) { return fock_ws_layout(K).total; }
+
+int build_fock(const cpphf_kernel* K, const double2* P, double2* Sigma, double2* F, double* hd_out,
+               double* energy, double2* Hdense, void* ws, size_t wsb, cudaStream_t st) {
+    CPPHF_TRY(validate_kernel(K));
+    if (!P || !Sigma || !F) return fail(CPPHF_ERR_INVALID, "build_fock: null pointer");
+    const FockWs L = fock_ws_layout(K);
+    if (!ws || wsb < L.total)
+        return fail(CPPHF_ERR_INVALID, "build_fock: workspace too small (" + std::to_string(L.total) + " bytes needed)");
+    unsigned char* W = static_cast<unsigned char*>(ws);
+    double* part = reinterpret_cast<double*>(W + L.off_part);
+    double2* rho_part = reinterpret_cast<double2*>(W + L.off_rho_part);
+    double2* rho_bar = reinterpret_cast<double2*>(W + L.off_rho_bar);
+    double2* SC = reinterpret_cast<double2*>(W + L.off_sc);
+    double* hd = hd_out ? hd_out : reinterpret_cast<double*>(W + L.off_hd);
+    const int64_t nk = K->nk1 * K->nk2;
+    const int nb = (int)K->nb, nb2 = nb * nb;
+    const double2* refP = K->has_refP ? static_cast<const double2*>(K->refP) : nullptr;
+    const bool need_pre = K->include_hartree || K->has_contact;
+    if (need_pre) {
+        const int CH = std::min(nb2, kRedThreads);
+        dim3 grid(L.Gk, (nb2 + CH - 1) / CH);
+        k_rho_bar_partial<<<grid, kRedThreads, 0, st>>>(P, refP, K->w2d, nk, nb2, CH, rho_part);
+        CPPHF_LAUNCH_CHECK("rho_bar partial");
+        k_hartree_contact<<<1, 256, 0, st>>>(rho_part, L.Gk, nb, K->HH, K->include_hartree,
+                                             K->has_contact, K->n_contact, K->contact_g,
+                                             static_cast<const double2*>(K->contact_Oi),
+                                             static_cast<const double2*>(K->contact_Oj), rho_bar,
+                                             hd, SC);
+        CPPHF_LAUNCH_CHECK("hartree/contact");
+    } else {
+        CPPHF_CUDA(cudaMemsetAsync(hd, 0, sizeof(double) * nb, st));
+    }
+    if (K->include_exchange) {
+        const int hcp = (K->exchange_hcp && K->dv == 1) ? 1 : 0;
+        CPPHF_TRY(exchange(P, refP, static_cast<const double2*>(K->VR), Sigma, K->nk1, K->nk2, K->nb,
+                           K->dv, hcp, 0, K->exchange_precision, W + L.off_exch,
+                           wsb - L.off_exch, st));
+    } else {
+        CPPHF_CUDA(cudaMemsetAsync(Sigma, 0, sizeof(double2) * (size_t)nk * nb2, st));
+    }
+    AsmArgs a;
+    a.h = static_cast<const double2*>(K->h);
+    a.Sigma = Sigma;
+    a.F = F;
+    a.P = P;
+    a.refP = refP;
+    a.w = K->w2d;
+    a.hd = K->include_hartree ? hd : nullptr;
+    a.SC = K->has_contact ? SC : nullptr;
+    a.Hdense = Hdense;
+    a.nk = nk;
+    a.nb = nb;
+    a.part = part;
+    k_assemble<<<L.Gasm, kAsmThreads, 0, st>>>(a);
+    CPPHF_LAUNCH_CHECK("assemble");
+    if (energy) {
+        k_sum_partials<<<1, 32, 0, st>>>(part, L.Gasm, energy);
+        CPPHF_LAUNCH_CHECK("energy sum");
+    }
+    return CPPHF_OK;
+}
+
+}  // namespace cpphf
+
+extern "C" {
+
+size_t cpphf_build_fock_workspace_bytes(const cpphf_kernel* K) {
+    return K ? cpphf::build_fock_workspace_bytes(K) : 0;
+}
+
+int cpphf_build_fock(const cpphf_kernel* K, const void* P, void* Sigma, void* F, double* hartree_diag,
+                     double* energy, void* H_dense, void* workspace, size_t workspace_bytes,
+                     void* stream) {
+    return cpphf::build_fock(K, static_cast<const double2*>(P), static_cast<double2*>(Sigma),
+                             static_cast<double2*>(F), hartree_diag, energy,
+                             static_cast<double2*>(H_dense), workspace, workspace_bytes,
+                             static_cast<cudaStream_t>(stream));
+}
+
+}  // extern "C"

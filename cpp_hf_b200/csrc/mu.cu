@@ -1,0 +1,220 @@
+// Chemical-potential solvers as one cooperative persistent kernel each
+// (cpp_hf utils.hpp:49-116).
+//
+// Every block owns a contiguous slice of the (nk*nb) eigenvalues.  Per
+// iteration a block reduces its slice (fixed tree) into a partial, the grid
+// meets at a bounded barrier, and every block then sums all partials in block
+// order and replays the reference's scalar update rule itself, so the whole
+// grid agrees on (lo, hi, mu) without a second barrier.  Partials are double
+// buffered by iteration parity.  Fixed iteration counts are kept exactly
+// (30 bisection steps by default, mu_maxiter Newton steps).
+#include "common.cuh"
+#include "mu.cuh"
+
+#include <mutex>
+
+namespace cpphf {
+
+namespace {
+
+constexpr int kMuThreads = 256;
+constexpr int kMuMaxGrid = 1024;
+
+__device__ __forceinline__ double expit(double x) {
+    if (x >= 0.0) return 1.0 / (1.0 + exp(-x));
+    const double e = exp(x);
+    return e / (1.0 + e);
+}
+
+struct MuArgs {
+    const double* eps;
+    const double* w;  // per-k weights
+    int64_t n;        // nk * nb
+    int nb;
+    double target;
+    const double* mu0;  // device warm start (newton) or null
+    double T;
+    int maxiter;
+    int mode;  // 0 bisection (utils.hpp:49-75), 1 in-loop newton (utils.hpp:79-116)
+    double* mu_out;
+    double* part;     // [2][grid][2]
+    unsigned* sync;   // [0] count [1] gen [2] error
+};
+
+__global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
+    __shared__ double red[64];
+    GridBarrier bar;
+    bar.init(a.sync);
+    const int G = gridDim.x;
+    const int64_t per = (a.n + G - 1) / G;
+    const int64_t b0 = (int64_t)blockIdx.x * per;
+    const int64_t b1 = min(a.n, b0 + per);
+
+    // 1. global min / max of eps
+    double lmin = INFINITY, lmax = -INFINITY;
+    for (int64_t i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
+        const double e = a.eps[i];
+        lmin = fmin(lmin, e);
+        lmax = fmax(lmax, e);
+    }
+    {
+        double v[2] = {-lmin, lmax};
+        // max-reduce through the sum scratch: use warp max then smem
+        v[0] = warp_max(v[0]);
+        v[1] = warp_max(v[1]);
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        if (lane == 0) {
+            red[wid] = v[0];
+            red[32 + wid] = v[1];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double m0 = -INFINITY, m1 = -INFINITY;
+            for (int i = 0; i < nw; ++i) {
+                m0 = fmax(m0, red[i]);
+                m1 = fmax(m1, red[32 + i]);
+            }
+            a.part[2 * blockIdx.x] = m0;
+            a.part[2 * blockIdx.x + 1] = m1;
+        }
+    }
+    if (!bar.wait()) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) *a.mu_out = NAN;
+        return;
+    }
+    double emin = INFINITY, emax = -INFINITY;
+    for (int b = 0; b < G; ++b) {
+        emin = fmin(emin, -__ldcg(&a.part[2 * b]));
+        emax = fmax(emax, __ldcg(&a.part[2 * b + 1]));
+    }
+    const double Tj = fmax(a.T, 1.0e-12);
+    double lo, hi, mu = 0.0;
+    if (a.mode == 0) {
+        const double span = emax - emin + 10.0 * fmax(Tj, 1.0e-6);
+        lo = emin - span;
+        hi = emax + span;
+    } else {
+        lo = emin - 50.0 * Tj;
+        hi = emax + 50.0 * Tj;
+        mu = fmin(fmax(*a.mu0, lo), hi);
+    }
+    const double Tfd = Tj + 1.0e-12;  // fermidirac_scalar(x, Tj) = expit(-x / (Tj + 1e-12))
+    for (int it = 0; it < a.maxiter; ++it) {
+        double* part = a.part + 2 * G + (size_t)(it & 1) * 2 * G;
+        const double mid = 0.5 * (lo + hi);
+        double v[2] = {0.0, 0.0};
+        for (int64_t i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
+            const double wk = a.w[i / a.nb];
+            const double e = a.eps[i];
+            if (a.mode == 0) {
+                v[0] += wk * expit(-(e - mid) / Tfd);
+            } else {
+                const double p = expit((mu - e) / Tj);
+                v[0] += wk * p;
+                v[1] += wk * p * (1.0 - p) / Tj;
+            }
+        }
+        block_sum<2>(v, red);
+        if (threadIdx.x == 0) {
+            part[2 * blockIdx.x] = v[0];
+            part[2 * blockIdx.x + 1] = v[1];
+        }
+        if (!bar.wait()) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) *a.mu_out = NAN;
+            return;
+        }
+        double N = 0.0, Z = 0.0;
+        for (int b = 0; b < G; ++b) {
+            N += __ldcg(&part[2 * b]);
+            Z += __ldcg(&part[2 * b + 1]);
+        }
+        if (a.mode == 0) {
+            if (N > a.target)
+                hi = mid;
+            else
+                lo = mid;
+        } else {
+            const double g = N - a.target;
+            if (g < 0.0) lo = mu;
+            if (g > 0.0) hi = mu;
+            const double Zs = fmax(Z, 1.0e-18);
+            double mn = mu - g / Zs;
+            const double mb = 0.5 * (lo + hi);
+            if (mn <= lo || mn >= hi) mn = mb;
+            mn = fmin(fmax(mn, lo), hi);
+            if (!isfinite(mn)) mn = mb;
+            mu = mn;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *a.mu_out = (a.mode == 0) ? 0.5 * (lo + hi) : mu;
+}
+
+int max_coop_grid() {
+    static int g = 0;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        int per = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_mu, kMuThreads, 0);
+        if (per < 1) per = 1;
+        g = std::min(kMuMaxGrid, per * num_sms());
+    });
+    return g;
+}
+
+}  // namespace
+
+size_t mu_workspace_bytes(int64_t, int64_t) {
+    return 64 + sizeof(double) * 6 * (size_t)kMuMaxGrid;
+}
+
+int mu_solve(const double* eps, const double* w, int64_t nk, int64_t nb, double target,
+             const double* mu0, double T, int maxiter, int mode, double* mu_out, void* ws,
+             size_t wsb, cudaStream_t st) {
+    if (nk < 1 || nb < 1) return fail(CPPHF_ERR_INVALID, "mu: empty eigenvalue array");
+    if (!eps || !w || !mu_out) return fail(CPPHF_ERR_INVALID, "mu: null pointer");
+    if (mode == 1 && !mu0) return fail(CPPHF_ERR_INVALID, "mu: null warm start");
+    if (!ws || wsb < mu_workspace_bytes(nk, nb)) return fail(CPPHF_ERR_INVALID, "mu: workspace too small");
+    const int64_t n = nk * nb;
+    int grid = (int)std::min<int64_t>(max_coop_grid(), (n + 4 * kMuThreads - 1) / (4 * kMuThreads));
+    if (grid < 1) grid = 1;
+    MuArgs a;
+    a.eps = eps;
+    a.w = w;
+    a.n = n;
+    a.nb = (int)nb;
+    a.target = target;
+    a.mu0 = mu0;
+    a.T = T;
+    a.maxiter = maxiter;
+    a.mode = mode;
+    a.mu_out = mu_out;
+    a.sync = reinterpret_cast<unsigned*>(ws);
+    a.part = reinterpret_cast<double*>(static_cast<unsigned char*>(ws) + 64);
+    CPPHF_CUDA(cudaMemsetAsync(ws, 0, 64, st));
+    void* args[] = {&a};
+    CPPHF_CUDA(cudaLaunchCooperativeKernel((const void*)k_mu, dim3(grid), dim3(kMuThreads), args, 0, st));
+    return CPPHF_OK;
+}
+
+}  // namespace cpphf
+
+extern "C" {
+
+size_t cpphf_mu_workspace_bytes(int64_t nk, int64_t nb) { return cpphf::mu_workspace_bytes(nk, nb); }
+
+int cpphf_find_mu_bisection(const double* eps, const double* weights, int64_t nk, int64_t nb,
+                            double n_e, double T, int maxiter, double* mu_out, void* workspace,
+                            size_t workspace_bytes, void* stream) {
+    if (maxiter <= 0) maxiter = 30;
+    return cpphf::mu_solve(eps, weights, nk, nb, n_e, nullptr, T, maxiter, 0, mu_out, workspace,
+                           workspace_bytes, static_cast<cudaStream_t>(stream));
+}
+
+int cpphf_solve_mu_inloop(const double* eps, const double* w_norm, int64_t nk, int64_t nb,
+                          double n_target_norm, const double* mu0, double T, int maxiter,
+                          double* mu_out, void* workspace, size_t workspace_bytes, void* stream) {
+    return cpphf::mu_solve(eps, w_norm, nk, nb, n_target_norm, mu0, T, maxiter, 1, mu_out, workspace,
+                           workspace_bytes, static_cast<cudaStream_t>(stream));
+}
+
+}  // extern "C"

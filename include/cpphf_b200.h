@@ -1,0 +1,226 @@
+/* cpphf_b200.h - C ABI of the B200 (sm_100a) Fock-build library.
+ *
+ * Drop-in device back end for cpp_hf's native operator module
+ * (cpp/cpp_hf_native.cpp of skilledwolf/cpp_hf).  Every entry point takes plain
+ * device pointers and sizes, runs on the given CUDA stream (NULL = legacy
+ * default stream), never allocates device memory (callers pass workspace
+ * sized by the matching *_workspace_bytes query) and returns a status code:
+ *
+ *   CPPHF_OK (0), CPPHF_ERR_INVALID (-1, maps to ValueError),
+ *   CPPHF_ERR_CUDA (-2), CPPHF_ERR_TIMEOUT (-3, a bounded device wait gave up),
+ *   CPPHF_ERR_NONFINITE (-4), CPPHF_ERR_UNSUPPORTED (-5).
+ *
+ * cpphf_last_error() returns the calling thread's last error text.
+ *
+ * Complex arrays are interleaved complex128 (double re, double im), C order,
+ * with the (nk1, nk2, nb, nb) layout of the reference (channel index fastest).
+ */
+#ifndef CPPHF_B200_H
+#define CPPHF_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CPPHF_ABI_VERSION 1
+
+#define CPPHF_OK 0
+#define CPPHF_ERR_INVALID -1
+#define CPPHF_ERR_CUDA -2
+#define CPPHF_ERR_TIMEOUT -3
+#define CPPHF_ERR_NONFINITE -4
+#define CPPHF_ERR_UNSUPPORTED -5
+
+const char* cpphf_last_error(void);
+int cpphf_version(void);
+
+/* Synchronous host <-> device copies on `stream` (for projector callbacks). */
+int cpphf_copy_d2h(void* dst_host, const void* src_device, size_t bytes, void* stream);
+int cpphf_copy_h2d(void* dst_device, const void* src_host, size_t bytes, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Exchange self-energy.  Replaces _native.selfenergy_fft_full
+ * (cpp/cpp_hf_native.cpp:246-278 -> selfenergy.hpp:83-171).
+ *   Sigma = -IFFT2[FFT2(P - refP) * VR], VR of orbital width dv (1 or nb);
+ *   hcp = Hermitian upper-triangle packing (requires dv == 1);
+ *   apply_ifftshift as selfenergy.hpp:174-190; precision 64 (complex128
+ *   throughout) or 32 (complex64 FFT, complex128 in/out).
+ *   refP may be NULL; Sigma may alias P.
+ * ---------------------------------------------------------------------- */
+size_t cpphf_exchange_workspace_bytes(int64_t nk1, int64_t nk2, int64_t nb, int hcp,
+                                      int precision);
+int cpphf_exchange(const void* P, const void* refP, const void* VR, void* Sigma, int64_t nk1,
+                   int64_t nk2, int64_t nb, int64_t dv, int hcp, int apply_ifftshift,
+                   int precision, void* workspace, size_t workspace_bytes, void* stream);
+/* Replaces _native.clear_fft_plan_cache (cpp_hf_native.cpp:280-284).  Plans
+ * hold no device memory here (twiddles are built per block), so it is a no-op. */
+int cpphf_clear_fft_plan_cache(void);
+
+/* ------------------------------------------------------------------------
+ * Batched Hermitian eigendecomposition.  Replaces _native.eigh_batched
+ * (cpp_hf_native.cpp:287-312 -> linalg.hpp:39-66): hermitise, then ascending
+ * eigenvalues w (batch, nb) and eigenvector columns V (batch, nb, nb).
+ * Cyclic complex Jacobi, one warp (nb <= 16) or one CTA per matrix.
+ * ---------------------------------------------------------------------- */
+int cpphf_eigh_batched(const void* M, double* w, void* V, int64_t batch, int64_t nb, void* stream);
+/* Replaces _native.eigh_block_sizes (cpp_hf_native.cpp:314-343 ->
+ * linalg.hpp:72-120).  sizes is a HOST array of n_sizes positive block sizes. */
+int cpphf_eigh_block_sizes(const void* M, double* w, void* V, int64_t batch, int64_t nb,
+                           const int64_t* sizes, int64_t n_sizes, int sort, void* stream);
+/* Replaces _native.max_offblock_sizes (cpp_hf_native.cpp:345-358 ->
+ * linalg.hpp:123-140).  Writes the result to the device scalar *out. */
+int cpphf_max_offblock_sizes(const void* M, int64_t batch, int64_t nb, const int64_t* sizes,
+                             int64_t n_sizes, double* out, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Chemical potential.  Replaces _native.find_mu_bisection
+ * (cpp_hf_native.cpp:361-377 -> utils.hpp:49-75) and the in-loop
+ * Newton-in-bracket solver of utils.hpp:79-116.  eps (nk, nb) and weights (nk)
+ * are device arrays; the result goes to the device scalar *mu_out.  Both run
+ * as one cooperative persistent kernel with bounded grid barriers.
+ * ---------------------------------------------------------------------- */
+size_t cpphf_mu_workspace_bytes(int64_t nk, int64_t nb);
+int cpphf_find_mu_bisection(const double* eps, const double* weights, int64_t nk, int64_t nb,
+                            double n_e, double T, int maxiter, double* mu_out, void* workspace,
+                            size_t workspace_bytes, void* stream);
+/* mu0 is a device scalar (the warm start). */
+int cpphf_solve_mu_inloop(const double* eps, const double* w_norm, int64_t nk, int64_t nb,
+                          double n_target_norm, const double* mu0, double T, int maxiter,
+                          double* mu_out, void* workspace, size_t workspace_bytes, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Kernel view: POD mirror of HFKernel (cpp/include/cpp_hf/kernel.hpp:10-84)
+ * with DEVICE pointers.  has_contact is fock.hpp:25-29 evaluated by the caller
+ * (any contact_g != 0 or n_contact > 1).  exchange_precision: 64 or 32.
+ * ---------------------------------------------------------------------- */
+typedef struct cpphf_kernel {
+    int64_t nk1, nk2, nb;
+    int64_t dv;
+    int32_t include_hartree;
+    int32_t include_exchange;
+    int32_t exchange_hcp;
+    int32_t has_refP;
+    int32_t has_contact;
+    int32_t n_contact;
+    int32_t exchange_precision;
+    int32_t reserved0;
+    double T;
+    double weight_sum;
+    const void* h;          /* complex128 (nk1, nk2, nb, nb) */
+    const void* VR;         /* complex128 (nk1, nk2, dv, dv) */
+    const void* refP;       /* complex128 (nk1, nk2, nb, nb) or NULL */
+    const double* w2d;      /* (nk1, nk2) */
+    const double* HH;       /* (nb, nb) */
+    const double* contact_g;  /* (n_contact) */
+    const void* contact_Oi;   /* complex128 (n_contact, nb, nb) */
+    const void* contact_Oj;   /* complex128 (n_contact, nb, nb) */
+} cpphf_kernel;
+
+/* ------------------------------------------------------------------------
+ * Fock build.  Replaces _native.build_fock_apply (cpp_hf_native.cpp:380-415 ->
+ * fock.hpp:34-351): Sigma, F = herm(h + Sigma + diag(H) + contact), the
+ * k-independent Hartree diagonal hartree_diag (nb) and the energy
+ * E = sum_k w_k Re Tr[h P + (Sigma + H)(P - refP)/2] (device scalar *energy).
+ * H_dense (complex128 field, may be NULL) receives the dense Hartree term.
+ * ---------------------------------------------------------------------- */
+size_t cpphf_build_fock_workspace_bytes(const cpphf_kernel* K);
+int cpphf_build_fock(const cpphf_kernel* K, const void* P, void* Sigma, void* F,
+                     double* hartree_diag, double* energy, void* H_dense, void* workspace,
+                     size_t workspace_bytes, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Spectral Cayley helpers of the direct-minimisation solver.  Replace
+ * _native._cayley_spectral_setup, _cayley_unitary_from_spectrum and
+ * _diag_UFU_from_spectrum (cpp_hf_native.cpp:585-651 -> solver_dm.hpp:206-303).
+ * ---------------------------------------------------------------------- */
+int cpphf_cayley_spectral_setup(const void* d, void* V, double* lam, int64_t batch, int64_t nb,
+                                void* stream);
+int cpphf_cayley_unitary(const void* V, const double* lam, double tau, void* U, int64_t batch,
+                         int64_t nb, void* stream);
+int cpphf_diag_ufu(const void* V, const void* Ft_eig, const double* lam, double tau,
+                   double* diag, int64_t batch, int64_t nb, void* stream);
+
+
+/* ------------------------------------------------------------------------
+ * Solvers.  The optional projector callback replaces the Python project_fn
+ * of the reference (cpp_hf_native.cpp:215-238): it receives a DEVICE field
+ * (nk1, nk2, nb, nb) on `stream`, must overwrite it in place before
+ * returning, and returns 0 on success.
+ * ---------------------------------------------------------------------- */
+typedef int (*cpphf_project_fn)(void* user, void* M, int64_t nk1, int64_t nk2, int64_t nb,
+                                void* stream);
+
+/* SolverConfig of solver_dm.hpp:22-63 (optimizer 0 = preconditioned CG;
+ * block_sizes is a HOST array, validated as the reference does and otherwise
+ * ignored: the dense path returns the same density). */
+typedef struct cpphf_dm_config {
+    int64_t max_iter;
+    double tol_E;
+    double tol_grad;
+    int64_t plateau_window;
+    double denom_scale;
+    double max_step;
+    int64_t cg_restart;
+    double bt_shrink;
+    int64_t bt_max;
+    int32_t mu_maxiter;
+    int32_t optimizer;
+    const int64_t* block_sizes;
+    int64_t n_block_sizes;
+} cpphf_dm_config;
+
+typedef struct cpphf_dm_result {
+    double mu;
+    double energy;
+    int64_t n_iter;
+    int32_t converged;
+    int32_t reserved;
+} cpphf_dm_result;
+
+/* Replaces _native.solve_dm (cpp_hf_native.cpp:488-582 -> solver_dm.hpp:392-653).
+ * Q_out, density_out, fock_out (device fields) may be NULL; p_out (device,
+ * (nk1, nk2, nb)); hist_E / hist_grad are HOST arrays of max_iter doubles. */
+size_t cpphf_solve_dm_workspace_bytes(const cpphf_kernel* K);
+int cpphf_solve_dm(const cpphf_kernel* K, const cpphf_dm_config* cfg, const void* P0, double n_e,
+                   cpphf_project_fn project, void* project_user, void* Q_out, double* p_out,
+                   void* density_out, void* fock_out, double* hist_E, double* hist_grad,
+                   cpphf_dm_result* result, void* workspace, size_t workspace_bytes,
+                   void* stream);
+
+/* SCFConfig of solver_scf.hpp:20-50; acceleration 0 = linear mixing. */
+typedef struct cpphf_scf_config {
+    int64_t max_iter;
+    double density_tol;
+    double comm_tol;
+    double mixing;
+    double level_shift;
+    int32_t acceleration;
+    int32_t reserved;
+} cpphf_scf_config;
+
+typedef struct cpphf_scf_result {
+    double energy;
+    double mu;
+    int64_t iterations;
+    int32_t converged;
+    int32_t reserved;
+} cpphf_scf_result;
+
+/* Replaces _native.solve_scf (cpp_hf_native.cpp:418-485 -> solver_scf.hpp:156-444).
+ * density_out / fock_out device fields (may be NULL); hist_* HOST arrays of
+ * max_iter doubles. */
+size_t cpphf_solve_scf_workspace_bytes(const cpphf_kernel* K);
+int cpphf_solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const void* P0, double n_e,
+                    cpphf_project_fn project, void* project_user, void* density_out,
+                    void* fock_out, double* hist_E, double* hist_density, double* hist_comm,
+                    cpphf_scf_result* result, void* workspace, size_t workspace_bytes,
+                    void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CPPHF_B200_H */

@@ -1,0 +1,90 @@
+"""Pin the oracle against the reference's own tests and stored regression data.
+
+Test infrastructure.  Runs in a container where the reference checkout is
+present (default ``/root/reference``; override with ``CPPHF_REFERENCE``):
+
+1. the reference's pytest suite (``tests/``) with ``oracle.native_np`` installed
+   as ``cpp_hf._native`` (tests of the trust-region Newton / deflation
+   optimiser and the ``contimod``-gated regression are outside this build's
+   scope and are deselected by name);
+2. the stored SCF regression case ``tests/data/meshgrid_regression_case_v1.npz``
+   through the reference's own ``cpp_hf.solve_scf`` with the same settings as
+   ``examples/contimod_example_meshgrid_offline.py:36-60``, checked at 1e-6.
+
+Usage: ``python -m oracle.pin_reference_suite``  (exit code 0 = pinned).
+"""
+
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+REPO = Path(__file__).resolve().parents[1]
+REF = Path(os.environ.get("CPPHF_REFERENCE", "/root/reference"))
+
+# Outside the hot-path scope: optimizer="newton" (solver_rtr.hpp) and the
+# deflation driver built on it.
+DESELECT = ["test_solver_rtr.py", "test_deflation.py"]
+
+
+def run_suite() -> int:
+    env = dict(os.environ)
+    env["PYTHONPATH"] = os.pathsep.join([str(REPO), str(REF / "src"), env.get("PYTHONPATH", "")])
+    env["PYTHONDONTWRITEBYTECODE"] = "1"
+    cmd = [sys.executable, "-m", "pytest", str(REF / "tests"), "-q", "-p", "no:cacheprovider",
+           "-p", "oracle._inject_native", "--rootdir", str(REF / "tests")]
+    for name in DESELECT:
+        cmd += ["--ignore", str(REF / "tests" / name)]
+    print("$", " ".join(cmd), flush=True)
+    return subprocess.call(cmd, env=env, cwd=str(REPO))
+
+
+def run_meshgrid_case() -> int:
+    sys.path.insert(0, str(REPO))
+    sys.path.insert(0, str(REF / "src"))
+    import numpy as np
+    from oracle import native_np
+
+    sys.modules["cpp_hf._native"] = native_np
+    import cpp_hf
+
+    d = np.load(REF / "tests" / "data" / "meshgrid_regression_case_v1.npz")
+    kernel = cpp_hf.HartreeFockKernel(
+        weights=d["weights"], hamiltonian=d["hamiltonian"], coulomb_q=d["coulomb_q"],
+        T=float(d["T"]), include_hartree=True, include_exchange=True,
+        reference_density=d["reference_density"], hartree_matrix=d["hartree_matrix"])
+    res = cpp_hf.solve_scf(kernel, np.asarray(d["P0"]), float(d["electrondensity0"]),
+                           config=cpp_hf.SCFConfig(max_iter=int(d["max_iter"]),
+                                                   density_tol=float(d["comm_tol"]),
+                                                   comm_tol=float(d["comm_tol"]), mixing=0.5))
+    P_exp = d["P_expected"].astype(np.complex128)
+    dP = float(np.max(np.abs(res.density_matrix - P_exp)))
+    dF = float(np.max(np.abs(res.fock_matrix - d["F_expected"])))
+    dmu = abs(float(res.chemical_potential) - float(d["mu_expected"]))
+    dC0 = abs(float(res.history["commutator_residual"][0]) - float(d["hist_dC_expected"][0]))
+    # The v1 fixture stores energies in the older convention
+    # E_v1 = sum_k w_k Re Tr[h P + (Sigma + H) P / 2]  (P, not P - refP, in the
+    # interaction term); it is recomputed here from the oracle's own Fock parts.
+    from cpp_hf.solver import _kernel_args_for_native
+    S, H, _F, _E = native_np.build_fock_apply(_kernel_args_for_native(kernel), P_exp, None)
+    w = kernel.w2d
+
+    def tr(A, B):
+        return float(np.sum(w * np.real(np.einsum("...ij,...ji->...", A, B))))
+
+    E_v1 = tr(kernel.h, P_exp) + 0.5 * tr(S + H, P_exp)
+    dE = abs(E_v1 - float(d["E_expected"]))
+    print(f"meshgrid case: iterations {res.iterations} (stored {int(d['k_expected'])}, "
+          f"advisory: the stored run used the v1 DIIS settings), max|dP| {dP:.2e}, "
+          f"max|dF| {dF:.2e}, |dmu| {dmu:.2e}, |dE_v1| {dE:.2e}, |d dC[0]| {dC0:.2e}")
+    ok = dP <= 1e-6 and dF <= 1e-6 and dE <= 1e-6 and dmu <= 1e-6 and dC0 <= 1e-6
+    print("meshgrid case:", "PASS" if ok else "FAIL")
+    return 0 if ok else 1
+
+
+if __name__ == "__main__":
+    rc1 = run_suite()
+    rc2 = run_meshgrid_case()
+    sys.exit(rc1 or rc2)
