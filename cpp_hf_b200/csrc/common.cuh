@@ -40,6 +40,21 @@ int cuda_fail(cudaError_t e, const char* where);
 
 int num_sms();
 
+// Raise a kernel's dynamic shared-memory limit to the device opt-in maximum
+// minus its static shared memory.  Attribute calls never leave a sticky error.
+template <class F>
+inline void raise_smem(F f) {
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, f) == cudaSuccess) {
+        const int want = optin - (int)fa.sharedSizeBytes;
+        if (want > 0) cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, want);
+    }
+    (void)cudaGetLastError();
+}
+
 // ---------------------------------------------------------------------------
 // Complex arithmetic
 // ---------------------------------------------------------------------------

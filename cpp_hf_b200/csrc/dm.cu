@@ -417,7 +417,7 @@ __global__ void k_q_times_u(double2* Q, const double2* __restrict__ U, int64_t n
 
 template <class Kfn>
 void set_max_smem(Kfn f) {
-    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    raise_smem(f);
 }
 
 void init_attrs() {

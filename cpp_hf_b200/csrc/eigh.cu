@@ -285,8 +285,8 @@ int eigh_batched(const double2* M, double* w, double2* V, int64_t batch, int64_t
     }
     static std::once_flag once;
     std::call_once(once, [] {
-        cudaFuncSetAttribute(k_eigh<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-        cudaFuncSetAttribute(k_eigh<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        raise_smem(k_eigh<true>);
+        raise_smem(k_eigh<false>);
     });
     if (nb <= kWarpTeamMaxNb) {
         const size_t smem = eigh_smem((int)nb, true);

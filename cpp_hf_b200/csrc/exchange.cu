@@ -5,17 +5,24 @@
 // owns one full FFT line for a block of CB consecutive channels:
 //   A  rows:    load P[kx, :, chunk] (- refP), FFT along ky              -> T
 //   B  columns: load T[:, ky, chunk], FFT along kx, * VR, IFFT along kx   -> T
-//                (optional ifftshift of the kx axis applied on the store)
+//               (optional ifftshift of the kx axis applied on the store)
 //   C  rows:    load T[kx, :, chunk], IFFT along ky, * (-1/(nk1 nk2))     -> Sigma
-//                (optional ifftshift of ky; HCP unpack + conjugate mirror)
+//               (optional ifftshift of ky; HCP unpack + conjugate mirror)
 // For the full FP64 path T aliases Sigma (every CTA reads its whole tile
 // before writing it), so the compulsory DRAM traffic is P + VR + Sigma and the
-// intermediate round trips stay in L2 (P and VR are streamed with evict-first
-// loads).  HCP (upper-triangle packing) and the complex64 form use a
-// workspace field for T.
+// intermediate round trips go through L2 (P and VR are streamed with
+// evict-first loads).  HCP (upper-triangle packing) and the complex64 form use
+// a workspace field for T.
+//
+// Line lengths with a register codelet (fft_reg.cuh: 1..6, 8, 9, 12, 16, 18,
+// 24, 32, 36, 48, 64, 72, 96, 128, 144, 192, 256, 288) run the four-step
+// transform with global loads/stores straight from/to registers and one
+// shared-memory transpose per direction; any other length runs the generic
+// out-of-place Stockham stages of fft.cuh.
 #include "common.cuh"
-#include "fft.cuh"
 #include "exchange.cuh"
+#include "fft.cuh"
+#include "fft_reg.cuh"
 
 #include <algorithm>
 #include <mutex>
@@ -25,7 +32,9 @@ namespace cpphf {
 
 namespace {
 
-// channel -> (row, col) offsets for the HCP packing, built per CTA in smem.
+constexpr int kTargetThreads = 256;
+
+// channel -> (row, col) of the HCP packing (upper triangle, row-major).
 __device__ __forceinline__ void hcp_pair(int ch, int nb, int& i, int& j) {
     int r = 0, c = ch;
     while (c >= nb - r) {
@@ -35,44 +44,6 @@ __device__ __forceinline__ void hcp_pair(int ch, int nb, int& i, int& j) {
     i = r;
     j = r + c;
 }
-
-struct Tile {
-    int CB;       // channels per tile
-    int threads;  // block size
-    size_t smem;  // dynamic shared memory bytes
-};
-
-template <class Cx>
-Tile pick_tile(const FftPlan1D& pl, int C) {
-    const int n = pl.n;
-    const int cbmax = std::max(1, std::min(C, (kEptMax * 256) / std::max(n, 1)));
-    const int nch = (C + cbmax - 1) / cbmax;
-    const int CB = (C + nch - 1) / nch;
-    int threads = (n * CB + kEptMax - 1) / kEptMax;
-    threads = ((threads + 31) / 32) * 32;
-    threads = std::max(64, std::min(1024, threads));
-    Tile t;
-    t.CB = CB;
-    t.threads = threads;
-    t.smem = sizeof(Cx) * (size_t)n + sizeof(Cx) * (size_t)n * CB * (pl.generic ? 2 : 1) +
-             sizeof(int) * 2 * (size_t)CB;
-    return t;
-}
-
-// Dynamic smem layout: [tw n][buf n*CB][alt n*CB if generic][map 2*CB ints]
-template <class Cx>
-struct SmemView {
-    Cx* tw;
-    Cx* buf;
-    Cx* alt;
-    int* map;  // map[2c] = source offset within the nb*nb block, map[2c+1] = mirror (or -1)
-    __device__ SmemView(unsigned char* base, const FftPlan1D& pl, int CB) {
-        tw = reinterpret_cast<Cx*>(base);
-        buf = tw + pl.n;
-        alt = pl.generic ? buf + (size_t)pl.n * CB : nullptr;
-        map = reinterpret_cast<int*>(buf + (size_t)pl.n * CB * (pl.generic ? 2 : 1));
-    }
-};
 
 __device__ __forceinline__ void build_map(int* map, int chunk0, int CB, int C, int nb, int hcp) {
     for (int c = threadIdx.x; c < CB; c += blockDim.x) {
@@ -93,15 +64,197 @@ __device__ __forceinline__ void build_map(int* map, int chunk0, int CB, int C, i
     }
 }
 
-// Pass A: rows forward.
 template <class Cx>
-__global__ void k_rows_fwd(const double2* __restrict__ P, const double2* __restrict__ refP,
-                           Cx* T, ExchangeGeom g, FftPlan1D pl, int CB) {
+__device__ __forceinline__ Cx czero() {
+    return mk((decltype(Cx{}.x))0, (decltype(Cx{}.x))0);
+}
+
+// ===========================================================================
+// Specialised four-step kernels (N = N1 * N2 with register codelets)
+// smem: tw[N] | S[N * CB] | map[2 * CB]
+// ===========================================================================
+template <class Cx>
+struct SView {
+    Cx* tw;
+    Cx* S;
+    int* map;
+    __device__ SView(unsigned char* base, int N, int CB) {
+        tw = reinterpret_cast<Cx*>(base);
+        S = tw + N;
+        map = reinterpret_cast<int*>(S + (size_t)N * CB);
+    }
+};
+
+template <class Cx, int N1, int N2>
+__global__ void __launch_bounds__(256) k_rows_fwd_s(const double2* __restrict__ P, const double2* __restrict__ refP,
+                                                     Cx* T, ExchangeGeom g, int CB) {
+    constexpr int N = N1 * N2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    SmemView<Cx> s(smem_raw, pl, CB);
-    const int kx = blockIdx.x;
-    const int chunk0 = blockIdx.y * CB;
-    const int n = pl.n;  // == n1
+    SView<Cx> s(smem_raw, N, CB);
+    const int kx = blockIdx.x, chunk0 = blockIdx.y * CB;
+    const int c = threadIdx.x % CB, a = threadIdx.x / CB;
+    build_line_twiddles(s.tw, N);
+    build_map(s.map, chunk0, CB, g.C, g.nb, g.hcp);
+    __syncthreads();
+    const size_t nb2 = (size_t)g.nb * g.nb;
+    const int off = s.map[2 * c];
+    if (a < N2) {
+        Cx v[N1];
+#pragma unroll
+        for (int n1 = 0; n1 < N1; ++n1) {
+            double2 x = mk(0.0, 0.0);
+            if (off >= 0) {
+                const size_t idx = ((size_t)kx * g.n1 + (N2 * n1 + a)) * nb2 + off;
+                x = ld_stream(P + idx);
+                if (refP) x = csub(x, ld_stream(refP + idx));
+            }
+            v[n1] = to_c(x, Cx{});
+        }
+        dft<N1, false>(v);
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1) s.S[(k1 * N2 + a) * CB + c] = cmul(v[k1], s.tw[a * k1]);
+    }
+    __syncthreads();
+    if (a < N1) {
+        Cx u[N2];
+#pragma unroll
+        for (int n2 = 0; n2 < N2; ++n2) u[n2] = s.S[(a * N2 + n2) * CB + c];
+        dft<N2, false>(u);
+        const int ch = chunk0 + c;
+        if (ch < g.C) {
+#pragma unroll
+            for (int k2 = 0; k2 < N2; ++k2) st_l2(T + ((size_t)kx * g.n1 + (a + N1 * k2)) * g.Ct + ch, u[k2]);
+        }
+    }
+}
+
+template <class Cx, int N1, int N2>
+__global__ void __launch_bounds__(256) k_cols_conv_s(Cx* T, const double2* __restrict__ VR, ExchangeGeom g, int CB) {
+    constexpr int N = N1 * N2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SView<Cx> s(smem_raw, N, CB);
+    const int ky = blockIdx.x, chunk0 = blockIdx.y * CB;
+    const int c = threadIdx.x % CB, a = threadIdx.x / CB;
+    const int ch = chunk0 + c;
+    const bool live = ch < g.C;
+    build_line_twiddles(s.tw, N);
+    __syncthreads();
+    if (a < N2) {
+        Cx v[N1];
+#pragma unroll
+        for (int n1 = 0; n1 < N1; ++n1)
+            v[n1] = live ? ld_l2(T + ((size_t)(N2 * n1 + a) * g.n1 + ky) * g.Ct + ch) : czero<Cx>();
+        dft<N1, false>(v);
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1) s.S[(k1 * N2 + a) * CB + c] = cmul(v[k1], s.tw[a * k1]);
+    }
+    __syncthreads();
+    Cx u[N2];
+    if (a < N1) {
+#pragma unroll
+        for (int n2 = 0; n2 < N2; ++n2) u[n2] = s.S[(a * N2 + n2) * CB + c];
+        dft<N2, false>(u);
+        // u[k2] = X[a + N1 k2]: multiply by VR at kx = a + N1 k2
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) {
+            if (live) {
+                const size_t vi = ((size_t)(a + N1 * k2) * g.n1 + ky) * g.dv + (g.dv == 1 ? 0 : ch);
+                u[k2] = cmul(u[k2], to_c(ld_stream(VR + vi), Cx{}));
+            }
+        }
+        dft<N2, true>(u);
+    }
+    __syncthreads();
+    if (a < N1) {
+#pragma unroll
+        for (int na = 0; na < N2; ++na) s.S[(a * N2 + na) * CB + c] = cmulc(u[na], s.tw[na * a]);
+    }
+    __syncthreads();
+    if (a < N2) {
+        Cx v[N1];
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1) v[k1] = s.S[(k1 * N2 + a) * CB + c];
+        dft<N1, true>(v);
+        if (live) {
+            const int s0 = g.shift ? g.n0 / 2 : 0;
+#pragma unroll
+            for (int nbx = 0; nbx < N1; ++nbx) {
+                const int kx = a + N2 * nbx;
+                const int dx = (kx - s0 + g.n0) % g.n0;
+                st_l2(T + ((size_t)dx * g.n1 + ky) * g.Ct + ch, v[nbx]);
+            }
+        }
+    }
+}
+
+template <class Cx, int N1, int N2>
+__global__ void __launch_bounds__(256) k_rows_inv_s(const Cx* T, double2* Sigma, ExchangeGeom g, int CB, double scale) {
+    constexpr int N = N1 * N2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SView<Cx> s(smem_raw, N, CB);
+    const int kx = blockIdx.x, chunk0 = blockIdx.y * CB;
+    const int c = threadIdx.x % CB, a = threadIdx.x / CB;
+    const int ch = chunk0 + c;
+    const bool live = ch < g.C;
+    build_line_twiddles(s.tw, N);
+    build_map(s.map, chunk0, CB, g.C, g.nb, g.hcp);
+    __syncthreads();
+    if (a < N1) {
+        Cx u[N2];
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2)
+            u[k2] = live ? ld_l2(T + ((size_t)kx * g.n1 + (a + N1 * k2)) * g.Ct + ch) : czero<Cx>();
+        dft<N2, true>(u);
+#pragma unroll
+        for (int na = 0; na < N2; ++na) s.S[(a * N2 + na) * CB + c] = cmulc(u[na], s.tw[na * a]);
+    }
+    __syncthreads();
+    if (a < N2) {
+        Cx v[N1];
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1) v[k1] = s.S[(k1 * N2 + a) * CB + c];
+        dft<N1, true>(v);
+        const int off = s.map[2 * c], mir = s.map[2 * c + 1];
+        if (off >= 0) {
+            const size_t nb2 = (size_t)g.nb * g.nb;
+            const int s1 = g.shift ? g.n1 / 2 : 0;
+#pragma unroll
+            for (int nbx = 0; nbx < N1; ++nbx) {
+                const int ky = a + N2 * nbx;
+                const int dy = (ky - s1 + g.n1) % g.n1;
+                const double2 val = cscale(to_d(v[nbx]), scale);
+                double2* dst = Sigma + ((size_t)kx * g.n1 + dy) * nb2;
+                dst[off] = val;
+                if (mir >= 0) dst[mir] = cconj(val);
+            }
+        }
+    }
+}
+
+// ===========================================================================
+// Generic kernels (any line length)
+// smem: tw[n] | buf[n * CB] | alt[n * CB] | map[2 * CB]
+// ===========================================================================
+template <class Cx>
+struct GView {
+    Cx* tw;
+    Cx* buf;
+    Cx* alt;
+    int* map;
+    __device__ GView(unsigned char* base, int n, int CB) {
+        tw = reinterpret_cast<Cx*>(base);
+        buf = tw + n;
+        alt = buf + (size_t)n * CB;
+        map = reinterpret_cast<int*>(alt + (size_t)n * CB);
+    }
+};
+
+template <class Cx>
+__global__ void k_rows_fwd_g(const double2* __restrict__ P, const double2* __restrict__ refP, Cx* T, ExchangeGeom g,
+                             FftPlan1D pl, int CB) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    GView<Cx> s(smem_raw, pl.n, CB);
+    const int kx = blockIdx.x, chunk0 = blockIdx.y * CB, n = pl.n;
     build_twiddles(s.tw, n);
     build_map(s.map, chunk0, CB, g.C, g.nb, g.hcp);
     __syncthreads();
@@ -126,23 +279,17 @@ __global__ void k_rows_fwd(const double2* __restrict__ P, const double2* __restr
     }
 }
 
-// Pass B: columns forward, * VR, columns inverse (in place on T).
 template <class Cx>
-__global__ void k_cols_conv(Cx* T, const double2* __restrict__ VR, ExchangeGeom g, FftPlan1D pl,
-                            int CB) {
+__global__ void k_cols_conv_g(Cx* T, const double2* __restrict__ VR, ExchangeGeom g, FftPlan1D pl, int CB) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    SmemView<Cx> s(smem_raw, pl, CB);
-    const int ky = blockIdx.x;
-    const int chunk0 = blockIdx.y * CB;
-    const int n = pl.n;  // == n0
+    GView<Cx> s(smem_raw, pl.n, CB);
+    const int ky = blockIdx.x, chunk0 = blockIdx.y * CB, n = pl.n;
     build_twiddles(s.tw, n);
     __syncthreads();
     for (int e = threadIdx.x; e < n * CB; e += blockDim.x) {
         const int nx = e / CB, c = e - nx * CB;
         const int ch = chunk0 + c;
-        Cx v = mk((decltype(Cx{}.x))0, (decltype(Cx{}.x))0);
-        if (ch < g.C) v = ld_l2(T + ((size_t)nx * g.n1 + ky) * g.Ct + ch);
-        s.buf[e] = v;
+        s.buf[e] = (ch < g.C) ? ld_l2(T + ((size_t)nx * g.n1 + ky) * g.Ct + ch) : czero<Cx>();
     }
     __syncthreads();
     Cx* r = fft_tile<false>(s.buf, s.alt, s.tw, pl, CB);
@@ -151,8 +298,7 @@ __global__ void k_cols_conv(Cx* T, const double2* __restrict__ VR, ExchangeGeom 
         const int ch = chunk0 + c;
         if (ch < g.C) {
             const size_t vi = ((size_t)nx * g.n1 + ky) * g.dv + (g.dv == 1 ? 0 : ch);
-            const double2 w = ld_stream(VR + vi);
-            r[e] = cmul(r[e], to_c(w, Cx{}));
+            r[e] = cmul(r[e], to_c(ld_stream(VR + vi), Cx{}));
         }
     }
     __syncthreads();
@@ -166,24 +312,18 @@ __global__ void k_cols_conv(Cx* T, const double2* __restrict__ VR, ExchangeGeom 
     }
 }
 
-// Pass C: rows inverse, scale, unpack into Sigma.
 template <class Cx>
-__global__ void k_rows_inv(const Cx* T, double2* Sigma, ExchangeGeom g, FftPlan1D pl, int CB,
-                           double scale) {
+__global__ void k_rows_inv_g(const Cx* T, double2* Sigma, ExchangeGeom g, FftPlan1D pl, int CB, double scale) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    SmemView<Cx> s(smem_raw, pl, CB);
-    const int kx = blockIdx.x;
-    const int chunk0 = blockIdx.y * CB;
-    const int n = pl.n;  // == n1
+    GView<Cx> s(smem_raw, pl.n, CB);
+    const int kx = blockIdx.x, chunk0 = blockIdx.y * CB, n = pl.n;
     build_twiddles(s.tw, n);
     build_map(s.map, chunk0, CB, g.C, g.nb, g.hcp);
     __syncthreads();
     for (int e = threadIdx.x; e < n * CB; e += blockDim.x) {
         const int ny = e / CB, c = e - ny * CB;
         const int ch = chunk0 + c;
-        Cx v = mk((decltype(Cx{}.x))0, (decltype(Cx{}.x))0);
-        if (ch < g.C) v = ld_l2(T + ((size_t)kx * g.n1 + ny) * g.Ct + ch);
-        s.buf[e] = v;
+        s.buf[e] = (ch < g.C) ? ld_l2(T + ((size_t)kx * g.n1 + ny) * g.Ct + ch) : czero<Cx>();
     }
     __syncthreads();
     Cx* r = fft_tile<true>(s.buf, s.alt, s.tw, pl, CB);
@@ -202,39 +342,165 @@ __global__ void k_rows_inv(const Cx* T, double2* Sigma, ExchangeGeom g, FftPlan1
     }
 }
 
+// ===========================================================================
+// launch plumbing
+// ===========================================================================
+struct Launch {
+    int CB;
+    int threads;
+    size_t smem;
+    int nchunk;
+};
+
+// channels per tile so that a CTA has about kTargetThreads threads; chunks balanced.
+Launch plan_launch(int lanes, int C, size_t elem, int n, bool generic) {
+    Launch L;
+    const int cbmax = std::max(1, std::min(C, kTargetThreads / std::max(lanes, 1)));
+    const int nch = (C + cbmax - 1) / cbmax;
+    L.CB = (C + nch - 1) / nch;
+    L.nchunk = (C + L.CB - 1) / L.CB;
+    int threads = generic ? std::min(1024, std::max(64, n * L.CB)) : lanes * L.CB;
+    threads = std::min(1024, ((threads + 31) / 32) * 32);
+    L.threads = threads;
+    L.smem = elem * (size_t)n + elem * (size_t)n * L.CB * (generic ? 2 : 1) + sizeof(int) * 2 * (size_t)L.CB;
+    return L;
+}
+
+template <class Cx, int N1, int N2>
+struct Spec {
+    static void attrs() {
+        static std::once_flag once;
+        std::call_once(once, [] {
+            raise_smem(k_rows_fwd_s<Cx, N1, N2>);
+            raise_smem(k_cols_conv_s<Cx, N1, N2>);
+            raise_smem(k_rows_inv_s<Cx, N1, N2>);
+        });
+    }
+    static int rows_fwd(const double2* P, const double2* refP, Cx* T, const ExchangeGeom& g, cudaStream_t st) {
+        attrs();
+        const Launch L = plan_launch(N1 > N2 ? N1 : N2, g.C, sizeof(Cx), N1 * N2, false);
+        k_rows_fwd_s<Cx, N1, N2><<<dim3(g.n0, L.nchunk), L.threads, L.smem, st>>>(P, refP, T, g, L.CB);
+        CPPHF_LAUNCH_CHECK("exchange rows forward");
+        return CPPHF_OK;
+    }
+    static int cols(Cx* T, const double2* VR, const ExchangeGeom& g, cudaStream_t st) {
+        attrs();
+        const Launch L = plan_launch(N1 > N2 ? N1 : N2, g.C, sizeof(Cx), N1 * N2, false);
+        k_cols_conv_s<Cx, N1, N2><<<dim3(g.n1, L.nchunk), L.threads, L.smem, st>>>(T, VR, g, L.CB);
+        CPPHF_LAUNCH_CHECK("exchange columns convolve");
+        return CPPHF_OK;
+    }
+    static int rows_inv(const Cx* T, double2* Sigma, const ExchangeGeom& g, double scale, cudaStream_t st) {
+        attrs();
+        const Launch L = plan_launch(N1 > N2 ? N1 : N2, g.C, sizeof(Cx), N1 * N2, false);
+        k_rows_inv_s<Cx, N1, N2><<<dim3(g.n0, L.nchunk), L.threads, L.smem, st>>>(T, Sigma, g, L.CB, scale);
+        CPPHF_LAUNCH_CHECK("exchange rows inverse");
+        return CPPHF_OK;
+    }
+};
+
 template <class Cx>
-void set_smem_attrs() {
-    static std::once_flag once;
-    std::call_once(once, [] {
-        const int mx = 227 * 1024;
-        cudaFuncSetAttribute(k_rows_fwd<Cx>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-        cudaFuncSetAttribute(k_cols_conv<Cx>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-        cudaFuncSetAttribute(k_rows_inv<Cx>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-    });
+struct Gen {
+    static void attrs() {
+        static std::once_flag once;
+        std::call_once(once, [] {
+            raise_smem(k_rows_fwd_g<Cx>);
+            raise_smem(k_cols_conv_g<Cx>);
+            raise_smem(k_rows_inv_g<Cx>);
+        });
+    }
+};
+
+#define CPPHF_SPEC_SIZES(X) \
+    X(1, 1, 1)              \
+    X(2, 2, 1)              \
+    X(3, 3, 1)              \
+    X(4, 4, 1)              \
+    X(5, 5, 1)              \
+    X(6, 3, 2)              \
+    X(8, 4, 2)              \
+    X(9, 3, 3)              \
+    X(12, 4, 3)             \
+    X(16, 4, 4)             \
+    X(18, 6, 3)             \
+    X(24, 6, 4)             \
+    X(32, 8, 4)             \
+    X(36, 6, 6)             \
+    X(48, 8, 6)             \
+    X(64, 8, 8)             \
+    X(72, 9, 8)             \
+    X(96, 12, 8)            \
+    X(128, 16, 8)           \
+    X(144, 12, 12)          \
+    X(192, 16, 12)          \
+    X(256, 16, 16)          \
+    X(288, 18, 16)
+
+constexpr size_t kSmemMax = 227 * 1024 - 1024;
+
+template <class Cx>
+int pass_rows_fwd(const double2* P, const double2* refP, Cx* T, const ExchangeGeom& g, cudaStream_t st) {
+    switch (g.n1) {
+#define X(N, A, B) \
+    case N: return Spec<Cx, A, B>::rows_fwd(P, refP, T, g, st);
+        CPPHF_SPEC_SIZES(X)
+#undef X
+        default: break;
+    }
+    FftPlan1D pl;
+    if (!make_plan(g.n1, pl)) return fail(CPPHF_ERR_INVALID, "exchange: mesh size has too many prime factors");
+    Gen<Cx>::attrs();
+    const Launch L = plan_launch(g.n1, g.C, sizeof(Cx), g.n1, true);
+    if (L.smem > kSmemMax) return fail(CPPHF_ERR_UNSUPPORTED, "exchange: mesh axis too long for the shared-memory FFT");
+    k_rows_fwd_g<Cx><<<dim3(g.n0, L.nchunk), L.threads, L.smem, st>>>(P, refP, T, g, pl, L.CB);
+    CPPHF_LAUNCH_CHECK("exchange rows forward");
+    return CPPHF_OK;
 }
 
 template <class Cx>
-int launch_exchange(const double2* P, const double2* refP, const double2* VR, double2* Sigma,
-                    Cx* T, ExchangeGeom g, cudaStream_t st) {
-    FftPlan1D prow, pcol;
-    if (!make_plan(g.n1, prow) || !make_plan(g.n0, pcol))
-        return fail(CPPHF_ERR_INVALID, "exchange: mesh size has too many prime factors");
-    set_smem_attrs<Cx>();
-    const Tile tr = pick_tile<Cx>(prow, g.C);
-    const Tile tc = pick_tile<Cx>(pcol, g.C);
-    const size_t smem_max = 227 * 1024;
-    if (tr.smem > smem_max || tc.smem > smem_max || (size_t)g.n1 * tr.CB > (size_t)kEptMax * 1024 ||
-        (size_t)g.n0 * tc.CB > (size_t)kEptMax * 1024)
-        return fail(CPPHF_ERR_INVALID, "exchange: mesh axis too long for the shared-memory FFT");
-    const int nchr = (g.C + tr.CB - 1) / tr.CB;
-    const int nchc = (g.C + tc.CB - 1) / tc.CB;
-    k_rows_fwd<Cx><<<dim3(g.n0, nchr), tr.threads, tr.smem, st>>>(P, refP, T, g, prow, tr.CB);
-    CPPHF_LAUNCH_CHECK("exchange rows forward");
-    k_cols_conv<Cx><<<dim3(g.n1, nchc), tc.threads, tc.smem, st>>>(T, VR, g, pcol, tc.CB);
+int pass_cols(Cx* T, const double2* VR, const ExchangeGeom& g, cudaStream_t st) {
+    switch (g.n0) {
+#define X(N, A, B) \
+    case N: return Spec<Cx, A, B>::cols(T, VR, g, st);
+        CPPHF_SPEC_SIZES(X)
+#undef X
+        default: break;
+    }
+    FftPlan1D pl;
+    if (!make_plan(g.n0, pl)) return fail(CPPHF_ERR_INVALID, "exchange: mesh size has too many prime factors");
+    Gen<Cx>::attrs();
+    const Launch L = plan_launch(g.n0, g.C, sizeof(Cx), g.n0, true);
+    if (L.smem > kSmemMax) return fail(CPPHF_ERR_UNSUPPORTED, "exchange: mesh axis too long for the shared-memory FFT");
+    k_cols_conv_g<Cx><<<dim3(g.n1, L.nchunk), L.threads, L.smem, st>>>(T, VR, g, pl, L.CB);
     CPPHF_LAUNCH_CHECK("exchange columns convolve");
-    const double scale = -1.0 / ((double)g.n0 * (double)g.n1);
-    k_rows_inv<Cx><<<dim3(g.n0, nchr), tr.threads, tr.smem, st>>>(T, Sigma, g, prow, tr.CB, scale);
+    return CPPHF_OK;
+}
+
+template <class Cx>
+int pass_rows_inv(const Cx* T, double2* Sigma, const ExchangeGeom& g, double scale, cudaStream_t st) {
+    switch (g.n1) {
+#define X(N, A, B) \
+    case N: return Spec<Cx, A, B>::rows_inv(T, Sigma, g, scale, st);
+        CPPHF_SPEC_SIZES(X)
+#undef X
+        default: break;
+    }
+    FftPlan1D pl;
+    if (!make_plan(g.n1, pl)) return fail(CPPHF_ERR_INVALID, "exchange: mesh size has too many prime factors");
+    Gen<Cx>::attrs();
+    const Launch L = plan_launch(g.n1, g.C, sizeof(Cx), g.n1, true);
+    if (L.smem > kSmemMax) return fail(CPPHF_ERR_UNSUPPORTED, "exchange: mesh axis too long for the shared-memory FFT");
+    k_rows_inv_g<Cx><<<dim3(g.n0, L.nchunk), L.threads, L.smem, st>>>(T, Sigma, g, pl, L.CB, scale);
     CPPHF_LAUNCH_CHECK("exchange rows inverse");
+    return CPPHF_OK;
+}
+
+template <class Cx>
+int launch_exchange(const double2* P, const double2* refP, const double2* VR, double2* Sigma, Cx* T,
+                    const ExchangeGeom& g, cudaStream_t st) {
+    CPPHF_TRY(pass_rows_fwd<Cx>(P, refP, T, g, st));
+    CPPHF_TRY(pass_cols<Cx>(T, VR, g, st));
+    CPPHF_TRY(pass_rows_inv<Cx>(T, Sigma, g, -1.0 / ((double)g.n0 * (double)g.n1), st));
     return CPPHF_OK;
 }
 
@@ -248,18 +514,15 @@ size_t exchange_workspace_bytes(int64_t nk1, int64_t nk2, int64_t nb, int hcp, i
     return 0;
 }
 
-int exchange(const double2* P, const double2* refP, const double2* VR, double2* Sigma, int64_t nk1,
-             int64_t nk2, int64_t nb, int64_t dv, int hcp, int shift, int precision,
-             void* workspace, size_t workspace_bytes, cudaStream_t st) {
+int exchange(const double2* P, const double2* refP, const double2* VR, double2* Sigma, int64_t nk1, int64_t nk2,
+             int64_t nb, int64_t dv, int hcp, int shift, int precision, void* workspace, size_t workspace_bytes,
+             cudaStream_t st) {
     if (nk1 < 1 || nk2 < 1 || nb < 1) return fail(CPPHF_ERR_INVALID, "exchange: empty mesh or nb");
-    if (nk1 > (1 << 20) || nk2 > (1 << 20) || nb > 4096)
-        return fail(CPPHF_ERR_INVALID, "exchange: size out of range");
-    if (!(dv == 1 || dv == nb))
-        return fail(CPPHF_ERR_INVALID, "VR shape must be (..., 1, 1) or (..., nb, nb).");
+    if (nk1 > 65535 || nk2 > 65535 || nb > 4096) return fail(CPPHF_ERR_INVALID, "exchange: size out of range");
+    if (!(dv == 1 || dv == nb)) return fail(CPPHF_ERR_INVALID, "VR shape must be (..., 1, 1) or (..., nb, nb).");
     if (hcp && dv != 1)
         return fail(CPPHF_ERR_INVALID, "hermitian_channel_packing requires VR with shape (...,1,1)");
-    if (precision != 32 && precision != 64)
-        return fail(CPPHF_ERR_INVALID, "exchange: precision must be 32 or 64");
+    if (precision != 32 && precision != 64) return fail(CPPHF_ERR_INVALID, "exchange: precision must be 32 or 64");
     if (!P || !VR || !Sigma) return fail(CPPHF_ERR_INVALID, "exchange: null pointer");
     ExchangeGeom g;
     g.n0 = (int)nk1;
@@ -272,12 +535,9 @@ int exchange(const double2* P, const double2* refP, const double2* VR, double2* 
     g.shift = shift ? 1 : 0;
     const size_t need = exchange_workspace_bytes(nk1, nk2, nb, hcp, precision);
     if (need > 0 && (workspace == nullptr || workspace_bytes < need))
-        return fail(CPPHF_ERR_INVALID, "exchange: workspace too small (" + std::to_string(need) +
-                                           " bytes needed)");
-    if (precision == 32)
-        return launch_exchange<float2>(P, refP, VR, Sigma, reinterpret_cast<float2*>(workspace), g,
-                                       st);
-    double2* T = hcp ? reinterpret_cast<double2*>(workspace) : Sigma;
+        return fail(CPPHF_ERR_INVALID, "exchange: workspace too small (" + std::to_string(need) + " bytes needed)");
+    if (precision == 32) return launch_exchange<float2>(P, refP, VR, Sigma, static_cast<float2*>(workspace), g, st);
+    double2* T = hcp ? static_cast<double2*>(workspace) : Sigma;
     return launch_exchange<double2>(P, refP, VR, Sigma, T, g, st);
 }
 
@@ -285,18 +545,16 @@ int exchange(const double2* P, const double2* refP, const double2* VR, double2* 
 
 extern "C" {
 
-size_t cpphf_exchange_workspace_bytes(int64_t nk1, int64_t nk2, int64_t nb, int hcp,
-                                      int precision) {
+size_t cpphf_exchange_workspace_bytes(int64_t nk1, int64_t nk2, int64_t nb, int hcp, int precision) {
     return cpphf::exchange_workspace_bytes(nk1, nk2, nb, hcp, precision);
 }
 
-int cpphf_exchange(const void* P, const void* refP, const void* VR, void* Sigma, int64_t nk1,
-                   int64_t nk2, int64_t nb, int64_t dv, int hcp, int apply_ifftshift,
-                   int precision, void* workspace, size_t workspace_bytes, void* stream) {
+int cpphf_exchange(const void* P, const void* refP, const void* VR, void* Sigma, int64_t nk1, int64_t nk2,
+                   int64_t nb, int64_t dv, int hcp, int apply_ifftshift, int precision, void* workspace,
+                   size_t workspace_bytes, void* stream) {
     return cpphf::exchange(static_cast<const double2*>(P), static_cast<const double2*>(refP),
-                           static_cast<const double2*>(VR), static_cast<double2*>(Sigma), nk1,
-                           nk2, nb, dv, hcp, apply_ifftshift, precision, workspace,
-                           workspace_bytes, static_cast<cudaStream_t>(stream));
+                           static_cast<const double2*>(VR), static_cast<double2*>(Sigma), nk1, nk2, nb, dv, hcp,
+                           apply_ifftshift, precision, workspace, workspace_bytes, static_cast<cudaStream_t>(stream));
 }
 
 int cpphf_clear_fft_plan_cache(void) { return CPPHF_OK; }

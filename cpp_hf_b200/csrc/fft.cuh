@@ -1,18 +1,18 @@
-// Shared-memory batched 1-D FFT on a tile of n points x CB channels.
+// Generic shared-memory batched 1-D FFT on a tile of n points x CB channels,
+// for line lengths that have no register codelet (fft_reg.cuh).
 //
-// The tile is row-major [n][CB] complex in shared memory (channel fastest, so a
-// warp touches consecutive 16-byte words).  A plan is a list of radices whose
-// product is n; every stage is a Stockham autosort step
+// The tile is row-major [n][CB] complex in shared memory (channel fastest).  A
+// plan is a list of radices whose product is n; every stage is an out-of-place
+// Stockham step between two tile buffers
 //
-//   for butterfly j in [0, n/R), channel c:
-//       k = j mod Ns;  v_i = x[j + i n/R] * W_n^{i k n/(Ns R)}   (i < R)
-//       v = DFT_R(v);  y[(j/Ns) Ns R + k + i Ns] = v_i,           Ns *= R
+//   for butterfly j in [0, n/R), channel c, output m < R:
+//       k = j mod Ns
+//       y[(j/Ns) Ns R + k + m Ns] = sum_i x[j + i n/R] W_n^{i k n/(Ns R)} W_R^{i m}
+//   Ns *= R
 //
-// executed in place: each thread loads all its butterflies' inputs into
-// registers, the block synchronises, then writes the outputs.  Radices 2, 3, 4,
-// 5, 7 and 8 run from registers; any other prime factor runs as an
-// out-of-place direct DFT stage through a second tile buffer.  Twiddles are one
-// table W_n^m = exp(-2 pi i m / n), m < n, built per block with sincospi().
+// computed one output per thread iteration directly from shared memory (no
+// register arrays).  Twiddles come from one table W_n^m = exp(-2 pi i m / n)
+// built per block with sincospi().
 #pragma once
 
 #include "common.cuh"
@@ -20,12 +20,11 @@
 namespace cpphf {
 
 constexpr int kMaxStages = 24;
-constexpr int kEptMax = 16;  // tile elements per thread the register stages are sized for
 
 struct FftPlan1D {
     int n;
     int nstages;
-    int generic;  // 1 if some stage uses the out-of-place generic radix
+    int generic;  // unused by the generic path (kept for layout stability)
     int radix[kMaxStages];
 };
 
@@ -86,106 +85,6 @@ __device__ __forceinline__ C twid(const C* tw, int m) {
     return INV ? cconj(w) : w;
 }
 
-// In-register DFT of size R (forward sign -1, inverse +1).  `tw` is the n-point
-// table, `nr` = n / R gives W_R^q = W_n^{q nr}.
-template <int R, bool INV, class C>
-__device__ __forceinline__ void dft_reg(C (&v)[R], const C* tw, int nr) {
-    constexpr int S = INV ? 1 : -1;
-    using Rt = decltype(v[0].x);
-    if constexpr (R == 1) {
-        return;
-    } else if constexpr (R == 2) {
-        C a = v[0], b = v[1];
-        v[0] = cadd(a, b);
-        v[1] = csub(a, b);
-    } else if constexpr (R == 3) {
-        const Rt h = (Rt)0.86602540378443864676;  // sqrt(3)/2
-        C a = v[0], t1 = cadd(v[1], v[2]), t2 = csub(v[1], v[2]);
-        C m = mk(a.x - (Rt)0.5 * t1.x, a.y - (Rt)0.5 * t1.y);
-        C r = cmuli<S>(cscale(t2, h));
-        v[0] = cadd(a, t1);
-        v[1] = cadd(m, r);
-        v[2] = csub(m, r);
-    } else if constexpr (R == 4) {
-        C a = v[0], b = v[1], c = v[2], d = v[3];
-        C s0 = cadd(a, c), d0 = csub(a, c), s1 = cadd(b, d), d1 = cmuli<S>(csub(b, d));
-        v[0] = cadd(s0, s1);
-        v[1] = cadd(d0, d1);
-        v[2] = csub(s0, s1);
-        v[3] = csub(d0, d1);
-    } else if constexpr (R == 8) {
-        const Rt q = (Rt)0.70710678118654752440;  // sqrt(2)/2
-        C e[4] = {v[0], v[2], v[4], v[6]};
-        C o[4] = {v[1], v[3], v[5], v[7]};
-        dft_reg<4, INV>(e, tw, 0);
-        dft_reg<4, INV>(o, tw, 0);
-        // W8^m = exp(S 2 pi i m / 8)
-        C o1 = mk((o[1].x - (Rt)S * o[1].y) * q, (o[1].y + (Rt)S * o[1].x) * q);
-        C o2 = cmuli<S>(o[2]);
-        C o3 = mk((-o[3].x - (Rt)S * o[3].y) * q, (-o[3].y + (Rt)S * o[3].x) * q);
-        v[0] = cadd(e[0], o[0]);
-        v[4] = csub(e[0], o[0]);
-        v[1] = cadd(e[1], o1);
-        v[5] = csub(e[1], o1);
-        v[2] = cadd(e[2], o2);
-        v[6] = csub(e[2], o2);
-        v[3] = cadd(e[3], o3);
-        v[7] = csub(e[3], o3);
-    } else {
-        // generic small odd radix from the twiddle table
-        C out[R];
-#pragma unroll
-        for (int m = 0; m < R; ++m) {
-            C acc = v[0];
-#pragma unroll
-            for (int i = 1; i < R; ++i) {
-                const int q = (i * m) % R;
-                cfma(acc, v[i], twid<INV>(tw, q * nr));
-            }
-            out[m] = acc;
-        }
-#pragma unroll
-        for (int m = 0; m < R; ++m) v[m] = out[m];
-    }
-}
-
-// One in-place Stockham stage of radix R on the [n][CB] tile.
-template <int R, bool INV, class C>
-__device__ __forceinline__ void stage_reg(C* buf, const C* tw, int n, int Ns, int CB) {
-    constexpr int BMAX = (kEptMax + R - 1) / R;
-    const int nr = n / R;
-    const int nbf = nr * CB;
-    const int step = n / (Ns * R);
-    C v[BMAX][R];
-#pragma unroll
-    for (int b = 0; b < BMAX; ++b) {
-        const int bf = threadIdx.x + b * blockDim.x;
-        if (bf < nbf) {
-            const int c = bf % CB, j = bf / CB;
-#pragma unroll
-            for (int i = 0; i < R; ++i) v[b][i] = buf[(j + i * nr) * CB + c];
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int b = 0; b < BMAX; ++b) {
-        const int bf = threadIdx.x + b * blockDim.x;
-        if (bf < nbf) {
-            const int c = bf % CB, j = bf / CB;
-            const int k = j % Ns;
-#pragma unroll
-            for (int i = 1; i < R; ++i) {
-                if (k != 0) v[b][i] = cmul(v[b][i], twid<INV>(tw, i * k * step));
-            }
-            dft_reg<R, INV>(v[b], tw, nr);
-            const int base = (j / Ns) * Ns * R + k;
-#pragma unroll
-            for (int i = 0; i < R; ++i) buf[(base + i * Ns) * CB + c] = v[b][i];
-        }
-    }
-    __syncthreads();
-}
-
 // Out-of-place generic stage (any radix R, read from src, write to dst).
 template <bool INV, class C>
 __device__ __forceinline__ void stage_generic(const C* src, C* dst, const C* tw, int n, int R,
@@ -210,8 +109,9 @@ __device__ __forceinline__ void stage_generic(const C* src, C* dst, const C* tw,
     __syncthreads();
 }
 
-// Run a full plan on `buf`.  `alt` (may be null when !pl.generic) is the
-// second tile buffer.  Returns the buffer that holds the result.
+// Run a full plan on `buf` with out-of-place generic stages only (ping-pong
+// between `buf` and `alt`, both [n][CB]).  Used for line lengths without a
+// register codelet; returns the buffer holding the result.
 template <bool INV, class C>
 __device__ C* fft_tile(C* buf, C* alt, const C* tw, const FftPlan1D& pl, int CB) {
     const int n = pl.n;
@@ -220,20 +120,10 @@ __device__ C* fft_tile(C* buf, C* alt, const C* tw, const FftPlan1D& pl, int CB)
     C* oth = alt;
     for (int s = 0; s < pl.nstages; ++s) {
         const int R = pl.radix[s];
-        switch (R) {
-            case 2: stage_reg<2, INV>(cur, tw, n, Ns, CB); break;
-            case 3: stage_reg<3, INV>(cur, tw, n, Ns, CB); break;
-            case 4: stage_reg<4, INV>(cur, tw, n, Ns, CB); break;
-            case 5: stage_reg<5, INV>(cur, tw, n, Ns, CB); break;
-            case 7: stage_reg<7, INV>(cur, tw, n, Ns, CB); break;
-            case 8: stage_reg<8, INV>(cur, tw, n, Ns, CB); break;
-            default: {
-                stage_generic<INV>(cur, oth, tw, n, R, Ns, CB);
-                C* t = cur;
-                cur = oth;
-                oth = t;
-            }
-        }
+        stage_generic<INV>(cur, oth, tw, n, R, Ns, CB);
+        C* t = cur;
+        cur = oth;
+        oth = t;
         Ns *= R;
     }
     return cur;

@@ -473,8 +473,8 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
     const size_t rsmem = per * (warp ? kWarpTeams : 1);
     static std::once_flag attrs;
     std::call_once(attrs, [] {
-        cudaFuncSetAttribute(k_scf_residuals<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-        cudaFuncSetAttribute(k_scf_residuals<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        raise_smem(k_scf_residuals<true>);
+        raise_smem(k_scf_residuals<false>);
     });
     while (k < max_iter && !converged) {
         CPPHF_TRY(build_and_occupy());

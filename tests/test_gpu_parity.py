@@ -146,7 +146,7 @@ def test_eigh_block_sizes(native, oracle, sort):
 # mu
 # ---------------------------------------------------------------------------
 
-@pytest.mark.parametrize("nk,nb,T", [(1, 2, 0.1), (16, 6, 0.05), (2304, 2, 0.1), (36864, 8, 0.05), (10, 3, 1e-5)])
+@pytest.mark.parametrize("nk,nb,T", [(1, 2, 0.1), (16, 6, 0.05), (2304, 2, 0.1), (36864, 8, 0.05)])
 def test_find_mu_bisection(native, oracle, nk, nb, T):
     rng = np.random.default_rng(nk + nb)
     bands = rng.normal(size=(nk, nb))
@@ -155,6 +155,20 @@ def test_find_mu_bisection(native, oracle, nk, nb, T):
     mu = native.find_mu_bisection(bands, w, n_e, T, 0)
     mu_ref = oracle.find_mu_bisection(bands, w, n_e, T, 0)
     assert abs(mu - mu_ref) < 1e-12 * max(1.0, abs(mu_ref))
+
+
+def test_find_mu_bisection_cold_limit_hits_target(native, oracle):
+    """T -> 0 with the target on a plateau of the count: mu is only defined up to
+    the plateau (serial, pairwise and tree sums decide count > n_e differently
+    when the count equals n_e to the last bit), so check the count itself, as
+    the reference's tests/test_main.py:227-234 does."""
+    rng = np.random.default_rng(13)
+    bands = rng.normal(size=(10, 3))
+    w = np.full(10, 0.1)
+    for T in (1e-5, 1e-3):
+        mu = native.find_mu_bisection(bands, w, 1.5, T, 0)
+        occ = 1.0 / (1.0 + np.exp((bands - mu) / (T + 1e-12)))
+        assert abs(float(np.sum(w[:, None] * occ)) - 1.5) < 1e-4
 
 
 def test_find_mu_bisection_float32_inputs(native, oracle):
@@ -264,7 +278,9 @@ def _check_dm(got, ref, e_tol=1e-9, f_tol=1e-8):
     print(f"iterations gpu {n} oracle {nr}; |dE| {abs(E - Er):.3e}; |dmu| {abs(mu - mur):.3e}")
     assert conv == convr
     assert abs(E - Er) < e_tol * max(1.0, abs(Er))
-    assert abs(mu - mur) < 1e-7
+    # mu is ill-conditioned when it sits in a gap (N(mu) flat); the occupations are not
+    assert abs(mu - mur) < 1e-4
+    assert rel(p, pr) < f_tol
     assert rel(D, Dr) < f_tol
     assert rel(F, Fr) < f_tol
     assert abs(n - nr) <= max(2, nr // 5)
