@@ -99,6 +99,8 @@ def _sync():
 
 def _exchange(VR_t, P_t, apply_ifftshift, hcp, precision=64):
     lib = _lib_handle()
+    P_t = P_t.contiguous()
+    VR_t = VR_t.contiguous()
     nk1, nk2, nb = P_t.shape[0], P_t.shape[1], P_t.shape[2]
     dv1, dv2 = VR_t.shape[2], VR_t.shape[3]
     if hcp and (dv1 != 1 or dv2 != 1):

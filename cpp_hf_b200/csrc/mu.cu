@@ -46,16 +46,20 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
     GridBarrier bar;
     bar.init(a.sync);
     const int G = gridDim.x;
-    const int64_t per = (a.n + G - 1) / G;
-    const int64_t b0 = (int64_t)blockIdx.x * per;
-    const int64_t b1 = min(a.n, b0 + per);
+    const int nb = a.nb;
+    const int64_t nk = a.n / nb;
+    const int64_t per = (nk + G - 1) / G;  // k-points per block
+    const int64_t k0 = (int64_t)blockIdx.x * per;
+    const int64_t k1 = min(nk, k0 + per);
 
     // 1. global min / max of eps
     double lmin = INFINITY, lmax = -INFINITY;
-    for (int64_t i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
-        const double e = a.eps[i];
-        lmin = fmin(lmin, e);
-        lmax = fmax(lmax, e);
+    for (int64_t k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+        for (int b = 0; b < nb; ++b) {
+            const double e = a.eps[k * nb + b];
+            lmin = fmin(lmin, e);
+            lmax = fmax(lmax, e);
+        }
     }
     {
         double v[2] = {-lmin, lmax};
@@ -82,11 +86,23 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
         if (blockIdx.x == 0 && threadIdx.x == 0) *a.mu_out = NAN;
         return;
     }
-    double emin = INFINITY, emax = -INFINITY;
-    for (int b = 0; b < G; ++b) {
-        emin = fmin(emin, -__ldcg(&a.part[2 * b]));
-        emax = fmax(emax, __ldcg(&a.part[2 * b + 1]));
+    // warp 0 reduces the block partials (fixed lane-strided order) and broadcasts
+    __shared__ double bc[2];
+    if (threadIdx.x < 32) {
+        double m0 = -INFINITY, m1 = -INFINITY;
+        for (int b = threadIdx.x; b < G; b += 32) {
+            m0 = fmax(m0, __ldcg(&a.part[2 * b]));
+            m1 = fmax(m1, __ldcg(&a.part[2 * b + 1]));
+        }
+        m0 = warp_max(m0);
+        m1 = warp_max(m1);
+        if (threadIdx.x == 0) {
+            bc[0] = -m0;
+            bc[1] = m1;
+        }
     }
+    __syncthreads();
+    const double emin = bc[0], emax = bc[1];
     const double Tj = fmax(a.T, 1.0e-12);
     double lo, hi, mu = 0.0;
     if (a.mode == 0) {
@@ -103,15 +119,17 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
         double* part = a.part + 2 * G + (size_t)(it & 1) * 2 * G;
         const double mid = 0.5 * (lo + hi);
         double v[2] = {0.0, 0.0};
-        for (int64_t i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
-            const double wk = a.w[i / a.nb];
-            const double e = a.eps[i];
-            if (a.mode == 0) {
-                v[0] += wk * expit(-(e - mid) / Tfd);
-            } else {
-                const double p = expit((mu - e) / Tj);
-                v[0] += wk * p;
-                v[1] += wk * p * (1.0 - p) / Tj;
+        for (int64_t k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+            const double wk = a.w[k];
+            for (int b = 0; b < nb; ++b) {
+                const double e = a.eps[k * nb + b];
+                if (a.mode == 0) {
+                    v[0] += wk * expit(-(e - mid) / Tfd);
+                } else {
+                    const double p = expit((mu - e) / Tj);
+                    v[0] += wk * p;
+                    v[1] += wk * p * (1.0 - p) / Tj;
+                }
             }
         }
         block_sum<2>(v, red);
@@ -123,11 +141,22 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
             if (blockIdx.x == 0 && threadIdx.x == 0) *a.mu_out = NAN;
             return;
         }
-        double N = 0.0, Z = 0.0;
-        for (int b = 0; b < G; ++b) {
-            N += __ldcg(&part[2 * b]);
-            Z += __ldcg(&part[2 * b + 1]);
+        if (threadIdx.x < 32) {
+            double n0 = 0.0, z0 = 0.0;
+            for (int b = threadIdx.x; b < G; b += 32) {
+                n0 += __ldcg(&part[2 * b]);
+                z0 += __ldcg(&part[2 * b + 1]);
+            }
+            n0 = warp_sum(n0);
+            z0 = warp_sum(z0);
+            if (threadIdx.x == 0) {
+                bc[0] = n0;
+                bc[1] = z0;
+            }
         }
+        __syncthreads();
+        const double N = bc[0], Z = bc[1];
+        __syncthreads();
         if (a.mode == 0) {
             if (N > a.target)
                 hi = mid;
@@ -175,7 +204,7 @@ int mu_solve(const double* eps, const double* w, int64_t nk, int64_t nb, double 
     if (mode == 1 && !mu0) return fail(CPPHF_ERR_INVALID, "mu: null warm start");
     if (!ws || wsb < mu_workspace_bytes(nk, nb)) return fail(CPPHF_ERR_INVALID, "mu: workspace too small");
     const int64_t n = nk * nb;
-    int grid = (int)std::min<int64_t>(max_coop_grid(), (n + 4 * kMuThreads - 1) / (4 * kMuThreads));
+    int grid = (int)std::min<int64_t>(max_coop_grid(), (nk + kMuThreads - 1) / kMuThreads);
     if (grid < 1) grid = 1;
     MuArgs a;
     a.eps = eps;
