@@ -1,5 +1,8 @@
 // Library-wide C-ABI plumbing: version, thread-local error text, SM count.
 #include "common.cuh"
+#include "bulk.cuh"
+
+#include <cudaTypedefs.h>
 
 #include <mutex>
 #include <string>
@@ -28,6 +31,30 @@ int num_sms() {
     int n = 0;
     cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
     return n > 0 ? n : 1;
+}
+
+bool make_tensor_map_3d(CUtensorMap* map, const void* base, CUtensorMapDataType dt, unsigned long long d0,
+                        unsigned long long d1, unsigned long long d2, unsigned long long stride1_bytes,
+                        unsigned long long stride2_bytes, unsigned b0, unsigned b1, unsigned b2) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+        (void)cudaGetLastError();
+    });
+    if (!encode) return false;
+    const cuuint64_t dims[3] = {d0, d1, d2};
+    const cuuint64_t strides[2] = {stride1_bytes, stride2_bytes};
+    const cuuint32_t box[3] = {b0, b1, b2};
+    const cuuint32_t es[3] = {1, 1, 1};
+    const CUresult r = encode(map, dt, 3, const_cast<void*>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
 }
 
 }  // namespace cpphf
@@ -59,3 +86,4 @@ int cpphf_copy_h2d(void* dst, const void* src, size_t bytes, void* stream) {
 }
 
 }  // extern "C"
+

@@ -23,8 +23,10 @@
 #include "exchange.cuh"
 #include "fft.cuh"
 #include "fft_reg.cuh"
+#include "bulk.cuh"
 
 #include <algorithm>
+#include <cstdlib>
 #include <mutex>
 #include <string>
 
@@ -231,6 +233,268 @@ __global__ void __launch_bounds__(256) k_rows_inv_s(const Cx* T, double2* Sigma,
     }
 }
 
+
+// ===========================================================================
+// Pipelined four-step kernels (full channel set, no HCP).  Persistent CTAs
+// walk the tiles (line, channel chunk) with a stride of gridDim.x; thread 0
+// fetches the NEXT tile's rows with cp.async.bulk into the other shared-memory
+// stage while the CTA transforms the current one.  The transpose of the
+// four-step runs in place in the current stage.
+// smem: tw[N] | mbar[2] | stage[2] = { in tile [N][CB] (double2, or Cx for T),
+//                                       second tile [N][CB] double2 (refP or VR) }
+// ===========================================================================
+struct PipeLayout {
+    size_t tw, bar, stage0, stage_bytes, in_bytes, total;
+};
+
+// Offsets are relative to a 128-byte aligned base (TMA tensor copies need
+// 128-byte aligned shared-memory destinations); `total` includes the slack
+// for aligning the dynamic shared-memory base.
+__host__ __device__ inline PipeLayout pipe_layout(int N, int CB, size_t in_elem, bool second) {
+    PipeLayout L;
+    L.tw = 0;
+    L.bar = (sizeof(double2) * (size_t)N + 15) & ~(size_t)15;
+    L.stage0 = (L.bar + 16 + 127) & ~(size_t)127;
+    L.in_bytes = ((in_elem * (size_t)N * CB) + 127) & ~(size_t)127;
+    L.stage_bytes = L.in_bytes + (second ? sizeof(double2) * (size_t)N * CB : 0);
+    L.stage_bytes = (L.stage_bytes + 127) & ~(size_t)127;
+    L.total = L.stage0 + 2 * L.stage_bytes + 128;
+    return L;
+}
+
+__device__ __forceinline__ unsigned char* align128(unsigned char* p) {
+    return reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(p) + 127) & ~(uintptr_t)127);
+}
+
+// pass A: rows forward.  Tile t -> (kx = t / nchunk, chunk = t % nchunk).
+template <class Cx, int N1, int N2>
+__global__ void __launch_bounds__(256, 2) k_rows_fwd_p(const __grid_constant__ CUtensorMap mP,
+                                                       const __grid_constant__ CUtensorMap mR, int has_refP, Cx* T,
+                                                       ExchangeGeom g, int CB, int nchunk, int ntiles) {
+    constexpr int N = N1 * N2;
+    extern __shared__ __align__(16) unsigned char smem_dyn[];
+    unsigned char* smem_raw = align128(smem_dyn);
+    const bool has_ref = has_refP != 0;
+    const PipeLayout L = pipe_layout(N, CB, sizeof(double2), has_ref);
+    Cx* tw = reinterpret_cast<Cx*>(smem_raw + L.tw);
+    unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem_raw + L.bar);
+    const int c = threadIdx.x % CB, a = threadIdx.x / CB;
+    build_line_twiddles(tw, N);
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    auto issue = [&](int t, int stage) {
+        if (threadIdx.x != 0) return;
+        const int kx = t / nchunk, c0 = (t - kx * nchunk) * CB;
+        const unsigned box = (unsigned)(N * CB * sizeof(double2));
+        unsigned char* st = smem_raw + L.stage0 + (size_t)stage * L.stage_bytes;
+        fence_proxy_async_smem();
+        mbar_arrive_expect_tx(&bar[stage], box * (has_ref ? 2u : 1u));
+        tma_load_3d(st, &mP, 2 * c0, 0, kx, &bar[stage]);
+        if (has_ref) tma_load_3d(st + L.in_bytes, &mR, 2 * c0, 0, kx, &bar[stage]);
+    };
+    int i = 0;
+    if ((int)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
+        const int stage = i & 1;
+        if (t + (int)gridDim.x < ntiles) issue(t + gridDim.x, stage ^ 1);
+        if (!mbar_wait(&bar[stage], (i >> 1) & 1)) return;
+        unsigned char* st = smem_raw + L.stage0 + (size_t)stage * L.stage_bytes;
+        const double2* in = reinterpret_cast<const double2*>(st);
+        const double2* rin = reinterpret_cast<const double2*>(st + L.in_bytes);
+        const int kx = t / nchunk, c0 = (t - kx * nchunk) * CB;
+        Cx v[N1];
+        if (a < N2) {
+#pragma unroll
+            for (int n1 = 0; n1 < N1; ++n1) {
+                double2 x = in[(N2 * n1 + a) * CB + c];
+                if (has_ref) x = csub(x, rin[(N2 * n1 + a) * CB + c]);
+                v[n1] = to_c(x, Cx{});
+            }
+            dft<N1, false>(v);
+        }
+        __syncthreads();
+        Cx* S = reinterpret_cast<Cx*>(st);
+        if (a < N2) {
+#pragma unroll
+            for (int k1 = 0; k1 < N1; ++k1) S[(k1 * N2 + a) * CB + c] = cmul(v[k1], tw[a * k1]);
+        }
+        __syncthreads();
+        if (a < N1) {
+            Cx u[N2];
+#pragma unroll
+            for (int n2 = 0; n2 < N2; ++n2) u[n2] = S[(a * N2 + n2) * CB + c];
+            dft<N2, false>(u);
+            const int ch = c0 + c;
+            if (ch < g.C) {
+#pragma unroll
+                for (int k2 = 0; k2 < N2; ++k2) st_l2(T + ((size_t)kx * g.n1 + (a + N1 * k2)) * g.Ct + ch, u[k2]);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// pass B: columns forward, * VR, inverse.  Tile t -> (ky, chunk).
+template <class Cx, int N1, int N2>
+__global__ void __launch_bounds__(256) k_cols_conv_p(const __grid_constant__ CUtensorMap mT,
+                                                     const __grid_constant__ CUtensorMap mV, Cx* T, ExchangeGeom g,
+                                                     int CB, int nchunk, int ntiles) {
+    constexpr int N = N1 * N2;
+    extern __shared__ __align__(16) unsigned char smem_dyn[];
+    unsigned char* smem_raw = align128(smem_dyn);
+    const PipeLayout L = pipe_layout(N, CB, sizeof(Cx), true);
+    Cx* tw = reinterpret_cast<Cx*>(smem_raw + L.tw);
+    unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem_raw + L.bar);
+    const int c = threadIdx.x % CB, a = threadIdx.x / CB;
+    build_line_twiddles(tw, N);
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    auto issue = [&](int t, int stage) {
+        if (threadIdx.x != 0) return;
+        const int ky = t / nchunk, c0 = (t - ky * nchunk) * CB;
+        const unsigned boxT = (unsigned)(N * CB * sizeof(Cx));
+        const unsigned boxV = (unsigned)(N * (g.dv == 1 ? 1 : CB) * sizeof(double2));
+        unsigned char* st = smem_raw + L.stage0 + (size_t)stage * L.stage_bytes;
+        fence_proxy_async_smem();
+        mbar_arrive_expect_tx(&bar[stage], boxT + boxV);
+        tma_load_3d(st, &mT, 2 * c0, ky, 0, &bar[stage]);
+        tma_load_3d(st + L.in_bytes, &mV, g.dv == 1 ? 0 : 2 * c0, ky, 0, &bar[stage]);
+    };
+    const int s0 = g.shift ? g.n0 / 2 : 0;
+    int i = 0;
+    if ((int)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
+        const int stage = i & 1;
+        if (t + (int)gridDim.x < ntiles) issue(t + gridDim.x, stage ^ 1);
+        if (!mbar_wait(&bar[stage], (i >> 1) & 1)) return;
+        unsigned char* st = smem_raw + L.stage0 + (size_t)stage * L.stage_bytes;
+        Cx* S = reinterpret_cast<Cx*>(st);
+        const double2* Vt = reinterpret_cast<const double2*>(st + L.in_bytes);
+        const int ky = t / nchunk, c0 = (t - ky * nchunk) * CB;
+        const int ch = c0 + c;
+        Cx v[N1];
+        if (a < N2) {
+#pragma unroll
+            for (int n1 = 0; n1 < N1; ++n1) v[n1] = S[(N2 * n1 + a) * CB + c];
+            dft<N1, false>(v);
+        }
+        __syncthreads();
+        if (a < N2) {
+#pragma unroll
+            for (int k1 = 0; k1 < N1; ++k1) S[(k1 * N2 + a) * CB + c] = cmul(v[k1], tw[a * k1]);
+        }
+        __syncthreads();
+        Cx u[N2];
+        if (a < N1) {
+#pragma unroll
+            for (int n2 = 0; n2 < N2; ++n2) u[n2] = S[(a * N2 + n2) * CB + c];
+            dft<N2, false>(u);
+#pragma unroll
+            for (int k2 = 0; k2 < N2; ++k2) {
+                const double2 w = g.dv == 1 ? Vt[a + N1 * k2] : Vt[(a + N1 * k2) * CB + c];
+                u[k2] = cmul(u[k2], to_c(w, Cx{}));
+            }
+            dft<N2, true>(u);
+        }
+        __syncthreads();
+        if (a < N1) {
+#pragma unroll
+            for (int na = 0; na < N2; ++na) S[(a * N2 + na) * CB + c] = cmulc(u[na], tw[na * a]);
+        }
+        __syncthreads();
+        if (a < N2) {
+#pragma unroll
+            for (int k1 = 0; k1 < N1; ++k1) v[k1] = S[(k1 * N2 + a) * CB + c];
+            dft<N1, true>(v);
+            if (ch < g.C) {
+#pragma unroll
+                for (int nbx = 0; nbx < N1; ++nbx) {
+                    const int kx = a + N2 * nbx;
+                    const int dx = (kx - s0 + g.n0) % g.n0;
+                    st_l2(T + ((size_t)dx * g.n1 + ky) * g.Ct + ch, v[nbx]);
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// pass C: rows inverse, scale, shift, store Sigma.  Tile t -> (kx, chunk).
+template <class Cx, int N1, int N2>
+__global__ void __launch_bounds__(256, 2) k_rows_inv_p(const __grid_constant__ CUtensorMap mT, double2* Sigma,
+                                                       ExchangeGeom g, int CB, int nchunk, int ntiles, double scale) {
+    constexpr int N = N1 * N2;
+    extern __shared__ __align__(16) unsigned char smem_dyn[];
+    unsigned char* smem_raw = align128(smem_dyn);
+    const PipeLayout L = pipe_layout(N, CB, sizeof(Cx), false);
+    Cx* tw = reinterpret_cast<Cx*>(smem_raw + L.tw);
+    unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem_raw + L.bar);
+    const int c = threadIdx.x % CB, a = threadIdx.x / CB;
+    const size_t nb2 = (size_t)g.nb * g.nb;
+    build_line_twiddles(tw, N);
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    auto issue = [&](int t, int stage) {
+        if (threadIdx.x != 0) return;
+        const int kx = t / nchunk, c0 = (t - kx * nchunk) * CB;
+        unsigned char* st = smem_raw + L.stage0 + (size_t)stage * L.stage_bytes;
+        fence_proxy_async_smem();
+        mbar_arrive_expect_tx(&bar[stage], (unsigned)(N * CB * sizeof(Cx)));
+        tma_load_3d(st, &mT, 2 * c0, 0, kx, &bar[stage]);
+    };
+    const int s1 = g.shift ? g.n1 / 2 : 0;
+    int i = 0;
+    if ((int)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
+        const int stage = i & 1;
+        if (t + (int)gridDim.x < ntiles) issue(t + gridDim.x, stage ^ 1);
+        if (!mbar_wait(&bar[stage], (i >> 1) & 1)) return;
+        unsigned char* st = smem_raw + L.stage0 + (size_t)stage * L.stage_bytes;
+        Cx* S = reinterpret_cast<Cx*>(st);
+        const int kx = t / nchunk, c0 = (t - kx * nchunk) * CB;
+        const int ch = c0 + c;
+        Cx u[N2];
+        if (a < N1) {
+#pragma unroll
+            for (int k2 = 0; k2 < N2; ++k2) u[k2] = S[(a + N1 * k2) * CB + c];
+            dft<N2, true>(u);
+        }
+        __syncthreads();
+        if (a < N1) {
+#pragma unroll
+            for (int na = 0; na < N2; ++na) S[(a * N2 + na) * CB + c] = cmulc(u[na], tw[na * a]);
+        }
+        __syncthreads();
+        if (a < N2) {
+            Cx v[N1];
+#pragma unroll
+            for (int k1 = 0; k1 < N1; ++k1) v[k1] = S[(k1 * N2 + a) * CB + c];
+            dft<N1, true>(v);
+            if (ch < g.C) {
+#pragma unroll
+                for (int nbx = 0; nbx < N1; ++nbx) {
+                    const int ky = a + N2 * nbx;
+                    const int dy = (ky - s1 + g.n1) % g.n1;
+                    Sigma[((size_t)kx * g.n1 + dy) * nb2 + ch] = cscale(to_d(v[nbx]), scale);
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
 // ===========================================================================
 // Generic kernels (any line length)
 // smem: tw[n] | buf[n * CB] | alt[n * CB] | map[2 * CB]
@@ -366,6 +630,17 @@ Launch plan_launch(int lanes, int C, size_t elem, int n, bool generic) {
     return L;
 }
 
+constexpr size_t kSmemMax = 227 * 1024 - 1024;
+
+// CPPHF_EXCHANGE_PIPELINE=0 selects the non-pipelined kernels (for A/B timing).
+bool pipeline_enabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("CPPHF_EXCHANGE_PIPELINE");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
 template <class Cx, int N1, int N2>
 struct Spec {
     static void attrs() {
@@ -374,10 +649,59 @@ struct Spec {
             raise_smem(k_rows_fwd_s<Cx, N1, N2>);
             raise_smem(k_cols_conv_s<Cx, N1, N2>);
             raise_smem(k_rows_inv_s<Cx, N1, N2>);
+            raise_smem(k_rows_fwd_p<Cx, N1, N2>);
+            raise_smem(k_cols_conv_p<Cx, N1, N2>);
+            raise_smem(k_rows_inv_p<Cx, N1, N2>);
         });
+    }
+    // persistent grid size for a pipelined kernel with `smem` bytes
+    template <class K>
+    static int pgrid(K kern, int threads, size_t smem, int ntiles) {
+        int per = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, threads, smem);
+        (void)cudaGetLastError();
+        if (per < 1) per = 1;
+        return std::max(1, std::min(ntiles, per * num_sms()));
+    }
+    // TMA boxes need 16-byte multiples for the inner extent, the row stride and
+    // the x coordinate (2 c0 scalars): for complex64 T that means even CB and Ct.
+    static bool pipelined(const ExchangeGeom& g) {
+        if (g.hcp || !pipeline_enabled() || N1 * N2 > 256) return false;
+        if (sizeof(Cx) == 8) {
+            const Launch L = plan_launch(N1 > N2 ? N1 : N2, g.C, sizeof(Cx), N1 * N2, false);
+            if ((L.CB % 2) != 0 || (g.Ct % 2) != 0) return false;
+        }
+        return true;
+    }
+    static CUtensorMapDataType tdt() { return sizeof(Cx) == 16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32; }
+    // field (n0, n1, C complex) as a 3-D tensor {2C scalars, n1, n0}
+    static bool field_map(CUtensorMap* m, const void* base, CUtensorMapDataType dt, size_t scal, int C,
+                          const ExchangeGeom& g, unsigned b0, unsigned b1, unsigned b2) {
+        const unsigned long long row = 2ull * C * scal;
+        return make_tensor_map_3d(m, base, dt, 2ull * C, (unsigned long long)g.n1, (unsigned long long)g.n0, row,
+                                  row * (unsigned long long)g.n1, b0, b1, b2);
     }
     static int rows_fwd(const double2* P, const double2* refP, Cx* T, const ExchangeGeom& g, cudaStream_t st) {
         attrs();
+        if (pipelined(g)) {
+            const Launch L = plan_launch(N1 > N2 ? N1 : N2, g.C, sizeof(Cx), N1 * N2, false);
+            const PipeLayout PL = pipe_layout(N1 * N2, L.CB, sizeof(double2), refP != nullptr);
+            if (PL.total <= kSmemMax) {
+                CUtensorMap mP, mR;
+                const int nb2 = g.nb * g.nb;
+                bool ok = field_map(&mP, P, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, nb2, g, 2 * L.CB, N1 * N2, 1);
+                ok = ok && field_map(&mR, refP ? refP : P, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, nb2, g, 2 * L.CB,
+                                     N1 * N2, 1);
+                if (ok) {
+                    const int nt = g.n0 * L.nchunk;
+                    const int grid = pgrid(k_rows_fwd_p<Cx, N1, N2>, L.threads, PL.total, nt);
+                    k_rows_fwd_p<Cx, N1, N2><<<grid, L.threads, PL.total, st>>>(mP, mR, refP != nullptr, T, g, L.CB,
+                                                                                L.nchunk, nt);
+                    CPPHF_LAUNCH_CHECK("exchange rows forward (pipelined)");
+                    return CPPHF_OK;
+                }
+            }
+        }
         const Launch L = plan_launch(N1 > N2 ? N1 : N2, g.C, sizeof(Cx), N1 * N2, false);
         k_rows_fwd_s<Cx, N1, N2><<<dim3(g.n0, L.nchunk), L.threads, L.smem, st>>>(P, refP, T, g, L.CB);
         CPPHF_LAUNCH_CHECK("exchange rows forward");
@@ -385,6 +709,25 @@ struct Spec {
     }
     static int cols(Cx* T, const double2* VR, const ExchangeGeom& g, cudaStream_t st) {
         attrs();
+        if (pipelined(g)) {
+            const Launch L = plan_launch(N1 > N2 ? N1 : N2, g.C, sizeof(Cx), N1 * N2, false);
+            const PipeLayout PL = pipe_layout(N1 * N2, L.CB, sizeof(Cx), true);
+            if (PL.total <= kSmemMax) {
+                CUtensorMap mT, mV;
+                bool ok = field_map(&mT, T, tdt(), sizeof(Cx) / 2, g.Ct, g, 2 * L.CB, 1, N1 * N2);
+                if (g.dv == 1)
+                    ok = ok && field_map(&mV, VR, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, 1, g, 2, 1, N1 * N2);
+                else
+                    ok = ok && field_map(&mV, VR, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, g.dv, g, 2 * L.CB, 1, N1 * N2);
+                if (ok) {
+                    const int nt = g.n1 * L.nchunk;
+                    const int grid = pgrid(k_cols_conv_p<Cx, N1, N2>, L.threads, PL.total, nt);
+                    k_cols_conv_p<Cx, N1, N2><<<grid, L.threads, PL.total, st>>>(mT, mV, T, g, L.CB, L.nchunk, nt);
+                    CPPHF_LAUNCH_CHECK("exchange columns convolve (pipelined)");
+                    return CPPHF_OK;
+                }
+            }
+        }
         const Launch L = plan_launch(N1 > N2 ? N1 : N2, g.C, sizeof(Cx), N1 * N2, false);
         k_cols_conv_s<Cx, N1, N2><<<dim3(g.n1, L.nchunk), L.threads, L.smem, st>>>(T, VR, g, L.CB);
         CPPHF_LAUNCH_CHECK("exchange columns convolve");
@@ -392,6 +735,21 @@ struct Spec {
     }
     static int rows_inv(const Cx* T, double2* Sigma, const ExchangeGeom& g, double scale, cudaStream_t st) {
         attrs();
+        if (pipelined(g)) {
+            const Launch L = plan_launch(N1 > N2 ? N1 : N2, g.C, sizeof(Cx), N1 * N2, false);
+            const PipeLayout PL = pipe_layout(N1 * N2, L.CB, sizeof(Cx), false);
+            if (PL.total <= kSmemMax) {
+                CUtensorMap mT;
+                if (field_map(&mT, T, tdt(), sizeof(Cx) / 2, g.Ct, g, 2 * L.CB, N1 * N2, 1)) {
+                    const int nt = g.n0 * L.nchunk;
+                    const int grid = pgrid(k_rows_inv_p<Cx, N1, N2>, L.threads, PL.total, nt);
+                    k_rows_inv_p<Cx, N1, N2><<<grid, L.threads, PL.total, st>>>(mT, Sigma, g, L.CB, L.nchunk, nt,
+                                                                                scale);
+                    CPPHF_LAUNCH_CHECK("exchange rows inverse (pipelined)");
+                    return CPPHF_OK;
+                }
+            }
+        }
         const Launch L = plan_launch(N1 > N2 ? N1 : N2, g.C, sizeof(Cx), N1 * N2, false);
         k_rows_inv_s<Cx, N1, N2><<<dim3(g.n0, L.nchunk), L.threads, L.smem, st>>>(T, Sigma, g, L.CB, scale);
         CPPHF_LAUNCH_CHECK("exchange rows inverse");
@@ -436,7 +794,6 @@ struct Gen {
     X(256, 16, 16)          \
     X(288, 18, 16)
 
-constexpr size_t kSmemMax = 227 * 1024 - 1024;
 
 template <class Cx>
 int pass_rows_fwd(const double2* P, const double2* refP, Cx* T, const ExchangeGeom& g, cudaStream_t st) {
@@ -558,5 +915,19 @@ int cpphf_exchange(const void* P, const void* refP, const void* VR, void* Sigma,
 }
 
 int cpphf_clear_fft_plan_cache(void) { return CPPHF_OK; }
+
+// Read (and with clear != 0 reset) the device-side flag set by bounded waits
+// that gave up.  Synchronises the device.  Returns the flag (0 = none) or a
+// negative status on a CUDA error.
+int cpphf_device_error(int clear) {
+    unsigned v = 0;
+    CPPHF_CUDA(cudaDeviceSynchronize());
+    CPPHF_CUDA(cudaMemcpyFromSymbol(&v, cpphf::g_cpphf_device_error, sizeof(v)));
+    if (clear) {
+        const unsigned z = 0;
+        CPPHF_CUDA(cudaMemcpyToSymbol(cpphf::g_cpphf_device_error, &z, sizeof(z)));
+    }
+    return (int)v;
+}
 
 }  // extern "C"
