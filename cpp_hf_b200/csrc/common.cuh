@@ -153,7 +153,11 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double* scratch) {
 // A wait that exceeds the spin limit records CPPHF_ERR_TIMEOUT and every later
 // barrier returns at once, so no block can wait forever.
 // ---------------------------------------------------------------------------
-constexpr long long kBarrierSpinLimit = 20000000LL;  // x ~64 ns sleep -> > 1 s
+constexpr long long kBarrierSpinLimit = 20000000LL;  // polls (each an L2 round trip) -> seconds
+#ifndef CPPHF_POLL_SLEEP_NS
+#define CPPHF_POLL_SLEEP_NS 0
+#endif
+constexpr unsigned kPollSleepNs = CPPHF_POLL_SLEEP_NS;
 
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
     unsigned v;
@@ -190,7 +194,7 @@ struct GridBarrier {
                             ok = 0;
                             break;
                         }
-                        __nanosleep(64);
+                        if (kPollSleepNs) __nanosleep(kPollSleepNs);
                     }
                 }
                 __threadfence();
@@ -198,6 +202,58 @@ struct GridBarrier {
             gen += 1;
             ok_sh = ok;
         }
+        __syncthreads();
+        return ok_sh != 0;
+    }
+
+    // Barrier whose last arriving block first sums the (2 x nblocks) partials
+    // `part` with warp 0 in a fixed lane-strided order and writes the two totals
+    // to `tot`, so the released blocks read two numbers instead of all partials.
+    // Ordering uses release/acquire atomics (no full fences).
+    __device__ bool wait_reduce(const double* part, int nblocks, double* tot) {
+        __syncthreads();
+        __shared__ int ok_sh, last_sh;
+        if (threadIdx.x == 0) {
+            ok_sh = 1;
+            last_sh = 0;
+            if (ld_acquire_u32(&sync[2]) != 0u) {
+                ok_sh = 0;
+            } else {
+                unsigned arrived;
+                asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(arrived) : "l"(&sync[0]) : "memory");
+                last_sh = (arrived == (unsigned)nblocks - 1) ? 1 : 0;
+            }
+        }
+        __syncthreads();
+        if (!ok_sh) return false;
+        if (last_sh) {
+            if (threadIdx.x < 32) {
+                double s0 = 0.0, s1 = 0.0;
+                for (int b = threadIdx.x; b < nblocks; b += 32) {
+                    s0 += __ldcg(&part[2 * b]);
+                    s1 += __ldcg(&part[2 * b + 1]);
+                }
+                s0 = warp_sum(s0);
+                s1 = warp_sum(s1);
+                if (threadIdx.x == 0) {
+                    __stcg(&tot[0], s0);
+                    __stcg(&tot[1], s1);
+                    sync[0] = 0u;
+                    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(&sync[1]) : "memory");
+                }
+            }
+        } else if (threadIdx.x == 0) {
+            long long spins = 0;
+            while (ld_acquire_u32(&sync[1]) == gen) {
+                if (++spins > kBarrierSpinLimit) {
+                    atomicExch(&sync[2], 1u);
+                    ok_sh = 0;
+                    break;
+                }
+                if (kPollSleepNs) __nanosleep(kPollSleepNs);
+            }
+        }
+        if (threadIdx.x == 0) gen += 1;
         __syncthreads();
         return ok_sh != 0;
     }

@@ -388,6 +388,145 @@ __global__ void k_retract(double2* Q, const double2* __restrict__ V, const doubl
     }
 }
 
+
+// ---------------------------------------------------------------------------
+// Cayley unitary by elimination: U(tau) = (I + tau d / 2)^{-1} (I - tau d / 2).
+// With H = i d Hermitian this equals V diag(c(tau, lam)) V^H of the spectral
+// form (solver_dm.hpp:251-272), so every backtracking trial and the retraction
+// need no eigendecomposition.  I + tau d / 2 has Hermitian part I (d is
+// skew-Hermitian), so Gauss-Jordan elimination without pivoting is stable.
+// On return Rs holds U (Ms is clobbered).
+// ---------------------------------------------------------------------------
+template <bool WARP>
+__device__ __forceinline__ void team_cayley_lu(const double2* Ds, double2* Ms, double2* Rs, double2* fs, double tau,
+                                               int nb, const Team<WARP>& t) {
+    const int ld = nb + 1;
+    const double h = 0.5 * tau;
+    for (int e = t.tid; e < nb * nb; e += t.nt) {
+        const int i = e / nb, j = e - i * nb;
+        const double2 a = cscale(Ds[i * ld + j], h);
+        const double one = (i == j) ? 1.0 : 0.0;
+        Ms[i * ld + j] = mk(one + a.x, a.y);
+        Rs[i * ld + j] = mk(one - a.x, -a.y);
+    }
+    t.sync();
+    for (int p = 0; p < nb; ++p) {
+        const double2 piv = Ms[p * ld + p];
+        const double inv = 1.0 / (piv.x * piv.x + piv.y * piv.y);
+        for (int r = t.tid; r < nb; r += t.nt) {
+            const double2 a = Ms[r * ld + p];
+            fs[r] = (r == p) ? mk(0.0, 0.0) : cscale(cmulc(a, piv), inv);  // a / piv
+        }
+        t.sync();
+        for (int e = t.tid; e < nb * nb; e += t.nt) {
+            const int r = e / nb, j = e - r * nb;
+            if (r == p) continue;
+            const double2 f = fs[r];
+            Ms[r * ld + j] = csub(Ms[r * ld + j], cmul(f, Ms[p * ld + j]));
+            Rs[r * ld + j] = csub(Rs[r * ld + j], cmul(f, Rs[p * ld + j]));
+        }
+        t.sync();
+    }
+    for (int e = t.tid; e < nb * nb; e += t.nt) {
+        const int r = e / nb, j = e - r * nb;
+        const double2 d = Ms[r * ld + r];
+        const double inv = 1.0 / (d.x * d.x + d.y * d.y);
+        Rs[r * ld + j] = cscale(cmulc(Rs[r * ld + j], d), inv);
+    }
+    t.sync();
+}
+
+// diag(U^H Ft U)_i = Re sum_j conj(U_ji) (Ft U)_ji ; Ws scratch
+template <bool WARP>
+__device__ __forceinline__ void team_diag_uhfu(const double2* Us, const double2* Fs, double2* Ws, double* out, int nb,
+                                               const Team<WARP>& t) {
+    const int ld = nb + 1;
+    tmm<false, false, WARP>(Ws, Fs, Us, nb, t);
+    t.sync();
+    for (int i = t.tid; i < nb; i += t.nt) {
+        double s = 0.0;
+        for (int j = 0; j < nb; ++j) {
+            const double2 u = Us[j * ld + i], w = Ws[j * ld + i];
+            s += u.x * w.x + u.y * w.y;  // Re(conj(u) w)
+        }
+        out[i] = s;
+    }
+}
+
+// One backtracking trial by elimination (solver_dm.hpp:577-589).
+template <bool WARP>
+__global__ void k_trial_lu(const double2* __restrict__ dQ, const double2* __restrict__ Ft,
+                           const double* __restrict__ p, const double* __restrict__ d_p,
+                           const double* __restrict__ w, int64_t nk, int nb, double T_r, double shrink,
+                           int last_trial, double fallback, DmScalars* S) {
+    if (S->accepted) return;  // grid-uniform
+    extern __shared__ __align__(16) unsigned char raw[];
+    __shared__ double red[64];
+    Team<WARP> t;
+    double2* Ds = team_mats<WARP>(raw, nb, 4, 3 * nb, t.team);
+    double2* Ms = Ds + team_mat_elems(nb);
+    double2* Rs = Ms + team_mat_elems(nb);
+    double2* Fs = Rs + team_mat_elems(nb);
+    double2* fs = Fs + team_mat_elems(nb);
+    double* ds = reinterpret_cast<double*>(fs + nb);
+    const double tau = S->tau_cur;
+    double v[2] = {0.0, 0.0};
+    for (int64_t k = (int64_t)blockIdx.x * t.nteams + t.team; k < nk; k += (int64_t)gridDim.x * t.nteams) {
+        tload<WARP>(Ds, dQ + (size_t)k * nb * nb, nb, t);
+        tload<WARP>(Fs, Ft + (size_t)k * nb * nb, nb, t);
+        t.sync();
+        team_cayley_lu<WARP>(Ds, Ms, Rs, fs, tau, nb, t);
+        team_diag_uhfu<WARP>(Rs, Fs, Ms, ds, nb, t);
+        t.sync();
+        const double wk = w[k];
+        for (int i = t.tid; i < nb; i += t.nt) {
+            const double pv = fmin(fmax(p[(size_t)k * nb + i] - tau * d_p[(size_t)k * nb + i], OCC_CLIP), 1.0 - OCC_CLIP);
+            v[0] += wk * pv * ds[i];
+            v[1] -= wk * (pv * log(pv) + (1.0 - pv) * log1p(-pv));
+        }
+        t.sync();
+    }
+    double out[2];
+    if (reduce_last_block<2>(v, S->part, &S->counter, out, red) && threadIdx.x == 0) {
+        const double om = out[0] - fmax(T_r, 1.0e-14) * out[1];
+        if (om < S->omega0) {
+            S->accepted = 1;
+            S->tau_final = tau;
+        } else {
+            S->tau_cur = tau * shrink;
+            if (last_trial) S->tau_final = S->tau0 * fallback;
+        }
+    }
+}
+
+// Retraction by elimination: Q <- Q U(tau_final), eps_work = diag(U^H Ft U).
+template <bool WARP>
+__global__ void k_retract_lu(double2* Q, const double2* __restrict__ dQ, const double2* __restrict__ Ft,
+                             double* __restrict__ ew, int64_t nk, int nb, const DmScalars* S) {
+    extern __shared__ __align__(16) unsigned char raw[];
+    Team<WARP> t;
+    double2* Ds = team_mats<WARP>(raw, nb, 4, 2 * nb, t.team);
+    double2* Ms = Ds + team_mat_elems(nb);
+    double2* Rs = Ms + team_mat_elems(nb);
+    double2* Fs = Rs + team_mat_elems(nb);
+    double2* fs = Fs + team_mat_elems(nb);
+    const double tau = S->tau_final;
+    for (int64_t k = (int64_t)blockIdx.x * t.nteams + t.team; k < nk; k += (int64_t)gridDim.x * t.nteams) {
+        tload<WARP>(Ds, dQ + (size_t)k * nb * nb, nb, t);
+        tload<WARP>(Fs, Ft + (size_t)k * nb * nb, nb, t);
+        t.sync();
+        team_cayley_lu<WARP>(Ds, Ms, Rs, fs, tau, nb, t);
+        team_diag_uhfu<WARP>(Rs, Fs, Ms, ew + (size_t)k * nb, nb, t);
+        t.sync();
+        tload<WARP>(Ds, Q + (size_t)k * nb * nb, nb, t);
+        t.sync();
+        tmm<false, false, WARP>(Ms, Ds, Rs, nb, t);  // Q U
+        t.sync();
+        tstore<WARP>(Q + (size_t)k * nb * nb, Ms, nb, t);
+        t.sync();
+    }
+}
+
 // p = expit((mu - eps) / T_r)  (solver_dm.hpp:456-457, 598-599)
 __global__ void k_occupations(const double* __restrict__ eps, const double* __restrict__ mu, double T_r,
                               double* __restrict__ p, int64_t n) {
@@ -437,6 +576,10 @@ void init_attrs() {
         set_max_smem(k_retract<false>);
         set_max_smem(k_q_times_u<true>);
         set_max_smem(k_q_times_u<false>);
+        set_max_smem(k_trial_lu<true>);
+        set_max_smem(k_trial_lu<false>);
+        set_max_smem(k_retract_lu<true>);
+        set_max_smem(k_retract_lu<false>);
     });
 }
 
@@ -474,8 +617,8 @@ unsigned flat_grid(int64_t n, int threads) {
 
 int dm_check_nb(int64_t nb) {
     if (nb < 1) return fail(CPPHF_ERR_INVALID, "nb must be positive");
-    // three team matrices of nb x (nb + 1) complex128 must fit in 227 KB
-    if (sizeof(double2) * team_mat_elems((int)nb) * 3 + 64 * sizeof(double) + 3 * nb * sizeof(double) > 227 * 1024)
+    // four team matrices of nb x (nb + 1) complex128 must fit in 227 KB
+    if (sizeof(double2) * team_mat_elems((int)nb) * 4 + 64 * sizeof(double) + 3 * nb * sizeof(double) > 227 * 1024)
         return fail(CPPHF_ERR_UNSUPPORTED, "nb too large for the per-k shared-memory kernels");
     return CPPHF_OK;
 }
@@ -538,6 +681,23 @@ int dm_trial(const double2* V, const double2* Fe, const double* lam, const doubl
     TeamLaunch L = team_launch(nk, nb);
     L.grid = std::min<unsigned>(L.grid, kDmMaxPartials);
     TEAM_DISPATCH(L, k_trial, 3, 3 * nb, V, Fe, lam, p, d_p, w, nk, nb, T_r, shrink, last_trial, fallback, S);
+    return CPPHF_OK;
+}
+
+int dm_trial_lu(const double2* dQ, const double2* Ft, const double* p, const double* d_p, const double* w, int64_t nk,
+                int nb, double T_r, double shrink, int last_trial, double fallback, DmScalars* S, cudaStream_t st) {
+    init_attrs();
+    TeamLaunch L = team_launch(nk, nb);
+    L.grid = std::min<unsigned>(L.grid, kDmMaxPartials);
+    TEAM_DISPATCH(L, k_trial_lu, 4, 3 * nb, dQ, Ft, p, d_p, w, nk, nb, T_r, shrink, last_trial, fallback, S);
+    return CPPHF_OK;
+}
+
+int dm_retract_lu(double2* Q, const double2* dQ, const double2* Ft, double* ew, int64_t nk, int nb, const DmScalars* S,
+                  cudaStream_t st) {
+    init_attrs();
+    const TeamLaunch L = team_launch(nk, nb);
+    TEAM_DISPATCH(L, k_retract_lu, 4, 2 * nb, Q, dQ, Ft, ew, nk, nb, S);
     return CPPHF_OK;
 }
 

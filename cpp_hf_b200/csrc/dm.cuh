@@ -40,6 +40,10 @@ int dm_direction(const double2* G, const double2* dQp, const double* g_p, const 
 int dm_trial(const double2* V, const double2* Fe, const double* lam, const double* p, const double* d_p,
              const double* w, int64_t nk, int nb, double T_r, double shrink, int last_trial, double fallback,
              DmScalars* S, cudaStream_t st);
+int dm_trial_lu(const double2* dQ, const double2* Ft, const double* p, const double* d_p, const double* w, int64_t nk,
+                int nb, double T_r, double shrink, int last_trial, double fallback, DmScalars* S, cudaStream_t st);
+int dm_retract_lu(double2* Q, const double2* dQ, const double2* Ft, double* ew, int64_t nk, int nb, const DmScalars* S,
+                  cudaStream_t st);
 int dm_retract(double2* Q, const double2* V, const double2* Fe, const double* lam, double* ew, int64_t nk, int nb,
                const DmScalars* S, cudaStream_t st);
 

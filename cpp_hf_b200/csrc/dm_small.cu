@@ -1,0 +1,576 @@
+// Direct-minimisation per-k kernels specialised for small band counts
+// (nb in {2, 4, 6, 8}; cpp_hf solver_dm.hpp:117-344).
+//
+// A group of GS = (nb rounded up to a power of two) threads owns one k-point;
+// thread r owns row r of every matrix in registers.  A CTA processes KT = 128/GS
+// k-points per tile: whole k-blocks are staged through shared memory with
+// coalesced loads/stores, and the operand that a row-times-matrix product needs
+// in full is read from the group's shared copy (a broadcast within the group).
+// Groups live inside one warp, so group-level ordering uses __syncwarp().
+#include "common.cuh"
+#include "dm.cuh"
+#include "dm_small.cuh"
+#include "team.cuh"
+
+#include <algorithm>
+#include <mutex>
+
+namespace cpphf {
+
+namespace {
+
+constexpr double TINY_REAL = 1.0e-30;  // types.hpp:13
+constexpr double LOGIT_CLIP = 1.0e-6;  // types.hpp:14
+constexpr double OCC_CLIP = 1.0e-8;    // types.hpp:16
+constexpr int kThreads = 128;
+
+__device__ __forceinline__ double expit(double x) {
+    if (x >= 0.0) return 1.0 / (1.0 + exp(-x));
+    const double e = exp(x);
+    return e / (1.0 + e);
+}
+
+template <int NB>
+struct Geo {
+    static constexpr int GS = NB <= 2 ? 2 : (NB <= 4 ? 4 : 8);  // group size
+    static constexpr int KT = kThreads / GS;                     // k-points per CTA tile
+    static constexpr int NB2 = NB * NB;
+    static constexpr int TILE = KT * NB2;                        // complex elements per field tile
+};
+
+// coalesced copy of a tile of `n` complex elements global <-> shared
+__device__ __forceinline__ void tile_load(double2* s, const double2* __restrict__ g, int n) {
+    for (int e = threadIdx.x; e < n; e += blockDim.x) s[e] = g[e];
+}
+__device__ __forceinline__ void tile_store(double2* g, const double2* s, int n) {
+    for (int e = threadIdx.x; e < n; e += blockDim.x) g[e] = s[e];
+}
+
+// ---------------------------------------------------------------------------
+// P = herm(Q diag(p) Q^H) with p = expit((mu - ew) / T_r) computed here
+// (solver_dm.hpp:117-128 + 456-457/598-599); p written out.
+// ---------------------------------------------------------------------------
+template <int NB>
+__global__ void __launch_bounds__(kThreads) k_dens_occ(const double2* __restrict__ Q, const double* __restrict__ ew,
+                                                       const double* __restrict__ mu, double T_r, double* __restrict__ p,
+                                                       double2* __restrict__ P, int64_t nk) {
+    using G = Geo<NB>;
+    __shared__ double2 sQ[G::TILE];
+    __shared__ double2 sX[G::TILE];
+    __shared__ double sp[G::KT * NB];
+    const int grp = threadIdx.x / G::GS, r = threadIdx.x % G::GS;
+    const double m = *mu;
+    const int64_t ntiles = (nk + G::KT - 1) / G::KT;
+    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int64_t k0 = t * G::KT;
+        const int nkt = (int)((nk - k0) < G::KT ? (nk - k0) : G::KT);
+        tile_load(sQ, Q + (size_t)k0 * G::NB2, nkt * G::NB2);
+        for (int e = threadIdx.x; e < nkt * NB; e += blockDim.x) {
+            const double pv = expit((m - ew[k0 * NB + e]) / T_r);
+            sp[e] = pv;
+            p[k0 * NB + e] = pv;
+        }
+        __syncthreads();
+        if (grp < nkt && r < NB) {
+            const double2* q = sQ + grp * G::NB2;
+            const double* pk = sp + grp * NB;
+            double2 qr[NB];
+#pragma unroll
+            for (int l = 0; l < NB; ++l) qr[l] = cscale(q[r * NB + l], pk[l]);
+#pragma unroll
+            for (int j = 0; j < NB; ++j) {
+                double2 acc = mk(0.0, 0.0);
+#pragma unroll
+                for (int l = 0; l < NB; ++l) cfmac(acc, qr[l], q[j * NB + l]);
+                sX[grp * G::NB2 + r * NB + j] = acc;
+            }
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < nkt * G::NB2; e += blockDim.x) {
+            const int kl = e / G::NB2, rr = e - kl * G::NB2, i = rr / NB, j = rr - i * NB;
+            const double2 a = sX[e], b = sX[kl * G::NB2 + j * NB + i];
+            P[(size_t)k0 * G::NB2 + e] = mk(0.5 * (a.x + b.x), 0.5 * (a.y - b.y));
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Ft = Q^H F Q, eps = Re diag Ft, G = orbital gradient, g_p, and the
+// reductions grad_norm, lam_pc (solver_dm.hpp:130-160, 497-519).
+// Ft overwrites F.
+// ---------------------------------------------------------------------------
+template <int NB>
+__global__ void __launch_bounds__(kThreads) k_rot_grad(const double2* __restrict__ Q, double2* F,
+                                                       const double* __restrict__ p, const double* __restrict__ w,
+                                                       double* __restrict__ eps, double2* __restrict__ Gout,
+                                                       double* __restrict__ g_p, int64_t nk, double T_r,
+                                                       double denom_scale, DmScalars* S) {
+    using G = Geo<NB>;
+    __shared__ double2 sQ[G::TILE];
+    __shared__ double2 sT[G::TILE];  // F Q, then Ft
+    __shared__ double red[64];
+    const int grp = threadIdx.x / G::GS, r = threadIdx.x % G::GS;
+    const double mu = S->mu;
+    const int64_t ntiles = (nk + G::KT - 1) / G::KT;
+    double v[2] = {0.0, 0.0};
+    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int64_t k0 = t * G::KT;
+        const int nkt = (int)((nk - k0) < G::KT ? (nk - k0) : G::KT);
+        tile_load(sQ, Q + (size_t)k0 * G::NB2, nkt * G::NB2);
+        __syncthreads();
+        const bool live = grp < nkt && r < NB;
+        const int64_t k = k0 + grp;
+        if (live) {  // T = F Q (row r)
+            const double2* q = sQ + grp * G::NB2;
+            double2 fr[NB];
+#pragma unroll
+            for (int l = 0; l < NB; ++l) fr[l] = F[(size_t)k * G::NB2 + r * NB + l];
+#pragma unroll
+            for (int j = 0; j < NB; ++j) {
+                double2 acc = mk(0.0, 0.0);
+#pragma unroll
+                for (int l = 0; l < NB; ++l) cfma(acc, fr[l], q[l * NB + j]);
+                sT[grp * G::NB2 + r * NB + j] = acc;
+            }
+        }
+        __syncthreads();
+        double2 ftr[NB];
+        if (live) {  // Ft = Q^H T (row r): Ft_rj = sum_l conj(Q_lr) T_lj
+            const double2* q = sQ + grp * G::NB2;
+            const double2* tt = sT + grp * G::NB2;
+#pragma unroll
+            for (int j = 0; j < NB; ++j) {
+                double2 acc = mk(0.0, 0.0);
+#pragma unroll
+                for (int l = 0; l < NB; ++l) cfma(acc, cconj(q[l * NB + r]), tt[l * NB + j]);
+                ftr[j] = acc;
+            }
+        }
+        __syncthreads();
+        if (live) {
+#pragma unroll
+            for (int j = 0; j < NB; ++j) {
+                sT[grp * G::NB2 + r * NB + j] = ftr[j];
+                F[(size_t)k * G::NB2 + r * NB + j] = ftr[j];
+            }
+        }
+        __syncthreads();
+        if (live) {
+            const double2* ft = sT + grp * G::NB2;
+            const double pr = p[k * NB + r];
+            const double er = ft[r * NB + r].x;
+            eps[k * NB + r] = er;
+            double gsq = 0.0;
+#pragma unroll
+            for (int j = 0; j < NB; ++j) {
+                double2 gv = mk(0.0, 0.0);
+                if (j != r) {
+                    const double pj = p[k * NB + j];
+                    const double2 aij = cscale(ftr[j], pj - pr);
+                    const double2 aji = cscale(ft[j * NB + r], pr - pj);
+                    gv = mk(0.5 * (aij.x - aji.x), 0.5 * (aij.y + aji.y));
+                }
+                Gout[(size_t)k * G::NB2 + r * NB + j] = gv;
+                gsq += gv.x * gv.x + gv.y * gv.y;
+            }
+            v[0] += w[k] * gsq;
+            const double pv = fmin(fmax(pr, LOGIT_CLIP), 1.0 - LOGIT_CLIP);
+            g_p[k * NB + r] = er + T_r * (log(pv) - log1p(-pv)) - mu;
+            v[1] += er * er;
+        }
+        __syncthreads();
+    }
+    double out[2];
+    if (reduce_last_block<2>(v, S->part, &S->counter, out, red) && threadIdx.x == 0) {
+        S->grad_norm = sqrt(fmax(0.0, out[0]));
+        const double nv = (double)(nk * NB);
+        const double scale = sqrt(out[1] / (nv > 1.0 ? nv : 1.0) + TINY_REAL);
+        S->lam_pc = fmax(T_r, denom_scale * scale);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Cayley unitary U(tau) = (I + tau d/2)^{-1} (I - tau d/2) of one k-point by
+// Gauss-Jordan elimination, one row per thread (row r of the result in u[]).
+// The pivot row is broadcast through the group's shared slot `piv`.
+// ---------------------------------------------------------------------------
+template <int NB>
+__device__ __forceinline__ void row_cayley(const double2* d, double tau, int r, double2* piv, double2 (&u)[NB],
+                                           unsigned mask) {
+    double2 mrow[NB];
+    const double h = 0.5 * tau;
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+        const double2 a = cscale(d[r * NB + j], h);
+        const double one = (j == r) ? 1.0 : 0.0;
+        mrow[j] = mk(one + a.x, a.y);
+        u[j] = mk(one - a.x, -a.y);
+    }
+#pragma unroll
+    for (int pp = 0; pp < NB; ++pp) {
+        if (r == pp) {
+#pragma unroll
+            for (int j = 0; j < NB; ++j) {
+                piv[j] = mrow[j];
+                piv[NB + j] = u[j];
+            }
+        }
+        __syncwarp(mask);
+        if (r != pp) {
+            const double2 pv = piv[pp];
+            const double inv = 1.0 / (pv.x * pv.x + pv.y * pv.y);
+            const double2 f = cscale(cmulc(mrow[pp], pv), inv);
+#pragma unroll
+            for (int j = 0; j < NB; ++j) {
+                mrow[j] = csub(mrow[j], cmul(f, piv[j]));
+                u[j] = csub(u[j], cmul(f, piv[NB + j]));
+            }
+        }
+        __syncwarp(mask);
+    }
+    double2 dd = mrow[0];
+#pragma unroll
+    for (int j = 1; j < NB; ++j)
+        if (j == r) dd = mrow[j];
+    const double inv = 1.0 / (dd.x * dd.x + dd.y * dd.y);
+#pragma unroll
+    for (int j = 0; j < NB; ++j) u[j] = cscale(cmulc(u[j], dd), inv);
+}
+
+// diag(U^H Ft U) for the group: thread j holds Ft row j (ftj) and U row j
+// (uj); it forms c_jr = conj(U_jr) (Ft U)_jr for every r from the group's U in
+// shared memory `su`, and the group sums c_jr over j with xor-shuffles (fixed
+// tree).  Thread r returns diag_r.
+template <int NB, int GS>
+__device__ __forceinline__ double row_diag_uhfu(const double2 (&ftj)[NB], const double2* su, int r, unsigned mask,
+                                                bool live) {
+    double c[NB];
+    const int rr = live ? r : 0;
+#pragma unroll
+    for (int q = 0; q < NB; ++q) {
+        double2 wjq = mk(0.0, 0.0);
+#pragma unroll
+        for (int l = 0; l < NB; ++l) cfma(wjq, ftj[l], su[l * NB + q]);
+        const double2 ujq = su[rr * NB + q];
+        c[q] = live ? (ujq.x * wjq.x + ujq.y * wjq.y) : 0.0;
+    }
+#pragma unroll
+    for (int o = GS / 2; o > 0; o >>= 1)
+#pragma unroll
+        for (int q = 0; q < NB; ++q) c[q] += __shfl_xor_sync(mask, c[q], o);
+    double out = 0.0;
+#pragma unroll
+    for (int q = 0; q < NB; ++q)
+        if (q == r) out = c[q];
+    return out;
+}
+
+template <int NB>
+__device__ __forceinline__ unsigned group_mask(int lane) {
+    using G = Geo<NB>;
+    const unsigned base = (1u << G::GS) - 1u;
+    return G::GS == 32 ? 0xffffffffu : (base << ((lane / G::GS) * G::GS));
+}
+
+// One backtracking trial (solver_dm.hpp:577-589) by elimination.
+template <int NB>
+__global__ void __launch_bounds__(kThreads) k_trial_small(const double2* __restrict__ dQ, const double2* __restrict__ Ft,
+                                                          const double* __restrict__ p, const double* __restrict__ d_p,
+                                                          const double* __restrict__ w, int64_t nk, double T_r,
+                                                          double shrink, int last_trial, double fallback,
+                                                          DmScalars* S) {
+    if (S->accepted) return;  // grid-uniform
+    using G = Geo<NB>;
+    __shared__ double2 sD[G::TILE];
+    __shared__ double2 sU[G::TILE];
+    __shared__ double2 sPiv[G::KT * 2 * NB];
+    __shared__ double red[64];
+    const int grp = threadIdx.x / G::GS, r = threadIdx.x % G::GS;
+    const unsigned mask = group_mask<NB>(threadIdx.x & 31);
+    const double tau = S->tau_cur;
+    const int64_t ntiles = (nk + G::KT - 1) / G::KT;
+    double v[2] = {0.0, 0.0};
+    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int64_t k0 = t * G::KT;
+        const int nkt = (int)((nk - k0) < G::KT ? (nk - k0) : G::KT);
+        tile_load(sD, dQ + (size_t)k0 * G::NB2, nkt * G::NB2);
+        __syncthreads();
+        const bool live = grp < nkt && r < NB;
+        const int rr = r < NB ? r : 0;
+        const int64_t k = k0 + grp;
+        if (grp < nkt) {
+            double2 u[NB];
+            row_cayley<NB>(sD + grp * G::NB2, tau, rr, sPiv + grp * 2 * NB, u, mask);
+            if (live) {
+#pragma unroll
+                for (int j = 0; j < NB; ++j) sU[grp * G::NB2 + r * NB + j] = u[j];
+            }
+        }
+        __syncthreads();
+        if (grp < nkt) {
+            double2 ftj[NB];
+#pragma unroll
+            for (int l = 0; l < NB; ++l) ftj[l] = Ft[(size_t)k * G::NB2 + rr * NB + l];
+            const double dr = row_diag_uhfu<NB, G::GS>(ftj, sU + grp * G::NB2, r, mask, live);
+            if (live) {
+                const double pv = fmin(fmax(p[k * NB + r] - tau * d_p[k * NB + r], OCC_CLIP), 1.0 - OCC_CLIP);
+                const double wk = w[k];
+                v[0] += wk * pv * dr;
+                v[1] -= wk * (pv * log(pv) + (1.0 - pv) * log1p(-pv));
+            }
+        }
+        __syncthreads();
+    }
+    double out[2];
+    if (reduce_last_block<2>(v, S->part, &S->counter, out, red) && threadIdx.x == 0) {
+        const double om = out[0] - fmax(T_r, 1.0e-14) * out[1];
+        if (om < S->omega0) {
+            S->accepted = 1;
+            S->tau_final = tau;
+        } else {
+            S->tau_cur = tau * shrink;
+            if (last_trial) S->tau_final = S->tau0 * fallback;
+        }
+    }
+}
+
+// Retraction Q <- Q U(tau_final) and eps_work = diag(U^H Ft U).
+template <int NB>
+__global__ void __launch_bounds__(kThreads) k_retract_small(double2* Q, const double2* __restrict__ dQ,
+                                                            const double2* __restrict__ Ft, double* __restrict__ ew,
+                                                            int64_t nk, const DmScalars* S) {
+    using G = Geo<NB>;
+    __shared__ double2 sD[G::TILE];
+    __shared__ double2 sU[G::TILE];
+    __shared__ double2 sPiv[G::KT * 2 * NB];
+    const int grp = threadIdx.x / G::GS, r = threadIdx.x % G::GS;
+    const unsigned mask = group_mask<NB>(threadIdx.x & 31);
+    const double tau = S->tau_final;
+    const int64_t ntiles = (nk + G::KT - 1) / G::KT;
+    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int64_t k0 = t * G::KT;
+        const int nkt = (int)((nk - k0) < G::KT ? (nk - k0) : G::KT);
+        tile_load(sD, dQ + (size_t)k0 * G::NB2, nkt * G::NB2);
+        __syncthreads();
+        const bool live = grp < nkt && r < NB;
+        const int rr = r < NB ? r : 0;
+        const int64_t k = k0 + grp;
+        if (grp < nkt) {
+            double2 u[NB];
+            row_cayley<NB>(sD + grp * G::NB2, tau, rr, sPiv + grp * 2 * NB, u, mask);
+            if (live) {
+#pragma unroll
+                for (int j = 0; j < NB; ++j) sU[grp * G::NB2 + r * NB + j] = u[j];
+            }
+        }
+        __syncthreads();
+        if (grp < nkt) {
+            double2 ftj[NB];
+#pragma unroll
+            for (int l = 0; l < NB; ++l) ftj[l] = Ft[(size_t)k * G::NB2 + rr * NB + l];
+            const double dr = row_diag_uhfu<NB, G::GS>(ftj, sU + grp * G::NB2, r, mask, live);
+            if (live) {
+                ew[k * NB + r] = dr;
+                const double2* su = sU + grp * G::NB2;
+                double2 qr[NB];
+#pragma unroll
+                for (int l = 0; l < NB; ++l) qr[l] = Q[(size_t)k * G::NB2 + r * NB + l];
+#pragma unroll
+                for (int j = 0; j < NB; ++j) {
+                    double2 acc = mk(0.0, 0.0);
+#pragma unroll
+                    for (int l = 0; l < NB; ++l) cfma(acc, qr[l], su[l * NB + j]);
+                    Q[(size_t)k * G::NB2 + r * NB + j] = acc;
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// PR+ numerator / denominator -> beta (solver_dm.hpp:513-559), per k-point rows.
+template <int NB>
+__global__ void __launch_bounds__(kThreads) k_pr_beta_small(const double2* __restrict__ Gc, const double2* __restrict__ Gp,
+                                                            const double* __restrict__ g_p,
+                                                            const double* __restrict__ g_pp,
+                                                            const double* __restrict__ eps,
+                                                            const double* __restrict__ p, const double* __restrict__ w,
+                                                            int64_t nk, double T_r, int restart, int iter, DmScalars* S) {
+    __shared__ double red[96];
+    const double lam = S->lam_pc;
+    double v[3] = {0.0, 0.0, 0.0};
+    const int64_t nrows = nk * NB;
+    for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < nrows; row += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = row / NB;
+        const int i = (int)(row - k * NB);
+        const double wk = w[k];
+        const double ei = eps[row];
+        double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+        for (int j = 0; j < NB; ++j) {
+            const double gap = ei - eps[k * NB + j];
+            const double base = sqrt(gap * gap + lam * lam);
+            const double2 g = Gc[row * NB + j], gp = Gp[row * NB + j];
+            const double2 d = mk(g.x / base, g.y / base);
+            s0 += (g.x * d.x + g.y * d.y) - (gp.x * d.x + gp.y * d.y);
+            s1 += gp.x * gp.x + gp.y * gp.y;
+        }
+        v[0] += wk * s0;
+        v[1] += wk * s1;
+        const double ps = fmin(fmax(p[row], OCC_CLIP), 1.0 - OCC_CLIP);
+        const double h = g_p[row] / (T_r / (ps * (1.0 - ps)));
+        v[2] += wk * (g_p[row] * h - g_pp[row] * h);
+        v[1] += wk * (g_pp[row] * g_pp[row]);
+    }
+    double out[3];
+    if (reduce_last_block<3>(v, S->part, &S->counter, out, red) && threadIdx.x == 0) {
+        const double num = out[0] + out[2];
+        const double den = out[1];
+        double beta = (den > TINY_REAL) ? fmax(0.0, num / den) : 0.0;
+        beta = fmin(beta, 5.0);
+        if (iter == 0 || (restart > 0 && iter % restart == 0)) beta = 0.0;
+        S->beta = beta;
+    }
+}
+
+// direction + tau0 + Omega0 (solver_dm.hpp:556-573, 346-365), per k-point rows.
+template <int NB>
+__global__ void __launch_bounds__(kThreads) k_direction_small(const double2* __restrict__ Gc,
+                                                              const double2* __restrict__ dQp,
+                                                              const double* __restrict__ g_p,
+                                                              const double* __restrict__ dpp,
+                                                              const double* __restrict__ eps,
+                                                              const double* __restrict__ p,
+                                                              const double* __restrict__ w, double2* __restrict__ dQ,
+                                                              double* __restrict__ d_p, int64_t nk, double T_r,
+                                                              double max_step, DmScalars* S) {
+    __shared__ double red[96];
+    const double lam = S->lam_pc, beta = S->beta;
+    double v[3] = {0.0, 0.0, 0.0};
+    const int64_t nrows = nk * NB;
+    for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < nrows; row += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = row / NB;
+        const double wk = w[k];
+        const double ei = eps[row];
+        double s0 = 0.0;
+#pragma unroll
+        for (int j = 0; j < NB; ++j) {
+            const double gap = ei - eps[k * NB + j];
+            const double base = sqrt(gap * gap + lam * lam);
+            const double2 g = Gc[row * NB + j], q = dQp[row * NB + j];
+            const double2 d = mk(g.x / base + beta * q.x, g.y / base + beta * q.y);
+            dQ[row * NB + j] = d;
+            s0 += d.x * d.x + d.y * d.y;
+        }
+        v[0] += wk * s0;
+        const double ps = fmin(fmax(p[row], OCC_CLIP), 1.0 - OCC_CLIP);
+        const double h = g_p[row] / (T_r / (ps * (1.0 - ps)));
+        d_p[row] = h + beta * dpp[row];
+        v[1] += wk * ps * ei;
+        v[2] -= wk * (ps * log(ps) + (1.0 - ps) * log1p(-ps));
+    }
+    double out[3];
+    if (reduce_last_block<3>(v, S->part, &S->counter, out, red) && threadIdx.x == 0) {
+        const double nrm = sqrt(fmax(0.0, out[0]));
+        const double tau0 = fmin(1.0, max_step / fmax(nrm, TINY_REAL));
+        S->tau0 = tau0;
+        S->tau_cur = tau0;
+        S->tau_final = tau0;
+        S->accepted = 0;
+        S->omega0 = out[1] - fmax(T_r, 1.0e-14) * out[2];
+    }
+}
+
+unsigned tiles_grid(int64_t nk, int KT, int cap) {
+    const int64_t nt = (nk + KT - 1) / KT;
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>(nt, cap));
+}
+
+unsigned rows_grid(int64_t rows) {
+    const int64_t want = (rows + kThreads - 1) / kThreads;
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, std::min<int64_t>(kDmMaxPartials, 4 * num_sms())));
+}
+
+#define SMALL_DISPATCH(nb, X) \
+    switch (nb) {             \
+        case 2: X(2); break;  \
+        case 4: X(4); break;  \
+        case 6: X(6); break;  \
+        case 8: X(8); break;  \
+        default: return fail(CPPHF_ERR_UNSUPPORTED, "small-nb kernel called with unsupported nb"); \
+    }
+
+}  // namespace
+
+bool dm_small_supported(int nb) { return nb == 2 || nb == 4 || nb == 6 || nb == 8; }
+
+int dm_small_dens_occ(const double2* Q, const double* ew, const double* mu, double T_r, double* p, double2* P,
+                      int64_t nk, int nb, cudaStream_t st) {
+#define X(N)                                                                                                     \
+    k_dens_occ<N><<<tiles_grid(nk, Geo<N>::KT, 16 * num_sms()), kThreads, 0, st>>>(Q, ew, mu, T_r, p, P, nk); \
+    CPPHF_LAUNCH_CHECK("dens_occ");
+    SMALL_DISPATCH(nb, X)
+#undef X
+    return CPPHF_OK;
+}
+
+int dm_small_rot_grad(const double2* Q, double2* F, const double* p, const double* w, double* eps, double2* Gout,
+                      double* g_p, int64_t nk, int nb, double T_r, double denom_scale, DmScalars* S, cudaStream_t st) {
+#define X(N)                                                                                                    \
+    k_rot_grad<N><<<tiles_grid(nk, Geo<N>::KT, kDmMaxPartials), kThreads, 0, st>>>(Q, F, p, w, eps, Gout, g_p, nk, \
+                                                                                   T_r, denom_scale, S);        \
+    CPPHF_LAUNCH_CHECK("rot_grad");
+    SMALL_DISPATCH(nb, X)
+#undef X
+    return CPPHF_OK;
+}
+
+int dm_small_pr_beta(const double2* Gc, const double2* Gp, const double* g_p, const double* g_pp, const double* eps,
+                     const double* p, const double* w, int64_t nk, int nb, double T_r, int restart, int iter,
+                     DmScalars* S, cudaStream_t st) {
+#define X(N)                                                                                                 \
+    k_pr_beta_small<N><<<rows_grid(nk * N), kThreads, 0, st>>>(Gc, Gp, g_p, g_pp, eps, p, w, nk, T_r, restart, \
+                                                               iter, S);                                     \
+    CPPHF_LAUNCH_CHECK("pr_beta");
+    SMALL_DISPATCH(nb, X)
+#undef X
+    return CPPHF_OK;
+}
+
+int dm_small_direction(const double2* Gc, const double2* dQp, const double* g_p, const double* dpp, const double* eps,
+                       const double* p, const double* w, double2* dQ, double* d_p, int64_t nk, int nb, double T_r,
+                       double max_step, DmScalars* S, cudaStream_t st) {
+#define X(N)                                                                                                   \
+    k_direction_small<N><<<rows_grid(nk * N), kThreads, 0, st>>>(Gc, dQp, g_p, dpp, eps, p, w, dQ, d_p, nk, T_r, \
+                                                                 max_step, S);                                 \
+    CPPHF_LAUNCH_CHECK("direction");
+    SMALL_DISPATCH(nb, X)
+#undef X
+    return CPPHF_OK;
+}
+
+int dm_small_trial(const double2* dQ, const double2* Ft, const double* p, const double* d_p, const double* w,
+                   int64_t nk, int nb, double T_r, double shrink, int last_trial, double fallback, DmScalars* S,
+                   cudaStream_t st) {
+#define X(N)                                                                                                     \
+    k_trial_small<N><<<tiles_grid(nk, Geo<N>::KT, kDmMaxPartials), kThreads, 0, st>>>(dQ, Ft, p, d_p, w, nk, T_r, \
+                                                                                      shrink, last_trial,        \
+                                                                                      fallback, S);              \
+    CPPHF_LAUNCH_CHECK("trial");
+    SMALL_DISPATCH(nb, X)
+#undef X
+    return CPPHF_OK;
+}
+
+int dm_small_retract(double2* Q, const double2* dQ, const double2* Ft, double* ew, int64_t nk, int nb,
+                     const DmScalars* S, cudaStream_t st) {
+#define X(N)                                                                                                   \
+    k_retract_small<N><<<tiles_grid(nk, Geo<N>::KT, 16 * num_sms()), kThreads, 0, st>>>(Q, dQ, Ft, ew, nk, S); \
+    CPPHF_LAUNCH_CHECK("retract");
+    SMALL_DISPATCH(nb, X)
+#undef X
+    return CPPHF_OK;
+}
+
+}  // namespace cpphf

@@ -15,6 +15,7 @@
 #include "fock.cuh"
 
 #include <algorithm>
+#include <mutex>
 #include <string>
 
 namespace cpphf {
@@ -185,12 +186,73 @@ __global__ void __launch_bounds__(kAsmThreads) k_assemble(AsmArgs a) {
     if (threadIdx.x == 0) a.part[blockIdx.x] = e_acc[0];
 }
 
-__global__ void k_sum_partials(const double* __restrict__ part, int n, double* __restrict__ out) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) {
-        double s = 0.0;
-        for (int b = 0; b < n; ++b) s += part[b];
-        *out = s;
+
+// Tiled assembly: a CTA stages KT whole k-blocks (KT nb^2 contiguous elements)
+// of Sigma, h and P (and refP) in shared memory with coalesced loads, then
+// forms F = herm(h + Sigma + SC + diag(hd)) and the energy terms element by
+// element, reading transposed partners from shared memory.
+constexpr int kTileElems = 1024;
+
+__global__ void __launch_bounds__(kAsmThreads) k_assemble_tiled(AsmArgs a, int KT) {
+    extern __shared__ __align__(16) unsigned char smem_t[];
+    __shared__ double red[32];
+    const int nb = a.nb, nb2 = nb * nb;
+    const int tile = KT * nb2;
+    double2* sS = reinterpret_cast<double2*>(smem_t);
+    double2* sH = sS + tile;
+    double2* sP = sH + tile;
+    double2* sR = sP + tile;  // refP (only when present)
+    const int64_t ntiles = (a.nk + KT - 1) / KT;
+    double e_acc[1] = {0.0};
+    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int64_t k0 = t * KT;
+        const int nkt = (int)((a.nk - k0) < (int64_t)KT ? (a.nk - k0) : (int64_t)KT);
+        const int n = nkt * nb2;
+        const size_t base = (size_t)k0 * nb2;
+        for (int e = threadIdx.x; e < n; e += blockDim.x) {
+            double2 s = a.Sigma[base + e];
+            if (a.SC) s = cadd(s, a.SC[e % nb2]);
+            sS[e] = s;
+            sH[e] = a.h[base + e];
+            sP[e] = a.P[base + e];
+            if (a.refP) sR[e] = a.refP[base + e];
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < n; e += blockDim.x) {
+            const int kl = e / nb2, r = e - kl * nb2;
+            const int i = r / nb, j = r - i * nb;
+            const int eT = kl * nb2 + j * nb + i;
+            const double hdi = a.hd ? a.hd[i] : 0.0;
+            double2 Aij = cadd(sH[e], sS[e]);
+            double2 Aji = cadd(sH[eT], sS[eT]);
+            if (i == j) {
+                Aij.x += hdi;
+                Aji = Aij;
+            }
+            a.F[base + e] = mk(0.5 * (Aij.x + Aji.x), 0.5 * (Aij.y - Aji.y));
+            if (a.SC) a.Sigma[base + e] = sS[e];
+            if (a.Hdense) a.Hdense[base + e] = mk(i == j ? hdi : 0.0, 0.0);
+            const double2 pji = sP[eT];
+            const double2 dji = a.refP ? csub(pji, sR[eT]) : pji;
+            double2 inter = cscale(sS[e], 0.5);
+            if (i == j && a.hd) inter.x += 0.5 * hdi;
+            const double2 h = sH[e];
+            const double s = (h.x * pji.x - h.y * pji.y) + (inter.x * dji.x - inter.y * dji.y);
+            e_acc[0] += a.w[k0 + kl] * s;
+        }
+        __syncthreads();
     }
+    block_sum<1>(e_acc, red);
+    if (threadIdx.x == 0) a.part[blockIdx.x] = e_acc[0];
+}
+
+// Fixed-order sum of block partials by one warp (lane-strided, then a
+// shuffle tree): deterministic for a given partial count.
+__global__ void k_sum_partials(const double* __restrict__ part, int n, double* __restrict__ out) {
+    double s = 0.0;
+    for (int b = threadIdx.x; b < n; b += 32) s += part[b];
+    s = warp_sum(s);
+    if (threadIdx.x == 0) *out = s;
 }
 
 struct FockWs {
@@ -295,8 +357,17 @@ int build_fock(const cpphf_kernel* K, const double2* P, double2* Sigma, double2*
     a.nk = nk;
     a.nb = nb;
     a.part = part;
-    k_assemble<<<L.Gasm, kAsmThreads, 0, st>>>(a);
-    CPPHF_LAUNCH_CHECK("assemble");
+    if (nb2 <= kTileElems) {
+        static std::once_flag once;
+        std::call_once(once, [] { raise_smem(k_assemble_tiled); });
+        const int KT = std::max(1, kTileElems / nb2);
+        const size_t smem = sizeof(double2) * (size_t)KT * nb2 * (refP ? 4 : 3);
+        k_assemble_tiled<<<L.Gasm, kAsmThreads, smem, st>>>(a, KT);
+        CPPHF_LAUNCH_CHECK("assemble (tiled)");
+    } else {
+        k_assemble<<<L.Gasm, kAsmThreads, 0, st>>>(a);
+        CPPHF_LAUNCH_CHECK("assemble");
+    }
     if (energy) {
         k_sum_partials<<<1, 32, 0, st>>>(part, L.Gasm, energy);
         CPPHF_LAUNCH_CHECK("energy sum");

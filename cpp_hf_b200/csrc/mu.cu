@@ -11,13 +11,14 @@
 #include "common.cuh"
 #include "mu.cuh"
 
+#include <cstdlib>
 #include <mutex>
 
 namespace cpphf {
 
 namespace {
 
-constexpr int kMuThreads = 256;
+constexpr int kMuThreads = 1024;
 constexpr int kMuMaxGrid = 1024;
 
 __device__ __forceinline__ double expit(double x) {
@@ -46,20 +47,18 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
     GridBarrier bar;
     bar.init(a.sync);
     const int G = gridDim.x;
-    const int nb = a.nb;
-    const int64_t nk = a.n / nb;
-    const int64_t per = (nk + G - 1) / G;  // k-points per block
-    const int64_t k0 = (int64_t)blockIdx.x * per;
-    const int64_t k1 = min(nk, k0 + per);
+    const unsigned nb = (unsigned)a.nb;
+    const unsigned n = (unsigned)a.n;
+    const unsigned per = (n + G - 1) / G;  // (k, band) elements per block
+    const unsigned e0 = blockIdx.x * per;
+    const unsigned e1 = min(n, e0 + per);
 
     // 1. global min / max of eps
     double lmin = INFINITY, lmax = -INFINITY;
-    for (int64_t k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
-        for (int b = 0; b < nb; ++b) {
-            const double e = a.eps[k * nb + b];
-            lmin = fmin(lmin, e);
-            lmax = fmax(lmax, e);
-        }
+    for (unsigned i = e0 + threadIdx.x; i < e1; i += blockDim.x) {
+        const double e = a.eps[i];
+        lmin = fmin(lmin, e);
+        lmax = fmax(lmax, e);
     }
     {
         double v[2] = {-lmin, lmax};
@@ -119,40 +118,32 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
         double* part = a.part + 2 * G + (size_t)(it & 1) * 2 * G;
         const double mid = 0.5 * (lo + hi);
         double v[2] = {0.0, 0.0};
-        for (int64_t k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
-            const double wk = a.w[k];
-            for (int b = 0; b < nb; ++b) {
-                const double e = a.eps[k * nb + b];
-                if (a.mode == 0) {
-                    v[0] += wk * expit(-(e - mid) / Tfd);
-                } else {
-                    const double p = expit((mu - e) / Tj);
-                    v[0] += wk * p;
-                    v[1] += wk * p * (1.0 - p) / Tj;
-                }
+        for (unsigned i = e0 + threadIdx.x; i < e1; i += blockDim.x) {
+            const double wk = a.w[i / nb];
+            const double e = a.eps[i];
+            if (a.mode == 0) {
+                v[0] += wk * expit(-(e - mid) / Tfd);
+            } else {
+                const double p = expit((mu - e) / Tj);
+                v[0] += wk * p;
+                v[1] += wk * p * (1.0 - p) / Tj;
             }
         }
         block_sum<2>(v, red);
         if (threadIdx.x == 0) {
-            part[2 * blockIdx.x] = v[0];
-            part[2 * blockIdx.x + 1] = v[1];
+            __stcg(&part[2 * blockIdx.x], v[0]);
+            __stcg(&part[2 * blockIdx.x + 1], v[1]);
         }
-        if (!bar.wait()) {
+        // the last block to arrive sums the partials (fixed lane-strided order)
+        // and publishes the totals before releasing the grid
+        double* tot = a.part + 6 * (size_t)G + (it & 1) * 2;
+        if (!bar.wait_reduce(part, G, tot)) {
             if (blockIdx.x == 0 && threadIdx.x == 0) *a.mu_out = NAN;
             return;
         }
-        if (threadIdx.x < 32) {
-            double n0 = 0.0, z0 = 0.0;
-            for (int b = threadIdx.x; b < G; b += 32) {
-                n0 += __ldcg(&part[2 * b]);
-                z0 += __ldcg(&part[2 * b + 1]);
-            }
-            n0 = warp_sum(n0);
-            z0 = warp_sum(z0);
-            if (threadIdx.x == 0) {
-                bc[0] = n0;
-                bc[1] = z0;
-            }
+        if (threadIdx.x == 0) {
+            bc[0] = __ldcg(&tot[0]);
+            bc[1] = __ldcg(&tot[1]);
         }
         __syncthreads();
         const double N = bc[0], Z = bc[1];
@@ -178,6 +169,13 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
     if (blockIdx.x == 0 && threadIdx.x == 0) *a.mu_out = (a.mode == 0) ? 0.5 * (lo + hi) : mu;
 }
 
+// Tuning knobs (read once): CPPHF_MU_THREADS_PER_K spreads a k-point's bands
+// over more blocks; CPPHF_MU_MAXGRID caps the cooperative grid.
+int env_int(const char* name, int dflt) {
+    const char* e = std::getenv(name);
+    return e ? std::atoi(e) : dflt;
+}
+
 int max_coop_grid() {
     static int g = 0;
     static std::once_flag once;
@@ -186,6 +184,8 @@ int max_coop_grid() {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_mu, kMuThreads, 0);
         if (per < 1) per = 1;
         g = std::min(kMuMaxGrid, per * num_sms());
+        const int cap = env_int("CPPHF_MU_MAXGRID", 0);
+        if (cap > 0) g = std::min(g, cap);
     });
     return g;
 }
@@ -193,18 +193,19 @@ int max_coop_grid() {
 }  // namespace
 
 size_t mu_workspace_bytes(int64_t, int64_t) {
-    return 64 + sizeof(double) * 6 * (size_t)kMuMaxGrid;
+    return 64 + sizeof(double) * (6 * (size_t)kMuMaxGrid + 8);
 }
 
 int mu_solve(const double* eps, const double* w, int64_t nk, int64_t nb, double target,
              const double* mu0, double T, int maxiter, int mode, double* mu_out, void* ws,
              size_t wsb, cudaStream_t st) {
     if (nk < 1 || nb < 1) return fail(CPPHF_ERR_INVALID, "mu: empty eigenvalue array");
+    if (nk * nb >= (int64_t)1 << 31) return fail(CPPHF_ERR_INVALID, "mu: more than 2^31 eigenvalues");
     if (!eps || !w || !mu_out) return fail(CPPHF_ERR_INVALID, "mu: null pointer");
     if (mode == 1 && !mu0) return fail(CPPHF_ERR_INVALID, "mu: null warm start");
     if (!ws || wsb < mu_workspace_bytes(nk, nb)) return fail(CPPHF_ERR_INVALID, "mu: workspace too small");
     const int64_t n = nk * nb;
-    int grid = (int)std::min<int64_t>(max_coop_grid(), (nk + kMuThreads - 1) / kMuThreads);
+    int grid = (int)std::min<int64_t>(max_coop_grid(), (n + kMuThreads - 1) / kMuThreads);
     if (grid < 1) grid = 1;
     MuArgs a;
     a.eps = eps;

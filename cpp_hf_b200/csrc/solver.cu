@@ -6,6 +6,7 @@
 // few scalars its convergence test needs.
 #include "common.cuh"
 #include "dm.cuh"
+#include "dm_small.cuh"
 #include "eigh.cuh"
 #include "fock.cuh"
 #include "mu.cuh"
@@ -265,12 +266,27 @@ int solve_dm(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* P
         CPPHF_CUDA(cudaMemsetAsync(dp[b], 0, vbytes, st));
     }
 
+    const bool small = dm_small_supported(nb);
+    // density from (Q, occupations); small nb fuses p = expit((mu - ew)/T_r)
+    auto density = [&](const double* ewv) -> int {
+        if (small) {
+            CPPHF_TRY(dm_small_dens_occ(Q, ewv, &S->mu, T_r, p, P, nk, nb, st));
+        } else {
+            CPPHF_TRY(dm_occupations(ewv, &S->mu, T_r, p, nk * nb, st));
+            CPPHF_TRY(dm_density(Q, p, P, nk, nb, st));
+        }
+        if (project) {
+            CPPHF_TRY(call_project(project, puser, P, K, st));
+            CPPHF_TRY(hermitize(P, P, nk, nb, st));
+        }
+        return CPPHF_OK;
+    };
+
     // ---- init (solver_dm.hpp:436-459) ----
     CPPHF_TRY(hermitize(P0, P, nk, nb, st));
     CPPHF_TRY(build_fock(K, P, Sig, F, nullptr, nullptr, nullptr, fws, L.fock_bytes, st));
-    CPPHF_TRY(eigh_batched(F, eps, Q, nk, nb, 0, nullptr, st));
-    CPPHF_TRY(mu_solve(eps, wn, nk, nb, n_t, &S->mu, T_r, mu_it, 1, &S->mu, mws, L.mu_bytes, st));
-    CPPHF_TRY(dm_occupations(eps, &S->mu, T_r, p, nk * nb, st));
+    CPPHF_TRY(eigh_batched(F, ew, Q, nk, nb, 0, nullptr, st));
+    CPPHF_TRY(mu_solve(ew, wn, nk, nb, n_t, &S->mu, T_r, mu_it, 1, &S->mu, mws, L.mu_bytes, st));
 
     double hbuf[4] = {0.0, 0.0, 0.0, 0.0};  // scalar read-back (pageable; each read is followed by a sync)
 
@@ -291,30 +307,39 @@ int solve_dm(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* P
         if (!(e_nc || g_nc)) break;
         const int cur = (int)(k & 1), prv = cur ^ 1;
 
-        // 1. density + Fock + energy
-        CPPHF_TRY(dm_density(Q, p, P, nk, nb, st));
-        if (project) {
-            CPPHF_TRY(call_project(project, puser, P, K, st));
-            CPPHF_TRY(hermitize(P, P, nk, nb, st));
-        }
+        // 1. density (with occupations from the last eps_work and mu) + Fock + energy
+        CPPHF_TRY(density(ew));
         CPPHF_TRY(build_fock(K, P, Sig, F, nullptr, &S->energy, nullptr, fws, L.fock_bytes, st));
-        CPPHF_TRY(dm_rotate(Q, F, F, eps, nk, nb, st));
-        // 2.-4. gradient, preconditioner, PR+ direction
-        CPPHF_TRY(dm_gradient(F, p, eps, wn, G[cur], g[cur], nk, nb, T_r, cfg->denom_scale, S, st));
-        CPPHF_TRY(dm_pr_beta(G[cur], G[prv], g[cur], g[prv], eps, p, wn, nk, nb, T_r, (int)cfg->cg_restart, (int)k, S,
-                             st));
-        CPPHF_TRY(dm_direction(G[cur], dQ[prv], g[cur], dp[prv], eps, p, wn, dQ[cur], dp[cur], nk, nb, T_r,
-                               cfg->max_step, S, st));
-        // 5. spectral Cayley line search
-        CPPHF_TRY(eigh_batched(dQ[cur], lam, Vd, nk, nb, 1, nullptr, st));
-        CPPHF_TRY(dm_rotate(Vd, F, Sig, nullptr, nk, nb, st));
-        for (int64_t bt = 0; bt < cfg->bt_max; ++bt)
-            CPPHF_TRY(dm_trial(Vd, Sig, lam, p, dp[cur], wn, nk, nb, T_r, cfg->bt_shrink, bt == cfg->bt_max - 1,
-                               fallback, S, st));
-        // 6. retraction, mu, occupations
-        CPPHF_TRY(dm_retract(Q, Vd, Sig, lam, ew, nk, nb, S, st));
+        // 2.-4. Ft = Q^H F Q, gradient, preconditioner, PR+ direction
+        if (small) {
+            CPPHF_TRY(dm_small_rot_grad(Q, F, p, wn, eps, G[cur], g[cur], nk, nb, T_r, cfg->denom_scale, S, st));
+            CPPHF_TRY(dm_small_pr_beta(G[cur], G[prv], g[cur], g[prv], eps, p, wn, nk, nb, T_r, (int)cfg->cg_restart,
+                                       (int)k, S, st));
+            CPPHF_TRY(dm_small_direction(G[cur], dQ[prv], g[cur], dp[prv], eps, p, wn, dQ[cur], dp[cur], nk, nb, T_r,
+                                         cfg->max_step, S, st));
+        } else {
+            CPPHF_TRY(dm_rotate(Q, F, F, eps, nk, nb, st));
+            CPPHF_TRY(dm_gradient(F, p, eps, wn, G[cur], g[cur], nk, nb, T_r, cfg->denom_scale, S, st));
+            CPPHF_TRY(dm_pr_beta(G[cur], G[prv], g[cur], g[prv], eps, p, wn, nk, nb, T_r, (int)cfg->cg_restart, (int)k,
+                                 S, st));
+            CPPHF_TRY(dm_direction(G[cur], dQ[prv], g[cur], dp[prv], eps, p, wn, dQ[cur], dp[cur], nk, nb, T_r,
+                                   cfg->max_step, S, st));
+        }
+        // 5. Cayley line search (elimination form of the spectral Cayley factor)
+        for (int64_t bt = 0; bt < cfg->bt_max; ++bt) {
+            if (small)
+                CPPHF_TRY(dm_small_trial(dQ[cur], F, p, dp[cur], wn, nk, nb, T_r, cfg->bt_shrink,
+                                         bt == cfg->bt_max - 1, fallback, S, st));
+            else
+                CPPHF_TRY(dm_trial_lu(dQ[cur], F, p, dp[cur], wn, nk, nb, T_r, cfg->bt_shrink, bt == cfg->bt_max - 1,
+                                      fallback, S, st));
+        }
+        // 6. retraction and mu (occupations are formed by the next density step)
+        if (small)
+            CPPHF_TRY(dm_small_retract(Q, dQ[cur], F, ew, nk, nb, S, st));
+        else
+            CPPHF_TRY(dm_retract_lu(Q, dQ[cur], F, ew, nk, nb, S, st));
         CPPHF_TRY(mu_solve(ew, wn, nk, nb, n_t, &S->mu, T_r, mu_it, 1, &S->mu, mws, L.mu_bytes, st));
-        CPPHF_TRY(dm_occupations(ew, &S->mu, T_r, p, nk * nb, st));
         // 7. record
         CPPHF_CUDA(cudaMemcpyAsync(hbuf, &S->energy, sizeof(double), cudaMemcpyDeviceToHost, st));
         CPPHF_CUDA(cudaMemcpyAsync(hbuf + 1, &S->grad_norm, sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -332,22 +357,13 @@ int solve_dm(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* P
     }
 
     // ---- finalize (solver_dm.hpp:615-652) ----
-    CPPHF_TRY(dm_density(Q, p, P, nk, nb, st));
-    if (project) {
-        CPPHF_TRY(call_project(project, puser, P, K, st));
-        CPPHF_TRY(hermitize(P, P, nk, nb, st));
-    }
+    CPPHF_TRY(density(ew));
     CPPHF_TRY(build_fock(K, P, Sig, F, nullptr, nullptr, nullptr, fws, L.fock_bytes, st));
     CPPHF_TRY(dm_rotate(Q, F, F, nullptr, nk, nb, st));
     CPPHF_TRY(eigh_batched(F, ew, Vd, nk, nb, 0, nullptr, st));
     CPPHF_TRY(dm_q_times_u(Q, Vd, nk, nb, st));
     CPPHF_TRY(mu_solve(ew, wn, nk, nb, n_t, &S->mu, T_r, mu_it, 1, &S->mu, mws, L.mu_bytes, st));
-    CPPHF_TRY(dm_occupations(ew, &S->mu, T_r, p, nk * nb, st));
-    CPPHF_TRY(dm_density(Q, p, P, nk, nb, st));
-    if (project) {
-        CPPHF_TRY(call_project(project, puser, P, K, st));
-        CPPHF_TRY(hermitize(P, P, nk, nb, st));
-    }
+    CPPHF_TRY(density(ew));
     CPPHF_TRY(build_fock(K, P, Sig, F, nullptr, &S->energy, nullptr, fws, L.fock_bytes, st));
     if (Q_out) CPPHF_CUDA(cudaMemcpyAsync(Q_out, Q, fbytes, cudaMemcpyDeviceToDevice, st));
     if (p_out) CPPHF_CUDA(cudaMemcpyAsync(p_out, p, vbytes, cudaMemcpyDeviceToDevice, st));

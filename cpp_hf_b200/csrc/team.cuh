@@ -86,7 +86,8 @@ __device__ __forceinline__ double2 cayley_factor(double lam, double tau) {
 }
 
 // Last-block-done reduction: every block adds NV values; the last block to
-// arrive sums all partials in block order (deterministic) into out[0..NV) and
+// arrive sums all partials (thread-strided, then a fixed tree: deterministic for
+// a given grid) into out[0..NV) and
 // resets the counter.  Returns true in every thread of the last block.
 template <int NV>
 __device__ __forceinline__ bool reduce_last_block(double (&v)[NV], double* partials, unsigned* counter,
@@ -103,14 +104,19 @@ __device__ __forceinline__ bool reduce_last_block(double (&v)[NV], double* parti
     }
     __syncthreads();
     if (is_last) {
-        if (threadIdx.x == 0) {
-            __threadfence();
+        // whole last block: thread-strided partial sums, then the fixed block tree
+        __threadfence();
+        double acc[NV];
 #pragma unroll
-            for (int i = 0; i < NV; ++i) {
-                double s = 0.0;
-                for (int b = 0; b < G; ++b) s += __ldcg(&partials[(size_t)i * G + b]);
-                out[i] = s;
-            }
+        for (int i = 0; i < NV; ++i) {
+            double s = 0.0;
+            for (int b = threadIdx.x; b < G; b += blockDim.x) s += __ldcg(&partials[(size_t)i * G + b]);
+            acc[i] = s;
+        }
+        block_sum<NV>(acc, red);
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int i = 0; i < NV; ++i) out[i] = acc[i];
             atomicExch(counter, 0u);
         }
         __syncthreads();
