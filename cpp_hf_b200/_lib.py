@@ -83,6 +83,7 @@ _SIGS = {
     "cpphf_mu_workspace_bytes": (sz, [i64, i64]),
     "cpphf_find_mu_bisection": (C.c_int, [vp, vp, i64, i64, f64, f64, C.c_int, vp, vp, sz, vp]),
     "cpphf_solve_mu_inloop": (C.c_int, [vp, vp, i64, i64, f64, vp, f64, C.c_int, vp, vp, sz, vp]),
+    "cpphf_find_mu_bisection_noalloc": (C.c_int, [vp, vp, i64, i64, f64, f64, C.c_int, vp, vp]),
     "cpphf_build_fock_workspace_bytes": (sz, [C.POINTER(Kernel)]),
     "cpphf_build_fock": (C.c_int, [C.POINTER(Kernel), vp, vp, vp, vp, vp, vp, vp, sz, vp]),
     "cpphf_cayley_spectral_setup": (C.c_int, [vp, vp, vp, i64, i64, vp]),

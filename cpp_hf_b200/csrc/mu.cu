@@ -190,6 +190,17 @@ int max_coop_grid() {
     return g;
 }
 
+
+// ---------------------------------------------------------------------------
+// Allocation-free bisection entry point.  Its scratch (grid-barrier words and
+// block partials, the same layout the workspace variant uses) is this
+// file-scope array, sized for the largest cooperative grid the solver ever
+// launches.  Every GPU that loads the library holds it until the process
+// exits; every call shares it.
+// ---------------------------------------------------------------------------
+constexpr size_t kMuNoAllocScratchBytes = 64 + sizeof(double) * (6 * (size_t)kMuMaxGrid + 8);
+static __device__ __align__(256) unsigned char g_mu_noalloc_scratch[kMuNoAllocScratchBytes];
+
 }  // namespace
 
 size_t mu_workspace_bytes(int64_t, int64_t) {
@@ -238,6 +249,38 @@ int cpphf_find_mu_bisection(const double* eps, const double* weights, int64_t nk
     if (maxiter <= 0) maxiter = 30;
     return cpphf::mu_solve(eps, weights, nk, nb, n_e, nullptr, T, maxiter, 0, mu_out, workspace,
                            workspace_bytes, static_cast<cudaStream_t>(stream));
+}
+
+// The device address of g_mu_noalloc_scratch for the current device.  Host
+// code only sees a host-side stand-in for the array under that name, so the
+// address is looked up once per device with that device current (first call on
+// the device; keep that call outside stream capture) and cached.
+static int noalloc_scratch(void** out) {
+    static std::mutex mtx;
+    static void* ptrs[64] = {nullptr};
+    int dev = 0;
+    CPPHF_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return cpphf::fail(CPPHF_ERR_UNSUPPORTED, "find_mu_bisection_noalloc: device index >= 64");
+    std::lock_guard<std::mutex> lock(mtx);
+    if (!ptrs[dev]) {
+        void* p = nullptr;
+        CPPHF_CUDA(cudaGetSymbolAddress(&p, cpphf::g_mu_noalloc_scratch));
+        ptrs[dev] = p;
+    }
+    *out = ptrs[dev];
+    return CPPHF_OK;
+}
+
+int cpphf_find_mu_bisection_noalloc(const double* eps, const double* weights, int64_t nk, int64_t nb, double n_e,
+                                    double T, int maxiter, double* mu_out, void* stream) {
+    if (nk < 1 || nb < 1) return cpphf::fail(CPPHF_ERR_INVALID, "mu: empty eigenvalue array");
+    if (nk * nb > CPPHF_MU_NOALLOC_MAX_EIGENVALUES)
+        return cpphf::fail(CPPHF_ERR_INVALID, "find_mu_bisection_noalloc: nk*nb exceeds the maximum of 2^31-1 eigenvalues");
+    void* scratch = nullptr;
+    CPPHF_TRY(noalloc_scratch(&scratch));
+    if (maxiter <= 0) maxiter = 30;
+    return cpphf::mu_solve(eps, weights, nk, nb, n_e, nullptr, T, maxiter, 0, mu_out, scratch,
+                           cpphf::kMuNoAllocScratchBytes, static_cast<cudaStream_t>(stream));
 }
 
 int cpphf_solve_mu_inloop(const double* eps, const double* w_norm, int64_t nk, int64_t nb,

@@ -37,6 +37,10 @@ extern "C" {
 const char* cpphf_last_error(void);
 int cpphf_version(void);
 
+/* Device-side flag set by bounded in-kernel waits (TMA barriers) that gave up;
+ * synchronises the device, returns the flag (0 = none), clears it if clear != 0. */
+int cpphf_device_error(int clear);
+
 /* Synchronous host <-> device copies on `stream` (for projector callbacks). */
 int cpphf_copy_d2h(void* dst_host, const void* src_device, size_t bytes, void* stream);
 int cpphf_copy_h2d(void* dst_device, const void* src_host, size_t bytes, void* stream);
@@ -86,6 +90,24 @@ size_t cpphf_mu_workspace_bytes(int64_t nk, int64_t nb);
 int cpphf_find_mu_bisection(const double* eps, const double* weights, int64_t nk, int64_t nb,
                             double n_e, double T, int maxiter, double* mu_out, void* workspace,
                             size_t workspace_bytes, void* stream);
+/* Allocation-free variant of cpphf_find_mu_bisection.  No counterpart in the
+ * reference: it exists for callers that cannot allocate device memory at call
+ * time - a host plug-in whose device memory belongs to a fixed pool it may not
+ * grow, a runtime that forbids cudaMalloc/cudaFree in its critical path
+ * because they synchronise the device, or code issuing work from a stream
+ * callback where CUDA calls that allocate are not allowed.  Same arguments and
+ * result as cpphf_find_mu_bisection minus the workspace: the scratch (grid
+ * barrier words and block partials, about 49 KB) is a file-scope device array
+ * that every GPU loading the library holds until the process exits.  Limit:
+ * nk*nb <= CPPHF_MU_NOALLOC_MAX_EIGENVALUES; larger sizes are rejected with
+ * CPPHF_ERR_INVALID.  The first call on a device looks up the array's device
+ * address (with that device current) and should come before any stream
+ * capture.  Calls share the array: each call clears the words that must start
+ * at zero, and calls that overlap on the GPU race.  Calls no allocating
+ * routine. */
+#define CPPHF_MU_NOALLOC_MAX_EIGENVALUES 2147483647LL
+int cpphf_find_mu_bisection_noalloc(const double* eps, const double* weights, int64_t nk, int64_t nb,
+                                    double n_e, double T, int maxiter, double* mu_out, void* stream);
 /* mu0 is a device scalar (the warm start). */
 int cpphf_solve_mu_inloop(const double* eps, const double* w_norm, int64_t nk, int64_t nb,
                           double n_target_norm, const double* mu0, double T, int maxiter,
