@@ -20,6 +20,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import re
 import statistics
 import subprocess
 import sys
@@ -46,6 +47,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--n", type=int, default=N_MESH)
+    ap.add_argument("--solves", type=int, default=1, help="also time solve/solve_scf (1) or not (0)")
+    ap.add_argument("--solve-reps", type=int, default=2)
+    ap.add_argument("--oracle-solve", type=int, default=1, help="oracle DM solve estimate on the host")
     return ap.parse_args()
 
 
@@ -175,14 +179,84 @@ def run_reference(a):
     return 0
 
 
+def _dm_call(native, args, P0, n_e, tol_E=1e-10, max_iter=1000):
+    """cpp_hf's solve() defaults (SolverConfig, solver.py:19-64) with tol_E = 1e-10."""
+    import torch
+
+    nk1, nk2, nb = P0.shape[0], P0.shape[1], P0.shape[2]
+    empty = torch.empty((0, nk1, nk2, nb, nb), dtype=torch.complex128, device=P0.device)
+    return native.solve_dm(args, P0, n_e, max_iter, tol_E, 0.0, 0.6, 0.5, 1e-3, 8, 10, 5, 25, 0, 0.5, 20,
+                           empty, 0.0, 1.0, [], None, False, True, False)
+
+
+def _scf_call(native, args, P0, n_e, tol=1e-9, max_iter=1000):
+    """solve_scf with linear mixing 0.5 and density/commutator tolerances `tol`."""
+    return native.solve_scf(args, P0, n_e, max_iter, tol, tol, 0.5, 0.0, None, [], "linear", 6, 2, 1.0, 0.0,
+                            True, False)
+
+
+def time_solves(torch, native, args_dev, P0_dev, n_e, reps):
+    """solves/s of solve (DM) and solve_scf at FP64 and switched precision, device resident."""
+    stream = torch.cuda.current_stream()
+    out = {}
+    results = {}
+    for kind, call in (("dm", _dm_call), ("scf", _scf_call)):
+        for prec in ("fp64", "mixed"):
+            a = dict(args_dev)
+            if prec == "mixed":
+                a["exchange_precision"] = "mixed"
+            r = call(native, a, P0_dev, n_e)  # warm-up (and the result checked below)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                r = call(native, a, P0_dev, n_e)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            t = e0.elapsed_time(e1) / 1e3 / reps
+            E = r[5] if kind == "dm" else r[2]
+            it = r[6] if kind == "dm" else r[4]
+            conv = r[7] if kind == "dm" else r[5]
+            results[(kind, prec)] = (E, r[2] if kind == "dm" else r[0])
+            out[f"{kind}_{prec}"] = {"solves_per_s": 1.0 / t, "ms_per_solve": 1e3 * t, "iterations": int(it),
+                                     "converged": bool(conv), "energy": float(E),
+                                     "ms_per_iteration": 1e3 * t / max(int(it), 1)}
+        e64, d64 = results[(kind, "fp64")]
+        emx, dmx = results[(kind, "mixed")]
+        out[f"{kind}_mixed"]["abs_dE_vs_fp64_gpu"] = abs(emx - e64)
+        out[f"{kind}_mixed"]["speedup_vs_fp64"] = out[f"{kind}_mixed"]["solves_per_s"] / out[f"{kind}_fp64"]["solves_per_s"]
+    return out
+
+
+def oracle_solve_estimate(args, P0_np, n_e, n_iter_gpu):
+    """Oracle DM solve time from a bounded sample: init + 2 iterations, extrapolated to the
+    iteration count of the FP64 GPU solve (the trajectories agree to ~1e-8)."""
+    from oracle import native_np
+
+    nk1, nk2, nb = P0_np.shape[0], P0_np.shape[1], P0_np.shape[2]
+    empty = np.empty((0, nk1, nk2, nb, nb), np.complex128)
+
+    def run(m):
+        t0 = time.perf_counter()
+        native_np.solve_dm(args, P0_np, n_e, m, 1e-10, 0.0, 0.6, 0.5, 1e-3, 8, 10, 5, 25, 0, 0.5, 20, empty, 0.0,
+                           1.0, [], None, False, False, False)
+        return time.perf_counter() - t0
+
+    t1 = run(1)
+    t3 = run(3)
+    per_it = max((t3 - t1) / 2.0, 1e-9)
+    base = max(t1 - per_it, 0.0)
+    total = base + n_iter_gpu * per_it
+    return 1.0 / total, per_it, base, t1 + t3
+
+
 def load_traffic():
-    f = ROOT / "profiles" / "exchange_traffic.json"
-    if f.exists():
-        try:
-            return json.loads(f.read_text())
-        except Exception:
-            return None
-    return None
+    """DRAM bytes per exchange from the committed ncu summary of the 192x192 nb=8 exchange."""
+    f = ROOT / "profiles" / "exchange_fp64_layered192_nb8.md"
+    if not f.exists():
+        return None
+    m = re.search(r"^traffic_bytes_per_exchange:\s*(\d+)", f.read_text(), re.M)
+    return {"nk": [N_MESH, N_MESH], "nb": 2 * N_LAYERS, "dram_bytes_per_exchange": int(m.group(1))} if m else None
 
 
 def main():
@@ -278,6 +352,18 @@ def main():
     clocks = sampler.stop()
     t_e2e = g0.elapsed_time(g1) / 1e3
 
+    # ---- solves/s (DM and SCF, FP64 and switched precision), device resident ----
+    solves = None
+    if a.solves:
+        from cpp_hf_b200 import _native as native
+
+        args_dev = {k: (torch.from_numpy(v).to(dev) if isinstance(v, np.ndarray) and v.size > 64 else v)
+                    for k, v in args.items()}
+        P0_dev = torch.from_numpy(np.ascontiguousarray(_P0)).to(dev)
+        barrier()
+        solves = time_solves(torch, native, args_dev, P0_dev, _ne, a.solve_reps)
+        barrier()
+
     # max over ranks
     times = torch.tensor([t_dev, t_ex, t_e2e], dtype=torch.float64, device=dev)
     if pg is not None:
@@ -343,6 +429,19 @@ def main():
             "gpu_launches": a.steps * fb.launches_per_build,
             "clocks": clocks,
         }
+        if solves is not None:
+            solves["config"] = ("solve(): SolverConfig defaults with tol_E=1e-10 (plateau window 5); "
+                                "solve_scf(): linear mixing 0.5, density_tol=comm_tol=1e-9; "
+                                "mixed = complex64 exchange until gradient norm / commutator residual < 1e-5, "
+                                "then complex128; P0 and kernel arrays device resident; single solve per call")
+            if a.oracle_solve and (world == 1 or rank == 0):
+                v, per_it, base, spent = oracle_solve_estimate(args, _P0, _ne, solves["dm_fp64"]["iterations"])
+                solves["cpu_baseline_dm"] = {
+                    "solves_per_s": v, "cores": host_cores(), "kind": "port",
+                    "sample": f"oracle solve_dm init + 1 and 3 iterations ({spent:.1f} s), extrapolated to "
+                              f"{solves['dm_fp64']['iterations']} iterations: {per_it:.3f} s/iteration, "
+                              f"{base:.3f} s setup"}
+            line["solves"] = solves
         print(json.dumps(line), flush=True)
     if pg is not None:
         pg.barrier()

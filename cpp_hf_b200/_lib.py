@@ -46,7 +46,7 @@ class DmConfig(C.Structure):
         ("max_iter", i64), ("tol_E", f64), ("tol_grad", f64), ("plateau_window", i64),
         ("denom_scale", f64), ("max_step", f64), ("cg_restart", i64), ("bt_shrink", f64),
         ("bt_max", i64), ("mu_maxiter", i32), ("optimizer", i32),
-        ("block_sizes", C.POINTER(i64)), ("n_block_sizes", i64),
+        ("block_sizes", C.POINTER(i64)), ("n_block_sizes", i64), ("mixed_switch_grad", f64),
     ]
 
 
@@ -57,7 +57,7 @@ class DmResult(C.Structure):
 class ScfConfig(C.Structure):
     _fields_ = [
         ("max_iter", i64), ("density_tol", f64), ("comm_tol", f64), ("mixing", f64),
-        ("level_shift", f64), ("acceleration", i32), ("reserved", i32),
+        ("level_shift", f64), ("acceleration", i32), ("reserved", i32), ("mixed_switch_tol", f64),
     ]
 
 
@@ -92,6 +92,20 @@ _SIGS = {
     "cpphf_solve_dm_workspace_bytes": (sz, [C.POINTER(Kernel)]),
     "cpphf_solve_dm": (C.c_int, [C.POINTER(Kernel), C.POINTER(DmConfig), vp, f64, PROJECT_FN, vp,
                                  vp, vp, vp, vp, dp, dp, C.POINTER(DmResult), vp, sz, vp]),
+    "cpphf_density_from_fock_workspace_bytes": (sz, [i64, i64]),
+    "cpphf_density_from_fock": (C.c_int, [vp, vp, i64, i64, i64, f64, f64, f64, vp, vp, vp, vp, vp, sz, vp]),
+    "cpphf_exchange_adjoint": (C.c_int, [vp, vp, vp, i64, i64, i64, i64, vp]),
+    "cpphf_exchange_vr_grad_workspace_bytes": (sz, [i64, i64, i64]),
+    "cpphf_exchange_vr_grad": (C.c_int, [vp, vp, vp, vp, i64, i64, i64, i64, vp, sz, vp]),
+    "cpphf_fock_backward_prep": (C.c_int, [vp, vp, vp, vp, i64, i64, vp]),
+    "cpphf_reduce_workspace_bytes": (sz, []),
+    "cpphf_hf_energy": (C.c_int, [vp, vp, vp, C.c_int, vp, vp, vp, i64, i64, vp, vp, sz, vp]),
+    "cpphf_hf_energy_backward": (C.c_int, [vp, vp, vp, C.c_int, vp, vp, vp, vp, i64, i64, vp, vp, vp, vp, vp,
+                                           vp]),
+    "cpphf_occupation_entropy": (C.c_int, [vp, vp, i64, i64, vp, vp, sz, vp]),
+    "cpphf_occupation_entropy_backward": (C.c_int, [vp, vp, vp, i64, i64, vp, vp]),
+    "cpphf_density_from_fock_backward_workspace_bytes": (sz, []),
+    "cpphf_density_from_fock_backward": (C.c_int, [vp, vp, vp, f64, vp, vp, vp, i64, i64, vp, sz, vp]),
     "cpphf_solve_scf_workspace_bytes": (sz, [C.POINTER(Kernel)]),
     "cpphf_solve_scf": (C.c_int, [C.POINTER(Kernel), C.POINTER(ScfConfig), vp, f64, PROJECT_FN, vp,
                                   vp, vp, dp, dp, dp, C.POINTER(ScfResult), vp, sz, vp]),

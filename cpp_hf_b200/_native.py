@@ -44,7 +44,30 @@ __all__ = [
 
 # Exchange precision used by build_fock_apply / solve_* when the kernel_args
 # dict does not carry an "exchange_precision" entry (64 = complex128 FFT).
+# Extension keys of the kernel_args dict (absent from the reference, which
+# ignores them): "exchange_precision" = 64 | 32 | "mixed"; "mixed" runs solves
+# with a complex64 exchange until the gradient norm (DM), or both the density
+# and the commutator residuals (SCF), fall below "mixed_switch" (default 1e-5),
+# then complex128
+# to convergence; a single build_fock_apply under "mixed" is complex128.
 DEFAULT_EXCHANGE_PRECISION = 64
+DEFAULT_MIXED_SWITCH = 1.0e-5
+
+
+def _parse_precision(value):
+    """-> (exchange precision bits, switched?)"""
+    if isinstance(value, str):
+        v = value.lower()
+        if v == "mixed":
+            return 64, True
+        table = {"fp64": 64, "complex128": 64, "c128": 64, "fp32": 32, "complex64": 32, "c64": 32}
+        if v not in table:
+            raise ValueError(f"exchange_precision must be 64, 32 or 'mixed', got {value!r}")
+        return table[v], False
+    bits = int(value)
+    if bits not in (32, 64):
+        raise ValueError(f"exchange_precision must be 64, 32 or 'mixed', got {value!r}")
+    return bits, False
 
 
 def _lib_handle():
@@ -260,7 +283,8 @@ class _DeviceKernel:
         cOj = _to_dev(args["contact_Oj"], "c")
         if args.get("superlattice_fock_active", False) or args.get("superlattice_hartree_active", False):
             raise NotImplementedError("superlattice kernel_args are not supported by this entry point yet")
-        prec = int(args.get("exchange_precision", precision or DEFAULT_EXCHANGE_PRECISION))
+        prec, self.mixed = _parse_precision(args.get("exchange_precision", precision or DEFAULT_EXCHANGE_PRECISION))
+        self.mixed_switch = float(args.get("mixed_switch", DEFAULT_MIXED_SWITCH)) if self.mixed else 0.0
         self._keep = [h, VR, refP, w2d, HH, cg, cOi, cOj]
         self.shape = (nk1, nk2, nb)
         K = _lib.Kernel()
@@ -369,6 +393,7 @@ def solve_dm(kernel_args, P0, n_e, max_iter, tol_E, tol_grad, max_step, bt_shrin
     bs_arr, n_bs = _sizes_arr(block_sizes)
     cfg.block_sizes = C.cast(bs_arr, C.POINTER(_lib.i64))
     cfg.n_block_sizes = n_bs
+    cfg.mixed_switch_grad = dk.mixed_switch
     Q = torch.empty_like(P0_t) if return_Q else None
     D = torch.empty_like(P0_t) if return_density else None
     F = torch.empty_like(P0_t) if return_fock else None
@@ -411,6 +436,7 @@ def solve_scf(kernel_args, P0, n_e, max_iter, density_tol, comm_tol, mixing, lev
     cfg.density_tol, cfg.comm_tol = float(density_tol), float(comm_tol)
     cfg.mixing, cfg.level_shift = float(mixing), float(level_shift)
     cfg.acceleration = 0
+    cfg.mixed_switch_tol = dk.mixed_switch
     D = torch.empty_like(P0_t) if return_density else None
     F = torch.empty_like(P0_t) if return_fock else None
     hE = np.zeros(max(max_iter, 1))

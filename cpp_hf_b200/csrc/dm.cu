@@ -21,20 +21,6 @@ constexpr double TINY_REAL = 1.0e-30;  // types.hpp:13
 constexpr double LOGIT_CLIP = 1.0e-6;  // types.hpp:14
 constexpr double OCC_CLIP = 1.0e-8;    // types.hpp:16
 
-template <bool WARP>
-size_t team_smem(int nb, int nmat, int extra_doubles_per_team) {
-    const int teams = WARP ? kWarpTeams : 1;
-    const size_t per = (sizeof(double2) * team_mat_elems(nb) * nmat + sizeof(double) * extra_doubles_per_team + 15) &
-                       ~(size_t)15;
-    return per * teams + sizeof(double) * 64;
-}
-
-template <bool WARP>
-__device__ __forceinline__ double2* team_mats(unsigned char* raw, int nb, int nmat, int extra, int team) {
-    const size_t per = (sizeof(double2) * team_mat_elems(nb) * nmat + sizeof(double) * extra + 15) & ~(size_t)15;
-    return reinterpret_cast<double2*>(raw + per * team);
-}
-
 __device__ __forceinline__ double expit(double x) {
     if (x >= 0.0) return 1.0 / (1.0 + exp(-x));
     const double e = exp(x);
@@ -582,36 +568,6 @@ void init_attrs() {
         set_max_smem(k_retract_lu<false>);
     });
 }
-
-struct TeamLaunch {
-    bool warp;
-    int threads;
-    unsigned grid;
-};
-
-TeamLaunch team_launch(int64_t nk, int nb) {
-    TeamLaunch L;
-    L.warp = nb <= kTeamWarpMaxNb;
-    L.threads = L.warp ? 32 * kWarpTeams : kCtaTeamThreadsDense;
-    const int64_t teams = L.warp ? kWarpTeams : 1;
-    const int64_t want = (nk + teams - 1) / teams;
-    L.grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)num_sms() * 16));
-    return L;
-}
-
-unsigned flat_grid(int64_t n, int threads) {
-    const int64_t want = (n + threads - 1) / threads;
-    return (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, std::min<int64_t>(kDmMaxPartials, (int64_t)num_sms() * 4)));
-}
-
-#define TEAM_DISPATCH(L, kern, nmat, extra, ...)                                                  \
-    do {                                                                                          \
-        if (L.warp)                                                                               \
-            kern<true><<<L.grid, L.threads, team_smem<true>(nb, nmat, extra), st>>>(__VA_ARGS__);  \
-        else                                                                                      \
-            kern<false><<<L.grid, L.threads, team_smem<false>(nb, nmat, extra), st>>>(__VA_ARGS__); \
-        CPPHF_LAUNCH_CHECK(#kern);                                                                \
-    } while (0)
 
 }  // namespace
 

@@ -36,6 +36,12 @@ namespace {
 
 constexpr int kTargetThreads = 256;
 
+// column-pass modes: multiply by VR (the exchange), by conj(VR) (its adjoint),
+// or stop after the forward transform (2-D FFT of the input, for dL/dVR)
+constexpr int kColsVR = 0;
+constexpr int kColsConjVR = 1;
+constexpr int kColsForwardOnly = 2;
+
 // channel -> (row, col) of the HCP packing (upper triangle, row-major).
 __device__ __forceinline__ void hcp_pair(int ch, int nb, int& i, int& j) {
     int r = 0, c = ch;
@@ -131,7 +137,8 @@ __global__ void __launch_bounds__(256) k_rows_fwd_s(const double2* __restrict__ 
 }
 
 template <class Cx, int N1, int N2>
-__global__ void __launch_bounds__(256) k_cols_conv_s(Cx* T, const double2* __restrict__ VR, ExchangeGeom g, int CB) {
+__global__ void __launch_bounds__(256) k_cols_conv_s(Cx* T, const double2* __restrict__ VR, ExchangeGeom g, int CB,
+                                                      int vmode) {
     constexpr int N = N1 * N2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SView<Cx> s(smem_raw, N, CB);
@@ -156,16 +163,27 @@ __global__ void __launch_bounds__(256) k_cols_conv_s(Cx* T, const double2* __res
 #pragma unroll
         for (int n2 = 0; n2 < N2; ++n2) u[n2] = s.S[(a * N2 + n2) * CB + c];
         dft<N2, false>(u);
-        // u[k2] = X[a + N1 k2]: multiply by VR at kx = a + N1 k2
-#pragma unroll
-        for (int k2 = 0; k2 < N2; ++k2) {
+        if (vmode == kColsForwardOnly) {
+            // u[k2] = X[a + N1 k2]: the 2-D forward transform, stored in natural order
             if (live) {
-                const size_t vi = ((size_t)(a + N1 * k2) * g.n1 + ky) * g.dv + (g.dv == 1 ? 0 : ch);
-                u[k2] = cmul(u[k2], to_c(ld_stream(VR + vi), Cx{}));
+#pragma unroll
+                for (int k2 = 0; k2 < N2; ++k2) st_l2(T + ((size_t)(a + N1 * k2) * g.n1 + ky) * g.Ct + ch, u[k2]);
             }
+        } else {
+            // u[k2] = X[a + N1 k2]: multiply by VR (or conj VR) at kx = a + N1 k2
+#pragma unroll
+            for (int k2 = 0; k2 < N2; ++k2) {
+                if (live) {
+                    const size_t vi = ((size_t)(a + N1 * k2) * g.n1 + ky) * g.dv + (g.dv == 1 ? 0 : ch);
+                    double2 w = ld_stream(VR + vi);
+                    if (vmode == kColsConjVR) w = cconj(w);
+                    u[k2] = cmul(u[k2], to_c(w, Cx{}));
+                }
+            }
+            dft<N2, true>(u);
         }
-        dft<N2, true>(u);
     }
+    if (vmode == kColsForwardOnly) return;
     __syncthreads();
     if (a < N1) {
 #pragma unroll
@@ -342,7 +360,7 @@ __global__ void __launch_bounds__(256, 2) k_rows_fwd_p(const __grid_constant__ C
 template <class Cx, int N1, int N2>
 __global__ void __launch_bounds__(256) k_cols_conv_p(const __grid_constant__ CUtensorMap mT,
                                                      const __grid_constant__ CUtensorMap mV, Cx* T, ExchangeGeom g,
-                                                     int CB, int nchunk, int ntiles) {
+                                                     int CB, int nchunk, int ntiles, int conjv) {
     constexpr int N = N1 * N2;
     extern __shared__ __align__(16) unsigned char smem_dyn[];
     unsigned char* smem_raw = align128(smem_dyn);
@@ -399,7 +417,8 @@ __global__ void __launch_bounds__(256) k_cols_conv_p(const __grid_constant__ CUt
             dft<N2, false>(u);
 #pragma unroll
             for (int k2 = 0; k2 < N2; ++k2) {
-                const double2 w = g.dv == 1 ? Vt[a + N1 * k2] : Vt[(a + N1 * k2) * CB + c];
+                double2 w = g.dv == 1 ? Vt[a + N1 * k2] : Vt[(a + N1 * k2) * CB + c];
+                if (conjv) w = cconj(w);
                 u[k2] = cmul(u[k2], to_c(w, Cx{}));
             }
             dft<N2, true>(u);
@@ -544,7 +563,8 @@ __global__ void k_rows_fwd_g(const double2* __restrict__ P, const double2* __res
 }
 
 template <class Cx>
-__global__ void k_cols_conv_g(Cx* T, const double2* __restrict__ VR, ExchangeGeom g, FftPlan1D pl, int CB) {
+__global__ void k_cols_conv_g(Cx* T, const double2* __restrict__ VR, ExchangeGeom g, FftPlan1D pl, int CB,
+                              int vmode) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     GView<Cx> s(smem_raw, pl.n, CB);
     const int ky = blockIdx.x, chunk0 = blockIdx.y * CB, n = pl.n;
@@ -557,12 +577,22 @@ __global__ void k_cols_conv_g(Cx* T, const double2* __restrict__ VR, ExchangeGeo
     }
     __syncthreads();
     Cx* r = fft_tile<false>(s.buf, s.alt, s.tw, pl, CB);
+    if (vmode == kColsForwardOnly) {
+        for (int e = threadIdx.x; e < n * CB; e += blockDim.x) {
+            const int nx = e / CB, c = e - nx * CB;
+            const int ch = chunk0 + c;
+            if (ch < g.C) st_l2(T + ((size_t)nx * g.n1 + ky) * g.Ct + ch, r[e]);
+        }
+        return;
+    }
     for (int e = threadIdx.x; e < n * CB; e += blockDim.x) {
         const int nx = e / CB, c = e - nx * CB;
         const int ch = chunk0 + c;
         if (ch < g.C) {
             const size_t vi = ((size_t)nx * g.n1 + ky) * g.dv + (g.dv == 1 ? 0 : ch);
-            r[e] = cmul(r[e], to_c(ld_stream(VR + vi), Cx{}));
+            double2 w = ld_stream(VR + vi);
+            if (vmode == kColsConjVR) w = cconj(w);
+            r[e] = cmul(r[e], to_c(w, Cx{}));
         }
     }
     __syncthreads();
@@ -707,9 +737,9 @@ struct Spec {
         CPPHF_LAUNCH_CHECK("exchange rows forward");
         return CPPHF_OK;
     }
-    static int cols(Cx* T, const double2* VR, const ExchangeGeom& g, cudaStream_t st) {
+    static int cols(Cx* T, const double2* VR, const ExchangeGeom& g, int vmode, cudaStream_t st) {
         attrs();
-        if (pipelined(g)) {
+        if (pipelined(g) && vmode != kColsForwardOnly) {
             const Launch L = plan_launch(N1 > N2 ? N1 : N2, g.C, sizeof(Cx), N1 * N2, false);
             const PipeLayout PL = pipe_layout(N1 * N2, L.CB, sizeof(Cx), true);
             if (PL.total <= kSmemMax) {
@@ -722,14 +752,15 @@ struct Spec {
                 if (ok) {
                     const int nt = g.n1 * L.nchunk;
                     const int grid = pgrid(k_cols_conv_p<Cx, N1, N2>, L.threads, PL.total, nt);
-                    k_cols_conv_p<Cx, N1, N2><<<grid, L.threads, PL.total, st>>>(mT, mV, T, g, L.CB, L.nchunk, nt);
+                    k_cols_conv_p<Cx, N1, N2><<<grid, L.threads, PL.total, st>>>(mT, mV, T, g, L.CB, L.nchunk, nt,
+                                                                                 vmode == kColsConjVR ? 1 : 0);
                     CPPHF_LAUNCH_CHECK("exchange columns convolve (pipelined)");
                     return CPPHF_OK;
                 }
             }
         }
         const Launch L = plan_launch(N1 > N2 ? N1 : N2, g.C, sizeof(Cx), N1 * N2, false);
-        k_cols_conv_s<Cx, N1, N2><<<dim3(g.n1, L.nchunk), L.threads, L.smem, st>>>(T, VR, g, L.CB);
+        k_cols_conv_s<Cx, N1, N2><<<dim3(g.n1, L.nchunk), L.threads, L.smem, st>>>(T, VR, g, L.CB, vmode);
         CPPHF_LAUNCH_CHECK("exchange columns convolve");
         return CPPHF_OK;
     }
@@ -815,10 +846,10 @@ int pass_rows_fwd(const double2* P, const double2* refP, Cx* T, const ExchangeGe
 }
 
 template <class Cx>
-int pass_cols(Cx* T, const double2* VR, const ExchangeGeom& g, cudaStream_t st) {
+int pass_cols(Cx* T, const double2* VR, const ExchangeGeom& g, int vmode, cudaStream_t st) {
     switch (g.n0) {
 #define X(N, A, B) \
-    case N: return Spec<Cx, A, B>::cols(T, VR, g, st);
+    case N: return Spec<Cx, A, B>::cols(T, VR, g, vmode, st);
         CPPHF_SPEC_SIZES(X)
 #undef X
         default: break;
@@ -828,7 +859,7 @@ int pass_cols(Cx* T, const double2* VR, const ExchangeGeom& g, cudaStream_t st) 
     Gen<Cx>::attrs();
     const Launch L = plan_launch(g.n0, g.C, sizeof(Cx), g.n0, true);
     if (L.smem > kSmemMax) return fail(CPPHF_ERR_UNSUPPORTED, "exchange: mesh axis too long for the shared-memory FFT");
-    k_cols_conv_g<Cx><<<dim3(g.n1, L.nchunk), L.threads, L.smem, st>>>(T, VR, g, pl, L.CB);
+    k_cols_conv_g<Cx><<<dim3(g.n1, L.nchunk), L.threads, L.smem, st>>>(T, VR, g, pl, L.CB, vmode);
     CPPHF_LAUNCH_CHECK("exchange columns convolve");
     return CPPHF_OK;
 }
@@ -854,9 +885,9 @@ int pass_rows_inv(const Cx* T, double2* Sigma, const ExchangeGeom& g, double sca
 
 template <class Cx>
 int launch_exchange(const double2* P, const double2* refP, const double2* VR, double2* Sigma, Cx* T,
-                    const ExchangeGeom& g, cudaStream_t st) {
+                    const ExchangeGeom& g, cudaStream_t st, int vmode = kColsVR) {
     CPPHF_TRY(pass_rows_fwd<Cx>(P, refP, T, g, st));
-    CPPHF_TRY(pass_cols<Cx>(T, VR, g, st));
+    CPPHF_TRY(pass_cols<Cx>(T, VR, g, vmode, st));
     CPPHF_TRY(pass_rows_inv<Cx>(T, Sigma, g, -1.0 / ((double)g.n0 * (double)g.n1), st));
     return CPPHF_OK;
 }
@@ -898,9 +929,106 @@ int exchange(const double2* P, const double2* refP, const double2* VR, double2* 
     return launch_exchange<double2>(P, refP, VR, Sigma, T, g, st);
 }
 
+namespace {
+
+// dL/dVR = -(1/nk) conj(X^)(q) G^(q) per channel (dv = nb*nb) or summed over the
+// channels (dv = 1); X^, G^ are the 2-D forward transforms, layout (q, C).
+__global__ void k_vr_grad(const double2* __restrict__ Xh, const double2* __restrict__ Gh, double2* __restrict__ gVR,
+                          int64_t nk, int C, int dv, double scale) {
+    if (dv != 1) {
+        const int64_t n = nk * C;
+        for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+            gVR[i] = cscale(cmul(cconj(Xh[i]), Gh[i]), scale);
+        return;
+    }
+    // one warp per q; fixed lane order -> deterministic
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t q = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < nk; q += warps) {
+        double2 acc = mk(0.0, 0.0);
+        for (int c = lane; c < C; c += 32) cfma(acc, cconj(Xh[q * C + c]), Gh[q * C + c]);
+        acc.x = warp_sum(acc.x);
+        acc.y = warp_sum(acc.y);
+        if (lane == 0) gVR[q] = cscale(acc, scale);
+    }
+}
+
+int check_adjoint_args(int64_t nk1, int64_t nk2, int64_t nb, int64_t dv) {
+    if (nk1 < 1 || nk2 < 1 || nb < 1) return fail(CPPHF_ERR_INVALID, "exchange: empty mesh or nb");
+    if (nk1 > 65535 || nk2 > 65535 || nb > 4096) return fail(CPPHF_ERR_INVALID, "exchange: size out of range");
+    if (!(dv == 1 || dv == nb)) return fail(CPPHF_ERR_INVALID, "VR shape must be (..., 1, 1) or (..., nb, nb).");
+    return CPPHF_OK;
+}
+
+ExchangeGeom full_geom(int64_t nk1, int64_t nk2, int64_t nb, int64_t dv) {
+    ExchangeGeom g;
+    g.n0 = (int)nk1;
+    g.n1 = (int)nk2;
+    g.nb = (int)nb;
+    g.hcp = 0;
+    g.C = (int)(nb * nb);
+    g.dv = dv == 1 ? 1 : (int)(nb * nb);
+    g.Ct = g.C;
+    g.shift = 0;
+    return g;
+}
+
+}  // namespace
+
+int exchange_adjoint(const double2* G, const double2* VR, double2* gP, int64_t nk1, int64_t nk2, int64_t nb,
+                     int64_t dv, cudaStream_t st) {
+    CPPHF_TRY(check_adjoint_args(nk1, nk2, nb, dv));
+    if (!G || !VR || !gP) return fail(CPPHF_ERR_INVALID, "exchange_adjoint: null pointer");
+    const ExchangeGeom g = full_geom(nk1, nk2, nb, dv);
+    return launch_exchange<double2>(G, nullptr, VR, gP, gP, g, st, kColsConjVR);
+}
+
+size_t exchange_vr_grad_workspace_bytes(int64_t nk1, int64_t nk2, int64_t nb) {
+    return 2 * (size_t)nk1 * nk2 * nb * nb * sizeof(double2);
+}
+
+int exchange_vr_grad(const double2* P, const double2* refP, const double2* G, double2* gVR, int64_t nk1, int64_t nk2,
+                     int64_t nb, int64_t dv, void* ws, size_t wsb, cudaStream_t st) {
+    CPPHF_TRY(check_adjoint_args(nk1, nk2, nb, dv));
+    if (!P || !G || !gVR) return fail(CPPHF_ERR_INVALID, "exchange_vr_grad: null pointer");
+    const size_t need = exchange_vr_grad_workspace_bytes(nk1, nk2, nb);
+    if (!ws || wsb < need)
+        return fail(CPPHF_ERR_INVALID, "exchange_vr_grad: workspace too small (" + std::to_string(need) + " bytes needed)");
+    const ExchangeGeom g = full_geom(nk1, nk2, nb, dv);
+    double2* Xh = static_cast<double2*>(ws);
+    double2* Gh = Xh + (size_t)nk1 * nk2 * g.C;
+    CPPHF_TRY(pass_rows_fwd<double2>(P, refP, Xh, g, st));
+    CPPHF_TRY(pass_cols<double2>(Xh, nullptr, g, kColsForwardOnly, st));
+    CPPHF_TRY(pass_rows_fwd<double2>(G, nullptr, Gh, g, st));
+    CPPHF_TRY(pass_cols<double2>(Gh, nullptr, g, kColsForwardOnly, st));
+    const int64_t nk = nk1 * nk2;
+    const int64_t work = dv == 1 ? nk * 32 : nk * g.C;
+    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>((work + 255) / 256, (int64_t)num_sms() * 8));
+    k_vr_grad<<<grid, 256, 0, st>>>(Xh, Gh, gVR, nk, g.C, g.dv, -1.0 / (double)nk);
+    CPPHF_LAUNCH_CHECK("exchange VR gradient");
+    return CPPHF_OK;
+}
+
 }  // namespace cpphf
 
 extern "C" {
+
+int cpphf_exchange_adjoint(const void* G, const void* VR, void* gP, int64_t nk1, int64_t nk2, int64_t nb, int64_t dv,
+                           void* stream) {
+    return cpphf::exchange_adjoint(static_cast<const double2*>(G), static_cast<const double2*>(VR),
+                                   static_cast<double2*>(gP), nk1, nk2, nb, dv, static_cast<cudaStream_t>(stream));
+}
+
+size_t cpphf_exchange_vr_grad_workspace_bytes(int64_t nk1, int64_t nk2, int64_t nb) {
+    return cpphf::exchange_vr_grad_workspace_bytes(nk1, nk2, nb);
+}
+
+int cpphf_exchange_vr_grad(const void* P, const void* refP, const void* G, void* gVR, int64_t nk1, int64_t nk2,
+                           int64_t nb, int64_t dv, void* workspace, size_t workspace_bytes, void* stream) {
+    return cpphf::exchange_vr_grad(static_cast<const double2*>(P), static_cast<const double2*>(refP),
+                                   static_cast<const double2*>(G), static_cast<double2*>(gVR), nk1, nk2, nb, dv,
+                                   workspace, workspace_bytes, static_cast<cudaStream_t>(stream));
+}
 
 size_t cpphf_exchange_workspace_bytes(int64_t nk1, int64_t nk2, int64_t nb, int hcp, int precision) {
     return cpphf::exchange_workspace_bytes(nk1, nk2, nb, hcp, precision);

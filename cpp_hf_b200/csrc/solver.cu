@@ -170,6 +170,22 @@ struct SolverWs {
     }
 };
 
+// Fock workspace large enough for the complex64 and the complex128 exchange, so
+// a switched-precision solve can build in either form from one workspace.
+size_t fock_bytes_any_precision(const cpphf_kernel* K) {
+    cpphf_kernel K32 = *K;
+    K32.exchange_precision = 32;
+    return std::max(build_fock_workspace_bytes(K), build_fock_workspace_bytes(&K32));
+}
+
+// Exchange precision of a switched solve: complex64 first, complex128 after.
+int check_mixed(const cpphf_kernel* K, double sw) {
+    if (!(sw >= 0.0)) return fail(CPPHF_ERR_INVALID, "mixed-precision switch threshold must be >= 0");
+    if (sw > 0.0 && K->exchange_precision != 64)
+        return fail(CPPHF_ERR_INVALID, "a switched-precision solve needs exchange_precision 64 in the kernel");
+    return CPPHF_OK;
+}
+
 struct DmLayout {
     size_t Q, P, Sig, F, G[2], dQ[2], Vd, p, eps, g[2], dp[2], lam, ew, wn, S, fock_ws, mu_ws, total;
     size_t fock_bytes, mu_bytes;
@@ -199,7 +215,7 @@ DmLayout dm_layout(const cpphf_kernel* K) {
     L.ew = W.take(vec);
     L.wn = W.take(sizeof(double) * nk);
     L.S = W.take(sizeof(DmScalars));
-    L.fock_bytes = build_fock_workspace_bytes(K);
+    L.fock_bytes = fock_bytes_any_precision(K);
     L.fock_ws = W.take(L.fock_bytes);
     L.mu_bytes = mu_workspace_bytes((int64_t)nk, (int64_t)nb);
     L.mu_ws = W.take(L.mu_bytes);
@@ -231,6 +247,7 @@ int solve_dm(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* P
         return fail(CPPHF_ERR_UNSUPPORTED, "optimizer='newton' (trust-region Newton) is not built into this library");
     CPPHF_TRY(check_block_sizes(cfg->block_sizes, cfg->n_block_sizes, K->nb));
     CPPHF_TRY(dm_check_nb(K->nb));
+    CPPHF_TRY(check_mixed(K, cfg->mixed_switch_grad));
     const DmLayout L = dm_layout(K);
     if (!ws || wsb < L.total)
         return fail(CPPHF_ERR_INVALID, "solve_dm: workspace too small (" + std::to_string(L.total) + " bytes needed)");
@@ -296,32 +313,48 @@ int solve_dm(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* P
     std::vector<double> hE((size_t)std::max<int64_t>(max_iter, 1)), hG((size_t)std::max<int64_t>(max_iter, 1));
     int64_t k = 0;
     const double fallback = std::pow(cfg->bt_shrink, (double)cfg->bt_max);
+    // Switched precision: complex64 exchange until the gradient norm falls below
+    // mixed_switch_grad (or the energy test would stop), then complex128.  The
+    // plateau window and the CG restart count restart at the switch (k0).
+    cpphf_kernel K32 = *K;
+    K32.exchange_precision = 32;
+    bool low = cfg->mixed_switch_grad > 0.0;
+    int64_t k0 = 0;
     while (k < max_iter) {
         bool e_nc;
-        if (cfg->plateau_window > 0 && k > cfg->plateau_window) {
+        const int64_t kk = k - k0;
+        if (cfg->plateau_window > 0 && kk > cfg->plateau_window) {
             e_nc = (hE[k - 1 - cfg->plateau_window] - hE[k - 1]) > cfg->tol_E;
         } else {
             e_nc = dE > cfg->tol_E;
         }
         const bool g_nc = (cfg->tol_grad > 0.0) && (grad_norm > cfg->tol_grad);
+        if (low && (!(e_nc || g_nc) || grad_norm < cfg->mixed_switch_grad)) {
+            low = false;
+            k0 = k;
+            dE = std::numeric_limits<double>::infinity();
+            E_prev = std::numeric_limits<double>::infinity();
+            continue;
+        }
         if (!(e_nc || g_nc)) break;
         const int cur = (int)(k & 1), prv = cur ^ 1;
+        const cpphf_kernel* Kb = low ? &K32 : K;
 
         // 1. density (with occupations from the last eps_work and mu) + Fock + energy
         CPPHF_TRY(density(ew));
-        CPPHF_TRY(build_fock(K, P, Sig, F, nullptr, &S->energy, nullptr, fws, L.fock_bytes, st));
+        CPPHF_TRY(build_fock(Kb, P, Sig, F, nullptr, &S->energy, nullptr, fws, L.fock_bytes, st));
         // 2.-4. Ft = Q^H F Q, gradient, preconditioner, PR+ direction
         if (small) {
             CPPHF_TRY(dm_small_rot_grad(Q, F, p, wn, eps, G[cur], g[cur], nk, nb, T_r, cfg->denom_scale, S, st));
             CPPHF_TRY(dm_small_pr_beta(G[cur], G[prv], g[cur], g[prv], eps, p, wn, nk, nb, T_r, (int)cfg->cg_restart,
-                                       (int)k, S, st));
+                                       (int)(k - k0), S, st));
             CPPHF_TRY(dm_small_direction(G[cur], dQ[prv], g[cur], dp[prv], eps, p, wn, dQ[cur], dp[cur], nk, nb, T_r,
                                          cfg->max_step, S, st));
         } else {
             CPPHF_TRY(dm_rotate(Q, F, F, eps, nk, nb, st));
             CPPHF_TRY(dm_gradient(F, p, eps, wn, G[cur], g[cur], nk, nb, T_r, cfg->denom_scale, S, st));
-            CPPHF_TRY(dm_pr_beta(G[cur], G[prv], g[cur], g[prv], eps, p, wn, nk, nb, T_r, (int)cfg->cg_restart, (int)k,
-                                 S, st));
+            CPPHF_TRY(dm_pr_beta(G[cur], G[prv], g[cur], g[prv], eps, p, wn, nk, nb, T_r, (int)cfg->cg_restart,
+                                 (int)(k - k0), S, st));
             CPPHF_TRY(dm_direction(G[cur], dQ[prv], g[cur], dp[prv], eps, p, wn, dQ[cur], dp[cur], nk, nb, T_r,
                                    cfg->max_step, S, st));
         }
@@ -410,7 +443,7 @@ ScfLayout scf_layout(const cpphf_kernel* K) {
     L.occ = W.take(vec);
     L.mu2 = W.take(4 * sizeof(double));
     L.S = W.take(sizeof(DmScalars));
-    L.fock_bytes = build_fock_workspace_bytes(K);
+    L.fock_bytes = fock_bytes_any_precision(K);
     L.fock_ws = W.take(L.fock_bytes);
     L.mu_bytes = mu_workspace_bytes((int64_t)nk, (int64_t)nb);
     L.mu_ws = W.take(L.mu_bytes);
@@ -430,6 +463,7 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
     if (cfg->acceleration != 0)
         return fail(CPPHF_ERR_UNSUPPORTED, "SCF acceleration 'diis'/'oda' is not built into this library");
     CPPHF_TRY(dm_check_nb(K->nb));
+    CPPHF_TRY(check_mixed(K, cfg->mixed_switch_tol));
     const ScfLayout L = scf_layout(K);
     if (!ws || wsb < L.total)
         return fail(CPPHF_ERR_INVALID, "solve_scf: workspace too small (" + std::to_string(L.total) + " bytes needed)");
@@ -450,11 +484,18 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
 
     double hbuf[4] = {0.0, 0.0, 0.0, 0.0};  // scalar read-back (pageable; each read is followed by a sync)
 
+    // switched precision: complex64 exchange until the density and commutator
+    // residuals both fall below mixed_switch_tol; convergence is only accepted
+    // in complex128
+    cpphf_kernel K32 = *K;
+    K32.exchange_precision = 32;
+    bool low = cfg->mixed_switch_tol > 0.0;
+
     // build_and_occupy (solver_scf.hpp:179-197); mu -> mu2[1], E -> S->energy
     auto build_and_occupy = [&]() -> int {
         if (project) CPPHF_TRY(call_project(project, puser, D, K, st));
         CPPHF_TRY(hermitize(D, D, nk, nb, st));
-        CPPHF_TRY(build_fock(K, D, Sig, F, nullptr, &S->energy, nullptr, fws, L.fock_bytes, st));
+        CPPHF_TRY(build_fock(low ? &K32 : K, D, Sig, F, nullptr, &S->energy, nullptr, fws, L.fock_bytes, st));
         if (project) {
             CPPHF_TRY(call_project(project, puser, F, K, st));
             CPPHF_TRY(hermitize(F, F, nk, nb, st));
@@ -509,6 +550,11 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
         const double d_res = std::sqrt(hbuf[1] / wsum);
         const double c_res = std::sqrt(hbuf[2] / wsum);
         converged = (d_res <= cfg->density_tol) && (c_res <= cfg->comm_tol);
+        if (low && (converged || std::max(d_res, c_res) < cfg->mixed_switch_tol)) {
+            // switch: mix as usual; the next build runs in complex128
+            low = false;
+            converged = false;
+        }
         if (converged) {
             CPPHF_CUDA(cudaMemcpyAsync(D, Pn, fbytes, cudaMemcpyDeviceToDevice, st));
         } else {
@@ -539,9 +585,68 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
     return CPPHF_OK;
 }
 
+// ---------------------------------------------------------------------------
+// density_from_fock (solver_scf.hpp:96-154, dense eigh branch)
+// ---------------------------------------------------------------------------
+size_t density_from_fock_workspace_bytes(int64_t nk, int64_t nb) {
+    SolverWs W;
+    W.take(sizeof(double) * (size_t)nk * nb);  // shifted energies
+    W.take(sizeof(double) * (size_t)nk * nb);  // occupations
+    W.take(4 * sizeof(double));                // mu_raw, mu
+    W.take(mu_workspace_bytes(nk, nb));
+    return W.total;
+}
+
+int density_from_fock(const double2* F, const double* w, int64_t nk1, int64_t nk2, int64_t nb, double n_e, double T,
+                      double level_shift, double2* P, double* eps, double2* V, double* mu_out, void* ws, size_t wsb,
+                      cudaStream_t st) {
+    if (nk1 < 1 || nk2 < 1 || nb < 1) return fail(CPPHF_ERR_INVALID, "density_from_fock: empty mesh or nb");
+    if (!F || !w || !P || !eps || !V || !mu_out) return fail(CPPHF_ERR_INVALID, "density_from_fock: null pointer");
+    CPPHF_TRY(dm_check_nb(nb));
+    const int64_t nk = nk1 * nk2;
+    const size_t need = density_from_fock_workspace_bytes(nk, nb);
+    if (!ws || wsb < need)
+        return fail(CPPHF_ERR_INVALID, "density_from_fock: workspace too small (" + std::to_string(need) + " bytes needed)");
+    SolverWs W;
+    unsigned char* base = static_cast<unsigned char*>(ws);
+    double* sh = reinterpret_cast<double*>(base + W.take(sizeof(double) * (size_t)nk * nb));
+    double* occ = reinterpret_cast<double*>(base + W.take(sizeof(double) * (size_t)nk * nb));
+    double* mu2 = reinterpret_cast<double*>(base + W.take(4 * sizeof(double)));
+    const size_t mb = mu_workspace_bytes(nk, nb);
+    void* mws = base + W.take(mb);
+    CPPHF_TRY(eigh_batched(F, eps, V, nk, (int)nb, 0, nullptr, st));
+    CPPHF_TRY(mu_solve(eps, w, nk, nb, n_e, nullptr, T, 30, 0, &mu2[0], mws, mb, st));
+    const double* e_occ = eps;
+    const double* mu = &mu2[0];
+    if (level_shift != 0.0) {
+        k_level_shift<<<grid_for(nk * nb, 256), 256, 0, st>>>(eps, &mu2[0], T, level_shift, sh, nk * nb);
+        CPPHF_LAUNCH_CHECK("level shift");
+        e_occ = sh;
+        CPPHF_TRY(mu_solve(e_occ, w, nk, nb, n_e, nullptr, T, 30, 0, &mu2[1], mws, mb, st));
+        mu = &mu2[1];
+    }
+    k_fermi<<<grid_for(nk * nb, 256), 256, 0, st>>>(e_occ, mu, T, occ, nk * nb);
+    CPPHF_LAUNCH_CHECK("fermi");
+    CPPHF_TRY(dm_density(V, occ, P, nk, (int)nb, st));
+    CPPHF_CUDA(cudaMemcpyAsync(mu_out, mu, sizeof(double), cudaMemcpyDeviceToDevice, st));
+    return CPPHF_OK;
+}
+
 }  // namespace cpphf
 
 extern "C" {
+
+size_t cpphf_density_from_fock_workspace_bytes(int64_t nk, int64_t nb) {
+    return cpphf::density_from_fock_workspace_bytes(nk, nb);
+}
+
+int cpphf_density_from_fock(const void* F, const double* w, int64_t nk1, int64_t nk2, int64_t nb, double n_e,
+                            double T, double level_shift, void* P, double* eps, void* V, double* mu, void* workspace,
+                            size_t workspace_bytes, void* stream) {
+    return cpphf::density_from_fock(static_cast<const double2*>(F), w, nk1, nk2, nb, n_e, T, level_shift,
+                                    static_cast<double2*>(P), eps, static_cast<double2*>(V), mu, workspace,
+                                    workspace_bytes, static_cast<cudaStream_t>(stream));
+}
 
 size_t cpphf_solve_dm_workspace_bytes(const cpphf_kernel* K) { return K ? cpphf::solve_dm_workspace_bytes(K) : 0; }
 

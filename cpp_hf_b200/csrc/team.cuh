@@ -41,6 +41,59 @@ struct Team {
 
 __host__ __device__ __forceinline__ size_t team_mat_elems(int nb) { return (size_t)nb * (nb + 1); }
 
+// dynamic shared memory of a team kernel: nmat team matrices + extra doubles
+// per team, plus 64 doubles of block-reduction scratch
+template <bool WARP>
+inline size_t team_smem(int nb, int nmat, int extra_doubles_per_team) {
+    const int teams = WARP ? kWarpTeams : 1;
+    const size_t per = (sizeof(double2) * team_mat_elems(nb) * nmat + sizeof(double) * extra_doubles_per_team + 15) &
+                       ~(size_t)15;
+    return per * teams + sizeof(double) * 64;
+}
+
+template <bool WARP>
+__device__ __forceinline__ double2* team_mats(unsigned char* raw, int nb, int nmat, int extra, int team) {
+    const size_t per = (sizeof(double2) * team_mat_elems(nb) * nmat + sizeof(double) * extra + 15) & ~(size_t)15;
+    return reinterpret_cast<double2*>(raw + per * team);
+}
+
+struct TeamLaunch {
+    bool warp;
+    int threads;
+    unsigned grid;
+};
+
+// grid-stride launch over nk k-points in teams; the grid is capped so that the
+// last-block reductions fit kTeamMaxPartials partials
+constexpr int kTeamMaxPartials = 1024;
+
+inline TeamLaunch team_launch(int64_t nk, int nb) {
+    TeamLaunch L;
+    L.warp = nb <= kTeamWarpMaxNb;
+    L.threads = L.warp ? 32 * kWarpTeams : kCtaTeamThreadsDense;
+    const int64_t teams = L.warp ? kWarpTeams : 1;
+    const int64_t want = (nk + teams - 1) / teams;
+    const int64_t cap = (int64_t)num_sms() * 16;
+    L.grid = (unsigned)(want < 1 ? 1 : (want < cap ? want : cap));
+    return L;
+}
+
+inline unsigned flat_grid(int64_t n, int threads) {
+    const int64_t want = (n + threads - 1) / threads;
+    int64_t cap = (int64_t)num_sms() * 4;
+    if (cap > kTeamMaxPartials) cap = kTeamMaxPartials;
+    return (unsigned)(want < 1 ? 1 : (want < cap ? want : cap));
+}
+
+#define TEAM_DISPATCH(L, kern, nmat, extra, ...)                                                  \
+    do {                                                                                          \
+        if (L.warp)                                                                               \
+            kern<true><<<L.grid, L.threads, team_smem<true>(nb, nmat, extra), st>>>(__VA_ARGS__);  \
+        else                                                                                      \
+            kern<false><<<L.grid, L.threads, team_smem<false>(nb, nmat, extra), st>>>(__VA_ARGS__); \
+        CPPHF_LAUNCH_CHECK(#kern);                                                                \
+    } while (0)
+
 template <bool WARP>
 __device__ __forceinline__ void tload(double2* S, const double2* __restrict__ G, int nb, const Team<WARP>& t) {
     const int ld = nb + 1;

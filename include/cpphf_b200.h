@@ -192,6 +192,12 @@ typedef struct cpphf_dm_config {
     int32_t optimizer;
     const int64_t* block_sizes;
     int64_t n_block_sizes;
+    /* Switched precision (no counterpart in the reference): > 0 runs the exchange
+     * in complex64 while the Riemannian gradient norm is >= this value, then in
+     * complex128 to the end (K->exchange_precision must be 64).  The energy test
+     * never ends the solve during the complex64 phase: it switches instead.
+     * 0 = plain solve at K->exchange_precision. */
+    double mixed_switch_grad;
 } cpphf_dm_config;
 
 typedef struct cpphf_dm_result {
@@ -221,6 +227,12 @@ typedef struct cpphf_scf_config {
     double level_shift;
     int32_t acceleration;
     int32_t reserved;
+    /* Switched precision (no counterpart in the reference): > 0 runs the exchange
+     * in complex64 until the density residual ||P_new - P||_w and the commutator
+     * residual ||[F,P]||_w are both below this value, then in complex128
+     * (K->exchange_precision must be 64); convergence is only accepted in the
+     * complex128 phase.  0 = plain. */
+    double mixed_switch_tol;
 } cpphf_scf_config;
 
 typedef struct cpphf_scf_result {
@@ -240,6 +252,70 @@ int cpphf_solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const vo
                     void* fock_out, double* hist_E, double* hist_density, double* hist_comm,
                     cpphf_scf_result* result, void* workspace, size_t workspace_bytes,
                     void* stream);
+
+/* Replaces density_from_fock (solver_scf.hpp:96-154, dense-eigh branch): eigh of
+ * herm(F), mu by bisection on the raw weights (30 iterations), optional level
+ * shift, P = herm(V diag(f) V^H).  P, V: device fields; eps (nk, nb) and the
+ * scalar mu: device.  The block_sizes fast path is not taken. */
+size_t cpphf_density_from_fock_workspace_bytes(int64_t nk, int64_t nb);
+int cpphf_density_from_fock(const void* F, const double* w, int64_t nk1, int64_t nk2, int64_t nb,
+                            double n_e, double T, double level_shift, void* P, double* eps, void* V,
+                            double* mu, void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---- Derivatives (no counterpart in the reference, which has no autograd) ----
+ * Gradients follow torch's convention for complex tensors: for a real loss L,
+ * grad z = dL/dRe z + i dL/dIm z.  Scalar upstream gradients (gE, gS) are device
+ * pointers so that a backward pass needs no host synchronisation. */
+
+/* Adjoint of the exchange map P -> Sigma (cpphf_exchange with refP = NULL, no
+ * ifftshift): gP = -IFFT2[FFT2(G) . conj(VR)].  Full channel set (no HCP). */
+int cpphf_exchange_adjoint(const void* G, const void* VR, void* gP, int64_t nk1, int64_t nk2,
+                           int64_t nb, int64_t dv, void* stream);
+
+/* dL/dVR = -(1/nk) conj(FFT2(P - refP)) . FFT2(G), per channel (dv = nb) or
+ * summed over the nb*nb channels (dv = 1).  Workspace: two fields. */
+size_t cpphf_exchange_vr_grad_workspace_bytes(int64_t nk1, int64_t nk2, int64_t nb);
+int cpphf_exchange_vr_grad(const void* P, const void* refP, const void* G, void* gVR,
+                           int64_t nk1, int64_t nk2, int64_t nb, int64_t dv, void* workspace,
+                           size_t workspace_bytes, void* stream);
+
+/* Backward of F = herm(h + Sigma + H): gS = gSigma + herm(gF) and gh = herm(gF).
+ * gSigma may be NULL; gS or gh may be NULL to skip them. */
+int cpphf_fock_backward_prep(const void* gSigma, const void* gF, void* gS, void* gh, int64_t nk,
+                             int64_t nb, void* stream);
+
+/* Workspace of the deterministic (last-block) reductions below. */
+size_t cpphf_reduce_workspace_bytes(void);
+
+/* E = sum_k w_k Re[Tr(h P) + 1/2 Tr((Sigma + H)(P - refP))] (fock.py:91-107,
+ * fock.hpp:324-383) into the device scalar E.  H is a field (H_per_k = 1) or
+ * one (nb, nb) matrix shared by all k (H_per_k = 0); Sigma, H, refP may be NULL. */
+int cpphf_hf_energy(const void* h, const void* Sigma, const void* H, int H_per_k, const void* P,
+                    const void* refP, const double* w, int64_t nk, int64_t nb, double* E,
+                    void* workspace, size_t workspace_bytes, void* stream);
+/* Gradients of E given the device scalar gE; any output may be NULL.  gH has
+ * the shape of H (field or shared (nb, nb)). */
+int cpphf_hf_energy_backward(const void* h, const void* Sigma, const void* H, int H_per_k,
+                             const void* P, const void* refP, const double* w, const double* gE,
+                             int64_t nk, int64_t nb, void* gP, void* gh, void* gSigma, void* gH,
+                             void* grefP, void* stream);
+
+/* S = -sum_k w_k sum_i [p ln p + (1 - p) ln(1 - p)], p clipped to [1e-14, 1 - 1e-14]
+ * (fock.py:110-115) into the device scalar S; and its gradient dS/dp times gS. */
+int cpphf_occupation_entropy(const double* p, const double* w_norm, int64_t nk, int64_t nb,
+                             double* S, void* workspace, size_t workspace_bytes, void* stream);
+int cpphf_occupation_entropy_backward(const double* p, const double* w_norm, const double* gS,
+                                      int64_t nk, int64_t nb, double* gp, void* stream);
+
+/* Vector-Jacobian product of cpphf_density_from_fock (level_shift = 0) with the
+ * electron count held fixed: gF = V [D o herm(V^H G V) - diag(w_k f'_i A / Z)] V^H,
+ * D_ij = (f_i - f_j)/(eps_i - eps_j), D_ii = f'_i, A = sum Re(G~_ii) f'_i,
+ * Z = sum w_k f'_i.  T is the temperature of the occupations f = expit((mu - eps)/T). */
+size_t cpphf_density_from_fock_backward_workspace_bytes(void);
+int cpphf_density_from_fock_backward(const void* V, const double* eps, const double* mu, double T,
+                                     const double* w, const void* G, void* gF, int64_t nk,
+                                     int64_t nb, void* workspace, size_t workspace_bytes,
+                                     void* stream);
 
 #ifdef __cplusplus
 }

@@ -380,3 +380,54 @@ def test_solve_scf_rejects_unknown_acceleration(native):
     args, P0, n_e = workloads.dirac(4, seed=0)
     with pytest.raises(ValueError, match="acceleration"):
         native.solve_scf(args, P0, n_e, 5, 1e-6, 1e-6, 0.5, 0.0, None, [], "bogus", 6, 2, 1.0, 0.0, True, True)
+
+
+# ---------------------------------------------------------------------------
+# switched precision (complex64 exchange, then complex128)
+# ---------------------------------------------------------------------------
+
+def _mixed(args, switch=1e-5):
+    a = dict(args)
+    a["exchange_precision"] = "mixed"
+    a["mixed_switch"] = switch
+    return a
+
+
+@pytest.mark.parametrize("case", ["dirac16", "layered12"])
+def test_solve_dm_mixed_precision_reaches_fp64_energy(native, oracle, case):
+    args, P0, n_e = workloads.dirac(16, seed=5) if case == "dirac16" else workloads.layered(12, n_layers=4, seed=2)
+    ref = _dm(oracle, args, P0, n_e, 300, 1e-11)
+    got = _dm(native, _mixed(args), P0, n_e, 300, 1e-11)
+    plain = _dm(native, args, P0, n_e, 300, 1e-11)
+    print(f"{case}: iterations mixed {got[6]} fp64 {plain[6]} oracle {ref[6]}; "
+          f"|dE| mixed {abs(got[5] - ref[5]):.3e} fp64 {abs(plain[5] - ref[5]):.3e}")
+    assert got[7] and ref[7]
+    # converged energies within 1e-9 of the FP64 oracle (the switched form's bar)
+    assert abs(got[5] - ref[5]) < 1e-9 * max(1.0, abs(ref[5]))
+    assert rel(got[2], ref[2]) < 1e-4
+    # the gradient history is recorded for both phases; the first iterations ran
+    # the complex64 exchange, so their energies differ from the FP64 run's
+    assert len(got[9]) == got[6]
+    assert got[8][0] != plain[8][0]
+    assert abs(got[8][0] - plain[8][0]) < 1e-5 * max(1.0, abs(plain[8][0]))
+
+
+def test_solve_dm_mixed_rejects_complex64_kernel(native):
+    args, P0, n_e = workloads.dirac(4, seed=0)
+    a = _mixed(args)
+    a["exchange_precision"] = "bogus"
+    with pytest.raises(ValueError, match="exchange_precision"):
+        _dm(native, a, P0, n_e, 5)
+
+
+def test_solve_scf_mixed_precision_reaches_fp64_energy(native, oracle):
+    args, P0, n_e = workloads.dirac(12, seed=3)
+    ref = _scf(oracle, args, P0, n_e, 300, 1e-10, 1e-10)
+    got = _scf(native, _mixed(args), P0, n_e, 300, 1e-10, 1e-10)
+    print(f"scf iterations mixed {got[4]} oracle {ref[4]}; |dE| {abs(got[2] - ref[2]):.3e}")
+    assert got[5] and ref[5]
+    # the second iteration (the first with a non-zero density) ran the complex64 exchange
+    assert got[6][1] != ref[6][1]
+    assert abs(got[6][1] - ref[6][1]) < 1e-5 * max(1.0, abs(ref[6][1]))
+    assert abs(got[2] - ref[2]) < 1e-9 * max(1.0, abs(ref[2]))
+    assert rel(got[0], ref[0]) < 1e-7
