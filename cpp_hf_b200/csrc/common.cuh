@@ -127,9 +127,11 @@ __device__ __forceinline__ double warp_min(double v) {
 }
 
 // Sum NV values per thread over the block; result valid in every thread.
-// `scratch` holds 32*NV doubles.  Fixed reduction tree -> bitwise reproducible.
-template <int NV>
-__device__ __forceinline__ void block_sum(double (&v)[NV], double* scratch) {
+// `scratch` holds at least 32*NV doubles (checked at compile time).  Fixed
+// reduction tree -> bitwise reproducible.
+template <int NV, int M>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double (&scratch)[M]) {
+    static_assert(M >= 32 * NV, "block_sum scratch needs 32 doubles per value");
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
 #pragma unroll
     for (int i = 0; i < NV; ++i) v[i] = warp_sum(v[i]);
@@ -206,10 +208,12 @@ struct GridBarrier {
         return ok_sh != 0;
     }
 
-    // Barrier whose last arriving block first sums the (2 x nblocks) partials
-    // `part` with warp 0 in a fixed lane-strided order and writes the two totals
-    // to `tot`, so the released blocks read two numbers instead of all partials.
-    // Ordering uses release/acquire atomics (no full fences).
+    // Barrier whose last arriving block first sums the (NV x nblocks) partials
+    // `part` (block b's values at part[NV b .. NV b + NV)) with warp 0 in a fixed
+    // lane-strided order and writes the NV totals to `tot`, so the released
+    // blocks read NV numbers instead of all partials.  Ordering uses
+    // release/acquire atomics (no full fences).
+    template <int NV = 2>
     __device__ bool wait_reduce(const double* part, int nblocks, double* tot) {
         __syncthreads();
         __shared__ int ok_sh, last_sh;
@@ -228,16 +232,18 @@ struct GridBarrier {
         if (!ok_sh) return false;
         if (last_sh) {
             if (threadIdx.x < 32) {
-                double s0 = 0.0, s1 = 0.0;
+                double sv[NV];
+#pragma unroll
+                for (int v = 0; v < NV; ++v) sv[v] = 0.0;
                 for (int b = threadIdx.x; b < nblocks; b += 32) {
-                    s0 += __ldcg(&part[2 * b]);
-                    s1 += __ldcg(&part[2 * b + 1]);
+#pragma unroll
+                    for (int v = 0; v < NV; ++v) sv[v] += __ldcg(&part[NV * b + v]);
                 }
-                s0 = warp_sum(s0);
-                s1 = warp_sum(s1);
+#pragma unroll
+                for (int v = 0; v < NV; ++v) sv[v] = warp_sum(sv[v]);
                 if (threadIdx.x == 0) {
-                    __stcg(&tot[0], s0);
-                    __stcg(&tot[1], s1);
+#pragma unroll
+                    for (int v = 0; v < NV; ++v) __stcg(&tot[v], sv[v]);
                     sync[0] = 0u;
                     asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(&sync[1]) : "memory");
                 }

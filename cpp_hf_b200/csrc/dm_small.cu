@@ -1,12 +1,17 @@
 // Direct-minimisation per-k kernels specialised for small band counts
 // (nb in {2, 4, 6, 8}; cpp_hf solver_dm.hpp:117-344).
 //
-// A group of GS = (nb rounded up to a power of two) threads owns one k-point;
-// thread r owns row r of every matrix in registers.  A CTA processes KT = 128/GS
-// k-points per tile: whole k-blocks are staged through shared memory with
-// coalesced loads/stores, and the operand that a row-times-matrix product needs
-// in full is read from the group's shared copy (a broadcast within the group).
-// Groups live inside one warp, so group-level ordering uses __syncwarp().
+// Tile kernels (density, rotation + gradient, Cayley trial, retraction): a
+// group of GS = (nb rounded up to a power of two) threads owns one k-point and
+// thread r owns row r of every matrix.  A CTA processes KT = 128/GS k-points
+// per tile: whole k-blocks are staged through shared memory with coalesced,
+// fully unrolled loads and stores into a padded layout (row stride nb + 1,
+// matrix stride MS chosen so that a warp's row reads and the groups' broadcast
+// reads fall in distinct banks).  Groups live inside one warp, so group-level
+// ordering uses __syncwarp().
+//
+// Element kernels (PR+ beta, direction): one thread per matrix element, so
+// every field access is coalesced; per-row terms are added by the j = 0 thread.
 #include "common.cuh"
 #include "dm.cuh"
 #include "dm_small.cuh"
@@ -30,20 +35,71 @@ __device__ __forceinline__ double expit(double x) {
     return e / (1.0 + e);
 }
 
+// Matrix stride in double2 units: >= nb * ld and, with 4 groups per warp
+// (gs = 8), congruent to 2 or 6 mod 8 so the groups' broadcast reads use
+// different banks; odd for smaller groups.
+constexpr int pad_ms(int nb, int ld, int gs) {
+    int m = nb * ld;
+    if (gs == 8) {
+        while (m % 8 != 2 && m % 8 != 6) ++m;
+    } else if (m % 2 == 0) {
+        ++m;
+    }
+    return m;
+}
+
 template <int NB>
 struct Geo {
-    static constexpr int GS = NB <= 2 ? 2 : (NB <= 4 ? 4 : 8);  // group size
-    static constexpr int KT = kThreads / GS;                     // k-points per CTA tile
+    static constexpr int GS = NB <= 2 ? 2 : (NB <= 4 ? 4 : 8);        // group size
+    static constexpr int KT = kThreads / GS;                           // k-points per CTA tile
     static constexpr int NB2 = NB * NB;
-    static constexpr int TILE = KT * NB2;                        // complex elements per field tile
+    static constexpr int LD = NB + 1;                                  // padded row stride
+    static constexpr int MS = pad_ms(NB, LD, GS);                      // padded matrix stride
+    static constexpr int TILE = KT * MS;                               // shared double2 per staged tile
+    static constexpr int PER = (KT * NB2 + kThreads - 1) / kThreads;  // elements per thread per tile
 };
 
-// coalesced copy of a tile of `n` complex elements global <-> shared
-__device__ __forceinline__ void tile_load(double2* s, const double2* __restrict__ g, int n) {
-    for (int e = threadIdx.x; e < n; e += blockDim.x) s[e] = g[e];
+// coalesced global (dense k-blocks) -> shared (padded) copy of one tile; all
+// loads are issued before the first shared store
+template <int NB>
+__device__ __forceinline__ void tile_load(double2* s, const double2* __restrict__ g, int nkt) {
+    using G = Geo<NB>;
+    const int n = nkt * G::NB2;
+    double2 v[G::PER];
+#pragma unroll
+    for (int u = 0; u < G::PER; ++u) {
+        const int e = threadIdx.x + u * kThreads;
+        v[u] = (e < n) ? g[e] : mk(0.0, 0.0);
+    }
+#pragma unroll
+    for (int u = 0; u < G::PER; ++u) {
+        const int e = threadIdx.x + u * kThreads;
+        if (e < n) {
+            const int kl = e / G::NB2, rem = e - kl * G::NB2, i = rem / NB, j = rem - i * NB;
+            s[kl * G::MS + i * G::LD + j] = v[u];
+        }
+    }
 }
-__device__ __forceinline__ void tile_store(double2* g, const double2* s, int n) {
-    for (int e = threadIdx.x; e < n; e += blockDim.x) g[e] = s[e];
+
+template <int NB>
+__device__ __forceinline__ void tile_store(double2* g, const double2* s, int nkt) {
+    using G = Geo<NB>;
+    const int n = nkt * G::NB2;
+#pragma unroll
+    for (int u = 0; u < G::PER; ++u) {
+        const int e = threadIdx.x + u * kThreads;
+        if (e < n) {
+            const int kl = e / G::NB2, rem = e - kl * G::NB2, i = rem / NB, j = rem - i * NB;
+            g[e] = s[kl * G::MS + i * G::LD + j];
+        }
+    }
+}
+
+template <int NB>
+__device__ __forceinline__ unsigned group_mask(int lane) {
+    using G = Geo<NB>;
+    const unsigned base = (1u << G::GS) - 1u;
+    return G::GS == 32 ? 0xffffffffu : (base << ((lane / G::GS) * G::GS));
 }
 
 // ---------------------------------------------------------------------------
@@ -64,7 +120,7 @@ __global__ void __launch_bounds__(kThreads) k_dens_occ(const double2* __restrict
     for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int64_t k0 = t * G::KT;
         const int nkt = (int)((nk - k0) < G::KT ? (nk - k0) : G::KT);
-        tile_load(sQ, Q + (size_t)k0 * G::NB2, nkt * G::NB2);
+        tile_load<NB>(sQ, Q + (size_t)k0 * G::NB2, nkt);
         for (int e = threadIdx.x; e < nkt * NB; e += blockDim.x) {
             const double pv = expit((m - ew[k0 * NB + e]) / T_r);
             sp[e] = pv;
@@ -72,24 +128,29 @@ __global__ void __launch_bounds__(kThreads) k_dens_occ(const double2* __restrict
         }
         __syncthreads();
         if (grp < nkt && r < NB) {
-            const double2* q = sQ + grp * G::NB2;
+            const double2* q = sQ + grp * G::MS;
             const double* pk = sp + grp * NB;
             double2 qr[NB];
 #pragma unroll
-            for (int l = 0; l < NB; ++l) qr[l] = cscale(q[r * NB + l], pk[l]);
+            for (int l = 0; l < NB; ++l) qr[l] = cscale(q[r * G::LD + l], pk[l]);
 #pragma unroll
             for (int j = 0; j < NB; ++j) {
                 double2 acc = mk(0.0, 0.0);
 #pragma unroll
-                for (int l = 0; l < NB; ++l) cfmac(acc, qr[l], q[j * NB + l]);
-                sX[grp * G::NB2 + r * NB + j] = acc;
+                for (int l = 0; l < NB; ++l) cfmac(acc, qr[l], q[j * G::LD + l]);
+                sX[grp * G::MS + r * G::LD + j] = acc;
             }
         }
         __syncthreads();
-        for (int e = threadIdx.x; e < nkt * G::NB2; e += blockDim.x) {
-            const int kl = e / G::NB2, rr = e - kl * G::NB2, i = rr / NB, j = rr - i * NB;
-            const double2 a = sX[e], b = sX[kl * G::NB2 + j * NB + i];
-            P[(size_t)k0 * G::NB2 + e] = mk(0.5 * (a.x + b.x), 0.5 * (a.y - b.y));
+        const int n = nkt * G::NB2;
+#pragma unroll
+        for (int u = 0; u < G::PER; ++u) {
+            const int e = threadIdx.x + u * kThreads;
+            if (e < n) {
+                const int kl = e / G::NB2, rr = e - kl * G::NB2, i = rr / NB, j = rr - i * NB;
+                const double2 a = sX[kl * G::MS + i * G::LD + j], b = sX[kl * G::MS + j * G::LD + i];
+                P[(size_t)k0 * G::NB2 + e] = mk(0.5 * (a.x + b.x), 0.5 * (a.y - b.y));
+            }
         }
         __syncthreads();
     }
@@ -107,8 +168,8 @@ __global__ void __launch_bounds__(kThreads) k_rot_grad(const double2* __restrict
                                                        double* __restrict__ g_p, int64_t nk, double T_r,
                                                        double denom_scale, DmScalars* S) {
     using G = Geo<NB>;
-    __shared__ double2 sQ[G::TILE];
-    __shared__ double2 sT[G::TILE];  // F Q, then Ft
+    __shared__ double2 sQ[G::TILE];  // Q, then the gradient
+    __shared__ double2 sT[G::TILE];  // F, then F Q, then Ft
     __shared__ double red[64];
     const int grp = threadIdx.x / G::GS, r = threadIdx.x % G::GS;
     const double mu = S->mu;
@@ -117,49 +178,48 @@ __global__ void __launch_bounds__(kThreads) k_rot_grad(const double2* __restrict
     for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int64_t k0 = t * G::KT;
         const int nkt = (int)((nk - k0) < G::KT ? (nk - k0) : G::KT);
-        tile_load(sQ, Q + (size_t)k0 * G::NB2, nkt * G::NB2);
+        tile_load<NB>(sQ, Q + (size_t)k0 * G::NB2, nkt);
+        tile_load<NB>(sT, F + (size_t)k0 * G::NB2, nkt);
         __syncthreads();
         const bool live = grp < nkt && r < NB;
         const int64_t k = k0 + grp;
-        if (live) {  // T = F Q (row r)
-            const double2* q = sQ + grp * G::NB2;
+        double2* tt = sT + grp * G::MS;
+        double2* q = sQ + grp * G::MS;
+        if (live) {  // row r of F Q replaces row r of F (only this thread touches that row)
             double2 fr[NB];
 #pragma unroll
-            for (int l = 0; l < NB; ++l) fr[l] = F[(size_t)k * G::NB2 + r * NB + l];
+            for (int l = 0; l < NB; ++l) fr[l] = tt[r * G::LD + l];
 #pragma unroll
             for (int j = 0; j < NB; ++j) {
                 double2 acc = mk(0.0, 0.0);
 #pragma unroll
-                for (int l = 0; l < NB; ++l) cfma(acc, fr[l], q[l * NB + j]);
-                sT[grp * G::NB2 + r * NB + j] = acc;
+                for (int l = 0; l < NB; ++l) cfma(acc, fr[l], q[l * G::LD + j]);
+                tt[r * G::LD + j] = acc;
             }
         }
         __syncthreads();
         double2 ftr[NB];
         if (live) {  // Ft = Q^H T (row r): Ft_rj = sum_l conj(Q_lr) T_lj
-            const double2* q = sQ + grp * G::NB2;
-            const double2* tt = sT + grp * G::NB2;
 #pragma unroll
             for (int j = 0; j < NB; ++j) {
                 double2 acc = mk(0.0, 0.0);
 #pragma unroll
-                for (int l = 0; l < NB; ++l) cfma(acc, cconj(q[l * NB + r]), tt[l * NB + j]);
+                for (int l = 0; l < NB; ++l) cfma(acc, cconj(q[l * G::LD + r]), tt[l * G::LD + j]);
                 ftr[j] = acc;
             }
         }
-        __syncthreads();
+        __syncthreads();  // all reads of Q and of F Q are done
         if (live) {
 #pragma unroll
-            for (int j = 0; j < NB; ++j) {
-                sT[grp * G::NB2 + r * NB + j] = ftr[j];
-                F[(size_t)k * G::NB2 + r * NB + j] = ftr[j];
-            }
+            for (int j = 0; j < NB; ++j) tt[r * G::LD + j] = ftr[j];
         }
         __syncthreads();
         if (live) {
-            const double2* ft = sT + grp * G::NB2;
             const double pr = p[k * NB + r];
-            const double er = ft[r * NB + r].x;
+            double er = ftr[0].x;
+#pragma unroll
+            for (int j = 1; j < NB; ++j)
+                if (j == r) er = ftr[j].x;
             eps[k * NB + r] = er;
             double gsq = 0.0;
 #pragma unroll
@@ -168,10 +228,10 @@ __global__ void __launch_bounds__(kThreads) k_rot_grad(const double2* __restrict
                 if (j != r) {
                     const double pj = p[k * NB + j];
                     const double2 aij = cscale(ftr[j], pj - pr);
-                    const double2 aji = cscale(ft[j * NB + r], pr - pj);
+                    const double2 aji = cscale(tt[j * G::LD + r], pr - pj);
                     gv = mk(0.5 * (aij.x - aji.x), 0.5 * (aij.y + aji.y));
                 }
-                Gout[(size_t)k * G::NB2 + r * NB + j] = gv;
+                q[r * G::LD + j] = gv;  // the gradient row takes Q's place
                 gsq += gv.x * gv.x + gv.y * gv.y;
             }
             v[0] += w[k] * gsq;
@@ -179,6 +239,9 @@ __global__ void __launch_bounds__(kThreads) k_rot_grad(const double2* __restrict
             g_p[k * NB + r] = er + T_r * (log(pv) - log1p(-pv)) - mu;
             v[1] += er * er;
         }
+        __syncthreads();
+        tile_store<NB>(F + (size_t)k0 * G::NB2, sT, nkt);
+        tile_store<NB>(Gout + (size_t)k0 * G::NB2, sQ, nkt);
         __syncthreads();
     }
     double out[2];
@@ -193,16 +256,17 @@ __global__ void __launch_bounds__(kThreads) k_rot_grad(const double2* __restrict
 // ---------------------------------------------------------------------------
 // Cayley unitary U(tau) = (I + tau d/2)^{-1} (I - tau d/2) of one k-point by
 // Gauss-Jordan elimination, one row per thread (row r of the result in u[]).
-// The pivot row is broadcast through the group's shared slot `piv`.
+// d is the group's padded matrix; the pivot row is broadcast through the
+// group's shared slot `piv`.
 // ---------------------------------------------------------------------------
-template <int NB>
+template <int NB, int LD>
 __device__ __forceinline__ void row_cayley(const double2* d, double tau, int r, double2* piv, double2 (&u)[NB],
                                            unsigned mask) {
     double2 mrow[NB];
     const double h = 0.5 * tau;
 #pragma unroll
     for (int j = 0; j < NB; ++j) {
-        const double2 a = cscale(d[r * NB + j], h);
+        const double2 a = cscale(d[r * LD + j], h);
         const double one = (j == r) ? 1.0 : 0.0;
         mrow[j] = mk(one + a.x, a.y);
         u[j] = mk(one - a.x, -a.y);
@@ -238,11 +302,11 @@ __device__ __forceinline__ void row_cayley(const double2* d, double tau, int r, 
     for (int j = 0; j < NB; ++j) u[j] = cscale(cmulc(u[j], dd), inv);
 }
 
-// diag(U^H Ft U) for the group: thread j holds Ft row j (ftj) and U row j
-// (uj); it forms c_jr = conj(U_jr) (Ft U)_jr for every r from the group's U in
-// shared memory `su`, and the group sums c_jr over j with xor-shuffles (fixed
-// tree).  Thread r returns diag_r.
-template <int NB, int GS>
+// diag(U^H Ft U) for the group: thread j holds Ft row j (ftj); it forms
+// c_jq = conj(U_jq) (Ft U)_jq for every q from the group's padded U in shared
+// memory `su`, and the group sums c_jq over j with xor-shuffles (fixed tree).
+// Thread r returns diag_r.
+template <int NB, int GS, int LD>
 __device__ __forceinline__ double row_diag_uhfu(const double2 (&ftj)[NB], const double2* su, int r, unsigned mask,
                                                 bool live) {
     double c[NB];
@@ -251,8 +315,8 @@ __device__ __forceinline__ double row_diag_uhfu(const double2 (&ftj)[NB], const 
     for (int q = 0; q < NB; ++q) {
         double2 wjq = mk(0.0, 0.0);
 #pragma unroll
-        for (int l = 0; l < NB; ++l) cfma(wjq, ftj[l], su[l * NB + q]);
-        const double2 ujq = su[rr * NB + q];
+        for (int l = 0; l < NB; ++l) cfma(wjq, ftj[l], su[l * LD + q]);
+        const double2 ujq = su[rr * LD + q];
         c[q] = live ? (ujq.x * wjq.x + ujq.y * wjq.y) : 0.0;
     }
 #pragma unroll
@@ -266,14 +330,8 @@ __device__ __forceinline__ double row_diag_uhfu(const double2 (&ftj)[NB], const 
     return out;
 }
 
-template <int NB>
-__device__ __forceinline__ unsigned group_mask(int lane) {
-    using G = Geo<NB>;
-    const unsigned base = (1u << G::GS) - 1u;
-    return G::GS == 32 ? 0xffffffffu : (base << ((lane / G::GS) * G::GS));
-}
-
 // One backtracking trial (solver_dm.hpp:577-589) by elimination.
+// Dynamic shared memory: sD | sF | sU, TILE double2 each.
 template <int NB>
 __global__ void __launch_bounds__(kThreads) k_trial_small(const double2* __restrict__ dQ, const double2* __restrict__ Ft,
                                                           const double* __restrict__ p, const double* __restrict__ d_p,
@@ -282,8 +340,10 @@ __global__ void __launch_bounds__(kThreads) k_trial_small(const double2* __restr
                                                           DmScalars* S) {
     if (S->accepted) return;  // grid-uniform
     using G = Geo<NB>;
-    __shared__ double2 sD[G::TILE];
-    __shared__ double2 sU[G::TILE];
+    extern __shared__ __align__(16) double2 dyn[];
+    double2* sD = dyn;
+    double2* sF = dyn + G::TILE;
+    double2* sU = dyn + 2 * G::TILE;
     __shared__ double2 sPiv[G::KT * 2 * NB];
     __shared__ double red[64];
     const int grp = threadIdx.x / G::GS, r = threadIdx.x % G::GS;
@@ -294,25 +354,26 @@ __global__ void __launch_bounds__(kThreads) k_trial_small(const double2* __restr
     for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int64_t k0 = t * G::KT;
         const int nkt = (int)((nk - k0) < G::KT ? (nk - k0) : G::KT);
-        tile_load(sD, dQ + (size_t)k0 * G::NB2, nkt * G::NB2);
+        tile_load<NB>(sD, dQ + (size_t)k0 * G::NB2, nkt);
+        tile_load<NB>(sF, Ft + (size_t)k0 * G::NB2, nkt);
         __syncthreads();
         const bool live = grp < nkt && r < NB;
         const int rr = r < NB ? r : 0;
         const int64_t k = k0 + grp;
         if (grp < nkt) {
             double2 u[NB];
-            row_cayley<NB>(sD + grp * G::NB2, tau, rr, sPiv + grp * 2 * NB, u, mask);
+            row_cayley<NB, G::LD>(sD + grp * G::MS, tau, rr, sPiv + grp * 2 * NB, u, mask);
             if (live) {
 #pragma unroll
-                for (int j = 0; j < NB; ++j) sU[grp * G::NB2 + r * NB + j] = u[j];
+                for (int j = 0; j < NB; ++j) sU[grp * G::MS + r * G::LD + j] = u[j];
             }
         }
         __syncthreads();
         if (grp < nkt) {
             double2 ftj[NB];
 #pragma unroll
-            for (int l = 0; l < NB; ++l) ftj[l] = Ft[(size_t)k * G::NB2 + rr * NB + l];
-            const double dr = row_diag_uhfu<NB, G::GS>(ftj, sU + grp * G::NB2, r, mask, live);
+            for (int l = 0; l < NB; ++l) ftj[l] = sF[grp * G::MS + rr * G::LD + l];
+            const double dr = row_diag_uhfu<NB, G::GS, G::LD>(ftj, sU + grp * G::MS, r, mask, live);
             if (live) {
                 const double pv = fmin(fmax(p[k * NB + r] - tau * d_p[k * NB + r], OCC_CLIP), 1.0 - OCC_CLIP);
                 const double wk = w[k];
@@ -335,14 +396,110 @@ __global__ void __launch_bounds__(kThreads) k_trial_small(const double2* __restr
     }
 }
 
+// The remaining backtracking trials after a failed first one, all in one pass:
+// trial m (m = 0 .. nrest-1) uses tau_m = tau_cur * shrink^m (the sequence the
+// one-at-a-time trials produce), and the first trial whose Omega is below
+// Omega0 is taken, exactly as the sequential loop would (solver_dm.hpp:577-589).
+// Returns at once when the first trial was accepted.
+constexpr int kMaxRestTrials = 7;
+
+template <int NB>
+__global__ void __launch_bounds__(kThreads) k_trial_rest_small(const double2* __restrict__ dQ,
+                                                               const double2* __restrict__ Ft,
+                                                               const double* __restrict__ p,
+                                                               const double* __restrict__ d_p,
+                                                               const double* __restrict__ w, int64_t nk, double T_r,
+                                                               double shrink, int nrest, double fallback,
+                                                               DmScalars* S) {
+    if (S->accepted) return;  // grid-uniform
+    using G = Geo<NB>;
+    extern __shared__ __align__(16) double2 dyn[];
+    double2* sD = dyn;
+    double2* sF = dyn + G::TILE;
+    double2* sU = dyn + 2 * G::TILE;
+    __shared__ double2 sPiv[G::KT * 2 * NB];
+    __shared__ double red[32 * 2 * kMaxRestTrials];
+    const int grp = threadIdx.x / G::GS, r = threadIdx.x % G::GS;
+    const unsigned mask = group_mask<NB>(threadIdx.x & 31);
+    const double tau_first = S->tau_cur;
+    const int64_t ntiles = (nk + G::KT - 1) / G::KT;
+    double v[2 * kMaxRestTrials];
+#pragma unroll
+    for (int m = 0; m < 2 * kMaxRestTrials; ++m) v[m] = 0.0;
+    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int64_t k0 = t * G::KT;
+        const int nkt = (int)((nk - k0) < G::KT ? (nk - k0) : G::KT);
+        tile_load<NB>(sD, dQ + (size_t)k0 * G::NB2, nkt);
+        tile_load<NB>(sF, Ft + (size_t)k0 * G::NB2, nkt);
+        __syncthreads();
+        const bool live = grp < nkt && r < NB;
+        const int rr = r < NB ? r : 0;
+        const int64_t k = k0 + grp;
+        double2 ftj[NB];
+        if (grp < nkt) {
+#pragma unroll
+            for (int l = 0; l < NB; ++l) ftj[l] = sF[grp * G::MS + rr * G::LD + l];
+        }
+        double tau = tau_first;
+#pragma unroll
+        for (int m = 0; m < kMaxRestTrials; ++m) {
+            if (m < nrest) {
+                if (grp < nkt) {
+                    double2 u[NB];
+                    row_cayley<NB, G::LD>(sD + grp * G::MS, tau, rr, sPiv + grp * 2 * NB, u, mask);
+                    if (live) {
+#pragma unroll
+                        for (int j = 0; j < NB; ++j) sU[grp * G::MS + r * G::LD + j] = u[j];
+                    }
+                    __syncwarp(mask);
+                    const double dr = row_diag_uhfu<NB, G::GS, G::LD>(ftj, sU + grp * G::MS, r, mask, live);
+                    if (live) {
+                        const double pv =
+                            fmin(fmax(p[k * NB + r] - tau * d_p[k * NB + r], OCC_CLIP), 1.0 - OCC_CLIP);
+                        const double wk = w[k];
+                        v[2 * m] += wk * pv * dr;
+                        v[2 * m + 1] -= wk * (pv * log(pv) + (1.0 - pv) * log1p(-pv));
+                    }
+                    __syncwarp(mask);
+                }
+                tau *= shrink;
+            }
+        }
+        __syncthreads();
+    }
+    double out[2 * kMaxRestTrials];
+    if (reduce_last_block<2 * kMaxRestTrials>(v, S->part, &S->counter, out, red) && threadIdx.x == 0) {
+        double tau = tau_first;
+        int taken = 0;
+        for (int m = 0; m < nrest && !taken; ++m) {
+            const double om = out[2 * m] - fmax(T_r, 1.0e-14) * out[2 * m + 1];
+            if (om < S->omega0) {
+                S->accepted = 1;
+                S->tau_final = tau;
+                taken = 1;
+            } else {
+                tau *= shrink;
+            }
+        }
+        if (!taken) {
+            S->tau_cur = tau;
+            S->tau_final = S->tau0 * fallback;
+        }
+    }
+}
+
 // Retraction Q <- Q U(tau_final) and eps_work = diag(U^H Ft U).
+// Dynamic shared memory: sD | sF | sU | sQ, TILE double2 each.
 template <int NB>
 __global__ void __launch_bounds__(kThreads) k_retract_small(double2* Q, const double2* __restrict__ dQ,
                                                             const double2* __restrict__ Ft, double* __restrict__ ew,
                                                             int64_t nk, const DmScalars* S) {
     using G = Geo<NB>;
-    __shared__ double2 sD[G::TILE];
-    __shared__ double2 sU[G::TILE];
+    extern __shared__ __align__(16) double2 dyn[];
+    double2* sD = dyn;
+    double2* sF = dyn + G::TILE;
+    double2* sU = dyn + 2 * G::TILE;
+    double2* sQ = dyn + 3 * G::TILE;
     __shared__ double2 sPiv[G::KT * 2 * NB];
     const int grp = threadIdx.x / G::GS, r = threadIdx.x % G::GS;
     const unsigned mask = group_mask<NB>(threadIdx.x & 31);
@@ -351,77 +508,96 @@ __global__ void __launch_bounds__(kThreads) k_retract_small(double2* Q, const do
     for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int64_t k0 = t * G::KT;
         const int nkt = (int)((nk - k0) < G::KT ? (nk - k0) : G::KT);
-        tile_load(sD, dQ + (size_t)k0 * G::NB2, nkt * G::NB2);
+        tile_load<NB>(sD, dQ + (size_t)k0 * G::NB2, nkt);
+        tile_load<NB>(sF, Ft + (size_t)k0 * G::NB2, nkt);
+        tile_load<NB>(sQ, Q + (size_t)k0 * G::NB2, nkt);
         __syncthreads();
         const bool live = grp < nkt && r < NB;
         const int rr = r < NB ? r : 0;
         const int64_t k = k0 + grp;
         if (grp < nkt) {
             double2 u[NB];
-            row_cayley<NB>(sD + grp * G::NB2, tau, rr, sPiv + grp * 2 * NB, u, mask);
+            row_cayley<NB, G::LD>(sD + grp * G::MS, tau, rr, sPiv + grp * 2 * NB, u, mask);
             if (live) {
 #pragma unroll
-                for (int j = 0; j < NB; ++j) sU[grp * G::NB2 + r * NB + j] = u[j];
+                for (int j = 0; j < NB; ++j) sU[grp * G::MS + r * G::LD + j] = u[j];
             }
         }
         __syncthreads();
         if (grp < nkt) {
             double2 ftj[NB];
 #pragma unroll
-            for (int l = 0; l < NB; ++l) ftj[l] = Ft[(size_t)k * G::NB2 + rr * NB + l];
-            const double dr = row_diag_uhfu<NB, G::GS>(ftj, sU + grp * G::NB2, r, mask, live);
+            for (int l = 0; l < NB; ++l) ftj[l] = sF[grp * G::MS + rr * G::LD + l];
+            const double dr = row_diag_uhfu<NB, G::GS, G::LD>(ftj, sU + grp * G::MS, r, mask, live);
             if (live) {
                 ew[k * NB + r] = dr;
-                const double2* su = sU + grp * G::NB2;
+                const double2* su = sU + grp * G::MS;
+                double2* qrow = sQ + grp * G::MS + r * G::LD;
                 double2 qr[NB];
 #pragma unroll
-                for (int l = 0; l < NB; ++l) qr[l] = Q[(size_t)k * G::NB2 + r * NB + l];
+                for (int l = 0; l < NB; ++l) qr[l] = qrow[l];
 #pragma unroll
                 for (int j = 0; j < NB; ++j) {
                     double2 acc = mk(0.0, 0.0);
 #pragma unroll
-                    for (int l = 0; l < NB; ++l) cfma(acc, qr[l], su[l * NB + j]);
-                    Q[(size_t)k * G::NB2 + r * NB + j] = acc;
+                    for (int l = 0; l < NB; ++l) cfma(acc, qr[l], su[l * G::LD + j]);
+                    qrow[j] = acc;  // only this thread reads or writes this row
                 }
             }
         }
         __syncthreads();
+        tile_store<NB>(Q + (size_t)k0 * G::NB2, sQ, nkt);
+        __syncthreads();
     }
 }
 
-// PR+ numerator / denominator -> beta (solver_dm.hpp:513-559), per k-point rows.
+// Element kernels: 256 threads, grid-stride loops unrolled by kUnrollE so
+// each thread keeps several independent field loads in flight.
+constexpr int kThreadsE = 256;
+constexpr int kUnrollE = 4;
+
+// PR+ numerator / denominator -> beta (solver_dm.hpp:513-559), one thread per
+// matrix element (k, i, j); the row terms of g_p are added by the j = 0 thread.
 template <int NB>
-__global__ void __launch_bounds__(kThreads) k_pr_beta_small(const double2* __restrict__ Gc, const double2* __restrict__ Gp,
-                                                            const double* __restrict__ g_p,
-                                                            const double* __restrict__ g_pp,
-                                                            const double* __restrict__ eps,
-                                                            const double* __restrict__ p, const double* __restrict__ w,
-                                                            int64_t nk, double T_r, int restart, int iter, DmScalars* S) {
+__global__ void __launch_bounds__(kThreadsE) k_pr_beta_small(const double2* __restrict__ Gc, const double2* __restrict__ Gp,
+                                                             const double* __restrict__ g_p,
+                                                             const double* __restrict__ g_pp,
+                                                             const double* __restrict__ eps,
+                                                             const double* __restrict__ p, const double* __restrict__ w,
+                                                             int64_t nk, double T_r, int restart, int iter, DmScalars* S) {
     __shared__ double red[96];
     const double lam = S->lam_pc;
     double v[3] = {0.0, 0.0, 0.0};
-    const int64_t nrows = nk * NB;
-    for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < nrows; row += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t k = row / NB;
-        const int i = (int)(row - k * NB);
-        const double wk = w[k];
-        const double ei = eps[row];
-        double s0 = 0.0, s1 = 0.0;
+    const int64_t nel = nk * NB * NB;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t e0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e0 < nel; e0 += kUnrollE * stride) {
+        double2 g[kUnrollE], gp[kUnrollE];
 #pragma unroll
-        for (int j = 0; j < NB; ++j) {
-            const double gap = ei - eps[k * NB + j];
-            const double base = sqrt(gap * gap + lam * lam);
-            const double2 g = Gc[row * NB + j], gp = Gp[row * NB + j];
-            const double2 d = mk(g.x / base, g.y / base);
-            s0 += (g.x * d.x + g.y * d.y) - (gp.x * d.x + gp.y * d.y);
-            s1 += gp.x * gp.x + gp.y * gp.y;
+        for (int u = 0; u < kUnrollE; ++u) {
+            const int64_t e = e0 + u * stride;
+            g[u] = e < nel ? Gc[e] : mk(0.0, 0.0);
+            gp[u] = e < nel ? Gp[e] : mk(0.0, 0.0);
         }
-        v[0] += wk * s0;
-        v[1] += wk * s1;
-        const double ps = fmin(fmax(p[row], OCC_CLIP), 1.0 - OCC_CLIP);
-        const double h = g_p[row] / (T_r / (ps * (1.0 - ps)));
-        v[2] += wk * (g_p[row] * h - g_pp[row] * h);
-        v[1] += wk * (g_pp[row] * g_pp[row]);
+#pragma unroll
+        for (int u = 0; u < kUnrollE; ++u) {
+            const int64_t e = e0 + u * stride;
+            if (e >= nel) break;
+            const int64_t row = e / NB;
+            const int j = (int)(e - row * NB);
+            const int64_t k = row / NB;
+            const double wk = w[k];
+            const double gap = eps[row] - eps[k * NB + j];
+            const double base = sqrt(gap * gap + lam * lam);
+            const double2 d = mk(g[u].x / base, g[u].y / base);
+            v[0] += wk * ((g[u].x * d.x + g[u].y * d.y) - (gp[u].x * d.x + gp[u].y * d.y));
+            v[1] += wk * (gp[u].x * gp[u].x + gp[u].y * gp[u].y);
+            if (j == 0) {
+                const double ps = fmin(fmax(p[row], OCC_CLIP), 1.0 - OCC_CLIP);
+                const double h = g_p[row] / (T_r / (ps * (1.0 - ps)));
+                v[2] += wk * (g_p[row] * h - g_pp[row] * h);
+                v[1] += wk * (g_pp[row] * g_pp[row]);
+            }
+        }
     }
     double out[3];
     if (reduce_last_block<3>(v, S->part, &S->counter, out, red) && threadIdx.x == 0) {
@@ -434,41 +610,53 @@ __global__ void __launch_bounds__(kThreads) k_pr_beta_small(const double2* __res
     }
 }
 
-// direction + tau0 + Omega0 (solver_dm.hpp:556-573, 346-365), per k-point rows.
+// direction + tau0 + Omega0 (solver_dm.hpp:556-573, 346-365), one thread per
+// matrix element; the occupation direction and Omega0 terms by the j = 0 thread.
 template <int NB>
-__global__ void __launch_bounds__(kThreads) k_direction_small(const double2* __restrict__ Gc,
-                                                              const double2* __restrict__ dQp,
-                                                              const double* __restrict__ g_p,
-                                                              const double* __restrict__ dpp,
-                                                              const double* __restrict__ eps,
-                                                              const double* __restrict__ p,
-                                                              const double* __restrict__ w, double2* __restrict__ dQ,
-                                                              double* __restrict__ d_p, int64_t nk, double T_r,
-                                                              double max_step, DmScalars* S) {
+__global__ void __launch_bounds__(kThreadsE) k_direction_small(const double2* __restrict__ Gc,
+                                                               const double2* __restrict__ dQp,
+                                                               const double* __restrict__ g_p,
+                                                               const double* __restrict__ dpp,
+                                                               const double* __restrict__ eps,
+                                                               const double* __restrict__ p,
+                                                               const double* __restrict__ w, double2* __restrict__ dQ,
+                                                               double* __restrict__ d_p, int64_t nk, double T_r,
+                                                               double max_step, DmScalars* S) {
     __shared__ double red[96];
     const double lam = S->lam_pc, beta = S->beta;
     double v[3] = {0.0, 0.0, 0.0};
-    const int64_t nrows = nk * NB;
-    for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < nrows; row += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t k = row / NB;
-        const double wk = w[k];
-        const double ei = eps[row];
-        double s0 = 0.0;
+    const int64_t nel = nk * NB * NB;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t e0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e0 < nel; e0 += kUnrollE * stride) {
+        double2 g[kUnrollE], q[kUnrollE];
 #pragma unroll
-        for (int j = 0; j < NB; ++j) {
+        for (int u = 0; u < kUnrollE; ++u) {
+            const int64_t e = e0 + u * stride;
+            g[u] = e < nel ? Gc[e] : mk(0.0, 0.0);
+            q[u] = (e < nel && beta != 0.0) ? dQp[e] : mk(0.0, 0.0);
+        }
+#pragma unroll
+        for (int u = 0; u < kUnrollE; ++u) {
+            const int64_t e = e0 + u * stride;
+            if (e >= nel) break;
+            const int64_t row = e / NB;
+            const int j = (int)(e - row * NB);
+            const int64_t k = row / NB;
+            const double wk = w[k];
+            const double ei = eps[row];
             const double gap = ei - eps[k * NB + j];
             const double base = sqrt(gap * gap + lam * lam);
-            const double2 g = Gc[row * NB + j], q = dQp[row * NB + j];
-            const double2 d = mk(g.x / base + beta * q.x, g.y / base + beta * q.y);
-            dQ[row * NB + j] = d;
-            s0 += d.x * d.x + d.y * d.y;
+            const double2 d = mk(g[u].x / base + beta * q[u].x, g[u].y / base + beta * q[u].y);
+            dQ[e] = d;
+            v[0] += wk * (d.x * d.x + d.y * d.y);
+            if (j == 0) {
+                const double ps = fmin(fmax(p[row], OCC_CLIP), 1.0 - OCC_CLIP);
+                const double h = g_p[row] / (T_r / (ps * (1.0 - ps)));
+                d_p[row] = h + beta * dpp[row];
+                v[1] += wk * ps * ei;
+                v[2] -= wk * (ps * log(ps) + (1.0 - ps) * log1p(-ps));
+            }
         }
-        v[0] += wk * s0;
-        const double ps = fmin(fmax(p[row], OCC_CLIP), 1.0 - OCC_CLIP);
-        const double h = g_p[row] / (T_r / (ps * (1.0 - ps)));
-        d_p[row] = h + beta * dpp[row];
-        v[1] += wk * ps * ei;
-        v[2] -= wk * (ps * log(ps) + (1.0 - ps) * log1p(-ps));
     }
     double out[3];
     if (reduce_last_block<3>(v, S->part, &S->counter, out, red) && threadIdx.x == 0) {
@@ -487,9 +675,19 @@ unsigned tiles_grid(int64_t nk, int KT, int cap) {
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>(nt, cap));
 }
 
-unsigned rows_grid(int64_t rows) {
-    const int64_t want = (rows + kThreads - 1) / kThreads;
-    return (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, std::min<int64_t>(kDmMaxPartials, 4 * num_sms())));
+unsigned elems_grid(int64_t n) {
+    const int64_t want = (n + (int64_t)kThreadsE * kUnrollE - 1) / ((int64_t)kThreadsE * kUnrollE);
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, std::min<int64_t>(kDmMaxPartials, 8 * num_sms())));
+}
+
+template <int NB>
+void small_attrs() {
+    static std::once_flag once;
+    std::call_once(once, [] {
+        raise_smem(k_trial_small<NB>);
+        raise_smem(k_trial_rest_small<NB>);
+        raise_smem(k_retract_small<NB>);
+    });
 }
 
 #define SMALL_DISPATCH(nb, X) \
@@ -529,9 +727,9 @@ int dm_small_rot_grad(const double2* Q, double2* F, const double* p, const doubl
 int dm_small_pr_beta(const double2* Gc, const double2* Gp, const double* g_p, const double* g_pp, const double* eps,
                      const double* p, const double* w, int64_t nk, int nb, double T_r, int restart, int iter,
                      DmScalars* S, cudaStream_t st) {
-#define X(N)                                                                                                 \
-    k_pr_beta_small<N><<<rows_grid(nk * N), kThreads, 0, st>>>(Gc, Gp, g_p, g_pp, eps, p, w, nk, T_r, restart, \
-                                                               iter, S);                                     \
+#define X(N)                                                                                                     \
+    k_pr_beta_small<N><<<elems_grid(nk * N * N), kThreadsE, 0, st>>>(Gc, Gp, g_p, g_pp, eps, p, w, nk, T_r, restart, \
+                                                                    iter, S);                                    \
     CPPHF_LAUNCH_CHECK("pr_beta");
     SMALL_DISPATCH(nb, X)
 #undef X
@@ -541,9 +739,9 @@ int dm_small_pr_beta(const double2* Gc, const double2* Gp, const double* g_p, co
 int dm_small_direction(const double2* Gc, const double2* dQp, const double* g_p, const double* dpp, const double* eps,
                        const double* p, const double* w, double2* dQ, double* d_p, int64_t nk, int nb, double T_r,
                        double max_step, DmScalars* S, cudaStream_t st) {
-#define X(N)                                                                                                   \
-    k_direction_small<N><<<rows_grid(nk * N), kThreads, 0, st>>>(Gc, dQp, g_p, dpp, eps, p, w, dQ, d_p, nk, T_r, \
-                                                                 max_step, S);                                 \
+#define X(N)                                                                                                        \
+    k_direction_small<N><<<elems_grid(nk * N * N), kThreadsE, 0, st>>>(Gc, dQp, g_p, dpp, eps, p, w, dQ, d_p, nk, T_r, \
+                                                                      max_step, S);                                 \
     CPPHF_LAUNCH_CHECK("direction");
     SMALL_DISPATCH(nb, X)
 #undef X
@@ -553,20 +751,41 @@ int dm_small_direction(const double2* Gc, const double2* dQp, const double* g_p,
 int dm_small_trial(const double2* dQ, const double2* Ft, const double* p, const double* d_p, const double* w,
                    int64_t nk, int nb, double T_r, double shrink, int last_trial, double fallback, DmScalars* S,
                    cudaStream_t st) {
-#define X(N)                                                                                                     \
-    k_trial_small<N><<<tiles_grid(nk, Geo<N>::KT, kDmMaxPartials), kThreads, 0, st>>>(dQ, Ft, p, d_p, w, nk, T_r, \
-                                                                                      shrink, last_trial,        \
-                                                                                      fallback, S);              \
+#define X(N)                                                                                                         \
+    small_attrs<N>();                                                                                                \
+    k_trial_small<N><<<tiles_grid(nk, Geo<N>::KT, kDmMaxPartials), kThreads, 3 * sizeof(double2) * Geo<N>::TILE,    \
+                       st>>>(dQ, Ft, p, d_p, w, nk, T_r, shrink, last_trial, fallback, S);                           \
     CPPHF_LAUNCH_CHECK("trial");
     SMALL_DISPATCH(nb, X)
 #undef X
     return CPPHF_OK;
 }
 
+int dm_small_trial_rest(const double2* dQ, const double2* Ft, const double* p, const double* d_p, const double* w,
+                        int64_t nk, int nb, double T_r, double shrink, int nrest, double fallback, DmScalars* S,
+                        cudaStream_t st) {
+    if (nrest < 1) return CPPHF_OK;
+    if (nrest > kMaxRestTrials) return fail(CPPHF_ERR_INVALID, "trial_rest: too many trials for one pass");
+    // partials: 2 * kMaxRestTrials values per block must fit S->part (3 * kDmMaxPartials)
+    const int cap = (3 * kDmMaxPartials) / (2 * kMaxRestTrials);
+#define X(N)                                                                                                     \
+    small_attrs<N>();                                                                                            \
+    k_trial_rest_small<N><<<tiles_grid(nk, Geo<N>::KT, cap), kThreads, 3 * sizeof(double2) * Geo<N>::TILE, st>>>( \
+        dQ, Ft, p, d_p, w, nk, T_r, shrink, nrest, fallback, S);                                                 \
+    CPPHF_LAUNCH_CHECK("trial_rest");
+    SMALL_DISPATCH(nb, X)
+#undef X
+    return CPPHF_OK;
+}
+
+int dm_small_max_rest_trials() { return kMaxRestTrials; }
+
 int dm_small_retract(double2* Q, const double2* dQ, const double2* Ft, double* ew, int64_t nk, int nb,
                      const DmScalars* S, cudaStream_t st) {
-#define X(N)                                                                                                   \
-    k_retract_small<N><<<tiles_grid(nk, Geo<N>::KT, 16 * num_sms()), kThreads, 0, st>>>(Q, dQ, Ft, ew, nk, S); \
+#define X(N)                                                                                                      \
+    small_attrs<N>();                                                                                             \
+    k_retract_small<N><<<tiles_grid(nk, Geo<N>::KT, 16 * num_sms()), kThreads, 4 * sizeof(double2) * Geo<N>::TILE, \
+                         st>>>(Q, dQ, Ft, ew, nk, S);                                                             \
     CPPHF_LAUNCH_CHECK("retract");
     SMALL_DISPATCH(nb, X)
 #undef X

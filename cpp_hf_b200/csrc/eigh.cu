@@ -10,8 +10,9 @@
 // (c, s) the real symmetric Schur rotation of [[A_pp, |A_pq|], [|A_pq|, A_qq]],
 // applied as A <- J^H A (rows), A <- A J and V <- V J (columns); the 2x2 pivot
 // block is then written exactly (A_pp - t|A_pq|, A_qq + t|A_pq|, zeros).
-// Sweeps stop when the off-diagonal Frobenius norm falls below 1e-17 of the
-// total (or after kMaxSweeps).  Eigenvalues are sorted ascending (stable),
+// Sweeps stop when the off-diagonal Frobenius norm falls to nb * eps of the
+// total (the rounding level of the rotations), when a sweep no longer reduces
+// it, or after kMaxSweeps.  Eigenvalues are sorted ascending (stable),
 // eigenvector columns permuted to match.
 #include "common.cuh"
 #include "eigh.cuh"
@@ -49,7 +50,7 @@ template <bool WARP>
 __device__ __forceinline__ double team_sum(double v, double* red) {
     if (WARP) return warp_sum(v);
     double a[1] = {v};
-    block_sum<1>(a, red);
+    block_sum<1>(a, *reinterpret_cast<double(*)[32]>(red));  // red: the kernel's 32-double scratch
     return a[0];
 }
 
@@ -81,6 +82,11 @@ __device__ void jacobi(double2* A, double2* V, int nb, int ld, PairParam* pp, do
     if (nb == 1) return;
     const int m = nb + (nb & 1);
     const int npair = m / 2;
+    // converged once the off-diagonal norm is at the rounding level of the
+    // rotations, (nb eps)^2 of the total (squared Frobenius norms), or once a
+    // sweep no longer reduces it
+    const double thr = (double)nb * 2.220446049250313e-16;
+    double off_prev = INFINITY;
     for (int sweep = 0; sweep < kMaxSweeps; ++sweep) {
         double off = 0.0, tot = 0.0;
         for (int e = tid; e < nb * nb; e += nt) {
@@ -92,7 +98,8 @@ __device__ void jacobi(double2* A, double2* V, int nb, int ld, PairParam* pp, do
         }
         off = team_sum<WARP>(off, red);
         tot = team_sum<WARP>(tot, red);
-        if (!(off > 1e-34 * tot) || off == 0.0) break;
+        if (!(off > thr * thr * tot) || off == 0.0 || !(off < off_prev)) break;
+        off_prev = off;
         for (int r = 0; r < m - 1; ++r) {
             for (int k = tid; k < npair; k += nt) {
                 int p, q;

@@ -10,11 +10,14 @@
 //            w_k Re[h_ij P_ji + (Sigma_ij + H_ij)/2 (P - refP)_ji] (+ the
 //            mirrored term); optional dense H.
 //   energy   fixed-order sum of the block partials.
+#include "bulk.cuh"
 #include "common.cuh"
 #include "exchange.cuh"
 #include "fock.cuh"
+#include "team.cuh"
 
 #include <algorithm>
+#include <cstdlib>
 #include <mutex>
 #include <string>
 
@@ -246,6 +249,92 @@ __global__ void __launch_bounds__(kAsmThreads) k_assemble_tiled(AsmArgs a, int K
     if (threadIdx.x == 0) a.part[blockIdx.x] = e_acc[0];
 }
 
+// Pipelined assembly: persistent CTAs walk tiles of KT whole k-blocks; thread
+// 0 brings the NEXT tile's Sigma, h, P (and refP) segments into the other
+// shared-memory stage with three (four) bulk copies while the CTA assembles the
+// current one, so each SM keeps two tiles of loads in flight.  The energy is
+// reduced in the same launch (last-block sum in a fixed order).
+template <bool REF>
+__global__ void __launch_bounds__(kAsmThreads) k_assemble_bulk(AsmArgs a, int KT, int64_t ntiles,
+                                                               unsigned* counter, double* energy_out) {
+    constexpr int NARR = REF ? 4 : 3;
+    extern __shared__ __align__(16) unsigned char smem_dyn[];
+    __shared__ double red[32];
+    __shared__ __align__(8) unsigned long long bar[2];
+    const int nb = a.nb, nb2 = nb * nb;
+    const int tile = KT * nb2;
+    double2* stg = reinterpret_cast<double2*>(
+        (reinterpret_cast<uintptr_t>(smem_dyn) + 127) & ~(uintptr_t)127);
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    auto issue = [&](int64_t t, int s) {
+        if (threadIdx.x != 0) return;
+        const int64_t k0 = t * KT;
+        const int nkt = (int)((a.nk - k0) < (int64_t)KT ? (a.nk - k0) : (int64_t)KT);
+        const unsigned bytes = (unsigned)(sizeof(double2) * (size_t)nkt * nb2);
+        const size_t off = (size_t)k0 * nb2;
+        double2* d = stg + (size_t)s * NARR * tile;
+        fence_proxy_async_smem();
+        mbar_arrive_expect_tx(&bar[s], bytes * NARR);
+        bulk_g2s(d, a.Sigma + off, bytes, &bar[s]);
+        bulk_g2s(d + tile, a.h + off, bytes, &bar[s]);
+        bulk_g2s(d + 2 * tile, a.P + off, bytes, &bar[s]);
+        if (REF) bulk_g2s(d + 3 * tile, a.refP + off, bytes, &bar[s]);
+    };
+    double e_acc[1] = {0.0};
+    int i = 0;
+    if ((int64_t)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
+        const int s = i & 1;
+        if (t + gridDim.x < ntiles) issue(t + gridDim.x, s ^ 1);
+        if (!mbar_wait(&bar[s], (unsigned)((i >> 1) & 1))) return;
+        const double2* sS = stg + (size_t)s * NARR * tile;
+        const double2* sH = sS + tile;
+        const double2* sP = sS + 2 * tile;
+        const double2* sR = sS + 3 * tile;
+        const int64_t k0 = t * KT;
+        const int nkt = (int)((a.nk - k0) < (int64_t)KT ? (a.nk - k0) : (int64_t)KT);
+        const int n = nkt * nb2;
+        const size_t base = (size_t)k0 * nb2;
+        for (int e = threadIdx.x; e < n; e += blockDim.x) {
+            const int kl = e / nb2, r = e - kl * nb2;
+            const int ii = r / nb, j = r - ii * nb;
+            const int eT = kl * nb2 + j * nb + ii;
+            const double hdi = a.hd ? a.hd[ii] : 0.0;
+            double2 se = sS[e], sT = sS[eT];
+            if (a.SC) {
+                se = cadd(se, a.SC[r]);
+                sT = cadd(sT, a.SC[j * nb + ii]);
+            }
+            double2 Aij = cadd(sH[e], se);
+            double2 Aji = cadd(sH[eT], sT);
+            if (ii == j) {
+                Aij.x += hdi;
+                Aji = Aij;
+            }
+            a.F[base + e] = mk(0.5 * (Aij.x + Aji.x), 0.5 * (Aij.y - Aji.y));
+            if (a.SC) a.Sigma[base + e] = se;
+            if (a.Hdense) a.Hdense[base + e] = mk(ii == j ? hdi : 0.0, 0.0);
+            const double2 pji = sP[eT];
+            const double2 dji = REF ? csub(pji, sR[eT]) : pji;
+            double2 inter = cscale(se, 0.5);
+            if (ii == j && a.hd) inter.x += 0.5 * hdi;
+            const double2 hv = sH[e];
+            const double sv = (hv.x * pji.x - hv.y * pji.y) + (inter.x * dji.x - inter.y * dji.y);
+            e_acc[0] += a.w[k0 + kl] * sv;
+        }
+        __syncthreads();
+    }
+    if (energy_out) {
+        double out[1];
+        if (reduce_last_block<1>(e_acc, a.part, counter, out, red) && threadIdx.x == 0) *energy_out = out[0];
+    }
+}
+
 // Fixed-order sum of block partials by one warp (lane-strided, then a
 // shuffle tree): deterministic for a given partial count.
 __global__ void k_sum_partials(const double* __restrict__ part, int n, double* __restrict__ out) {
@@ -256,9 +345,18 @@ __global__ void k_sum_partials(const double* __restrict__ part, int n, double* _
 }
 
 struct FockWs {
-    size_t off_part, off_rho_part, off_rho_bar, off_sc, off_hd, off_exch, total;
+    size_t off_part, off_counter, off_rho_part, off_rho_bar, off_sc, off_hd, off_exch, total;
     int Gasm, Gk;
 };
+
+// CPPHF_ASSEMBLY_BULK=0 selects the non-pipelined assembly (for A/B timing).
+bool bulk_assembly_enabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("CPPHF_ASSEMBLY_BULK");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
 
 FockWs fock_ws_layout(const cpphf_kernel* K) {
     FockWs L;
@@ -275,6 +373,7 @@ FockWs fock_ws_layout(const cpphf_kernel* K) {
         return at;
     };
     L.off_part = take(sizeof(double) * kMaxPartials);
+    L.off_counter = take(sizeof(unsigned));
     L.off_rho_part = take(sizeof(double2) * (size_t)L.Gk * nb2);
     L.off_rho_bar = take(sizeof(double2) * nb2);
     L.off_sc = take(sizeof(double2) * nb2);
@@ -333,7 +432,7 @@ int build_fock(const cpphf_kernel* K, const double2* P, double2* Sigma, double2*
                                              static_cast<const double2*>(K->contact_Oj), rho_bar,
                                              hd, SC);
         CPPHF_LAUNCH_CHECK("hartree/contact");
-    } else {
+    } else if (hd_out) {
         CPPHF_CUDA(cudaMemsetAsync(hd, 0, sizeof(double) * nb, st));
     }
     if (K->include_exchange) {
@@ -357,6 +456,35 @@ int build_fock(const cpphf_kernel* K, const double2* P, double2* Sigma, double2*
     a.nk = nk;
     a.nb = nb;
     a.part = part;
+    if (nb2 <= kTileElems && bulk_assembly_enabled()) {
+        // whole k-blocks per stage: 1024 elements (3 arrays) or 512 (4 arrays with refP)
+        const int elems = refP ? 512 : kTileElems;
+        const int KT = std::max(1, elems / nb2);
+        const int64_t ntiles = (nk + KT - 1) / KT;
+        const int narr = refP ? 4 : 3;
+        const size_t smem = sizeof(double2) * (size_t)KT * nb2 * narr * 2 + 128;
+        static std::once_flag once_b;
+        std::call_once(once_b, [] {
+            raise_smem(k_assemble_bulk<false>);
+            raise_smem(k_assemble_bulk<true>);
+        });
+        int per = 0;
+        if (refP)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_assemble_bulk<true>, kAsmThreads, smem);
+        else
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_assemble_bulk<false>, kAsmThreads, smem);
+        (void)cudaGetLastError();
+        per = std::max(1, per);
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(ntiles, std::min<int64_t>(kMaxPartials, (int64_t)per * num_sms())));
+        unsigned* counter = reinterpret_cast<unsigned*>(W + L.off_counter);
+        if (energy) CPPHF_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned), st));
+        if (refP)
+            k_assemble_bulk<true><<<grid, kAsmThreads, smem, st>>>(a, KT, ntiles, counter, energy);
+        else
+            k_assemble_bulk<false><<<grid, kAsmThreads, smem, st>>>(a, KT, ntiles, counter, energy);
+        CPPHF_LAUNCH_CHECK("assemble (bulk pipelined)");
+        return CPPHF_OK;
+    }
     if (nb2 <= kTileElems) {
         static std::once_flag once;
         std::call_once(once, [] { raise_smem(k_assemble_tiled); });

@@ -1,13 +1,16 @@
 // Chemical-potential solvers as one cooperative persistent kernel each
 // (cpp_hf utils.hpp:49-116).
 //
-// Every block owns a contiguous slice of the (nk*nb) eigenvalues.  Per
-// iteration a block reduces its slice (fixed tree) into a partial, the grid
-// meets at a bounded barrier, and every block then sums all partials in block
-// order and replays the reference's scalar update rule itself, so the whole
-// grid agrees on (lo, hi, mu) without a second barrier.  Partials are double
-// buffered by iteration parity.  Fixed iteration counts are kept exactly
-// (30 bisection steps by default, mu_maxiter Newton steps).
+// Every block owns a contiguous slice of the (nk*nb) eigenvalues.  Per round
+// a block reduces its slice (fixed tree) into partials, the grid meets at a
+// bounded barrier whose last block sums the partials in block order, and every
+// block replays the reference's scalar update rule itself, so the whole grid
+// agrees on (lo, hi, mu).  The results are those of the reference's fixed
+// iteration counts (30 bisection steps by default, mu_maxiter Newton steps):
+// bisection evaluates the counts at all midpoints of the next kBisectLevels
+// levels of its decision tree per round and walks the tree exactly, and Newton
+// stops early only once its state (mu, lo, hi) repeats with period 1 or 2, when
+// the state after the remaining iterations is already known.
 #include "common.cuh"
 #include "mu.cuh"
 
@@ -20,6 +23,8 @@ namespace {
 
 constexpr int kMuThreads = 1024;
 constexpr int kMuMaxGrid = 1024;
+constexpr int kBisectLevels = 3;                      // bisection steps per grid barrier
+constexpr int kMuNV = (1 << kBisectLevels) - 1;       // midpoints evaluated per barrier
 
 __device__ __forceinline__ double expit(double x) {
     if (x >= 0.0) return 1.0 / (1.0 + exp(-x));
@@ -38,12 +43,12 @@ struct MuArgs {
     int maxiter;
     int mode;  // 0 bisection (utils.hpp:49-75), 1 in-loop newton (utils.hpp:79-116)
     double* mu_out;
-    double* part;     // [2][grid][2]
+    double* part;     // [grid][2] min/max, [grid][kMuNV] partials, [2][kMuNV] totals
     unsigned* sync;   // [0] count [1] gen [2] error
 };
 
 __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
-    __shared__ double red[64];
+    __shared__ double red[32 * kMuNV];  // block_sum<kMuNV> scratch (32 doubles per value)
     GridBarrier bar;
     bar.init(a.sync);
     const int G = gridDim.x;
@@ -114,46 +119,109 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
         mu = fmin(fmax(*a.mu0, lo), hi);
     }
     const double Tfd = Tj + 1.0e-12;  // fermidirac_scalar(x, Tj) = expit(-x / (Tj + 1e-12))
-    for (int it = 0; it < a.maxiter; ++it) {
-        double* part = a.part + 2 * G + (size_t)(it & 1) * 2 * G;
-        const double mid = 0.5 * (lo + hi);
-        double v[2] = {0.0, 0.0};
-        for (unsigned i = e0 + threadIdx.x; i < e1; i += blockDim.x) {
-            const double wk = a.w[i / nb];
-            const double e = a.eps[i];
-            if (a.mode == 0) {
-                v[0] += wk * expit(-(e - mid) / Tfd);
-            } else {
+    double* part = a.part + 2 * G;                  // [G][kMuNV] partials of the current round
+    double* tots = part + (size_t)kMuNV * G;        // [2][kMuNV] totals, by round parity
+    __shared__ double bc_tot[kMuNV];
+    int round = 0;
+    if (a.mode == 0) {
+        // Bisection, kBisectLevels steps per grid barrier: the counts at all
+        // midpoints of the next levels of the bisection tree are evaluated in one
+        // pass, then the tree is walked exactly as the sequential steps would
+        // (each midpoint is 0.5 * (lo + hi) of the interval the sequence reaches).
+        int it = 0;
+        while (it < a.maxiter) {
+            const int L = min(kBisectLevels, a.maxiter - it);
+            const int nodes = (1 << L) - 1;
+            double nlo[kMuNV], nhi[kMuNV], mid[kMuNV];
+            nlo[0] = lo;
+            nhi[0] = hi;
+#pragma unroll
+            for (int j = 0; j < kMuNV; ++j) {
+                if (j < nodes) {
+                    mid[j] = 0.5 * (nlo[j] + nhi[j]);
+                    const int l = 2 * j + 1, r = 2 * j + 2;
+                    if (l < kMuNV) {
+                        nlo[l] = nlo[j];
+                        nhi[l] = mid[j];
+                    }
+                    if (r < kMuNV) {
+                        nlo[r] = mid[j];
+                        nhi[r] = nhi[j];
+                    }
+                } else {
+                    mid[j] = 0.0;
+                }
+            }
+            double v[kMuNV];
+#pragma unroll
+            for (int j = 0; j < kMuNV; ++j) v[j] = 0.0;
+            for (unsigned i = e0 + threadIdx.x; i < e1; i += blockDim.x) {
+                const double wk = a.w[i / nb];
+                const double e = a.eps[i];
+#pragma unroll
+                for (int j = 0; j < kMuNV; ++j)
+                    if (j < nodes) v[j] += wk * expit(-(e - mid[j]) / Tfd);
+            }
+            block_sum<kMuNV>(v, red);
+            if (threadIdx.x == 0) {
+#pragma unroll
+                for (int j = 0; j < kMuNV; ++j) __stcg(&part[kMuNV * blockIdx.x + j], v[j]);
+            }
+            double* tot = tots + (round & 1) * kMuNV;
+            if (!bar.wait_reduce<kMuNV>(part, G, tot)) {
+                if (blockIdx.x == 0 && threadIdx.x == 0) *a.mu_out = NAN;
+                return;
+            }
+            if (threadIdx.x < kMuNV) bc_tot[threadIdx.x] = __ldcg(&tot[threadIdx.x]);
+            __syncthreads();
+            int node = 0;
+            for (int l = 0; l < L; ++l) {
+                double m = mid[0];
+#pragma unroll
+                for (int j = 1; j < kMuNV; ++j)
+                    if (j == node) m = mid[j];
+                if (bc_tot[node] > a.target) {
+                    hi = m;
+                    node = 2 * node + 1;
+                } else {
+                    lo = m;
+                    node = 2 * node + 2;
+                }
+            }
+            __syncthreads();
+            it += L;
+            ++round;
+        }
+    } else {
+        // Newton in a bracket.  The update is a deterministic function of the
+        // state (mu, lo, hi); once the state repeats with period 1 or 2 the
+        // remaining iterations are known, so the loop stops there with the state
+        // the full iteration count would end in.
+        double mu1 = NAN, lo1 = NAN, hi1 = NAN;  // state one iteration back
+        for (int it = 0; it < a.maxiter; ++it) {
+            double v[2] = {0.0, 0.0};
+            for (unsigned i = e0 + threadIdx.x; i < e1; i += blockDim.x) {
+                const double wk = a.w[i / nb];
+                const double e = a.eps[i];
                 const double p = expit((mu - e) / Tj);
                 v[0] += wk * p;
                 v[1] += wk * p * (1.0 - p) / Tj;
             }
-        }
-        block_sum<2>(v, red);
-        if (threadIdx.x == 0) {
-            __stcg(&part[2 * blockIdx.x], v[0]);
-            __stcg(&part[2 * blockIdx.x + 1], v[1]);
-        }
-        // the last block to arrive sums the partials (fixed lane-strided order)
-        // and publishes the totals before releasing the grid
-        double* tot = a.part + 6 * (size_t)G + (it & 1) * 2;
-        if (!bar.wait_reduce(part, G, tot)) {
-            if (blockIdx.x == 0 && threadIdx.x == 0) *a.mu_out = NAN;
-            return;
-        }
-        if (threadIdx.x == 0) {
-            bc[0] = __ldcg(&tot[0]);
-            bc[1] = __ldcg(&tot[1]);
-        }
-        __syncthreads();
-        const double N = bc[0], Z = bc[1];
-        __syncthreads();
-        if (a.mode == 0) {
-            if (N > a.target)
-                hi = mid;
-            else
-                lo = mid;
-        } else {
+            block_sum<2>(v, red);
+            if (threadIdx.x == 0) {
+                __stcg(&part[2 * blockIdx.x], v[0]);
+                __stcg(&part[2 * blockIdx.x + 1], v[1]);
+            }
+            double* tot = tots + (it & 1) * kMuNV;
+            if (!bar.wait_reduce<2>(part, G, tot)) {
+                if (blockIdx.x == 0 && threadIdx.x == 0) *a.mu_out = NAN;
+                return;
+            }
+            if (threadIdx.x < 2) bc_tot[threadIdx.x] = __ldcg(&tot[threadIdx.x]);
+            __syncthreads();
+            const double N = bc_tot[0], Z = bc_tot[1];
+            __syncthreads();
+            const double mu0 = mu, lo0 = lo, hi0 = hi;
             const double g = N - a.target;
             if (g < 0.0) lo = mu;
             if (g > 0.0) hi = mu;
@@ -164,6 +232,15 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
             mn = fmin(fmax(mn, lo), hi);
             if (!isfinite(mn)) mn = mb;
             mu = mn;
+            const int rest = a.maxiter - (it + 1);
+            if (mu == mu0 && lo == lo0 && hi == hi0) break;  // fixed point
+            if (mu == mu1 && lo == lo1 && hi == hi1) {       // period 2: (s1, s0) repeats
+                if (rest & 1) mu = mu0;
+                break;
+            }
+            mu1 = mu0;
+            lo1 = lo0;
+            hi1 = hi0;
         }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) *a.mu_out = (a.mode == 0) ? 0.5 * (lo + hi) : mu;
@@ -198,13 +275,13 @@ int max_coop_grid() {
 // launches.  Every GPU that loads the library holds it until the process
 // exits; every call shares it.
 // ---------------------------------------------------------------------------
-constexpr size_t kMuNoAllocScratchBytes = 64 + sizeof(double) * (6 * (size_t)kMuMaxGrid + 8);
+constexpr size_t kMuNoAllocScratchBytes = 64 + sizeof(double) * ((2 + kMuNV) * (size_t)kMuMaxGrid + 2 * kMuNV);
 static __device__ __align__(256) unsigned char g_mu_noalloc_scratch[kMuNoAllocScratchBytes];
 
 }  // namespace
 
 size_t mu_workspace_bytes(int64_t, int64_t) {
-    return 64 + sizeof(double) * (6 * (size_t)kMuMaxGrid + 8);
+    return 64 + sizeof(double) * ((2 + kMuNV) * (size_t)kMuMaxGrid + 2 * kMuNV);
 }
 
 int mu_solve(const double* eps, const double* w, int64_t nk, int64_t nb, double target,

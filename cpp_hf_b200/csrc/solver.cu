@@ -359,13 +359,20 @@ int solve_dm(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* P
                                    cfg->max_step, S, st));
         }
         // 5. Cayley line search (elimination form of the spectral Cayley factor)
-        for (int64_t bt = 0; bt < cfg->bt_max; ++bt) {
-            if (small)
-                CPPHF_TRY(dm_small_trial(dQ[cur], F, p, dp[cur], wn, nk, nb, T_r, cfg->bt_shrink,
-                                         bt == cfg->bt_max - 1, fallback, S, st));
-            else
-                CPPHF_TRY(dm_trial_lu(dQ[cur], F, p, dp[cur], wn, nk, nb, T_r, cfg->bt_shrink, bt == cfg->bt_max - 1,
-                                      fallback, S, st));
+        if (small && cfg->bt_max >= 2 && cfg->bt_max - 1 <= dm_small_max_rest_trials()) {
+            // first trial, then (if it failed) all remaining trials in one pass
+            CPPHF_TRY(dm_small_trial(dQ[cur], F, p, dp[cur], wn, nk, nb, T_r, cfg->bt_shrink, 0, fallback, S, st));
+            CPPHF_TRY(dm_small_trial_rest(dQ[cur], F, p, dp[cur], wn, nk, nb, T_r, cfg->bt_shrink,
+                                          (int)(cfg->bt_max - 1), fallback, S, st));
+        } else {
+            for (int64_t bt = 0; bt < cfg->bt_max; ++bt) {
+                if (small)
+                    CPPHF_TRY(dm_small_trial(dQ[cur], F, p, dp[cur], wn, nk, nb, T_r, cfg->bt_shrink,
+                                             bt == cfg->bt_max - 1, fallback, S, st));
+                else
+                    CPPHF_TRY(dm_trial_lu(dQ[cur], F, p, dp[cur], wn, nk, nb, T_r, cfg->bt_shrink,
+                                          bt == cfg->bt_max - 1, fallback, S, st));
+            }
         }
         // 6. retraction and mu (occupations are formed by the next density step)
         if (small)

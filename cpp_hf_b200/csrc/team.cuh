@@ -142,9 +142,9 @@ __device__ __forceinline__ double2 cayley_factor(double lam, double tau) {
 // arrive sums all partials (thread-strided, then a fixed tree: deterministic for
 // a given grid) into out[0..NV) and
 // resets the counter.  Returns true in every thread of the last block.
-template <int NV>
+template <int NV, int M>
 __device__ __forceinline__ bool reduce_last_block(double (&v)[NV], double* partials, unsigned* counter,
-                                                  double* out, double* red) {
+                                                  double* out, double (&red)[M]) {
     block_sum<NV>(v, red);
     __shared__ int is_last;
     const int G = gridDim.x;

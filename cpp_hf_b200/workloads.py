@@ -54,8 +54,9 @@ def dirac(n: int = 48, *, seed: int = 0, m: float = -0.5, U: float = 1.0, T: flo
     return args, P0, 1.0 * float(np.sum(w))
 
 
-def layered(n: int = 192, *, n_layers: int = 4, seed: int = 0, U: float = 1.0, T: float = 0.05,
-            Delta: float = 0.2, gamma1: float = 0.4, noise: float = 0.005, filling=None):
+def layered_model(n: int = 192, *, n_layers: int = 4, seed: int = 0, U: float = 1.0, Delta: float = 0.2,
+                  gamma1: float = 0.4, noise: float = 0.005):
+    """(h, Vq, w) of the layered model; h is affine in (Delta, gamma1) and Vq linear in U."""
     nb = 2 * n_layers
     k = kgrid(n)
     kx, ky = np.meshgrid(k, k, indexing="ij")
@@ -80,6 +81,12 @@ def layered(n: int = 192, *, n_layers: int = 4, seed: int = 0, U: float = 1.0, T
     Vq = 2.0 * np.pi * U / (q + 0.05)
     Vq = Vq[..., None, None] * np.exp(-0.3 * q[..., None, None] * dl[None, None])
     w = np.full((n, n), 1.0 / (n * n))
+    return h, Vq, w
+
+
+def layered(n: int = 192, *, n_layers: int = 4, seed: int = 0, U: float = 1.0, T: float = 0.05,
+            Delta: float = 0.2, gamma1: float = 0.4, noise: float = 0.005, filling=None):
+    h, Vq, w = layered_model(n, n_layers=n_layers, seed=seed, U=U, Delta=Delta, gamma1=gamma1, noise=noise)
     args = kernel_args(w, h, Vq, T, include_exchange=True, include_hartree=False)
     P0 = np.zeros_like(h)
     n_fill = n_layers if filling is None else int(filling)

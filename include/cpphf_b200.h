@@ -97,7 +97,7 @@ int cpphf_find_mu_bisection(const double* eps, const double* weights, int64_t nk
  * because they synchronise the device, or code issuing work from a stream
  * callback where CUDA calls that allocate are not allowed.  Same arguments and
  * result as cpphf_find_mu_bisection minus the workspace: the scratch (grid
- * barrier words and block partials, about 49 KB) is a file-scope device array
+ * barrier words and block partials, about 74 KB) is a file-scope device array
  * that every GPU loading the library holds until the process exits.  Limit:
  * nk*nb <= CPPHF_MU_NOALLOC_MAX_EIGENVALUES; larger sizes are rejected with
  * CPPHF_ERR_INVALID.  The first call on a device looks up the array's device
