@@ -290,6 +290,7 @@ int eigh_batched(const double2* M, double* w, double2* V, int64_t batch, int64_t
         bs.start[1] = (short)nb;
         for (int i = 0; i < nb; ++i) bs.blk[i] = 0;
     }
+    if (bs.nblocks <= 1 && eigh_small_enabled(nb)) return eigh_small(M, w, V, batch, nb, mode, st);
     static std::once_flag once;
     std::call_once(once, [] {
         raise_smem(k_eigh<true>);

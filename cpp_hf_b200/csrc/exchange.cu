@@ -26,6 +26,7 @@
 #include "bulk.cuh"
 
 #include <algorithm>
+#include <cstdio>
 #include <cstdlib>
 #include <mutex>
 #include <string>
@@ -255,11 +256,11 @@ __global__ void __launch_bounds__(256) k_rows_inv_s(const Cx* T, double2* Sigma,
 // ===========================================================================
 // Pipelined four-step kernels (full channel set, no HCP).  Persistent CTAs
 // walk the tiles (line, channel chunk) with a stride of gridDim.x; thread 0
-// fetches the NEXT tile's rows with cp.async.bulk into the other shared-memory
-// stage while the CTA transforms the current one.  The transpose of the
-// four-step runs in place in the current stage.
-// smem: tw[N] | mbar[2] | stage[2] = { in tile [N][CB] (double2, or Cx for T),
-//                                       second tile [N][CB] double2 (refP or VR) }
+// keeps the next nst-1 tiles in flight (TMA tensor copies into a ring of nst
+// shared-memory stages) while the CTA transforms the current one.  The
+// transpose of the four-step runs in place in the current stage.
+// smem: tw[N] | mbar[kMaxPipeStages] | stage[nst] = { in tile [N][CB] (double2,
+//       or Cx for T), second tile [N][CB] double2 (refP or VR) }
 // ===========================================================================
 struct PipeLayout {
     size_t tw, bar, stage0, stage_bytes, in_bytes, total;
@@ -268,15 +269,17 @@ struct PipeLayout {
 // Offsets are relative to a 128-byte aligned base (TMA tensor copies need
 // 128-byte aligned shared-memory destinations); `total` includes the slack
 // for aligning the dynamic shared-memory base.
-__host__ __device__ inline PipeLayout pipe_layout(int N, int CB, size_t in_elem, bool second) {
+constexpr int kMaxPipeStages = 4;
+
+__host__ __device__ inline PipeLayout pipe_layout(int N, int CB, size_t in_elem, bool second, int nst) {
     PipeLayout L;
     L.tw = 0;
     L.bar = (sizeof(double2) * (size_t)N + 15) & ~(size_t)15;
-    L.stage0 = (L.bar + 16 + 127) & ~(size_t)127;
+    L.stage0 = (L.bar + 8 * kMaxPipeStages + 127) & ~(size_t)127;
     L.in_bytes = ((in_elem * (size_t)N * CB) + 127) & ~(size_t)127;
     L.stage_bytes = L.in_bytes + (second ? sizeof(double2) * (size_t)N * CB : 0);
     L.stage_bytes = (L.stage_bytes + 127) & ~(size_t)127;
-    L.total = L.stage0 + 2 * L.stage_bytes + 128;
+    L.total = L.stage0 + (size_t)nst * L.stage_bytes + 128;
     return L;
 }
 
@@ -288,19 +291,18 @@ __device__ __forceinline__ unsigned char* align128(unsigned char* p) {
 template <class Cx, int N1, int N2>
 __global__ void __launch_bounds__(256, 2) k_rows_fwd_p(const __grid_constant__ CUtensorMap mP,
                                                        const __grid_constant__ CUtensorMap mR, int has_refP, Cx* T,
-                                                       ExchangeGeom g, int CB, int nchunk, int ntiles) {
+                                                       ExchangeGeom g, int CB, int nchunk, int ntiles, int nst) {
     constexpr int N = N1 * N2;
     extern __shared__ __align__(16) unsigned char smem_dyn[];
     unsigned char* smem_raw = align128(smem_dyn);
     const bool has_ref = has_refP != 0;
-    const PipeLayout L = pipe_layout(N, CB, sizeof(double2), has_ref);
+    const PipeLayout L = pipe_layout(N, CB, sizeof(double2), has_ref, nst);
     Cx* tw = reinterpret_cast<Cx*>(smem_raw + L.tw);
     unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem_raw + L.bar);
     const int c = threadIdx.x % CB, a = threadIdx.x / CB;
     build_line_twiddles(tw, N);
     if (threadIdx.x == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
+        for (int b = 0; b < nst; ++b) mbar_init(&bar[b], 1);
         fence_mbar_init();
     }
     __syncthreads();
@@ -315,11 +317,15 @@ __global__ void __launch_bounds__(256, 2) k_rows_fwd_p(const __grid_constant__ C
         if (has_ref) tma_load_3d(st + L.in_bytes, &mR, 2 * c0, 0, kx, &bar[stage]);
     };
     int i = 0;
-    if ((int)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+    for (int j = 0; j < nst - 1; ++j)
+        if ((int)blockIdx.x + j * (int)gridDim.x < ntiles) issue(blockIdx.x + j * gridDim.x, j);
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
-        const int stage = i & 1;
-        if (t + (int)gridDim.x < ntiles) issue(t + gridDim.x, stage ^ 1);
-        if (!mbar_wait(&bar[stage], (i >> 1) & 1)) return;
+        const int stage = i % nst;
+        {
+            const int ahead = t + (nst - 1) * (int)gridDim.x;
+            if (ahead < ntiles) issue(ahead, (i + nst - 1) % nst);
+        }
+        if (!mbar_wait(&bar[stage], (unsigned)((i / nst) & 1))) return;
         unsigned char* st = smem_raw + L.stage0 + (size_t)stage * L.stage_bytes;
         const double2* in = reinterpret_cast<const double2*>(st);
         const double2* rin = reinterpret_cast<const double2*>(st + L.in_bytes);
@@ -360,18 +366,17 @@ __global__ void __launch_bounds__(256, 2) k_rows_fwd_p(const __grid_constant__ C
 template <class Cx, int N1, int N2>
 __global__ void __launch_bounds__(256) k_cols_conv_p(const __grid_constant__ CUtensorMap mT,
                                                      const __grid_constant__ CUtensorMap mV, Cx* T, ExchangeGeom g,
-                                                     int CB, int nchunk, int ntiles, int conjv) {
+                                                     int CB, int nchunk, int ntiles, int conjv, int nst) {
     constexpr int N = N1 * N2;
     extern __shared__ __align__(16) unsigned char smem_dyn[];
     unsigned char* smem_raw = align128(smem_dyn);
-    const PipeLayout L = pipe_layout(N, CB, sizeof(Cx), true);
+    const PipeLayout L = pipe_layout(N, CB, sizeof(Cx), true, nst);
     Cx* tw = reinterpret_cast<Cx*>(smem_raw + L.tw);
     unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem_raw + L.bar);
     const int c = threadIdx.x % CB, a = threadIdx.x / CB;
     build_line_twiddles(tw, N);
     if (threadIdx.x == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
+        for (int b = 0; b < nst; ++b) mbar_init(&bar[b], 1);
         fence_mbar_init();
     }
     __syncthreads();
@@ -388,11 +393,15 @@ __global__ void __launch_bounds__(256) k_cols_conv_p(const __grid_constant__ CUt
     };
     const int s0 = g.shift ? g.n0 / 2 : 0;
     int i = 0;
-    if ((int)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+    for (int j = 0; j < nst - 1; ++j)
+        if ((int)blockIdx.x + j * (int)gridDim.x < ntiles) issue(blockIdx.x + j * gridDim.x, j);
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
-        const int stage = i & 1;
-        if (t + (int)gridDim.x < ntiles) issue(t + gridDim.x, stage ^ 1);
-        if (!mbar_wait(&bar[stage], (i >> 1) & 1)) return;
+        const int stage = i % nst;
+        {
+            const int ahead = t + (nst - 1) * (int)gridDim.x;
+            if (ahead < ntiles) issue(ahead, (i + nst - 1) % nst);
+        }
+        if (!mbar_wait(&bar[stage], (unsigned)((i / nst) & 1))) return;
         unsigned char* st = smem_raw + L.stage0 + (size_t)stage * L.stage_bytes;
         Cx* S = reinterpret_cast<Cx*>(st);
         const double2* Vt = reinterpret_cast<const double2*>(st + L.in_bytes);
@@ -449,19 +458,19 @@ __global__ void __launch_bounds__(256) k_cols_conv_p(const __grid_constant__ CUt
 // pass C: rows inverse, scale, shift, store Sigma.  Tile t -> (kx, chunk).
 template <class Cx, int N1, int N2>
 __global__ void __launch_bounds__(256, 2) k_rows_inv_p(const __grid_constant__ CUtensorMap mT, double2* Sigma,
-                                                       ExchangeGeom g, int CB, int nchunk, int ntiles, double scale) {
+                                                       ExchangeGeom g, int CB, int nchunk, int ntiles, double scale,
+                                                       int nst) {
     constexpr int N = N1 * N2;
     extern __shared__ __align__(16) unsigned char smem_dyn[];
     unsigned char* smem_raw = align128(smem_dyn);
-    const PipeLayout L = pipe_layout(N, CB, sizeof(Cx), false);
+    const PipeLayout L = pipe_layout(N, CB, sizeof(Cx), false, nst);
     Cx* tw = reinterpret_cast<Cx*>(smem_raw + L.tw);
     unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem_raw + L.bar);
     const int c = threadIdx.x % CB, a = threadIdx.x / CB;
     const size_t nb2 = (size_t)g.nb * g.nb;
     build_line_twiddles(tw, N);
     if (threadIdx.x == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
+        for (int b = 0; b < nst; ++b) mbar_init(&bar[b], 1);
         fence_mbar_init();
     }
     __syncthreads();
@@ -475,11 +484,15 @@ __global__ void __launch_bounds__(256, 2) k_rows_inv_p(const __grid_constant__ C
     };
     const int s1 = g.shift ? g.n1 / 2 : 0;
     int i = 0;
-    if ((int)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+    for (int j = 0; j < nst - 1; ++j)
+        if ((int)blockIdx.x + j * (int)gridDim.x < ntiles) issue(blockIdx.x + j * gridDim.x, j);
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
-        const int stage = i & 1;
-        if (t + (int)gridDim.x < ntiles) issue(t + gridDim.x, stage ^ 1);
-        if (!mbar_wait(&bar[stage], (i >> 1) & 1)) return;
+        const int stage = i % nst;
+        {
+            const int ahead = t + (nst - 1) * (int)gridDim.x;
+            if (ahead < ntiles) issue(ahead, (i + nst - 1) % nst);
+        }
+        if (!mbar_wait(&bar[stage], (unsigned)((i / nst) & 1))) return;
         unsigned char* st = smem_raw + L.stage0 + (size_t)stage * L.stage_bytes;
         Cx* S = reinterpret_cast<Cx*>(st);
         const int kx = t / nchunk, c0 = (t - kx * nchunk) * CB;
@@ -646,10 +659,10 @@ struct Launch {
     int nchunk;
 };
 
-// channels per tile so that a CTA has about kTargetThreads threads; chunks balanced.
-Launch plan_launch(int lanes, int C, size_t elem, int n, bool generic) {
+// channels per tile so that a CTA has about `target` threads; chunks balanced.
+Launch plan_launch(int lanes, int C, size_t elem, int n, bool generic, int target = kTargetThreads) {
     Launch L;
-    const int cbmax = std::max(1, std::min(C, kTargetThreads / std::max(lanes, 1)));
+    const int cbmax = std::max(1, std::min(C, target / std::max(lanes, 1)));
     const int nch = (C + cbmax - 1) / cbmax;
     L.CB = (C + nch - 1) / nch;
     L.nchunk = (C + L.CB - 1) / L.CB;
@@ -661,6 +674,34 @@ Launch plan_launch(int lanes, int C, size_t elem, int n, bool generic) {
 }
 
 constexpr size_t kSmemMax = 227 * 1024 - 1024;
+
+// Pipelined-pass shape: threads per CTA (sets the channels per tile) and the
+// number of shared-memory stages.  CPPHF_PIPE_ROWS / CPPHF_PIPE_COLS =
+// "threads,stages" override the defaults (for tuning sweeps).
+struct PipeCfg {
+    int threads;
+    int nst;
+};
+
+PipeCfg pipe_cfg_env(const char* name, PipeCfg dflt) {
+    const char* e = std::getenv(name);
+    if (!e) return dflt;
+    PipeCfg c = dflt;
+    if (std::sscanf(e, "%d,%d", &c.threads, &c.nst) != 2) return dflt;
+    if (c.threads < 32 || c.threads > 1024) c.threads = dflt.threads;
+    if (c.nst < 2 || c.nst > kMaxPipeStages) c.nst = dflt.nst;
+    return c;
+}
+
+PipeCfg rows_cfg() {
+    static const PipeCfg c = pipe_cfg_env("CPPHF_PIPE_ROWS", PipeCfg{128, 2});
+    return c;
+}
+
+PipeCfg cols_cfg() {
+    static const PipeCfg c = pipe_cfg_env("CPPHF_PIPE_COLS", PipeCfg{128, 2});
+    return c;
+}
 
 // CPPHF_EXCHANGE_PIPELINE=0 selects the non-pipelined kernels (for A/B timing).
 bool pipeline_enabled() {
@@ -695,12 +736,14 @@ struct Spec {
     }
     // TMA boxes need 16-byte multiples for the inner extent, the row stride and
     // the x coordinate (2 c0 scalars): for complex64 T that means even CB and Ct.
-    static bool pipelined(const ExchangeGeom& g) {
+    static Launch pipe_launch(const ExchangeGeom& g, const PipeCfg& cfg) {
+        return plan_launch(N1 > N2 ? N1 : N2, g.C, sizeof(Cx), N1 * N2, false, cfg.threads);
+    }
+    static bool pipelined(const ExchangeGeom& g, const PipeCfg& cfg) {
         if (g.hcp || !pipeline_enabled() || N1 * N2 > 256) return false;
-        if (sizeof(Cx) == 8) {
-            const Launch L = plan_launch(N1 > N2 ? N1 : N2, g.C, sizeof(Cx), N1 * N2, false);
-            if ((L.CB % 2) != 0 || (g.Ct % 2) != 0) return false;
-        }
+        const Launch L = pipe_launch(g, cfg);
+        if (L.threads > 256) return false;  // __launch_bounds__(256)
+        if (sizeof(Cx) == 8 && ((L.CB % 2) != 0 || (g.Ct % 2) != 0)) return false;
         return true;
     }
     static CUtensorMapDataType tdt() { return sizeof(Cx) == 16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32; }
@@ -713,9 +756,10 @@ struct Spec {
     }
     static int rows_fwd(const double2* P, const double2* refP, Cx* T, const ExchangeGeom& g, cudaStream_t st) {
         attrs();
-        if (pipelined(g)) {
-            const Launch L = plan_launch(N1 > N2 ? N1 : N2, g.C, sizeof(Cx), N1 * N2, false);
-            const PipeLayout PL = pipe_layout(N1 * N2, L.CB, sizeof(double2), refP != nullptr);
+        const PipeCfg cfg = rows_cfg();
+        if (pipelined(g, cfg)) {
+            const Launch L = pipe_launch(g, cfg);
+            const PipeLayout PL = pipe_layout(N1 * N2, L.CB, sizeof(double2), refP != nullptr, cfg.nst);
             if (PL.total <= kSmemMax) {
                 CUtensorMap mP, mR;
                 const int nb2 = g.nb * g.nb;
@@ -726,7 +770,7 @@ struct Spec {
                     const int nt = g.n0 * L.nchunk;
                     const int grid = pgrid(k_rows_fwd_p<Cx, N1, N2>, L.threads, PL.total, nt);
                     k_rows_fwd_p<Cx, N1, N2><<<grid, L.threads, PL.total, st>>>(mP, mR, refP != nullptr, T, g, L.CB,
-                                                                                L.nchunk, nt);
+                                                                                L.nchunk, nt, cfg.nst);
                     CPPHF_LAUNCH_CHECK("exchange rows forward (pipelined)");
                     return CPPHF_OK;
                 }
@@ -739,9 +783,10 @@ struct Spec {
     }
     static int cols(Cx* T, const double2* VR, const ExchangeGeom& g, int vmode, cudaStream_t st) {
         attrs();
-        if (pipelined(g) && vmode != kColsForwardOnly) {
-            const Launch L = plan_launch(N1 > N2 ? N1 : N2, g.C, sizeof(Cx), N1 * N2, false);
-            const PipeLayout PL = pipe_layout(N1 * N2, L.CB, sizeof(Cx), true);
+        const PipeCfg cfg = cols_cfg();
+        if (pipelined(g, cfg) && vmode != kColsForwardOnly) {
+            const Launch L = pipe_launch(g, cfg);
+            const PipeLayout PL = pipe_layout(N1 * N2, L.CB, sizeof(Cx), true, cfg.nst);
             if (PL.total <= kSmemMax) {
                 CUtensorMap mT, mV;
                 bool ok = field_map(&mT, T, tdt(), sizeof(Cx) / 2, g.Ct, g, 2 * L.CB, 1, N1 * N2);
@@ -753,7 +798,8 @@ struct Spec {
                     const int nt = g.n1 * L.nchunk;
                     const int grid = pgrid(k_cols_conv_p<Cx, N1, N2>, L.threads, PL.total, nt);
                     k_cols_conv_p<Cx, N1, N2><<<grid, L.threads, PL.total, st>>>(mT, mV, T, g, L.CB, L.nchunk, nt,
-                                                                                 vmode == kColsConjVR ? 1 : 0);
+                                                                                 vmode == kColsConjVR ? 1 : 0,
+                                                                                 cfg.nst);
                     CPPHF_LAUNCH_CHECK("exchange columns convolve (pipelined)");
                     return CPPHF_OK;
                 }
@@ -766,16 +812,17 @@ struct Spec {
     }
     static int rows_inv(const Cx* T, double2* Sigma, const ExchangeGeom& g, double scale, cudaStream_t st) {
         attrs();
-        if (pipelined(g)) {
-            const Launch L = plan_launch(N1 > N2 ? N1 : N2, g.C, sizeof(Cx), N1 * N2, false);
-            const PipeLayout PL = pipe_layout(N1 * N2, L.CB, sizeof(Cx), false);
+        const PipeCfg cfg = rows_cfg();
+        if (pipelined(g, cfg)) {
+            const Launch L = pipe_launch(g, cfg);
+            const PipeLayout PL = pipe_layout(N1 * N2, L.CB, sizeof(Cx), false, cfg.nst);
             if (PL.total <= kSmemMax) {
                 CUtensorMap mT;
                 if (field_map(&mT, T, tdt(), sizeof(Cx) / 2, g.Ct, g, 2 * L.CB, N1 * N2, 1)) {
                     const int nt = g.n0 * L.nchunk;
                     const int grid = pgrid(k_rows_inv_p<Cx, N1, N2>, L.threads, PL.total, nt);
                     k_rows_inv_p<Cx, N1, N2><<<grid, L.threads, PL.total, st>>>(mT, Sigma, g, L.CB, L.nchunk, nt,
-                                                                                scale);
+                                                                                scale, cfg.nst);
                     CPPHF_LAUNCH_CHECK("exchange rows inverse (pipelined)");
                     return CPPHF_OK;
                 }

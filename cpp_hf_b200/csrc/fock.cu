@@ -17,6 +17,7 @@
 #include "team.cuh"
 
 #include <algorithm>
+#include <cstdio>
 #include <cstdlib>
 #include <mutex>
 #include <string>
@@ -28,6 +29,7 @@ namespace {
 constexpr int kAsmThreads = 256;
 constexpr int kRedThreads = 256;
 constexpr int kMaxPartials = 2048;
+constexpr int kAsmMaxStages = 4;
 
 // rho_bar partials: grid (Gk, ceil(nb2 / CH)), CH channels per block, lanes =
 // blockDim / CH k-lanes.
@@ -256,18 +258,17 @@ __global__ void __launch_bounds__(kAsmThreads) k_assemble_tiled(AsmArgs a, int K
 // reduced in the same launch (last-block sum in a fixed order).
 template <bool REF>
 __global__ void __launch_bounds__(kAsmThreads) k_assemble_bulk(AsmArgs a, int KT, int64_t ntiles,
-                                                               unsigned* counter, double* energy_out) {
+                                                               unsigned* counter, double* energy_out, int nst) {
     constexpr int NARR = REF ? 4 : 3;
     extern __shared__ __align__(16) unsigned char smem_dyn[];
     __shared__ double red[32];
-    __shared__ __align__(8) unsigned long long bar[2];
+    __shared__ __align__(8) unsigned long long bar[kAsmMaxStages];
     const int nb = a.nb, nb2 = nb * nb;
     const int tile = KT * nb2;
     double2* stg = reinterpret_cast<double2*>(
         (reinterpret_cast<uintptr_t>(smem_dyn) + 127) & ~(uintptr_t)127);
     if (threadIdx.x == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
+        for (int b = 0; b < nst; ++b) mbar_init(&bar[b], 1);
         fence_mbar_init();
     }
     __syncthreads();
@@ -287,11 +288,12 @@ __global__ void __launch_bounds__(kAsmThreads) k_assemble_bulk(AsmArgs a, int KT
     };
     double e_acc[1] = {0.0};
     int i = 0;
-    if ((int64_t)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+    for (int j = 0; j < nst - 1; ++j)
+        if ((int64_t)blockIdx.x + (int64_t)j * gridDim.x < ntiles) issue(blockIdx.x + (int64_t)j * gridDim.x, j);
     for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
-        const int s = i & 1;
-        if (t + gridDim.x < ntiles) issue(t + gridDim.x, s ^ 1);
-        if (!mbar_wait(&bar[s], (unsigned)((i >> 1) & 1))) return;
+        const int s = i % nst;
+        if (t + (int64_t)(nst - 1) * gridDim.x < ntiles) issue(t + (int64_t)(nst - 1) * gridDim.x, (i + nst - 1) % nst);
+        if (!mbar_wait(&bar[s], (unsigned)((i / nst) & 1))) return;
         const double2* sS = stg + (size_t)s * NARR * tile;
         const double2* sH = sS + tile;
         const double2* sP = sS + 2 * tile;
@@ -348,6 +350,26 @@ struct FockWs {
     size_t off_part, off_counter, off_rho_part, off_rho_bar, off_sc, off_hd, off_exch, total;
     int Gasm, Gk;
 };
+
+// Bulk assembly shape: complex elements per array per stage and stage count;
+// CPPHF_ASSEMBLY="elems,stages" overrides (for tuning sweeps).
+struct AsmCfg {
+    int elems;
+    int nst;
+};
+
+AsmCfg asm_cfg() {
+    static const AsmCfg c = [] {
+        AsmCfg d{512, 2};
+        const char* e = std::getenv("CPPHF_ASSEMBLY");
+        AsmCfg v = d;
+        if (e && std::sscanf(e, "%d,%d", &v.elems, &v.nst) == 2 && v.elems >= 64 && v.elems <= 4096 && v.nst >= 2 &&
+            v.nst <= kAsmMaxStages)
+            return v;
+        return d;
+    }();
+    return c;
+}
 
 // CPPHF_ASSEMBLY_BULK=0 selects the non-pipelined assembly (for A/B timing).
 bool bulk_assembly_enabled() {
@@ -458,11 +480,12 @@ int build_fock(const cpphf_kernel* K, const double2* P, double2* Sigma, double2*
     a.part = part;
     if (nb2 <= kTileElems && bulk_assembly_enabled()) {
         // whole k-blocks per stage: 1024 elements (3 arrays) or 512 (4 arrays with refP)
-        const int elems = refP ? 512 : kTileElems;
+        const AsmCfg cfg = asm_cfg();
+        const int elems = refP ? cfg.elems / 2 : cfg.elems;
         const int KT = std::max(1, elems / nb2);
         const int64_t ntiles = (nk + KT - 1) / KT;
         const int narr = refP ? 4 : 3;
-        const size_t smem = sizeof(double2) * (size_t)KT * nb2 * narr * 2 + 128;
+        const size_t smem = sizeof(double2) * (size_t)KT * nb2 * narr * cfg.nst + 128;
         static std::once_flag once_b;
         std::call_once(once_b, [] {
             raise_smem(k_assemble_bulk<false>);
@@ -479,9 +502,9 @@ int build_fock(const cpphf_kernel* K, const double2* P, double2* Sigma, double2*
         unsigned* counter = reinterpret_cast<unsigned*>(W + L.off_counter);
         if (energy) CPPHF_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned), st));
         if (refP)
-            k_assemble_bulk<true><<<grid, kAsmThreads, smem, st>>>(a, KT, ntiles, counter, energy);
+            k_assemble_bulk<true><<<grid, kAsmThreads, smem, st>>>(a, KT, ntiles, counter, energy, cfg.nst);
         else
-            k_assemble_bulk<false><<<grid, kAsmThreads, smem, st>>>(a, KT, ntiles, counter, energy);
+            k_assemble_bulk<false><<<grid, kAsmThreads, smem, st>>>(a, KT, ntiles, counter, energy, cfg.nst);
         CPPHF_LAUNCH_CHECK("assemble (bulk pipelined)");
         return CPPHF_OK;
     }

@@ -1,0 +1,52 @@
+"""GPU: batched sweeps (many independent solves of uneven mesh and band count on
+concurrent streams) against the same instances solved one by one in FP64 and
+against the oracle."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from cpp_hf_b200 import batch
+
+pytestmark = pytest.mark.gpu
+
+
+def _small_sweep(count=8, seed=3):
+    # the sweep's draws (nb, T, U, filling) on meshes small enough for the oracle
+    return batch.sweep_instances(count, seed=seed, meshes=(6, 8, 12))
+
+
+def test_sweep_draws_cover_models_and_fillings():
+    inst = batch.sweep_instances(96, seed=0)
+    nbs = {i.nb for i in inst}
+    assert nbs == {2, 4, 6, 8}
+    assert {i.n for i in inst} <= {36, 48, 72, 96, 144}
+    for i in inst:
+        assert 1 <= i.filling <= i.nb - 1
+        assert 0.02 <= i.T <= 0.2 and 0.5 <= i.U <= 2.0
+        assert i.args["h"].shape == (i.n, i.n, i.nb, i.nb)
+
+
+@pytest.mark.parametrize("solver", ["dm", "scf"])
+def test_batched_mixed_matches_sequential_fp64_and_oracle(oracle, solver):
+    inst = batch.upload(_small_sweep())
+    seq, t_seq = batch.solve_batch(inst, precision="fp64", solver=solver, streams=1, tol=1e-11)
+    bat, t_bat = batch.solve_batch(inst, precision="mixed", solver=solver, streams=4, tol=1e-11)
+    for i, (a, b) in enumerate(zip(seq, bat)):
+        x = inst[i]
+        if solver == "dm":
+            nb, n = x.nb, x.n
+            ref = oracle.solve_dm(x.args, x.P0, x.n_e, 1000, 1e-11, 0.0, 0.6, 0.5, 1e-3, 8, 10, 5, 25, 0, 0.5, 20,
+                                  np.empty((0, n, n, nb, nb), np.complex128), 0.0, 1.0, [], None, False, False, False)
+            E_ref, it_ref = ref[5], ref[6]
+        else:
+            ref = oracle.solve_scf(x.args, x.P0, x.n_e, 1000, 1e-11, 1e-11, 0.5, 0.0, None, [], "linear", 6, 2, 1.0,
+                                   0.0, False, False)
+            E_ref, it_ref = ref[2], ref[4]
+        print(f"{solver} #{i} {x.model} n={x.n} nb={x.nb} fill={x.filling}: fp64 {a['iterations']} it, "
+              f"mixed {b['iterations']} it, oracle {it_ref} it; |dE| fp64 {abs(a['energy'] - E_ref):.2e} "
+              f"mixed {abs(b['energy'] - E_ref):.2e}")
+        assert a["converged"] and b["converged"]
+        assert abs(a["energy"] - E_ref) < 1e-9 * max(1.0, abs(E_ref))
+        assert abs(b["energy"] - E_ref) < 1e-9 * max(1.0, abs(E_ref))
