@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--solves", type=int, default=1, help="also time solve/solve_scf (1) or not (0)")
     ap.add_argument("--solve-reps", type=int, default=2)
     ap.add_argument("--oracle-solve", type=int, default=1, help="oracle DM solve estimate on the host")
+    ap.add_argument("--sweep", type=int, default=96, help="batched-sweep instances (0 = skip)")
+    ap.add_argument("--sweep-streams", type=int, default=16)
     return ap.parse_args()
 
 
@@ -364,6 +366,37 @@ def main():
         solves = time_solves(torch, native, args_dev, P0_dev, _ne, a.solve_reps)
         barrier()
 
+    # ---- batched sweep: mixed precision on concurrent streams vs one by one in FP64 ----
+    sweep = None
+    if a.sweep > 0:
+        from cpp_hf_b200 import batch
+
+        inst = batch.upload(batch.sweep_instances(a.sweep, seed=rank))
+        batch.solve_batch(inst[:4], precision="fp64", streams=1)  # warm-up (kernel attributes, allocator)
+        barrier()
+        seq, t_seq = batch.solve_batch(inst, precision="fp64", streams=1)
+        bat, t_bat = batch.solve_batch(inst, precision="mixed", streams=a.sweep_streams)
+        barrier()
+        rel = [abs(x["energy"] - y["energy"]) / max(1.0, abs(x["energy"])) for x, y in zip(seq, bat)]
+        same = [r for r in rel if r <= 1e-9]
+        sweep = {
+            "instances": len(inst),
+            "batched_mixed_solves_per_s": len(inst) / t_bat,
+            "sequential_fp64_solves_per_s": len(inst) / t_seq,
+            "speedup": t_seq / t_bat,
+            "mixed_same_state_as_fp64": len(same),
+            "max_rel_dE_mixed_vs_fp64_same_state": max(same) if same else None,
+            "max_rel_dE_mixed_vs_fp64_all": max(rel),
+            "converged_fp64": int(sum(bool(x["converged"]) for x in seq)),
+            "converged_mixed": int(sum(bool(y["converged"]) for y in bat)),
+            "iterations_fp64": int(sum(x["iterations"] for x in seq)),
+            "iterations_mixed": int(sum(y["iterations"] for y in bat)),
+            "streams": a.sweep_streams,
+            "config": ("seeded instances: nb in {2,4,6,8} (Dirac for 2, layered for 4-8), mesh in "
+                       "{36,48,72,96,144}^2, T~U[0.02,0.2], U~U[0.5,2], integer filling; solve() with tol_E=1e-10; "
+                       "wall clock over the batch with device sync on both sides"),
+        }
+
     # max over ranks
     times = torch.tensor([t_dev, t_ex, t_e2e], dtype=torch.float64, device=dev)
     if pg is not None:
@@ -442,6 +475,8 @@ def main():
                               f"{solves['dm_fp64']['iterations']} iterations: {per_it:.3f} s/iteration, "
                               f"{base:.3f} s setup"}
             line["solves"] = solves
+        if sweep is not None:
+            line["sweep"] = sweep
         print(json.dumps(line), flush=True)
     if pg is not None:
         pg.barrier()

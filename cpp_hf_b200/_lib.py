@@ -27,6 +27,20 @@ dp = C.POINTER(C.c_double)
 sz = C.c_size_t
 
 
+class Superlattice(C.Structure):
+    """``cpphf_superlattice`` (layout index arrays on the host, Coulomb tables on the device)."""
+
+    _fields_ = [
+        ("fock_active", i32), ("hartree_active", i32),
+        ("n_G", i64), ("dim_orb", i64), ("n_delta", i64), ("N_ext_x", i64), ("N_ext_y", i64),
+        ("hartree_degeneracy", f64),
+        ("V_lag_fft", vp), ("V_lag_fft_orbital", vp),
+        ("g_a_off", C.POINTER(i64)), ("pair_i", C.POINTER(i64)), ("pair_j", C.POINTER(i64)),
+        ("pair_start", C.POINTER(i64)), ("pair_to_delta", C.POINTER(i64)),
+        ("HH_GG", vp), ("HH_GG_orbital", vp),
+    ]
+
+
 class Kernel(C.Structure):
     """``cpphf_kernel`` (device pointers)."""
 
@@ -38,6 +52,7 @@ class Kernel(C.Structure):
         ("T", f64), ("weight_sum", f64),
         ("h", vp), ("VR", vp), ("refP", vp), ("w2d", vp), ("HH", vp),
         ("contact_g", vp), ("contact_Oi", vp), ("contact_Oj", vp),
+        ("sl", C.POINTER(Superlattice)),
     ]
 
 
@@ -92,6 +107,10 @@ _SIGS = {
     "cpphf_solve_dm_workspace_bytes": (sz, [C.POINTER(Kernel)]),
     "cpphf_solve_dm": (C.c_int, [C.POINTER(Kernel), C.POINTER(DmConfig), vp, f64, PROJECT_FN, vp,
                                  vp, vp, vp, vp, dp, dp, C.POINTER(DmResult), vp, sz, vp]),
+    "cpphf_superlattice_workspace_bytes": (sz, [i64, i64, i64, i64, i64, C.c_int]),
+    "cpphf_superlattice_streamed": (C.c_int, [vp, vp, vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(i64),
+                                              C.POINTER(i64), i64, i64, i64, i64, i64, i64, i64, C.c_int, vp, vp,
+                                              sz, vp]),
     "cpphf_density_from_fock_workspace_bytes": (sz, [i64, i64]),
     "cpphf_density_from_fock": (C.c_int, [vp, vp, i64, i64, i64, f64, f64, f64, vp, vp, vp, vp, vp, sz, vp]),
     "cpphf_exchange_adjoint": (C.c_int, [vp, vp, vp, i64, i64, i64, i64, vp]),

@@ -281,8 +281,9 @@ class _DeviceKernel:
         cg = _to_dev(cg_host, "f")
         cOi = _to_dev(args["contact_Oi"], "c")
         cOj = _to_dev(args["contact_Oj"], "c")
+        self.sl = None
         if args.get("superlattice_fock_active", False) or args.get("superlattice_hartree_active", False):
-            raise NotImplementedError("superlattice kernel_args are not supported by this entry point yet")
+            self.sl = _superlattice_struct(args, nb)
         prec, self.mixed = _parse_precision(args.get("exchange_precision", precision or DEFAULT_EXCHANGE_PRECISION))
         self.mixed_switch = float(args.get("mixed_switch", DEFAULT_MIXED_SWITCH)) if self.mixed else 0.0
         self._keep = [h, VR, refP, w2d, HH, cg, cOi, cOj]
@@ -302,10 +303,76 @@ class _DeviceKernel:
         K.refP = refP.data_ptr() if refP is not None else None
         K.w2d, K.HH = w2d.data_ptr(), HH.data_ptr()
         K.contact_g, K.contact_Oi, K.contact_Oj = cg.data_ptr(), cOi.data_ptr(), cOj.data_ptr()
+        if self.sl is not None:
+            K.sl = C.pointer(self.sl[0])
         self.K = K
 
     def ref(self):
         return C.byref(self.K)
+
+
+def _i64_host(x, name):
+    a = np.ascontiguousarray(np.asarray(x.cpu() if _is_torch(x) else x), dtype=np.int64)
+    return a
+
+
+def _superlattice_struct(args, nb):
+    """``cpphf_superlattice`` from the superlattice_* kernel_args entries
+    (cpp_hf_native.cpp:109-213).  Returns (struct, kept arrays)."""
+    n_G = int(args["n_G"])
+    dim_orb = int(args["dim_orb"])
+    n_delta = int(args["n_delta"])
+    N_ext_x, N_ext_y = int(args["N_ext_x"]), int(args["N_ext_y"])
+    if n_G * dim_orb != nb:
+        raise ValueError("superlattice mode requires n_G × dim_orb == nb")
+    V = _to_dev(args["V_lag_fft"], "c")
+    if tuple(V.shape[:2]) != (N_ext_x, N_ext_y):
+        raise ValueError("V_lag_fft must have shape (N_ext_x, N_ext_y)")
+    g_a_off = _i64_host(args["g_a_off"], "g_a_off")
+    pair_i = _i64_host(args["pair_i"], "pair_i")
+    pair_j = _i64_host(args["pair_j"], "pair_j")
+    pair_start = _i64_host(args["pair_start"], "pair_start")
+    p2d = _i64_host(args["pair_to_delta"], "pair_to_delta")
+    if g_a_off.shape != (n_G, 2):
+        raise ValueError("g_a_off must be (n_G, 2)")
+    if pair_start.shape[0] != n_delta + 1:
+        raise ValueError("pair_start must have length n_delta + 1")
+    if pair_i.shape[0] != pair_j.shape[0]:
+        raise ValueError("pair_i and pair_j must have the same length")
+    if p2d.shape != (n_G, n_G):
+        raise ValueError("pair_to_delta must be (n_G, n_G)")
+    keep = [V, g_a_off, pair_i, pair_j, pair_start, p2d]
+    S = _lib.Superlattice()
+    S.fock_active = int(bool(args.get("superlattice_fock_active", False)))
+    S.hartree_active = int(bool(args.get("superlattice_hartree_active", False)))
+    S.n_G, S.dim_orb, S.n_delta, S.N_ext_x, S.N_ext_y = n_G, dim_orb, n_delta, N_ext_x, N_ext_y
+    S.hartree_degeneracy = float(args.get("hartree_degeneracy", 1.0))
+    S.V_lag_fft = V.data_ptr()
+    S.V_lag_fft_orbital = None
+    if "V_lag_fft_orbital" in args:
+        vo = _to_dev(args["V_lag_fft_orbital"], "c")
+        if tuple(vo.shape) != (N_ext_x, N_ext_y, dim_orb, dim_orb):
+            raise ValueError("V_lag_fft_orbital must be (N_ext_x, N_ext_y, dim_orb, dim_orb)")
+        keep.append(vo)
+        S.V_lag_fft_orbital = vo.data_ptr()
+    for name, arr in (("g_a_off", g_a_off), ("pair_i", pair_i), ("pair_j", pair_j), ("pair_start", pair_start),
+                      ("pair_to_delta", p2d)):
+        setattr(S, name, arr.ctypes.data_as(C.POINTER(_lib.i64)))
+    S.HH_GG = None
+    S.HH_GG_orbital = None
+    if S.hartree_active:
+        hg = _to_dev(args["HH_GG"], "f")
+        if tuple(hg.shape) != (n_G, n_G):
+            raise ValueError("HH_GG must be (n_G, n_G)")
+        keep.append(hg)
+        S.HH_GG = hg.data_ptr()
+        if "HH_GG_orbital" in args:
+            ho = _to_dev(args["HH_GG_orbital"], "f")
+            if tuple(ho.shape) != (n_G, n_G, dim_orb, dim_orb):
+                raise ValueError("HH_GG_orbital must be (n_G, n_G, dim_orb, dim_orb)")
+            keep.append(ho)
+            S.HH_GG_orbital = ho.data_ptr()
+    return (S, keep)
 
 
 def _host_project(project_fn, F):
@@ -528,8 +595,49 @@ def _deflation_bias(P, targets, w2d, sigma, length):
 
 def selfenergy_superlattice_streamed(rho, VR_fft, g_a_off, pair_i, pair_j, pair_start, nkx, nky, n_G,
                                      dim_orb, N_ext_x, N_ext_y, VR_fft_orbital=None, hermitian_rho=False):
-    """cpp_hf_native.cpp:719-816."""
-    raise NotImplementedError("selfenergy_superlattice_streamed is not built into cpp_hf_b200 yet")
+    """cpp_hf_native.cpp:719-816 (streamed superlattice Fock, superlattice.hpp:50-246)."""
+    lib = _lib_handle()
+    as_np = not _is_torch(rho)
+    rho_t = _to_dev(rho, "c")
+    V = _to_dev(VR_fft, "c")
+    g_a_off = _i64_host(g_a_off, "g_a_off")
+    pair_i = _i64_host(pair_i, "pair_i")
+    pair_j = _i64_host(pair_j, "pair_j")
+    pair_start = _i64_host(pair_start, "pair_start")
+    nkx, nky, n_G, dim_orb = int(nkx), int(nky), int(n_G), int(dim_orb)
+    N_ext_x, N_ext_y = int(N_ext_x), int(N_ext_y)
+    if rho_t.dim() != 6:
+        raise ValueError("rho must be (nkx, nky, n_G, dim_orb, n_G, dim_orb)")
+    if V.dim() != 2:
+        raise ValueError("VR_fft must be (N_ext_x, N_ext_y)")
+    if tuple(V.shape) != (N_ext_x, N_ext_y):
+        raise ValueError("VR_fft shape does not match (N_ext_x, N_ext_y)")
+    if g_a_off.ndim != 2 or g_a_off.shape != (n_G, 2):
+        raise ValueError("g_a_off must be (n_G, 2)")
+    if pair_start.ndim != 1 or pair_start.shape[0] < 1:
+        raise ValueError("pair_start must be 1-D, len >= 1")
+    if pair_i.ndim != 1 or pair_j.ndim != 1 or pair_i.shape[0] != pair_j.shape[0]:
+        raise ValueError("pair_i and pair_j must be 1-D with the same length")
+    if tuple(rho_t.shape) != (nkx, nky, n_G, dim_orb, n_G, dim_orb):
+        raise ValueError("rho must be (nkx, nky, n_G, dim_orb, n_G, dim_orb)")
+    vo = None
+    if VR_fft_orbital is not None:
+        vo = _to_dev(VR_fft_orbital, "c")
+        if vo.dim() != 4 or tuple(vo.shape) != (N_ext_x, N_ext_y, dim_orb, dim_orb):
+            raise ValueError("VR_fft_orbital must be (N_ext_x, N_ext_y, dim_orb, dim_orb)")
+    n_delta = pair_start.shape[0] - 1
+    if int(pair_start[-1]) > pair_i.shape[0]:
+        raise ValueError("pair_start exceeds the pair arrays")
+    sigma = torch.empty_like(rho_t)
+    ws = _ws(lib.cpphf_superlattice_workspace_bytes(int(pair_start[-1]), n_G, dim_orb, N_ext_x, N_ext_y,
+                                                    int(vo is not None)))
+    P64 = C.POINTER(_lib.i64)
+    check(lib.cpphf_superlattice_streamed(_ptr(rho_t), _ptr(V), _ptr(vo), g_a_off.ctypes.data_as(P64),
+                                          pair_i.ctypes.data_as(P64), pair_j.ctypes.data_as(P64),
+                                          pair_start.ctypes.data_as(P64), n_delta, nkx, nky, n_G, dim_orb,
+                                          N_ext_x, N_ext_y, int(bool(hermitian_rho)), _ptr(sigma), _ptr(ws),
+                                          ws.numel(), _stream()), "selfenergy_superlattice_streamed")
+    return _out(sigma, as_np)
 
 
 def resample_kgrid_2d(values, nk_new):

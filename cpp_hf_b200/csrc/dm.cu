@@ -383,14 +383,16 @@ __global__ void k_retract(double2* Q, const double2* __restrict__ V, const doubl
 // skew-Hermitian), so Gauss-Jordan elimination without pivoting is stable.
 // On return Rs holds U (Ms is clobbered).
 // ---------------------------------------------------------------------------
+// d is read straight from the k-block in global memory (dense, row stride nb),
+// so the team holds only M, the right-hand side R and one more matrix.
 template <bool WARP>
-__device__ __forceinline__ void team_cayley_lu(const double2* Ds, double2* Ms, double2* Rs, double2* fs, double tau,
-                                               int nb, const Team<WARP>& t) {
+__device__ __forceinline__ void team_cayley_lu(const double2* __restrict__ dk, double2* Ms, double2* Rs, double2* fs,
+                                               double tau, int nb, const Team<WARP>& t) {
     const int ld = nb + 1;
     const double h = 0.5 * tau;
     for (int e = t.tid; e < nb * nb; e += t.nt) {
         const int i = e / nb, j = e - i * nb;
-        const double2 a = cscale(Ds[i * ld + j], h);
+        const double2 a = cscale(dk[e], h);
         const double one = (i == j) ? 1.0 : 0.0;
         Ms[i * ld + j] = mk(one + a.x, a.y);
         Rs[i * ld + j] = mk(one - a.x, -a.y);
@@ -449,8 +451,7 @@ __global__ void k_trial_lu(const double2* __restrict__ dQ, const double2* __rest
     extern __shared__ __align__(16) unsigned char raw[];
     __shared__ double red[64];
     Team<WARP> t;
-    double2* Ds = team_mats<WARP>(raw, nb, 4, 3 * nb, t.team);
-    double2* Ms = Ds + team_mat_elems(nb);
+    double2* Ms = team_mats<WARP>(raw, nb, 3, 3 * nb, t.team);
     double2* Rs = Ms + team_mat_elems(nb);
     double2* Fs = Rs + team_mat_elems(nb);
     double2* fs = Fs + team_mat_elems(nb);
@@ -458,10 +459,8 @@ __global__ void k_trial_lu(const double2* __restrict__ dQ, const double2* __rest
     const double tau = S->tau_cur;
     double v[2] = {0.0, 0.0};
     for (int64_t k = (int64_t)blockIdx.x * t.nteams + t.team; k < nk; k += (int64_t)gridDim.x * t.nteams) {
-        tload<WARP>(Ds, dQ + (size_t)k * nb * nb, nb, t);
         tload<WARP>(Fs, Ft + (size_t)k * nb * nb, nb, t);
-        t.sync();
-        team_cayley_lu<WARP>(Ds, Ms, Rs, fs, tau, nb, t);
+        team_cayley_lu<WARP>(dQ + (size_t)k * nb * nb, Ms, Rs, fs, tau, nb, t);
         team_diag_uhfu<WARP>(Rs, Fs, Ms, ds, nb, t);
         t.sync();
         const double wk = w[k];
@@ -491,22 +490,19 @@ __global__ void k_retract_lu(double2* Q, const double2* __restrict__ dQ, const d
                              double* __restrict__ ew, int64_t nk, int nb, const DmScalars* S) {
     extern __shared__ __align__(16) unsigned char raw[];
     Team<WARP> t;
-    double2* Ds = team_mats<WARP>(raw, nb, 4, 2 * nb, t.team);
-    double2* Ms = Ds + team_mat_elems(nb);
+    double2* Ms = team_mats<WARP>(raw, nb, 3, 2 * nb, t.team);
     double2* Rs = Ms + team_mat_elems(nb);
     double2* Fs = Rs + team_mat_elems(nb);
     double2* fs = Fs + team_mat_elems(nb);
     const double tau = S->tau_final;
     for (int64_t k = (int64_t)blockIdx.x * t.nteams + t.team; k < nk; k += (int64_t)gridDim.x * t.nteams) {
-        tload<WARP>(Ds, dQ + (size_t)k * nb * nb, nb, t);
         tload<WARP>(Fs, Ft + (size_t)k * nb * nb, nb, t);
-        t.sync();
-        team_cayley_lu<WARP>(Ds, Ms, Rs, fs, tau, nb, t);
+        team_cayley_lu<WARP>(dQ + (size_t)k * nb * nb, Ms, Rs, fs, tau, nb, t);
         team_diag_uhfu<WARP>(Rs, Fs, Ms, ew + (size_t)k * nb, nb, t);
         t.sync();
-        tload<WARP>(Ds, Q + (size_t)k * nb * nb, nb, t);
+        tload<WARP>(Fs, Q + (size_t)k * nb * nb, nb, t);  // Ft is done: Q takes its place
         t.sync();
-        tmm<false, false, WARP>(Ms, Ds, Rs, nb, t);  // Q U
+        tmm<false, false, WARP>(Ms, Fs, Rs, nb, t);  // Q U
         t.sync();
         tstore<WARP>(Q + (size_t)k * nb * nb, Ms, nb, t);
         t.sync();
@@ -573,8 +569,8 @@ void init_attrs() {
 
 int dm_check_nb(int64_t nb) {
     if (nb < 1) return fail(CPPHF_ERR_INVALID, "nb must be positive");
-    // four team matrices of nb x (nb + 1) complex128 must fit in 227 KB
-    if (sizeof(double2) * team_mat_elems((int)nb) * 4 + 64 * sizeof(double) + 3 * nb * sizeof(double) > 227 * 1024)
+    // three team matrices of nb x (nb + 1) complex128 must fit in 227 KB (nb <= 68)
+    if (sizeof(double2) * team_mat_elems((int)nb) * 3 + 64 * sizeof(double) + 4 * nb * sizeof(double2) > 227 * 1024)
         return fail(CPPHF_ERR_UNSUPPORTED, "nb too large for the per-k shared-memory kernels");
     return CPPHF_OK;
 }
@@ -645,7 +641,7 @@ int dm_trial_lu(const double2* dQ, const double2* Ft, const double* p, const dou
     init_attrs();
     TeamLaunch L = team_launch(nk, nb);
     L.grid = std::min<unsigned>(L.grid, kDmMaxPartials);
-    TEAM_DISPATCH(L, k_trial_lu, 4, 3 * nb, dQ, Ft, p, d_p, w, nk, nb, T_r, shrink, last_trial, fallback, S);
+    TEAM_DISPATCH(L, k_trial_lu, 3, 3 * nb, dQ, Ft, p, d_p, w, nk, nb, T_r, shrink, last_trial, fallback, S);
     return CPPHF_OK;
 }
 
@@ -653,7 +649,7 @@ int dm_retract_lu(double2* Q, const double2* dQ, const double2* Ft, double* ew, 
                   cudaStream_t st) {
     init_attrs();
     const TeamLaunch L = team_launch(nk, nb);
-    TEAM_DISPATCH(L, k_retract_lu, 4, 2 * nb, Q, dQ, Ft, ew, nk, nb, S);
+    TEAM_DISPATCH(L, k_retract_lu, 3, 2 * nb, Q, dQ, Ft, ew, nk, nb, S);
     return CPPHF_OK;
 }
 

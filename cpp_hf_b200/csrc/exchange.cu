@@ -847,6 +847,19 @@ struct Gen {
     }
 };
 
+// The generic kernels loop over their tile with a block stride, so any block
+// size works: cap it at what the kernel's register use allows.
+template <class K>
+int cap_threads(K kern, int threads) {
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, kern) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return std::min(threads, 256);
+    }
+    const int m = (fa.maxThreadsPerBlock / 32) * 32;
+    return std::max(32, std::min(threads, m));
+}
+
 #define CPPHF_SPEC_SIZES(X) \
     X(1, 1, 1)              \
     X(2, 2, 1)              \
@@ -887,7 +900,8 @@ int pass_rows_fwd(const double2* P, const double2* refP, Cx* T, const ExchangeGe
     Gen<Cx>::attrs();
     const Launch L = plan_launch(g.n1, g.C, sizeof(Cx), g.n1, true);
     if (L.smem > kSmemMax) return fail(CPPHF_ERR_UNSUPPORTED, "exchange: mesh axis too long for the shared-memory FFT");
-    k_rows_fwd_g<Cx><<<dim3(g.n0, L.nchunk), L.threads, L.smem, st>>>(P, refP, T, g, pl, L.CB);
+    k_rows_fwd_g<Cx><<<dim3(g.n0, L.nchunk), cap_threads(k_rows_fwd_g<Cx>, L.threads), L.smem, st>>>(P, refP, T, g,
+                                                                                                     pl, L.CB);
     CPPHF_LAUNCH_CHECK("exchange rows forward");
     return CPPHF_OK;
 }
@@ -906,7 +920,8 @@ int pass_cols(Cx* T, const double2* VR, const ExchangeGeom& g, int vmode, cudaSt
     Gen<Cx>::attrs();
     const Launch L = plan_launch(g.n0, g.C, sizeof(Cx), g.n0, true);
     if (L.smem > kSmemMax) return fail(CPPHF_ERR_UNSUPPORTED, "exchange: mesh axis too long for the shared-memory FFT");
-    k_cols_conv_g<Cx><<<dim3(g.n1, L.nchunk), L.threads, L.smem, st>>>(T, VR, g, pl, L.CB, vmode);
+    k_cols_conv_g<Cx><<<dim3(g.n1, L.nchunk), cap_threads(k_cols_conv_g<Cx>, L.threads), L.smem, st>>>(T, VR, g, pl,
+                                                                                                       L.CB, vmode);
     CPPHF_LAUNCH_CHECK("exchange columns convolve");
     return CPPHF_OK;
 }
@@ -925,7 +940,8 @@ int pass_rows_inv(const Cx* T, double2* Sigma, const ExchangeGeom& g, double sca
     Gen<Cx>::attrs();
     const Launch L = plan_launch(g.n1, g.C, sizeof(Cx), g.n1, true);
     if (L.smem > kSmemMax) return fail(CPPHF_ERR_UNSUPPORTED, "exchange: mesh axis too long for the shared-memory FFT");
-    k_rows_inv_g<Cx><<<dim3(g.n0, L.nchunk), L.threads, L.smem, st>>>(T, Sigma, g, pl, L.CB, scale);
+    k_rows_inv_g<Cx><<<dim3(g.n0, L.nchunk), cap_threads(k_rows_inv_g<Cx>, L.threads), L.smem, st>>>(T, Sigma, g, pl,
+                                                                                                     L.CB, scale);
     CPPHF_LAUNCH_CHECK("exchange rows inverse");
     return CPPHF_OK;
 }

@@ -97,11 +97,19 @@ __device__ __forceinline__ void stage_generic(const C* src, C* dst, const C* tw,
         const int m = bf % R, j = bf / R;  // output m of butterfly j
         const int k = j % Ns;
         C acc = mk((decltype(tw[0].x))0, (decltype(tw[0].x))0);
+        // twiddle W_n^{i k step} times DFT factor W_R^{i m} = W_n^{(i m mod R) nr}; both
+        // exponents stay below n (k step < n / R, (i m mod R) nr < n), so the sum
+        // wraps at most once and the exponents advance by adding, with no division
+        const int a_step = k * step;
+        int a_tw = 0, im = 0;
         for (int i = 0; i < R; ++i) {
             C x = src[(j + i * nr) * CB + c];
-            // twiddle W_n^{i k step} then DFT factor W_R^{i m} = W_n^{(i m mod R) nr}
-            const long long q = ((long long)i * k * step + (long long)((i * m) % R) * nr) % n;
-            cfma(acc, x, twid<INV>(tw, (int)q));
+            int q = a_tw + im * nr;
+            if (q >= n) q -= n;
+            cfma(acc, x, twid<INV>(tw, q));
+            a_tw += a_step;
+            im += m;
+            if (im >= R) im -= R;
         }
         const int base = (j / Ns) * Ns * R + k;
         dst[(base + m * Ns) * CB + c] = acc;

@@ -14,6 +14,7 @@
 #include "common.cuh"
 #include "exchange.cuh"
 #include "fock.cuh"
+#include "superlattice.cuh"
 #include "team.cuh"
 
 #include <algorithm>
@@ -348,8 +349,12 @@ __global__ void k_sum_partials(const double* __restrict__ part, int n, double* _
 
 struct FockWs {
     size_t off_part, off_counter, off_rho_part, off_rho_bar, off_sc, off_hd, off_exch, total;
+    size_t off_sl, sl_bytes, off_slh, off_rho;
     int Gasm, Gk;
 };
+
+bool sl_fock(const cpphf_kernel* K) { return K->sl && K->sl->fock_active && K->include_exchange; }
+bool sl_hart(const cpphf_kernel* K) { return K->sl && K->sl->hartree_active && K->include_hartree; }
 
 // Bulk assembly shape: complex elements per array per stage and stage count;
 // CPPHF_ASSEMBLY="elems,stages" overrides (for tuning sweeps).
@@ -402,6 +407,16 @@ FockWs fock_ws_layout(const cpphf_kernel* K) {
     L.off_hd = take(sizeof(double) * nb);
     const int hcp = (K->exchange_hcp && K->dv == 1) ? 1 : 0;
     L.off_exch = take(exchange_workspace_bytes(K->nk1, K->nk2, K->nb, hcp, K->exchange_precision));
+    L.sl_bytes = 0;
+    L.off_sl = L.off_slh = L.off_rho = o;
+    if (sl_fock(K)) {
+        const cpphf_superlattice* sl = K->sl;
+        L.sl_bytes = superlattice_workspace_bytes(sl->pair_start[sl->n_delta], sl->n_G, sl->dim_orb, sl->N_ext_x,
+                                                  sl->N_ext_y, sl->V_lag_fft_orbital != nullptr);
+        L.off_sl = take(L.sl_bytes);
+        if (K->has_refP) L.off_rho = take(sizeof(double2) * (size_t)nk * nb2);
+    }
+    if (sl_hart(K)) L.off_slh = take(sl_hartree_workspace_bytes(K->sl));
     L.total = o;
     return L;
 }
@@ -421,6 +436,17 @@ int validate_kernel(const cpphf_kernel* K) {
     if (K->has_contact && K->nb > 64) return fail(CPPHF_ERR_UNSUPPORTED, "contact terms need nb <= 64");
     if (K->exchange_precision != 32 && K->exchange_precision != 64)
         return fail(CPPHF_ERR_INVALID, "kernel: exchange_precision must be 32 or 64");
+    if (K->sl && (K->sl->fock_active || K->sl->hartree_active)) {
+        const cpphf_superlattice* sl = K->sl;
+        if (sl->n_G < 1 || sl->dim_orb < 1 || sl->n_G * sl->dim_orb != K->nb)
+            return fail(CPPHF_ERR_INVALID, "superlattice mode requires n_G × dim_orb == nb");
+        if (sl->n_delta < 0 || !sl->pair_start || !sl->pair_to_delta || !sl->g_a_off)
+            return fail(CPPHF_ERR_INVALID, "superlattice: missing layout arrays");
+        if (sl->fock_active && (!sl->V_lag_fft || sl->N_ext_x < K->nk1 || sl->N_ext_y < K->nk2))
+            return fail(CPPHF_ERR_INVALID, "V_lag_fft must have shape (N_ext_x, N_ext_y)");
+        if (sl->hartree_active && K->include_hartree && !sl->HH_GG && !sl->HH_GG_orbital)
+            return fail(CPPHF_ERR_INVALID, "HH_GG must be (n_G, n_G)");
+    }
     return CPPHF_OK;
 }
 
@@ -443,21 +469,36 @@ int build_fock(const cpphf_kernel* K, const double2* P, double2* Sigma, double2*
     const int nb = (int)K->nb, nb2 = nb * nb;
     const double2* refP = K->has_refP ? static_cast<const double2*>(K->refP) : nullptr;
     const bool need_pre = K->include_hartree || K->has_contact;
+    const bool slh = sl_hart(K);
     if (need_pre) {
         const int CH = std::min(nb2, kRedThreads);
         dim3 grid(L.Gk, (nb2 + CH - 1) / CH);
         k_rho_bar_partial<<<grid, kRedThreads, 0, st>>>(P, refP, K->w2d, nk, nb2, CH, rho_part);
         CPPHF_LAUNCH_CHECK("rho_bar partial");
-        k_hartree_contact<<<1, 256, 0, st>>>(rho_part, L.Gk, nb, K->HH, K->include_hartree,
+        // the superlattice Hartree replaces the diagonal Hartree (fock.hpp:66-175)
+        k_hartree_contact<<<1, 256, 0, st>>>(rho_part, L.Gk, nb, K->HH, K->include_hartree && !slh,
                                              K->has_contact, K->n_contact, K->contact_g,
                                              static_cast<const double2*>(K->contact_Oi),
                                              static_cast<const double2*>(K->contact_Oj), rho_bar,
                                              hd, SC);
         CPPHF_LAUNCH_CHECK("hartree/contact");
+        if (slh) CPPHF_TRY(sl_hartree(K->sl, rho_bar, SC, K->has_contact, W + L.off_slh, st));
     } else if (hd_out) {
         CPPHF_CUDA(cudaMemsetAsync(hd, 0, sizeof(double) * nb, st));
     }
-    if (K->include_exchange) {
+    if (sl_fock(K)) {
+        const cpphf_superlattice* sl = K->sl;
+        const double2* rho = P;
+        if (refP) {
+            double2* tmp = reinterpret_cast<double2*>(W + L.off_rho);
+            CPPHF_TRY(field_diff(P, refP, tmp, nk * nb2, st));
+            rho = tmp;
+        }
+        CPPHF_TRY(superlattice_streamed(rho, static_cast<const double2*>(sl->V_lag_fft),
+                                        static_cast<const double2*>(sl->V_lag_fft_orbital), sl->g_a_off, sl->pair_i,
+                                        sl->pair_j, sl->pair_start, sl->n_delta, K->nk1, K->nk2, sl->n_G, sl->dim_orb,
+                                        sl->N_ext_x, sl->N_ext_y, 1, Sigma, W + L.off_sl, L.sl_bytes, st));
+    } else if (K->include_exchange) {
         const int hcp = (K->exchange_hcp && K->dv == 1) ? 1 : 0;
         CPPHF_TRY(exchange(P, refP, static_cast<const double2*>(K->VR), Sigma, K->nk1, K->nk2, K->nb,
                            K->dv, hcp, 0, K->exchange_precision, W + L.off_exch,
@@ -472,8 +513,8 @@ int build_fock(const cpphf_kernel* K, const double2* P, double2* Sigma, double2*
     a.P = P;
     a.refP = refP;
     a.w = K->w2d;
-    a.hd = K->include_hartree ? hd : nullptr;
-    a.SC = K->has_contact ? SC : nullptr;
+    a.hd = (K->include_hartree && !slh) ? hd : nullptr;
+    a.SC = (K->has_contact || slh) ? SC : nullptr;
     a.Hdense = Hdense;
     a.nk = nk;
     a.nb = nb;

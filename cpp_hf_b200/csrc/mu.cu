@@ -23,6 +23,7 @@ namespace {
 
 constexpr int kMuThreads = 1024;
 constexpr int kMuMaxGrid = 1024;
+constexpr int64_t kMuOneBlockMax = 32768;             // eigenvalues handled by a single CTA
 constexpr int kBisectLevels = 3;                      // bisection steps per grid barrier
 constexpr int kMuNV = (1 << kBisectLevels) - 1;       // midpoints evaluated per barrier
 
@@ -295,6 +296,9 @@ int mu_solve(const double* eps, const double* w, int64_t nk, int64_t nb, double 
     const int64_t n = nk * nb;
     int grid = (int)std::min<int64_t>(max_coop_grid(), (n + kMuThreads - 1) / kMuThreads);
     if (grid < 1) grid = 1;
+    // small problems: one CTA does it all (its barriers are block-local), launched
+    // as an ordinary kernel so that solves on other streams keep running beside it
+    if (n <= kMuOneBlockMax) grid = 1;
     MuArgs a;
     a.eps = eps;
     a.w = w;
@@ -309,6 +313,11 @@ int mu_solve(const double* eps, const double* w, int64_t nk, int64_t nb, double 
     a.sync = reinterpret_cast<unsigned*>(ws);
     a.part = reinterpret_cast<double*>(static_cast<unsigned char*>(ws) + 64);
     CPPHF_CUDA(cudaMemsetAsync(ws, 0, 64, st));
+    if (grid == 1) {
+        k_mu<<<1, kMuThreads, 0, st>>>(a);
+        CPPHF_LAUNCH_CHECK("mu (one block)");
+        return CPPHF_OK;
+    }
     void* args[] = {&a};
     CPPHF_CUDA(cudaLaunchCooperativeKernel((const void*)k_mu, dim3(grid), dim3(kMuThreads), args, 0, st));
     return CPPHF_OK;

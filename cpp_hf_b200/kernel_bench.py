@@ -14,6 +14,7 @@ from __future__ import annotations
 import argparse
 import ctypes as C
 
+import numpy as np
 import torch
 
 from . import _lib, workloads
@@ -23,7 +24,9 @@ from ._native import _DeviceKernel, _ptr, _stream, _ws
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--op", default="exchange",
-                    choices=["exchange", "exchange32", "exchange_hcp", "build", "eigh", "mu", "solve_dm", "solve_scf"])
+                    choices=["exchange", "exchange32", "exchange_hcp", "build", "eigh", "mu", "solve_dm", "solve_scf",
+                             "sl_build", "sl_mesh_build", "sl_dm"])
+    ap.add_argument("--pw", type=int, default=32, help="plane waves of the Dirac superlattice (sl_* ops)")
     ap.add_argument("--iters", type=int, default=10, help="solver iterations per call (solve_* ops)")
     ap.add_argument("--n", type=int, default=192)
     ap.add_argument("--layers", type=int, default=4)
@@ -33,6 +36,8 @@ def main():
     lib = _lib.load()
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
+    if a.op.startswith("sl_"):
+        return superlattice_op(a, lib, dev)
     nb = 2 * a.layers
     args, _P0, _ = workloads.layered(a.n, n_layers=a.layers, seed=0)
     P = torch.from_numpy(workloads.random_hermitian_density(a.n, nb, seed=1)).to(dev)
@@ -97,6 +102,50 @@ def main():
     e1.record()
     torch.cuda.synchronize()
     print(f"{a.op} n={a.n} nb={nb}: {1e3 * e0.elapsed_time(e1) / a.reps:.2f} us/call")
+
+
+def superlattice_op(a, lib, dev):
+    """Fock builds / DM iterations of the 2-component Dirac superlattice (nb = 2 * pw):
+    streamed superlattice form (sl_build, sl_dm) or plain-mesh form (sl_mesh_build)."""
+    from . import _native, superlattice
+
+    streamed = a.op != "sl_mesh_build"
+    args, P0, n_e = superlattice.dirac_superlattice(a.n, n_pw=a.pw, seed=0, streamed=streamed)
+    args = {k: (torch.from_numpy(v).to(dev) if isinstance(v, np.ndarray) and v.size > 4096 else v)
+            for k, v in args.items()}
+    nb = 2 * a.pw
+    st = _stream()
+    if a.op == "sl_dm":
+        P0_t = torch.from_numpy(P0).to(dev)
+        empty = torch.empty((0, a.n, a.n, nb, nb), dtype=torch.complex128, device=dev)
+
+        def op():
+            _native.solve_dm(args, P0_t, n_e, a.iters, 0.0, 0.0, 0.6, 0.5, 1e-3, 8, 10, 5, 25, 0, 0.5, 20, empty,
+                             0.0, 1.0, [], None, False, False, False)
+    else:
+        dk = _DeviceKernel(args)
+        rng = np.random.default_rng(1)
+        lam = torch.from_numpy(rng.uniform(0.0, 1.0, size=(a.n, a.n, nb))).to(dev)
+        P = torch.diag_embed(lam).to(torch.complex128)
+        S = torch.empty_like(P)
+        F = torch.empty_like(P)
+        E = torch.zeros(1, dtype=torch.float64, device=dev)
+        ws = _ws(lib.cpphf_build_fock_workspace_bytes(C.byref(dk.K)))
+
+        def op():
+            _lib.check(lib.cpphf_build_fock(C.byref(dk.K), _ptr(P), _ptr(S), _ptr(F), None, _ptr(E), None, _ptr(ws),
+                                            ws.numel(), st), "build")
+    for _ in range(a.warmup):
+        op()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.reps):
+        op()
+    e1.record()
+    torch.cuda.synchronize()
+    extra = f" iters={a.iters}" if a.op == "sl_dm" else ""
+    print(f"{a.op} n={a.n} nb={nb}{extra}: {1e3 * e0.elapsed_time(e1) / a.reps:.2f} us/call")
 
 
 if __name__ == "__main__":

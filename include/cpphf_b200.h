@@ -118,6 +118,28 @@ int cpphf_solve_mu_inloop(const double* eps, const double* w_norm, int64_t nk, i
  * with DEVICE pointers.  has_contact is fock.hpp:25-29 evaluated by the caller
  * (any contact_g != 0 or n_contact > 1).  exchange_precision: 64 or 32.
  * ---------------------------------------------------------------------- */
+/* Superlattice (moire plane-wave) data of a kernel, mirroring the
+ * superlattice_* entries of the reference's kernel_args dict
+ * (cpp_hf_native.cpp:109-213, superlattice.py:88-193).  nb = n_G * dim_orb.
+ * The CSR pair lists, tile offsets and pair_to_delta are HOST arrays (the
+ * channel plan is made on the host every call); the Coulomb tables are device
+ * arrays. */
+typedef struct cpphf_superlattice {
+    int32_t fock_active;     /* streamed superlattice exchange replaces the mesh exchange */
+    int32_t hartree_active;  /* superlattice Hartree replaces the diagonal Hartree */
+    int64_t n_G, dim_orb, n_delta, N_ext_x, N_ext_y;
+    double hartree_degeneracy;
+    const void* V_lag_fft;          /* device complex128 (N_ext_x, N_ext_y) */
+    const void* V_lag_fft_orbital;  /* device complex128 (N_ext_x, N_ext_y, dim_orb, dim_orb) or NULL */
+    const int64_t* g_a_off;         /* host (n_G, 2) */
+    const int64_t* pair_i;          /* host (n_pairs) */
+    const int64_t* pair_j;          /* host (n_pairs) */
+    const int64_t* pair_start;      /* host (n_delta + 1) */
+    const int64_t* pair_to_delta;   /* host (n_G, n_G) */
+    const double* HH_GG;            /* device (n_G, n_G) or NULL without Hartree */
+    const double* HH_GG_orbital;    /* device (n_G, n_G, dim_orb, dim_orb) or NULL */
+} cpphf_superlattice;
+
 typedef struct cpphf_kernel {
     int64_t nk1, nk2, nb;
     int64_t dv;
@@ -139,6 +161,7 @@ typedef struct cpphf_kernel {
     const double* contact_g;  /* (n_contact) */
     const void* contact_Oi;   /* complex128 (n_contact, nb, nb) */
     const void* contact_Oj;   /* complex128 (n_contact, nb, nb) */
+    const cpphf_superlattice* sl;  /* NULL for a plain mesh kernel */
 } cpphf_kernel;
 
 /* ------------------------------------------------------------------------
@@ -252,6 +275,23 @@ int cpphf_solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const vo
                     void* fock_out, double* hist_E, double* hist_density, double* hist_comm,
                     cpphf_scf_result* result, void* workspace, size_t workspace_bytes,
                     void* stream);
+
+/* Replaces _native.selfenergy_superlattice_streamed (cpp_hf_native.cpp:719-816 ->
+ * superlattice.hpp:50-246): per Delta-G channel, the (G_a, G_b) blocks of rho
+ * (nkx, nky, n_G, dim_orb, n_G, dim_orb; device) are placed on the extended
+ * (N_ext_x, N_ext_y) grid at offsets (nkx, nky) * g_a_off[G_a], convolved with
+ * V_lag_fft (or V_lag_fft_orbital per orbital pair) and read back into sigma
+ * (same shape, device).  With hermitian_rho a channel whose reversed pairs form
+ * another channel fills both (conjugate transpose).  g_a_off, pair_i, pair_j,
+ * pair_start are HOST arrays. */
+size_t cpphf_superlattice_workspace_bytes(int64_t n_pairs, int64_t n_G, int64_t dim_orb, int64_t N_ext_x,
+                                          int64_t N_ext_y, int orbital_vr);
+int cpphf_superlattice_streamed(const void* rho, const void* V_lag_fft, const void* V_lag_fft_orbital,
+                                const int64_t* g_a_off, const int64_t* pair_i, const int64_t* pair_j,
+                                const int64_t* pair_start, int64_t n_delta, int64_t nkx, int64_t nky,
+                                int64_t n_G, int64_t dim_orb, int64_t N_ext_x, int64_t N_ext_y,
+                                int hermitian_rho, void* sigma, void* workspace, size_t workspace_bytes,
+                                void* stream);
 
 /* Replaces density_from_fock (solver_scf.hpp:96-154, dense-eigh branch): eigh of
  * herm(F), mu by bisection on the raw weights (30 iterations), optional level

@@ -15,6 +15,10 @@ Writes
   own ``HartreeFockKernel`` + ``_kernel_args_for_native`` for small seeded
   problems (scalar / layer-resolved interaction, Hartree, contact terms), used
   to pin ``cpp_hf_b200.problem.kernel_args`` (the VR phase convention).
+* ``superlattice_ref.npz``: the extended-grid layout and superlattice_*
+  kernel_args of a small plane-wave problem from the reference's
+  ``build_extended_layout`` + ``SuperlatticeHartreeFockKernel``, used to pin
+  ``cpp_hf_b200.superlattice``.
 
 The reference's Python layer needs a ``_native`` module only for the
 embedded-reference option, which these cases do not use; the oracle is
@@ -87,6 +91,34 @@ def _ref_cases():
     return arrays
 
 
+def _superlattice_case():
+    """Layout + kernel_args of a small superlattice problem built through the
+    reference's build_extended_layout and SuperlatticeHartreeFockKernel."""
+    from cpp_hf.solver import _kernel_args_for_native
+    from cpp_hf.superlattice import SuperlatticeHartreeFockKernel, build_extended_layout
+    from cpp_hf_b200 import superlattice as sl
+
+    g, B = sl._triangular_shells(7)
+    n = 6
+    V = lambda q: 2 * np.pi * 0.5 / (q + 0.05) * np.tanh(5 * q)  # noqa: E731
+    layout = build_extended_layout(g, B, n, n, V, 1.0 / n ** 2)
+    rng = np.random.default_rng(5)
+    D = 2 * g.shape[0]
+    h = rng.normal(size=(n, n, D, D)) + 1j * rng.normal(size=(n, n, D, D))
+    h = 0.5 * (h + np.conj(np.swapaxes(h, -1, -2)))
+    HH_GG = rng.uniform(0.0, 1.0, size=(g.shape[0],) * 2)
+    HH_GG = 0.5 * (HH_GG + HH_GG.T)
+    np.fill_diagonal(HH_GG, 0.0)
+    kern = SuperlatticeHartreeFockKernel(np.full((n, n), 1.0 / n ** 2), h, layout, HH_GG=HH_GG, T=0.05,
+                                         hartree_degeneracy=2.0)
+    args = _kernel_args_for_native(kern)
+    arrays = {"in.g_frac": g, "in.B": B, "in.n": np.array(n), "in.h": h, "in.HH_GG": HH_GG,
+              "in.w_scalar": np.array(1.0 / n ** 2)}
+    for key, val in args.items():
+        arrays[f"out.{key}"] = np.asarray(val)
+    return arrays
+
+
 def main():
     sys.path.insert(0, str(REPO))
     sys.path.insert(0, str(REF / "src"))
@@ -101,7 +133,8 @@ def main():
             "hist_E_expected", "hist_dC_expected"]
     np.savez_compressed(HERE / "meshgrid_scf_v1.npz", **{k: d[k] for k in keep})
     np.savez_compressed(HERE / "kernel_args_ref.npz", **_ref_cases())
-    print("wrote", HERE / "meshgrid_scf_v1.npz", HERE / "kernel_args_ref.npz")
+    np.savez_compressed(HERE / "superlattice_ref.npz", **_superlattice_case())
+    print("wrote", HERE / "meshgrid_scf_v1.npz", HERE / "kernel_args_ref.npz", HERE / "superlattice_ref.npz")
 
 
 if __name__ == "__main__":

@@ -431,3 +431,19 @@ def test_solve_scf_mixed_precision_reaches_fp64_energy(native, oracle):
     assert abs(got[6][1] - ref[6][1]) < 1e-5 * max(1.0, abs(ref[6][1]))
     assert abs(got[2] - ref[2]) < 1e-9 * max(1.0, abs(ref[2]))
     assert rel(got[0], ref[0]) < 1e-7
+
+
+@pytest.mark.parametrize("layers", [5, 7, 9])
+def test_solve_dm_generic_team_path_matches_oracle(native, oracle, layers):
+    """nb = 10, 14 (warp teams) and 18 (CTA team): the general per-k kernels follow the
+    oracle's trajectory (energy history of 30 iterations)."""
+    args, P0, n_e = workloads.layered(6, n_layers=layers, seed=4)
+    got = native.solve_dm(args, P0, n_e, 30, 0.0, 0.0, 0.6, 0.5, 1e-3, 8, 10, 5, 25, 0, 0.5, 20,
+                          np.empty((0, 6, 6, 2 * layers, 2 * layers), np.complex128), 0.0, 1.0, [], None,
+                          False, True, False)
+    ref = oracle.solve_dm(args, P0, n_e, 30, 0.0, 0.0, 0.6, 0.5, 1e-3, 8, 10, 5, 25, 0, 0.5, 20,
+                          np.empty((0, 6, 6, 2 * layers, 2 * layers), np.complex128), 0.0, 1.0, [], None,
+                          False, True, False)
+    d = np.abs(np.asarray(got[8]) - np.asarray(ref[8]))
+    print(f"nb={2 * layers}: energy history |dE| per iteration {np.array2string(d[:8], precision=2)} ... max {d.max():.2e}")
+    assert d.max() < 1e-9 * max(1.0, float(np.max(np.abs(ref[8]))))

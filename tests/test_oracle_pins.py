@@ -117,3 +117,29 @@ def test_layered_workload_shapes_and_symmetry():
     assert not args["exchange_hcp"]
     np.testing.assert_allclose(args["h"], herm(args["h"]), atol=1e-15)
     assert abs(n_e - 2.0) < 1e-12
+
+
+def test_superlattice_layout_and_kernel_args_match_reference_fixture():
+    """cpp_hf_b200.superlattice against the reference's build_extended_layout +
+    SuperlatticeHartreeFockKernel (tests/golden/superlattice_ref.npz)."""
+    from cpp_hf_b200 import superlattice as sl
+
+    d = np.load(GOLDEN / "superlattice_ref.npz")
+    n = int(d["in.n"])
+    V = lambda q: 2 * np.pi * 0.5 / (q + 0.05) * np.tanh(5 * q)  # noqa: E731
+    lay = sl.extended_layout(d["in.g_frac"], d["in.B"], n, n, V, float(d["in.w_scalar"]))
+    args = sl.superlattice_kernel_args(np.full((n, n), 1.0 / n ** 2), d["in.h"], lay, 0.05, HH_GG=d["in.HH_GG"],
+                                       hartree_degeneracy=2.0)
+    for key in d.files:
+        if not key.startswith("out."):
+            continue
+        k = key[4:]
+        ref = d[key]
+        got = np.asarray(args[k])
+        if ref.size == 0 and got.size == 0:
+            continue
+        if k == "refP":  # the reference passes an empty refP without a reference density
+            assert not args["has_refP"] and ref.size == 0
+            continue
+        assert got.shape == ref.shape, k
+        np.testing.assert_allclose(got, ref, rtol=0, atol=1e-13, err_msg=k)
