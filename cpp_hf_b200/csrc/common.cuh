@@ -209,8 +209,8 @@ struct GridBarrier {
     }
 
     // Barrier whose last arriving block first sums the (NV x nblocks) partials
-    // `part` (block b's values at part[NV b .. NV b + NV)) with warp 0 in a fixed
-    // lane-strided order and writes the NV totals to `tot`, so the released
+    // `part` (block b's values at part[NV b .. NV b + NV)) with all its threads in
+    // a fixed order and writes the NV totals to `tot`, so the released
     // blocks read NV numbers instead of all partials.  Ordering uses
     // release/acquire atomics (no full fences).
     template <int NV = 2>
@@ -231,22 +231,22 @@ struct GridBarrier {
         __syncthreads();
         if (!ok_sh) return false;
         if (last_sh) {
-            if (threadIdx.x < 32) {
-                double sv[NV];
+            // the whole block loads the partials at once (one L2 round trip for
+            // up to blockDim blocks) and sums them with a fixed tree
+            __shared__ double red_wr[32 * NV];
+            double sv[NV];
 #pragma unroll
-                for (int v = 0; v < NV; ++v) sv[v] = 0.0;
-                for (int b = threadIdx.x; b < nblocks; b += 32) {
+            for (int v = 0; v < NV; ++v) sv[v] = 0.0;
+            for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
 #pragma unroll
-                    for (int v = 0; v < NV; ++v) sv[v] += __ldcg(&part[NV * b + v]);
-                }
+                for (int v = 0; v < NV; ++v) sv[v] += __ldcg(&part[NV * b + v]);
+            }
+            block_sum<NV>(sv, red_wr);
+            if (threadIdx.x == 0) {
 #pragma unroll
-                for (int v = 0; v < NV; ++v) sv[v] = warp_sum(sv[v]);
-                if (threadIdx.x == 0) {
-#pragma unroll
-                    for (int v = 0; v < NV; ++v) __stcg(&tot[v], sv[v]);
-                    sync[0] = 0u;
-                    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(&sync[1]) : "memory");
-                }
+                for (int v = 0; v < NV; ++v) __stcg(&tot[v], sv[v]);
+                sync[0] = 0u;
+                asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(&sync[1]) : "memory");
             }
         } else if (threadIdx.x == 0) {
             long long spins = 0;

@@ -396,98 +396,6 @@ __global__ void __launch_bounds__(kThreads) k_trial_small(const double2* __restr
     }
 }
 
-// The remaining backtracking trials after a failed first one, all in one pass:
-// trial m (m = 0 .. nrest-1) uses tau_m = tau_cur * shrink^m (the sequence the
-// one-at-a-time trials produce), and the first trial whose Omega is below
-// Omega0 is taken, exactly as the sequential loop would (solver_dm.hpp:577-589).
-// Returns at once when the first trial was accepted.
-constexpr int kMaxRestTrials = 7;
-
-template <int NB>
-__global__ void __launch_bounds__(kThreads) k_trial_rest_small(const double2* __restrict__ dQ,
-                                                               const double2* __restrict__ Ft,
-                                                               const double* __restrict__ p,
-                                                               const double* __restrict__ d_p,
-                                                               const double* __restrict__ w, int64_t nk, double T_r,
-                                                               double shrink, int nrest, double fallback,
-                                                               DmScalars* S) {
-    if (S->accepted) return;  // grid-uniform
-    using G = Geo<NB>;
-    extern __shared__ __align__(16) double2 dyn[];
-    double2* sD = dyn;
-    double2* sF = dyn + G::TILE;
-    double2* sU = dyn + 2 * G::TILE;
-    __shared__ double2 sPiv[G::KT * 2 * NB];
-    __shared__ double red[32 * 2 * kMaxRestTrials];
-    const int grp = threadIdx.x / G::GS, r = threadIdx.x % G::GS;
-    const unsigned mask = group_mask<NB>(threadIdx.x & 31);
-    const double tau_first = S->tau_cur;
-    const int64_t ntiles = (nk + G::KT - 1) / G::KT;
-    double v[2 * kMaxRestTrials];
-#pragma unroll
-    for (int m = 0; m < 2 * kMaxRestTrials; ++m) v[m] = 0.0;
-    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const int64_t k0 = t * G::KT;
-        const int nkt = (int)((nk - k0) < G::KT ? (nk - k0) : G::KT);
-        tile_load<NB>(sD, dQ + (size_t)k0 * G::NB2, nkt);
-        tile_load<NB>(sF, Ft + (size_t)k0 * G::NB2, nkt);
-        __syncthreads();
-        const bool live = grp < nkt && r < NB;
-        const int rr = r < NB ? r : 0;
-        const int64_t k = k0 + grp;
-        double2 ftj[NB];
-        if (grp < nkt) {
-#pragma unroll
-            for (int l = 0; l < NB; ++l) ftj[l] = sF[grp * G::MS + rr * G::LD + l];
-        }
-        double tau = tau_first;
-#pragma unroll
-        for (int m = 0; m < kMaxRestTrials; ++m) {
-            if (m < nrest) {
-                if (grp < nkt) {
-                    double2 u[NB];
-                    row_cayley<NB, G::LD>(sD + grp * G::MS, tau, rr, sPiv + grp * 2 * NB, u, mask);
-                    if (live) {
-#pragma unroll
-                        for (int j = 0; j < NB; ++j) sU[grp * G::MS + r * G::LD + j] = u[j];
-                    }
-                    __syncwarp(mask);
-                    const double dr = row_diag_uhfu<NB, G::GS, G::LD>(ftj, sU + grp * G::MS, r, mask, live);
-                    if (live) {
-                        const double pv =
-                            fmin(fmax(p[k * NB + r] - tau * d_p[k * NB + r], OCC_CLIP), 1.0 - OCC_CLIP);
-                        const double wk = w[k];
-                        v[2 * m] += wk * pv * dr;
-                        v[2 * m + 1] -= wk * (pv * log(pv) + (1.0 - pv) * log1p(-pv));
-                    }
-                    __syncwarp(mask);
-                }
-                tau *= shrink;
-            }
-        }
-        __syncthreads();
-    }
-    double out[2 * kMaxRestTrials];
-    if (reduce_last_block<2 * kMaxRestTrials>(v, S->part, &S->counter, out, red) && threadIdx.x == 0) {
-        double tau = tau_first;
-        int taken = 0;
-        for (int m = 0; m < nrest && !taken; ++m) {
-            const double om = out[2 * m] - fmax(T_r, 1.0e-14) * out[2 * m + 1];
-            if (om < S->omega0) {
-                S->accepted = 1;
-                S->tau_final = tau;
-                taken = 1;
-            } else {
-                tau *= shrink;
-            }
-        }
-        if (!taken) {
-            S->tau_cur = tau;
-            S->tau_final = S->tau0 * fallback;
-        }
-    }
-}
-
 // Retraction Q <- Q U(tau_final) and eps_work = diag(U^H Ft U).
 // Dynamic shared memory: sD | sF | sU | sQ, TILE double2 each.
 template <int NB>
@@ -552,12 +460,15 @@ __global__ void __launch_bounds__(kThreads) k_retract_small(double2* Q, const do
 }
 
 // Element kernels: 256 threads, grid-stride loops unrolled by kUnrollE so
-// each thread keeps several independent field loads in flight.
+// each thread keeps several independent field loads in flight.  The per-row
+// (occupation) terms run in a second, row-parallel loop of the same launch:
+// folded into the element loop they would make every warp execute the
+// log / division branch of its row leaders.
 constexpr int kThreadsE = 256;
 constexpr int kUnrollE = 4;
 
-// PR+ numerator / denominator -> beta (solver_dm.hpp:513-559), one thread per
-// matrix element (k, i, j); the row terms of g_p are added by the j = 0 thread.
+// PR+ numerator / denominator -> beta (solver_dm.hpp:513-559): matrix terms
+// one thread per element (k, i, j), occupation terms one thread per row (k, i).
 template <int NB>
 __global__ void __launch_bounds__(kThreadsE) k_pr_beta_small(const double2* __restrict__ Gc, const double2* __restrict__ Gp,
                                                              const double* __restrict__ g_p,
@@ -570,7 +481,8 @@ __global__ void __launch_bounds__(kThreadsE) k_pr_beta_small(const double2* __re
     double v[3] = {0.0, 0.0, 0.0};
     const int64_t nel = nk * NB * NB;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t e0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e0 < nel; e0 += kUnrollE * stride) {
+    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (int64_t e0 = tid; e0 < nel; e0 += kUnrollE * stride) {
         double2 g[kUnrollE], gp[kUnrollE];
 #pragma unroll
         for (int u = 0; u < kUnrollE; ++u) {
@@ -591,13 +503,16 @@ __global__ void __launch_bounds__(kThreadsE) k_pr_beta_small(const double2* __re
             const double2 d = mk(g[u].x / base, g[u].y / base);
             v[0] += wk * ((g[u].x * d.x + g[u].y * d.y) - (gp[u].x * d.x + gp[u].y * d.y));
             v[1] += wk * (gp[u].x * gp[u].x + gp[u].y * gp[u].y);
-            if (j == 0) {
-                const double ps = fmin(fmax(p[row], OCC_CLIP), 1.0 - OCC_CLIP);
-                const double h = g_p[row] / (T_r / (ps * (1.0 - ps)));
-                v[2] += wk * (g_p[row] * h - g_pp[row] * h);
-                v[1] += wk * (g_pp[row] * g_pp[row]);
-            }
         }
+    }
+    const int64_t nrow = nk * NB;
+    for (int64_t row = tid; row < nrow; row += stride) {
+        const double wk = w[row / NB];
+        const double ps = fmin(fmax(p[row], OCC_CLIP), 1.0 - OCC_CLIP);
+        const double gr = g_p[row], gq = g_pp[row];
+        const double h = gr / (T_r / (ps * (1.0 - ps)));
+        v[2] += wk * (gr * h - gq * h);
+        v[1] += wk * (gq * gq);
     }
     double out[3];
     if (reduce_last_block<3>(v, S->part, &S->counter, out, red) && threadIdx.x == 0) {
@@ -610,8 +525,8 @@ __global__ void __launch_bounds__(kThreadsE) k_pr_beta_small(const double2* __re
     }
 }
 
-// direction + tau0 + Omega0 (solver_dm.hpp:556-573, 346-365), one thread per
-// matrix element; the occupation direction and Omega0 terms by the j = 0 thread.
+// direction + tau0 + Omega0 (solver_dm.hpp:556-573, 346-365): matrix direction
+// one thread per element, occupation direction and Omega0 terms one per row.
 template <int NB>
 __global__ void __launch_bounds__(kThreadsE) k_direction_small(const double2* __restrict__ Gc,
                                                                const double2* __restrict__ dQp,
@@ -627,7 +542,8 @@ __global__ void __launch_bounds__(kThreadsE) k_direction_small(const double2* __
     double v[3] = {0.0, 0.0, 0.0};
     const int64_t nel = nk * NB * NB;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t e0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e0 < nel; e0 += kUnrollE * stride) {
+    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (int64_t e0 = tid; e0 < nel; e0 += kUnrollE * stride) {
         double2 g[kUnrollE], q[kUnrollE];
 #pragma unroll
         for (int u = 0; u < kUnrollE; ++u) {
@@ -643,20 +559,21 @@ __global__ void __launch_bounds__(kThreadsE) k_direction_small(const double2* __
             const int j = (int)(e - row * NB);
             const int64_t k = row / NB;
             const double wk = w[k];
-            const double ei = eps[row];
-            const double gap = ei - eps[k * NB + j];
+            const double gap = eps[row] - eps[k * NB + j];
             const double base = sqrt(gap * gap + lam * lam);
             const double2 d = mk(g[u].x / base + beta * q[u].x, g[u].y / base + beta * q[u].y);
             dQ[e] = d;
             v[0] += wk * (d.x * d.x + d.y * d.y);
-            if (j == 0) {
-                const double ps = fmin(fmax(p[row], OCC_CLIP), 1.0 - OCC_CLIP);
-                const double h = g_p[row] / (T_r / (ps * (1.0 - ps)));
-                d_p[row] = h + beta * dpp[row];
-                v[1] += wk * ps * ei;
-                v[2] -= wk * (ps * log(ps) + (1.0 - ps) * log1p(-ps));
-            }
         }
+    }
+    const int64_t nrow = nk * NB;
+    for (int64_t row = tid; row < nrow; row += stride) {
+        const double wk = w[row / NB];
+        const double ps = fmin(fmax(p[row], OCC_CLIP), 1.0 - OCC_CLIP);
+        const double h = g_p[row] / (T_r / (ps * (1.0 - ps)));
+        d_p[row] = h + beta * dpp[row];
+        v[1] += wk * ps * eps[row];
+        v[2] -= wk * (ps * log(ps) + (1.0 - ps) * log1p(-ps));
     }
     double out[3];
     if (reduce_last_block<3>(v, S->part, &S->counter, out, red) && threadIdx.x == 0) {
@@ -685,7 +602,6 @@ void small_attrs() {
     static std::once_flag once;
     std::call_once(once, [] {
         raise_smem(k_trial_small<NB>);
-        raise_smem(k_trial_rest_small<NB>);
         raise_smem(k_retract_small<NB>);
     });
 }
@@ -760,25 +676,6 @@ int dm_small_trial(const double2* dQ, const double2* Ft, const double* p, const 
 #undef X
     return CPPHF_OK;
 }
-
-int dm_small_trial_rest(const double2* dQ, const double2* Ft, const double* p, const double* d_p, const double* w,
-                        int64_t nk, int nb, double T_r, double shrink, int nrest, double fallback, DmScalars* S,
-                        cudaStream_t st) {
-    if (nrest < 1) return CPPHF_OK;
-    if (nrest > kMaxRestTrials) return fail(CPPHF_ERR_INVALID, "trial_rest: too many trials for one pass");
-    // partials: 2 * kMaxRestTrials values per block must fit S->part (3 * kDmMaxPartials)
-    const int cap = (3 * kDmMaxPartials) / (2 * kMaxRestTrials);
-#define X(N)                                                                                                     \
-    small_attrs<N>();                                                                                            \
-    k_trial_rest_small<N><<<tiles_grid(nk, Geo<N>::KT, cap), kThreads, 3 * sizeof(double2) * Geo<N>::TILE, st>>>( \
-        dQ, Ft, p, d_p, w, nk, T_r, shrink, nrest, fallback, S);                                                 \
-    CPPHF_LAUNCH_CHECK("trial_rest");
-    SMALL_DISPATCH(nb, X)
-#undef X
-    return CPPHF_OK;
-}
-
-int dm_small_max_rest_trials() { return kMaxRestTrials; }
 
 int dm_small_retract(double2* Q, const double2* dQ, const double2* Ft, double* ew, int64_t nk, int nb,
                      const DmScalars* S, cudaStream_t st) {

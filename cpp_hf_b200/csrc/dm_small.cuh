@@ -20,11 +20,6 @@ int dm_small_direction(const double2* Gc, const double2* dQp, const double* g_p,
 int dm_small_trial(const double2* dQ, const double2* Ft, const double* p, const double* d_p, const double* w,
                    int64_t nk, int nb, double T_r, double shrink, int last_trial, double fallback, DmScalars* S,
                    cudaStream_t st);
-// trials 2 .. 1 + nrest of a backtracking line search in one pass (after a failed first trial)
-int dm_small_trial_rest(const double2* dQ, const double2* Ft, const double* p, const double* d_p, const double* w,
-                        int64_t nk, int nb, double T_r, double shrink, int nrest, double fallback, DmScalars* S,
-                        cudaStream_t st);
-int dm_small_max_rest_trials();
 int dm_small_retract(double2* Q, const double2* dQ, const double2* Ft, double* ew, int64_t nk, int nb,
                      const DmScalars* S, cudaStream_t st);
 

@@ -33,6 +33,15 @@ __device__ __forceinline__ double expit(double x) {
     return e / (1.0 + e);
 }
 
+// Shortcut thresholds on the (approximate) logistic argument x: for x >= 37,
+// 1 + exp(-x) rounds to 1 in FP64, so expit(x) is exactly 1; for x <= -50,
+// expit(x) < 2e-22 and the term is dropped (far below the rounding of any sum
+// of weights it enters).  The approximate argument (difference times the
+// reciprocal temperature) is within a few ulp of the exact quotient, far from
+// either threshold's margin.
+constexpr double kFdOne = 37.0;
+constexpr double kFdZero = -50.0;
+
 struct MuArgs {
     const double* eps;
     const double* w;  // per-k weights
@@ -47,6 +56,17 @@ struct MuArgs {
     double* part;     // [grid][2] min/max, [grid][kMuNV] partials, [2][kMuNV] totals
     unsigned* sync;   // [0] count [1] gen [2] error
 };
+
+// Element i of a block's slice in band-major order (band = i / nk, k = i % nk):
+// the 32 lanes of a warp then hold one band at 32 neighbouring k-points, whose
+// eigenvalues mostly fall on the same side of a trial mu, so the shortcut
+// branches above stay warp-uniform.  eps is (nk, nb) row-major, w per k.
+__device__ __forceinline__ void band_major(const MuArgs& a, unsigned i, unsigned nb, double& wk, double& e) {
+    const unsigned nk = (unsigned)(a.n / nb);
+    const unsigned band = i / nk, k = i - band * nk;
+    wk = a.w[k];
+    e = a.eps[(size_t)k * nb + band];
+}
 
 __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
     __shared__ double red[32 * kMuNV];  // block_sum<kMuNV> scratch (32 doubles per value)
@@ -120,6 +140,7 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
         mu = fmin(fmax(*a.mu0, lo), hi);
     }
     const double Tfd = Tj + 1.0e-12;  // fermidirac_scalar(x, Tj) = expit(-x / (Tj + 1e-12))
+    const double invTfd = 1.0 / Tfd, invTj = 1.0 / Tj;
     double* part = a.part + 2 * G;                  // [G][kMuNV] partials of the current round
     double* tots = part + (size_t)kMuNV * G;        // [2][kMuNV] totals, by round parity
     __shared__ double bc_tot[kMuNV];
@@ -157,11 +178,20 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
 #pragma unroll
             for (int j = 0; j < kMuNV; ++j) v[j] = 0.0;
             for (unsigned i = e0 + threadIdx.x; i < e1; i += blockDim.x) {
-                const double wk = a.w[i / nb];
-                const double e = a.eps[i];
+                double wk, e;
+                band_major(a, i, nb, wk, e);
 #pragma unroll
-                for (int j = 0; j < kMuNV; ++j)
-                    if (j < nodes) v[j] += wk * expit(-(e - mid[j]) / Tfd);
+                for (int j = 0; j < kMuNV; ++j) {
+                    if (j < nodes) {
+                        // x = (mid - e) / Tfd: the term is exactly wk for x >= 37
+                        // and below 2e-22 wk (dropped) for x <= -50
+                        const double xa = (mid[j] - e) * invTfd;
+                        if (xa >= kFdOne)
+                            v[j] += wk;
+                        else if (xa > kFdZero)
+                            v[j] += wk * expit(-(e - mid[j]) / Tfd);
+                    }
+                }
             }
             block_sum<kMuNV>(v, red);
             if (threadIdx.x == 0) {
@@ -202,11 +232,18 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
         for (int it = 0; it < a.maxiter; ++it) {
             double v[2] = {0.0, 0.0};
             for (unsigned i = e0 + threadIdx.x; i < e1; i += blockDim.x) {
-                const double wk = a.w[i / nb];
-                const double e = a.eps[i];
-                const double p = expit((mu - e) / Tj);
-                v[0] += wk * p;
-                v[1] += wk * p * (1.0 - p) / Tj;
+                double wk, e;
+                band_major(a, i, nb, wk, e);
+                // p = expit((mu - e) / Tj) is exactly 1 (and p (1 - p) exactly 0)
+                // for an argument >= 37; below -50 both terms are dropped
+                const double xa = (mu - e) * invTj;
+                if (xa >= kFdOne) {
+                    v[0] += wk;
+                } else if (xa > kFdZero) {
+                    const double p = expit((mu - e) / Tj);
+                    v[0] += wk * p;
+                    v[1] += wk * p * (1.0 - p) / Tj;
+                }
             }
             block_sum<2>(v, red);
             if (threadIdx.x == 0) {

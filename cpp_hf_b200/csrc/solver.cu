@@ -358,21 +358,15 @@ int solve_dm(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* P
             CPPHF_TRY(dm_direction(G[cur], dQ[prv], g[cur], dp[prv], eps, p, wn, dQ[cur], dp[cur], nk, nb, T_r,
                                    cfg->max_step, S, st));
         }
-        // 5. Cayley line search (elimination form of the spectral Cayley factor)
-        if (small && cfg->bt_max >= 2 && cfg->bt_max - 1 <= dm_small_max_rest_trials()) {
-            // first trial, then (if it failed) all remaining trials in one pass
-            CPPHF_TRY(dm_small_trial(dQ[cur], F, p, dp[cur], wn, nk, nb, T_r, cfg->bt_shrink, 0, fallback, S, st));
-            CPPHF_TRY(dm_small_trial_rest(dQ[cur], F, p, dp[cur], wn, nk, nb, T_r, cfg->bt_shrink,
-                                          (int)(cfg->bt_max - 1), fallback, S, st));
-        } else {
-            for (int64_t bt = 0; bt < cfg->bt_max; ++bt) {
-                if (small)
-                    CPPHF_TRY(dm_small_trial(dQ[cur], F, p, dp[cur], wn, nk, nb, T_r, cfg->bt_shrink,
-                                             bt == cfg->bt_max - 1, fallback, S, st));
-                else
-                    CPPHF_TRY(dm_trial_lu(dQ[cur], F, p, dp[cur], wn, nk, nb, T_r, cfg->bt_shrink,
-                                          bt == cfg->bt_max - 1, fallback, S, st));
-            }
+        // 5. Cayley line search (elimination form of the spectral Cayley factor):
+        // one pass per trial; a pass after the accepted trial returns at once
+        for (int64_t bt = 0; bt < cfg->bt_max; ++bt) {
+            if (small)
+                CPPHF_TRY(dm_small_trial(dQ[cur], F, p, dp[cur], wn, nk, nb, T_r, cfg->bt_shrink,
+                                         bt == cfg->bt_max - 1, fallback, S, st));
+            else
+                CPPHF_TRY(dm_trial_lu(dQ[cur], F, p, dp[cur], wn, nk, nb, T_r, cfg->bt_shrink,
+                                      bt == cfg->bt_max - 1, fallback, S, st));
         }
         // 6. retraction and mu (occupations are formed by the next density step)
         if (small)
@@ -498,7 +492,9 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
     K32.exchange_precision = 32;
     bool low = cfg->mixed_switch_tol > 0.0;
 
-    // build_and_occupy (solver_scf.hpp:179-197); mu -> mu2[1], E -> S->energy
+    // the occupation mu: mu2[1] after a level shift, else mu2[0]
+    double* mu_fin = (cfg->level_shift != 0.0) ? &mu2[1] : &mu2[0];
+    // build_and_occupy (solver_scf.hpp:179-197); mu -> mu_fin, E -> S->energy
     auto build_and_occupy = [&]() -> int {
         if (project) CPPHF_TRY(call_project(project, puser, D, K, st));
         CPPHF_TRY(hermitize(D, D, nk, nb, st));
@@ -516,8 +512,11 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
             CPPHF_LAUNCH_CHECK("level shift");
             e_occ = sh;
         }
-        CPPHF_TRY(mu_solve(e_occ, K->w2d, nk, nb, n_e, nullptr, K->T, 30, 0, &mu2[1], mws, L.mu_bytes, st));
-        k_fermi<<<grid_for(nk * nb, 256), 256, 0, st>>>(e_occ, &mu2[1], K->T, occ, nk * nb);
+        // without a level shift the second bisection (solver_scf.hpp:136) runs on an
+        // unchanged copy of eps and returns mu_raw itself
+        if (cfg->level_shift != 0.0)
+            CPPHF_TRY(mu_solve(e_occ, K->w2d, nk, nb, n_e, nullptr, K->T, 30, 0, mu_fin, mws, L.mu_bytes, st));
+        k_fermi<<<grid_for(nk * nb, 256), 256, 0, st>>>(e_occ, mu_fin, K->T, occ, nk * nb);
         CPPHF_LAUNCH_CHECK("fermi");
         CPPHF_TRY(dm_density(V, occ, Pn, nk, nb, st));
         if (project) CPPHF_TRY(call_project(project, puser, Pn, K, st));
@@ -550,7 +549,7 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
         CPPHF_CUDA(cudaMemcpyAsync(hbuf, &S->energy, sizeof(double), cudaMemcpyDeviceToHost, st));
         CPPHF_CUDA(cudaMemcpyAsync(hbuf + 1, &S->grad_norm, sizeof(double), cudaMemcpyDeviceToHost, st));
         CPPHF_CUDA(cudaMemcpyAsync(hbuf + 2, &S->lam_pc, sizeof(double), cudaMemcpyDeviceToHost, st));
-        CPPHF_CUDA(cudaMemcpyAsync(hbuf + 3, &mu2[1], sizeof(double), cudaMemcpyDeviceToHost, st));
+        CPPHF_CUDA(cudaMemcpyAsync(hbuf + 3, mu_fin, sizeof(double), cudaMemcpyDeviceToHost, st));
         CPPHF_CUDA(cudaStreamSynchronize(st));
         if (!std::isfinite(hbuf[3]))
             return fail(CPPHF_ERR_TIMEOUT, "solve_scf: chemical-potential solve failed (device wait timeout or non-finite)");
@@ -581,7 +580,7 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
     if (D_out) CPPHF_CUDA(cudaMemcpyAsync(D_out, D, fbytes, cudaMemcpyDeviceToDevice, st));
     if (F_out) CPPHF_CUDA(cudaMemcpyAsync(F_out, F, fbytes, cudaMemcpyDeviceToDevice, st));
     CPPHF_CUDA(cudaMemcpyAsync(hbuf, &S->energy, sizeof(double), cudaMemcpyDeviceToHost, st));
-    CPPHF_CUDA(cudaMemcpyAsync(hbuf + 3, &mu2[1], sizeof(double), cudaMemcpyDeviceToHost, st));
+    CPPHF_CUDA(cudaMemcpyAsync(hbuf + 3, mu_fin, sizeof(double), cudaMemcpyDeviceToHost, st));
     CPPHF_CUDA(cudaStreamSynchronize(st));
     if (!std::isfinite(hbuf[3]))
         return fail(CPPHF_ERR_TIMEOUT, "solve_scf: chemical-potential solve failed (device wait timeout or non-finite)");
