@@ -366,7 +366,7 @@ def main():
         solves = time_solves(torch, native, args_dev, P0_dev, _ne, a.solve_reps)
         barrier()
 
-    # ---- batched sweep: mixed precision on concurrent streams vs one by one in FP64 ----
+    # ---- batched sweep: concurrent streams (mixed and FP64) vs one by one in FP64 ----
     sweep = None
     if a.sweep > 0:
         from cpp_hf_b200 import batch
@@ -375,6 +375,7 @@ def main():
         batch.solve_batch(inst[:4], precision="fp64", streams=1)  # warm-up (kernel attributes, allocator)
         barrier()
         seq, t_seq = batch.solve_batch(inst, precision="fp64", streams=1)
+        bat64, t_bat64 = batch.solve_batch(inst, precision="fp64", streams=a.sweep_streams)
         bat, t_bat = batch.solve_batch(inst, precision="mixed", streams=a.sweep_streams)
         barrier()
         rel = [abs(x["energy"] - y["energy"]) / max(1.0, abs(x["energy"])) for x, y in zip(seq, bat)]
@@ -382,11 +383,15 @@ def main():
         sweep = {
             "instances": len(inst),
             "batched_mixed_solves_per_s": len(inst) / t_bat,
+            "batched_fp64_solves_per_s": len(inst) / t_bat64,
             "sequential_fp64_solves_per_s": len(inst) / t_seq,
             "speedup": t_seq / t_bat,
+            "speedup_batched_fp64": t_seq / t_bat64,
             "mixed_same_state_as_fp64": len(same),
             "max_rel_dE_mixed_vs_fp64_same_state": max(same) if same else None,
             "max_rel_dE_mixed_vs_fp64_all": max(rel),
+            "batched_fp64_matches_sequential": int(sum(abs(x["energy"] - y["energy"]) <= 1e-9 * max(1.0, abs(x["energy"]))
+                                                        for x, y in zip(seq, bat64))),
             "converged_fp64": int(sum(bool(x["converged"]) for x in seq)),
             "converged_mixed": int(sum(bool(y["converged"]) for y in bat)),
             "iterations_fp64": int(sum(x["iterations"] for x in seq)),

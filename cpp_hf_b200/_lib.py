@@ -62,6 +62,7 @@ class DmConfig(C.Structure):
         ("denom_scale", f64), ("max_step", f64), ("cg_restart", i64), ("bt_shrink", f64),
         ("bt_max", i64), ("mu_maxiter", i32), ("optimizer", i32),
         ("block_sizes", C.POINTER(i64)), ("n_block_sizes", i64), ("mixed_switch_grad", f64),
+        ("graphs", i32), ("reserved_dm", i32),
     ]
 
 

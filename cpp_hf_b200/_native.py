@@ -50,6 +50,8 @@ __all__ = [
 # and the commutator residuals (SCF), fall below "mixed_switch" (default 1e-5),
 # then complex128
 # to convergence; a single build_fock_apply under "mixed" is complex128.
+# "solve_graphs" (default True): solve_dm replays each iteration as a captured
+# CUDA graph; False launches every kernel (better for many concurrent solves).
 DEFAULT_EXCHANGE_PRECISION = 64
 DEFAULT_MIXED_SWITCH = 1.0e-5
 
@@ -461,6 +463,7 @@ def solve_dm(kernel_args, P0, n_e, max_iter, tol_E, tol_grad, max_step, bt_shrin
     cfg.block_sizes = C.cast(bs_arr, C.POINTER(_lib.i64))
     cfg.n_block_sizes = n_bs
     cfg.mixed_switch_grad = dk.mixed_switch
+    cfg.graphs = 1 if kernel_args.get("solve_graphs", True) else 0
     Q = torch.empty_like(P0_t) if return_Q else None
     D = torch.empty_like(P0_t) if return_density else None
     F = torch.empty_like(P0_t) if return_fock else None

@@ -83,10 +83,11 @@ def upload(instances, device=None):
     return instances
 
 
-def _solve_one(inst, precision, solver, tol, max_iter):
+def _solve_one(inst, precision, solver, tol, max_iter, graphs=True):
     args = dict(inst.dev["args"])
     if precision == "mixed":
         args["exchange_precision"] = "mixed"
+    args["solve_graphs"] = graphs
     P0 = inst.dev["P0"]
     if solver == "dm":
         nb, n = inst.nb, inst.n
@@ -118,6 +119,8 @@ def solve_batch(instances, *, precision="mixed", solver="dm", streams=16, tol=1e
         for i in order:
             results[i] = _solve_one(instances[i], precision, solver, tol, max_iter)
     else:
+        # concurrent solves launch their kernels directly: per-solve graph
+        # instantiation from many host threads contends in the driver
         local = threading.local()
         lock = threading.Lock()
         queue = list(order)
@@ -132,7 +135,7 @@ def solve_batch(instances, *, precision="mixed", solver="dm", streams=16, tol=1e
                         if not queue:
                             break
                         i = queue.pop(0)
-                    results[i] = _solve_one(instances[i], precision, solver, tol, max_iter)
+                    results[i] = _solve_one(instances[i], precision, solver, tol, max_iter, graphs=False)
             local.stream.synchronize()
 
         with ThreadPoolExecutor(max_workers=streams) as ex:

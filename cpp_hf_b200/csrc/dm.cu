@@ -208,7 +208,7 @@ __global__ void k_pr_beta(const double2* __restrict__ G, const double2* __restri
                           const double* __restrict__ g_p, const double* __restrict__ g_pp,
                           const double* __restrict__ eps, const double* __restrict__ p,
                           const double* __restrict__ w, int64_t nk, int nb, double T_r, int restart,
-                          int iter, DmScalars* S) {
+                          DmScalars* S) {
     __shared__ double red[96];
     const int nb2 = nb * nb;
     const int64_t nel = nk * nb2;
@@ -241,7 +241,11 @@ __global__ void k_pr_beta(const double2* __restrict__ G, const double2* __restri
         const double den = out[1];
         double beta = (den > TINY_REAL) ? fmax(0.0, num / den) : 0.0;
         beta = fmin(beta, 5.0);
+        // the iteration count lives on the device (incremented here) so that an
+        // iteration's launches do not depend on it
+        const int iter = S->iter;
         if (iter == 0 || (restart > 0 && iter % restart == 0)) beta = 0.0;
+        S->iter = iter + 1;
         S->beta = beta;
     }
 }
@@ -610,9 +614,9 @@ int dm_gradient(const double2* Ft, const double* p, const double* eps, const dou
 }
 
 int dm_pr_beta(const double2* G, const double2* Gp, const double* g_p, const double* g_pp, const double* eps,
-               const double* p, const double* w, int64_t nk, int nb, double T_r, int restart, int iter,
-               DmScalars* S, cudaStream_t st) {
-    k_pr_beta<<<flat_grid(nk * nb * nb, 256), 256, 0, st>>>(G, Gp, g_p, g_pp, eps, p, w, nk, nb, T_r, restart, iter, S);
+               const double* p, const double* w, int64_t nk, int nb, double T_r, int restart, DmScalars* S,
+               cudaStream_t st) {
+    k_pr_beta<<<flat_grid(nk * nb * nb, 256), 256, 0, st>>>(G, Gp, g_p, g_pp, eps, p, w, nk, nb, T_r, restart, S);
     CPPHF_LAUNCH_CHECK("pr_beta");
     return CPPHF_OK;
 }

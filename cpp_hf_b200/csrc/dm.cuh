@@ -20,7 +20,9 @@ struct DmScalars {
     double omega0;
     int accepted;
     unsigned counter;  // last-block reduction counter (self-resetting)
-    double pad[2];
+    int iter;          // iterations since the start or the precision switch (CG restart count)
+    int iter_pad;
+    double pad[1];
     double part[3 * kDmMaxPartials];
 };
 
@@ -32,7 +34,7 @@ int dm_occupations(const double* eps, const double* mu, double T_r, double* p, i
 int dm_gradient(const double2* Ft, const double* p, const double* eps, const double* w, double2* G, double* g_p,
                 int64_t nk, int nb, double T_r, double denom_scale, DmScalars* S, cudaStream_t st);
 int dm_pr_beta(const double2* G, const double2* Gp, const double* g_p, const double* g_pp, const double* eps,
-               const double* p, const double* w, int64_t nk, int nb, double T_r, int restart, int iter,
+               const double* p, const double* w, int64_t nk, int nb, double T_r, int restart,
                DmScalars* S, cudaStream_t st);
 int dm_direction(const double2* G, const double2* dQp, const double* g_p, const double* dpp, const double* eps,
                  const double* p, const double* w, double2* dQ, double* d_p, int64_t nk, int nb, double T_r,

@@ -256,8 +256,11 @@ __global__ void __launch_bounds__(kThreads) k_rot_grad(const double2* __restrict
 // ---------------------------------------------------------------------------
 // Cayley unitary U(tau) = (I + tau d/2)^{-1} (I - tau d/2) of one k-point by
 // Gauss-Jordan elimination, one row per thread (row r of the result in u[]).
-// d is the group's padded matrix; the pivot row is broadcast through the
-// group's shared slot `piv`.
+// At step pp the owner of row pp divides its row by the pivot (one reciprocal
+// per step) and broadcasts it through the group's shared slot `piv`; the other
+// rows eliminate column pp, touching only the columns right of the pivot in
+// the left block (the ones left of it are already zero).  The rows end
+// normalised, so u[] is row r of U.
 // ---------------------------------------------------------------------------
 template <int NB, int LD>
 __device__ __forceinline__ void row_cayley(const double2* d, double tau, int r, double2* piv, double2 (&u)[NB],
@@ -274,32 +277,30 @@ __device__ __forceinline__ void row_cayley(const double2* d, double tau, int r, 
 #pragma unroll
     for (int pp = 0; pp < NB; ++pp) {
         if (r == pp) {
+            const double2 pv = mrow[pp];
+            const double inv = 1.0 / (pv.x * pv.x + pv.y * pv.y);
+            const double2 rp = mk(pv.x * inv, -pv.y * inv);
+#pragma unroll
+            for (int j = pp + 1; j < NB; ++j) {
+                mrow[j] = cmul(mrow[j], rp);
+                piv[j] = mrow[j];
+            }
 #pragma unroll
             for (int j = 0; j < NB; ++j) {
-                piv[j] = mrow[j];
+                u[j] = cmul(u[j], rp);
                 piv[NB + j] = u[j];
             }
         }
         __syncwarp(mask);
         if (r != pp) {
-            const double2 pv = piv[pp];
-            const double inv = 1.0 / (pv.x * pv.x + pv.y * pv.y);
-            const double2 f = cscale(cmulc(mrow[pp], pv), inv);
+            const double2 f = mrow[pp];
 #pragma unroll
-            for (int j = 0; j < NB; ++j) {
-                mrow[j] = csub(mrow[j], cmul(f, piv[j]));
-                u[j] = csub(u[j], cmul(f, piv[NB + j]));
-            }
+            for (int j = pp + 1; j < NB; ++j) mrow[j] = csub(mrow[j], cmul(f, piv[j]));
+#pragma unroll
+            for (int j = 0; j < NB; ++j) u[j] = csub(u[j], cmul(f, piv[NB + j]));
         }
         __syncwarp(mask);
     }
-    double2 dd = mrow[0];
-#pragma unroll
-    for (int j = 1; j < NB; ++j)
-        if (j == r) dd = mrow[j];
-    const double inv = 1.0 / (dd.x * dd.x + dd.y * dd.y);
-#pragma unroll
-    for (int j = 0; j < NB; ++j) u[j] = cscale(cmulc(u[j], dd), inv);
 }
 
 // diag(U^H Ft U) for the group: thread j holds Ft row j (ftj); it forms
@@ -332,12 +333,14 @@ __device__ __forceinline__ double row_diag_uhfu(const double2 (&ftj)[NB], const 
 
 // One backtracking trial (solver_dm.hpp:577-589) by elimination.
 // Dynamic shared memory: sD | sF | sU, TILE double2 each.
+// Every trial that runs writes its diag(U^H Ft U) to ew, so after the line
+// search ew holds the accepted trial's values (the retraction reuses them).
 template <int NB>
 __global__ void __launch_bounds__(kThreads) k_trial_small(const double2* __restrict__ dQ, const double2* __restrict__ Ft,
                                                           const double* __restrict__ p, const double* __restrict__ d_p,
-                                                          const double* __restrict__ w, int64_t nk, double T_r,
-                                                          double shrink, int last_trial, double fallback,
-                                                          DmScalars* S) {
+                                                          const double* __restrict__ w, double* __restrict__ ew,
+                                                          int64_t nk, double T_r, double shrink, int last_trial,
+                                                          double fallback, DmScalars* S) {
     if (S->accepted) return;  // grid-uniform
     using G = Geo<NB>;
     extern __shared__ __align__(16) double2 dyn[];
@@ -375,6 +378,7 @@ __global__ void __launch_bounds__(kThreads) k_trial_small(const double2* __restr
             for (int l = 0; l < NB; ++l) ftj[l] = sF[grp * G::MS + rr * G::LD + l];
             const double dr = row_diag_uhfu<NB, G::GS, G::LD>(ftj, sU + grp * G::MS, r, mask, live);
             if (live) {
+                ew[k * NB + r] = dr;
                 const double pv = fmin(fmax(p[k * NB + r] - tau * d_p[k * NB + r], OCC_CLIP), 1.0 - OCC_CLIP);
                 const double wk = w[k];
                 v[0] += wk * pv * dr;
@@ -412,12 +416,15 @@ __global__ void __launch_bounds__(kThreads) k_retract_small(double2* Q, const do
     const int grp = threadIdx.x / G::GS, r = threadIdx.x % G::GS;
     const unsigned mask = group_mask<NB>(threadIdx.x & 31);
     const double tau = S->tau_final;
+    // an accepted trial left its diag(U^H Ft U) in ew; only the fallback step
+    // (no trial accepted) needs it here (grid-uniform)
+    const bool need_diag = S->accepted == 0;
     const int64_t ntiles = (nk + G::KT - 1) / G::KT;
     for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int64_t k0 = t * G::KT;
         const int nkt = (int)((nk - k0) < G::KT ? (nk - k0) : G::KT);
         tile_load<NB>(sD, dQ + (size_t)k0 * G::NB2, nkt);
-        tile_load<NB>(sF, Ft + (size_t)k0 * G::NB2, nkt);
+        if (need_diag) tile_load<NB>(sF, Ft + (size_t)k0 * G::NB2, nkt);
         tile_load<NB>(sQ, Q + (size_t)k0 * G::NB2, nkt);
         __syncthreads();
         const bool live = grp < nkt && r < NB;
@@ -433,12 +440,14 @@ __global__ void __launch_bounds__(kThreads) k_retract_small(double2* Q, const do
         }
         __syncthreads();
         if (grp < nkt) {
-            double2 ftj[NB];
+            if (need_diag) {
+                double2 ftj[NB];
 #pragma unroll
-            for (int l = 0; l < NB; ++l) ftj[l] = sF[grp * G::MS + rr * G::LD + l];
-            const double dr = row_diag_uhfu<NB, G::GS, G::LD>(ftj, sU + grp * G::MS, r, mask, live);
+                for (int l = 0; l < NB; ++l) ftj[l] = sF[grp * G::MS + rr * G::LD + l];
+                const double dr = row_diag_uhfu<NB, G::GS, G::LD>(ftj, sU + grp * G::MS, r, mask, live);
+                if (live) ew[k * NB + r] = dr;
+            }
             if (live) {
-                ew[k * NB + r] = dr;
                 const double2* su = sU + grp * G::MS;
                 double2* qrow = sQ + grp * G::MS + r * G::LD;
                 double2 qr[NB];
@@ -459,55 +468,46 @@ __global__ void __launch_bounds__(kThreads) k_retract_small(double2* Q, const do
     }
 }
 
-// Element kernels: 256 threads, grid-stride loops unrolled by kUnrollE so
-// each thread keeps several independent field loads in flight.  The per-row
-// (occupation) terms run in a second, row-parallel loop of the same launch:
-// folded into the element loop they would make every warp execute the
-// log / division branch of its row leaders.
+// Row kernels (PR+ beta, direction): one thread per matrix row (k, i), which
+// loads the row's NB elements of each field (independent loads, all in
+// flight at once), its eigenvalue, weight and occupation terms, so the index
+// arithmetic and the row terms are paid once per row.  The preconditioner
+// 1 / sqrt(gap^2 + lambda^2) is one reciprocal square root per element.
 constexpr int kThreadsE = 256;
-constexpr int kUnrollE = 4;
 
-// PR+ numerator / denominator -> beta (solver_dm.hpp:513-559): matrix terms
-// one thread per element (k, i, j), occupation terms one thread per row (k, i).
+// PR+ numerator / denominator -> beta (solver_dm.hpp:513-559)
 template <int NB>
 __global__ void __launch_bounds__(kThreadsE) k_pr_beta_small(const double2* __restrict__ Gc, const double2* __restrict__ Gp,
                                                              const double* __restrict__ g_p,
                                                              const double* __restrict__ g_pp,
                                                              const double* __restrict__ eps,
                                                              const double* __restrict__ p, const double* __restrict__ w,
-                                                             int64_t nk, double T_r, int restart, int iter, DmScalars* S) {
+                                                             int64_t nk, double T_r, int restart, DmScalars* S) {
     __shared__ double red[96];
-    const double lam = S->lam_pc;
+    const double lam = S->lam_pc, lam2 = lam * lam;
     double v[3] = {0.0, 0.0, 0.0};
-    const int64_t nel = nk * NB * NB;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    for (int64_t e0 = tid; e0 < nel; e0 += kUnrollE * stride) {
-        double2 g[kUnrollE], gp[kUnrollE];
-#pragma unroll
-        for (int u = 0; u < kUnrollE; ++u) {
-            const int64_t e = e0 + u * stride;
-            g[u] = e < nel ? Gc[e] : mk(0.0, 0.0);
-            gp[u] = e < nel ? Gp[e] : mk(0.0, 0.0);
-        }
-#pragma unroll
-        for (int u = 0; u < kUnrollE; ++u) {
-            const int64_t e = e0 + u * stride;
-            if (e >= nel) break;
-            const int64_t row = e / NB;
-            const int j = (int)(e - row * NB);
-            const int64_t k = row / NB;
-            const double wk = w[k];
-            const double gap = eps[row] - eps[k * NB + j];
-            const double base = sqrt(gap * gap + lam * lam);
-            const double2 d = mk(g[u].x / base, g[u].y / base);
-            v[0] += wk * ((g[u].x * d.x + g[u].y * d.y) - (gp[u].x * d.x + gp[u].y * d.y));
-            v[1] += wk * (gp[u].x * gp[u].x + gp[u].y * gp[u].y);
-        }
-    }
     const int64_t nrow = nk * NB;
-    for (int64_t row = tid; row < nrow; row += stride) {
-        const double wk = w[row / NB];
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < nrow; row += stride) {
+        const int64_t k = row / NB;
+        double2 g[NB], gp[NB];
+#pragma unroll
+        for (int j = 0; j < NB; ++j) {
+            g[j] = Gc[row * NB + j];
+            gp[j] = Gp[row * NB + j];
+        }
+        const double wk = w[k], ei = eps[row];
+        double a0 = 0.0, a1 = 0.0;
+#pragma unroll
+        for (int j = 0; j < NB; ++j) {
+            const double gap = ei - eps[k * NB + j];
+            const double rb = rsqrt(gap * gap + lam2);
+            const double2 d = mk(g[j].x * rb, g[j].y * rb);
+            a0 += (g[j].x * d.x + g[j].y * d.y) - (gp[j].x * d.x + gp[j].y * d.y);
+            a1 += gp[j].x * gp[j].x + gp[j].y * gp[j].y;
+        }
+        v[0] += wk * a0;
+        v[1] += wk * a1;
         const double ps = fmin(fmax(p[row], OCC_CLIP), 1.0 - OCC_CLIP);
         const double gr = g_p[row], gq = g_pp[row];
         const double h = gr / (T_r / (ps * (1.0 - ps)));
@@ -520,13 +520,16 @@ __global__ void __launch_bounds__(kThreadsE) k_pr_beta_small(const double2* __re
         const double den = out[1];
         double beta = (den > TINY_REAL) ? fmax(0.0, num / den) : 0.0;
         beta = fmin(beta, 5.0);
+        // the iteration count lives on the device (incremented here) so that an
+        // iteration's launches do not depend on it
+        const int iter = S->iter;
         if (iter == 0 || (restart > 0 && iter % restart == 0)) beta = 0.0;
+        S->iter = iter + 1;
         S->beta = beta;
     }
 }
 
-// direction + tau0 + Omega0 (solver_dm.hpp:556-573, 346-365): matrix direction
-// one thread per element, occupation direction and Omega0 terms one per row.
+// direction + tau0 + Omega0 (solver_dm.hpp:556-573, 346-365)
 template <int NB>
 __global__ void __launch_bounds__(kThreadsE) k_direction_small(const double2* __restrict__ Gc,
                                                                const double2* __restrict__ dQp,
@@ -538,41 +541,33 @@ __global__ void __launch_bounds__(kThreadsE) k_direction_small(const double2* __
                                                                double* __restrict__ d_p, int64_t nk, double T_r,
                                                                double max_step, DmScalars* S) {
     __shared__ double red[96];
-    const double lam = S->lam_pc, beta = S->beta;
+    const double lam = S->lam_pc, lam2 = lam * lam, beta = S->beta;
     double v[3] = {0.0, 0.0, 0.0};
-    const int64_t nel = nk * NB * NB;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    for (int64_t e0 = tid; e0 < nel; e0 += kUnrollE * stride) {
-        double2 g[kUnrollE], q[kUnrollE];
-#pragma unroll
-        for (int u = 0; u < kUnrollE; ++u) {
-            const int64_t e = e0 + u * stride;
-            g[u] = e < nel ? Gc[e] : mk(0.0, 0.0);
-            q[u] = (e < nel && beta != 0.0) ? dQp[e] : mk(0.0, 0.0);
-        }
-#pragma unroll
-        for (int u = 0; u < kUnrollE; ++u) {
-            const int64_t e = e0 + u * stride;
-            if (e >= nel) break;
-            const int64_t row = e / NB;
-            const int j = (int)(e - row * NB);
-            const int64_t k = row / NB;
-            const double wk = w[k];
-            const double gap = eps[row] - eps[k * NB + j];
-            const double base = sqrt(gap * gap + lam * lam);
-            const double2 d = mk(g[u].x / base + beta * q[u].x, g[u].y / base + beta * q[u].y);
-            dQ[e] = d;
-            v[0] += wk * (d.x * d.x + d.y * d.y);
-        }
-    }
     const int64_t nrow = nk * NB;
-    for (int64_t row = tid; row < nrow; row += stride) {
-        const double wk = w[row / NB];
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < nrow; row += stride) {
+        const int64_t k = row / NB;
+        double2 g[NB], q[NB];
+#pragma unroll
+        for (int j = 0; j < NB; ++j) {
+            g[j] = Gc[row * NB + j];
+            q[j] = beta != 0.0 ? dQp[row * NB + j] : mk(0.0, 0.0);
+        }
+        const double wk = w[k], ei = eps[row];
+        double a0 = 0.0;
+#pragma unroll
+        for (int j = 0; j < NB; ++j) {
+            const double gap = ei - eps[k * NB + j];
+            const double rb = rsqrt(gap * gap + lam2);
+            const double2 d = mk(g[j].x * rb + beta * q[j].x, g[j].y * rb + beta * q[j].y);
+            dQ[row * NB + j] = d;
+            a0 += d.x * d.x + d.y * d.y;
+        }
+        v[0] += wk * a0;
         const double ps = fmin(fmax(p[row], OCC_CLIP), 1.0 - OCC_CLIP);
         const double h = g_p[row] / (T_r / (ps * (1.0 - ps)));
         d_p[row] = h + beta * dpp[row];
-        v[1] += wk * ps * eps[row];
+        v[1] += wk * ps * ei;
         v[2] -= wk * (ps * log(ps) + (1.0 - ps) * log1p(-ps));
     }
     double out[3];
@@ -592,8 +587,8 @@ unsigned tiles_grid(int64_t nk, int KT, int cap) {
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>(nt, cap));
 }
 
-unsigned elems_grid(int64_t n) {
-    const int64_t want = (n + (int64_t)kThreadsE * kUnrollE - 1) / ((int64_t)kThreadsE * kUnrollE);
+unsigned rows_grid(int64_t nrow) {
+    const int64_t want = (nrow + kThreadsE - 1) / kThreadsE;
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, std::min<int64_t>(kDmMaxPartials, 8 * num_sms())));
 }
 
@@ -641,11 +636,11 @@ int dm_small_rot_grad(const double2* Q, double2* F, const double* p, const doubl
 }
 
 int dm_small_pr_beta(const double2* Gc, const double2* Gp, const double* g_p, const double* g_pp, const double* eps,
-                     const double* p, const double* w, int64_t nk, int nb, double T_r, int restart, int iter,
-                     DmScalars* S, cudaStream_t st) {
+                     const double* p, const double* w, int64_t nk, int nb, double T_r, int restart, DmScalars* S,
+                     cudaStream_t st) {
 #define X(N)                                                                                                     \
-    k_pr_beta_small<N><<<elems_grid(nk * N * N), kThreadsE, 0, st>>>(Gc, Gp, g_p, g_pp, eps, p, w, nk, T_r, restart, \
-                                                                    iter, S);                                    \
+    k_pr_beta_small<N><<<rows_grid(nk * N), kThreadsE, 0, st>>>(Gc, Gp, g_p, g_pp, eps, p, w, nk, T_r, restart, \
+                                                                    S);                                          \
     CPPHF_LAUNCH_CHECK("pr_beta");
     SMALL_DISPATCH(nb, X)
 #undef X
@@ -656,7 +651,7 @@ int dm_small_direction(const double2* Gc, const double2* dQp, const double* g_p,
                        const double* p, const double* w, double2* dQ, double* d_p, int64_t nk, int nb, double T_r,
                        double max_step, DmScalars* S, cudaStream_t st) {
 #define X(N)                                                                                                        \
-    k_direction_small<N><<<elems_grid(nk * N * N), kThreadsE, 0, st>>>(Gc, dQp, g_p, dpp, eps, p, w, dQ, d_p, nk, T_r, \
+    k_direction_small<N><<<rows_grid(nk * N), kThreadsE, 0, st>>>(Gc, dQp, g_p, dpp, eps, p, w, dQ, d_p, nk, T_r, \
                                                                       max_step, S);                                 \
     CPPHF_LAUNCH_CHECK("direction");
     SMALL_DISPATCH(nb, X)
@@ -665,12 +660,12 @@ int dm_small_direction(const double2* Gc, const double2* dQp, const double* g_p,
 }
 
 int dm_small_trial(const double2* dQ, const double2* Ft, const double* p, const double* d_p, const double* w,
-                   int64_t nk, int nb, double T_r, double shrink, int last_trial, double fallback, DmScalars* S,
-                   cudaStream_t st) {
+                   double* ew, int64_t nk, int nb, double T_r, double shrink, int last_trial, double fallback,
+                   DmScalars* S, cudaStream_t st) {
 #define X(N)                                                                                                         \
     small_attrs<N>();                                                                                                \
     k_trial_small<N><<<tiles_grid(nk, Geo<N>::KT, kDmMaxPartials), kThreads, 3 * sizeof(double2) * Geo<N>::TILE,    \
-                       st>>>(dQ, Ft, p, d_p, w, nk, T_r, shrink, last_trial, fallback, S);                           \
+                       st>>>(dQ, Ft, p, d_p, w, ew, nk, T_r, shrink, last_trial, fallback, S);                       \
     CPPHF_LAUNCH_CHECK("trial");
     SMALL_DISPATCH(nb, X)
 #undef X

@@ -12,14 +12,14 @@ int dm_small_dens_occ(const double2* Q, const double* ew, const double* mu, doub
 int dm_small_rot_grad(const double2* Q, double2* F, const double* p, const double* w, double* eps, double2* Gout,
                       double* g_p, int64_t nk, int nb, double T_r, double denom_scale, DmScalars* S, cudaStream_t st);
 int dm_small_pr_beta(const double2* Gc, const double2* Gp, const double* g_p, const double* g_pp, const double* eps,
-                     const double* p, const double* w, int64_t nk, int nb, double T_r, int restart, int iter,
+                     const double* p, const double* w, int64_t nk, int nb, double T_r, int restart,
                      DmScalars* S, cudaStream_t st);
 int dm_small_direction(const double2* Gc, const double2* dQp, const double* g_p, const double* dpp, const double* eps,
                        const double* p, const double* w, double2* dQ, double* d_p, int64_t nk, int nb, double T_r,
                        double max_step, DmScalars* S, cudaStream_t st);
 int dm_small_trial(const double2* dQ, const double2* Ft, const double* p, const double* d_p, const double* w,
-                   int64_t nk, int nb, double T_r, double shrink, int last_trial, double fallback, DmScalars* S,
-                   cudaStream_t st);
+                   double* ew, int64_t nk, int nb, double T_r, double shrink, int last_trial, double fallback,
+                   DmScalars* S, cudaStream_t st);
 int dm_small_retract(double2* Q, const double2* dQ, const double2* Ft, double* ew, int64_t nk, int nb,
                      const DmScalars* S, cudaStream_t st);
 

@@ -6,11 +6,14 @@
 // bounded barrier whose last block sums the partials in block order, and every
 // block replays the reference's scalar update rule itself, so the whole grid
 // agrees on (lo, hi, mu).  The results are those of the reference's fixed
-// iteration counts (30 bisection steps by default, mu_maxiter Newton steps):
-// bisection evaluates the counts at all midpoints of the next kBisectLevels
-// levels of its decision tree per round and walks the tree exactly, and Newton
-// stops early only once its state (mu, lo, hi) repeats with period 1 or 2, when
-// the state after the remaining iterations is already known.
+// iteration counts (30 bisection steps by default, mu_maxiter Newton steps).
+// Bisection runs its first levels as exact multisection rounds, then finds
+// the root of N(mu) = n_e by Newton and replays the remaining levels against
+// it (a level whose midpoint lies within the rounding margin of the root is
+// counted exactly), which reproduces the bisection's decisions with a few
+// counts instead of one per level.  Newton stops early only once its state
+// (mu, lo, hi) repeats with period 1 or 2, when the state after the remaining
+// iterations is already known.
 #include "common.cuh"
 #include "mu.cuh"
 
@@ -26,6 +29,8 @@ constexpr int kMuMaxGrid = 1024;
 constexpr int64_t kMuOneBlockMax = 32768;             // eigenvalues handled by a single CTA
 constexpr int kBisectLevels = 3;                      // bisection steps per grid barrier
 constexpr int kMuNV = (1 << kBisectLevels) - 1;       // midpoints evaluated per barrier
+constexpr double kMuWide = 64.0;                      // exact multisection while the bracket exceeds 64 T
+constexpr int kMuRootMaxIter = 80;                    // safeguarded Newton rounds (bisection fallback)
 
 __device__ __forceinline__ double expit(double x) {
     if (x >= 0.0) return 1.0 / (1.0 + exp(-x));
@@ -146,12 +151,22 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
     __shared__ double bc_tot[kMuNV];
     int round = 0;
     if (a.mode == 0) {
-        // Bisection, kBisectLevels steps per grid barrier: the counts at all
-        // midpoints of the next levels of the bisection tree are evaluated in one
-        // pass, then the tree is walked exactly as the sequential steps would
-        // (each midpoint is 0.5 * (lo + hi) of the interval the sequence reaches).
+        // Bisection (utils.hpp:49-75) in three phases.
+        //  1. Exact multisection rounds while the bracket is wide: the counts at
+        //     all midpoints of the next kBisectLevels levels of the bisection
+        //     tree in one pass, then the tree is walked exactly as the
+        //     sequential steps would.
+        //  2. The root mu* of N(mu) = target by bracketed Newton from there.
+        //  3. The remaining levels replayed against mu*: a midpoint farther than
+        //     thr from mu* is decided by comparison (N is increasing, and there
+        //     |N(mid) - target| >= 7 eps_N), a nearer one by its exact count.  A
+        //     root with thr > T/8 (flat N, e.g. mu in a gap) runs the remaining
+        //     levels as exact multisection rounds instead.
+        const double epsN = 1.0e-13 * fmax(1.0, fabs(a.target));
         int it = 0;
-        while (it < a.maxiter) {
+        double Nlo = NAN, Nhi = NAN;  // counts at the bracket ends when evaluated
+        bool ok = true;
+        auto msec_round = [&]() {
             const int L = min(kBisectLevels, a.maxiter - it);
             const int nodes = (1 << L) - 1;
             double nlo[kMuNV], nhi[kMuNV], mid[kMuNV];
@@ -200,7 +215,7 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
             }
             double* tot = tots + (round & 1) * kMuNV;
             if (!bar.wait_reduce<kMuNV>(part, G, tot)) {
-                if (blockIdx.x == 0 && threadIdx.x == 0) *a.mu_out = NAN;
+                ok = false;
                 return;
             }
             if (threadIdx.x < kMuNV) bc_tot[threadIdx.x] = __ldcg(&tot[threadIdx.x]);
@@ -213,15 +228,104 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
                     if (j == node) m = mid[j];
                 if (bc_tot[node] > a.target) {
                     hi = m;
+                    Nhi = bc_tot[node];
                     node = 2 * node + 1;
                 } else {
                     lo = m;
+                    Nlo = bc_tot[node];
                     node = 2 * node + 2;
                 }
             }
             __syncthreads();
             it += L;
             ++round;
+        };
+        // count N and slope Z = dN/dmu at one mu (one grid round)
+        auto count_round = [&](double m, double& N, double& Z) {
+            double v[2] = {0.0, 0.0};
+            for (unsigned i = e0 + threadIdx.x; i < e1; i += blockDim.x) {
+                double wk, e;
+                band_major(a, i, nb, wk, e);
+                const double xa = (m - e) * invTfd;
+                if (xa >= kFdOne) {
+                    v[0] += wk;
+                } else if (xa > kFdZero) {
+                    const double pf = expit(-(e - m) / Tfd);
+                    v[0] += wk * pf;
+                    v[1] += wk * pf * (1.0 - pf) * invTfd;
+                }
+            }
+            block_sum<2>(v, red);
+            if (threadIdx.x == 0) {
+                __stcg(&part[2 * blockIdx.x], v[0]);
+                __stcg(&part[2 * blockIdx.x + 1], v[1]);
+            }
+            double* tot = tots + (round & 1) * kMuNV;
+            ++round;
+            if (!bar.wait_reduce<2>(part, G, tot)) {
+                ok = false;
+                return;
+            }
+            if (threadIdx.x < 2) bc_tot[threadIdx.x] = __ldcg(&tot[threadIdx.x]);
+            __syncthreads();
+            N = bc_tot[0];
+            Z = bc_tot[1];
+            __syncthreads();
+        };
+        while (ok && it < a.maxiter && (it == 0 || hi - lo > kMuWide * Tj)) msec_round();
+        if (ok && it < a.maxiter) {
+            // 2. root: secant start inside the bracket, then safeguarded Newton
+            double m = 0.5 * (lo + hi);
+            if (isfinite(Nlo) && isfinite(Nhi) && Nhi > Nlo) {
+                const double ms = lo + (a.target - Nlo) * (hi - lo) / (Nhi - Nlo);
+                if (ms > lo && ms < hi) m = ms;
+            }
+            double ra = lo, rb = hi, g = INFINITY, slope = 0.0;
+            bool conv = false;
+            for (int r = 0; ok && r < kMuRootMaxIter; ++r) {
+                double N = 0.0, Z = 0.0;
+                count_round(m, N, Z);
+                if (!ok) break;
+                g = N - a.target;
+                slope = Z;
+                if (fabs(g) <= epsN) {
+                    conv = true;
+                    break;
+                }
+                if (g > 0.0)
+                    rb = m;
+                else
+                    ra = m;
+                double mn = (Z > 0.0) ? m - g / Z : NAN;
+                if (!(mn > ra && mn < rb)) mn = 0.5 * (ra + rb);
+                if (mn == m) break;
+                m = mn;
+            }
+            const double thr = (conv && slope > 0.0) ? 8.0 * (fabs(g) + epsN) / slope : INFINITY;
+            if (ok && thr <= 0.125 * Tj) {
+                // 3. replay of the remaining levels
+                for (; ok && it < a.maxiter; ++it) {
+                    const double md = 0.5 * (lo + hi);
+                    bool up;
+                    if (fabs(md - m) > thr) {
+                        up = md > m;
+                    } else {
+                        double N = 0.0, Z = 0.0;
+                        count_round(md, N, Z);
+                        up = N > a.target;
+                    }
+                    if (up)
+                        hi = md;
+                    else
+                        lo = md;
+                }
+            } else {
+                while (ok && it < a.maxiter) msec_round();
+            }
+        }
+        if (!ok) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) *a.mu_out = NAN;
+            return;
         }
     } else {
         // Newton in a bracket.  The update is a deterministic function of the

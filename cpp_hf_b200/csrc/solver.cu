@@ -14,6 +14,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
+#include <cstdlib>
 #include <limits>
 #include <mutex>
 #include <string>
@@ -234,6 +236,57 @@ int check_block_sizes(const int64_t* sizes, int64_t n, int64_t nb) {
     return CPPHF_OK;
 }
 
+// The legacy default stream cannot be captured: a solve called on it runs on
+// its own non-blocking stream, ordered after the caller's stream on entry and
+// before it on exit.  A solve on any other stream runs (and is captured) on
+// that stream directly.  `capturable` is false when the private stream could
+// not be created; the solve then runs on the caller's stream without graphs.
+struct SolveStream {
+    cudaStream_t user = nullptr, s = nullptr;
+    cudaEvent_t ev = nullptr;
+    bool capturable = true;
+    explicit SolveStream(cudaStream_t u) : user(u) {
+        if (u != nullptr && u != cudaStreamLegacy) return;
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess ||
+            cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventRecord(ev, user) != cudaSuccess || cudaStreamWaitEvent(s, ev, 0) != cudaSuccess) {
+            (void)cudaGetLastError();
+            if (s) cudaStreamDestroy(s);
+            s = nullptr;
+            capturable = false;
+        }
+    }
+    ~SolveStream() {
+        if (s) {
+            cudaEventRecord(ev, s);
+            cudaStreamWaitEvent(user, ev, 0);
+            cudaStreamDestroy(s);
+        }
+        if (ev) cudaEventDestroy(ev);
+    }
+    cudaStream_t stream() const { return s ? s : user; }
+};
+
+// One DM iteration as an instantiated graph, per (buffer parity, precision).
+struct IterGraphs {
+    cudaGraphExec_t exec[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    bool failed[2][2] = {{false, false}, {false, false}};
+    ~IterGraphs() {
+        for (auto& row : exec)
+            for (auto& e : row)
+                if (e) cudaGraphExecDestroy(e);
+    }
+};
+
+// CPPHF_SOLVE_GRAPHS=0 launches every kernel of every iteration (for A/B timing).
+bool solve_graphs_enabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("CPPHF_SOLVE_GRAPHS");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
 }  // namespace
 
 size_t solve_dm_workspace_bytes(const cpphf_kernel* K) { return dm_layout(K).total; }
@@ -251,6 +304,14 @@ int solve_dm(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* P
     const DmLayout L = dm_layout(K);
     if (!ws || wsb < L.total)
         return fail(CPPHF_ERR_INVALID, "solve_dm: workspace too small (" + std::to_string(L.total) + " bytes needed)");
+    const SolveStream guard(st);
+    st = guard.stream();
+    // Not captured: projector callbacks (host round trips) and the superlattice
+    // exchange, whose per-call channel tables are copied from host buffers that
+    // a replayed graph would read after they are gone.
+    const bool sl_path = K->sl && (K->sl->fock_active || K->sl->hartree_active);
+    const bool use_graphs = cfg->graphs != 0 && guard.capturable && !project && !sl_path && solve_graphs_enabled();
+    IterGraphs graphs;
     unsigned char* W = static_cast<unsigned char*>(ws);
     auto fld = [&](size_t off) { return reinterpret_cast<double2*>(W + off); };
     auto vec = [&](size_t off) { return reinterpret_cast<double*>(W + off); };
@@ -320,6 +381,46 @@ int solve_dm(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* P
     K32.exchange_precision = 32;
     bool low = cfg->mixed_switch_grad > 0.0;
     int64_t k0 = 0;
+    // One iteration (solver_dm.hpp:460-611): every launch, no host decision.
+    auto iteration = [&](int cur, int prv, bool low_prec) -> int {
+        const cpphf_kernel* Kb = low_prec ? &K32 : K;
+
+        // 1. density (with occupations from the last eps_work and mu) + Fock + energy
+        CPPHF_TRY(density(ew));
+        CPPHF_TRY(build_fock(Kb, P, Sig, F, nullptr, &S->energy, nullptr, fws, L.fock_bytes, st));
+        // 2.-4. Ft = Q^H F Q, gradient, preconditioner, PR+ direction
+        if (small) {
+            CPPHF_TRY(dm_small_rot_grad(Q, F, p, wn, eps, G[cur], g[cur], nk, nb, T_r, cfg->denom_scale, S, st));
+            CPPHF_TRY(dm_small_pr_beta(G[cur], G[prv], g[cur], g[prv], eps, p, wn, nk, nb, T_r, (int)cfg->cg_restart,
+                                       S, st));
+            CPPHF_TRY(dm_small_direction(G[cur], dQ[prv], g[cur], dp[prv], eps, p, wn, dQ[cur], dp[cur], nk, nb, T_r,
+                                         cfg->max_step, S, st));
+        } else {
+            CPPHF_TRY(dm_rotate(Q, F, F, eps, nk, nb, st));
+            CPPHF_TRY(dm_gradient(F, p, eps, wn, G[cur], g[cur], nk, nb, T_r, cfg->denom_scale, S, st));
+            CPPHF_TRY(dm_pr_beta(G[cur], G[prv], g[cur], g[prv], eps, p, wn, nk, nb, T_r, (int)cfg->cg_restart, S,
+                                 st));
+            CPPHF_TRY(dm_direction(G[cur], dQ[prv], g[cur], dp[prv], eps, p, wn, dQ[cur], dp[cur], nk, nb, T_r,
+                                   cfg->max_step, S, st));
+        }
+        // 5. Cayley line search (elimination form of the spectral Cayley factor):
+        // one pass per trial; a pass after the accepted trial returns at once
+        for (int64_t bt = 0; bt < cfg->bt_max; ++bt) {
+            if (small)
+                CPPHF_TRY(dm_small_trial(dQ[cur], F, p, dp[cur], wn, ew, nk, nb, T_r, cfg->bt_shrink,
+                                         bt == cfg->bt_max - 1, fallback, S, st));
+            else
+                CPPHF_TRY(dm_trial_lu(dQ[cur], F, p, dp[cur], wn, nk, nb, T_r, cfg->bt_shrink,
+                                      bt == cfg->bt_max - 1, fallback, S, st));
+        }
+        // 6. retraction and mu (occupations are formed by the next density step)
+        if (small)
+            CPPHF_TRY(dm_small_retract(Q, dQ[cur], F, ew, nk, nb, S, st));
+        else
+            CPPHF_TRY(dm_retract_lu(Q, dQ[cur], F, ew, nk, nb, S, st));
+        CPPHF_TRY(mu_solve(ew, wn, nk, nb, n_t, &S->mu, T_r, mu_it, 1, &S->mu, mws, L.mu_bytes, st));
+        return CPPHF_OK;
+    };
     while (k < max_iter) {
         bool e_nc;
         const int64_t kk = k - k0;
@@ -332,57 +433,46 @@ int solve_dm(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* P
         if (low && (!(e_nc || g_nc) || grad_norm < cfg->mixed_switch_grad)) {
             low = false;
             k0 = k;
+            CPPHF_CUDA(cudaMemsetAsync(&S->iter, 0, sizeof(int), st));
             dE = std::numeric_limits<double>::infinity();
             E_prev = std::numeric_limits<double>::infinity();
             continue;
         }
         if (!(e_nc || g_nc)) break;
         const int cur = (int)(k & 1), prv = cur ^ 1;
-        const cpphf_kernel* Kb = low ? &K32 : K;
-
-        // 1. density (with occupations from the last eps_work and mu) + Fock + energy
-        CPPHF_TRY(density(ew));
-        CPPHF_TRY(build_fock(Kb, P, Sig, F, nullptr, &S->energy, nullptr, fws, L.fock_bytes, st));
-        // 2.-4. Ft = Q^H F Q, gradient, preconditioner, PR+ direction
-        if (small) {
-            CPPHF_TRY(dm_small_rot_grad(Q, F, p, wn, eps, G[cur], g[cur], nk, nb, T_r, cfg->denom_scale, S, st));
-            CPPHF_TRY(dm_small_pr_beta(G[cur], G[prv], g[cur], g[prv], eps, p, wn, nk, nb, T_r, (int)cfg->cg_restart,
-                                       (int)(k - k0), S, st));
-            CPPHF_TRY(dm_small_direction(G[cur], dQ[prv], g[cur], dp[prv], eps, p, wn, dQ[cur], dp[cur], nk, nb, T_r,
-                                         cfg->max_step, S, st));
-        } else {
-            CPPHF_TRY(dm_rotate(Q, F, F, eps, nk, nb, st));
-            CPPHF_TRY(dm_gradient(F, p, eps, wn, G[cur], g[cur], nk, nb, T_r, cfg->denom_scale, S, st));
-            CPPHF_TRY(dm_pr_beta(G[cur], G[prv], g[cur], g[prv], eps, p, wn, nk, nb, T_r, (int)cfg->cg_restart,
-                                 (int)(k - k0), S, st));
-            CPPHF_TRY(dm_direction(G[cur], dQ[prv], g[cur], dp[prv], eps, p, wn, dQ[cur], dp[cur], nk, nb, T_r,
-                                   cfg->max_step, S, st));
+        IterGraphs& gr = graphs;
+        const int lw = low ? 1 : 0;
+        if (use_graphs && !gr.exec[cur][lw] && !gr.failed[cur][lw] && k - k0 >= 1) {
+            // capture this parity and precision once (after an eager iteration
+            // has set every kernel attribute); a failed capture runs eagerly
+            cudaGraph_t g = nullptr;
+            if (cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+                gr.failed[cur][lw] = true;
+            } else {
+                const int rc = iteration(cur, prv, low);
+                const cudaError_t e = cudaStreamEndCapture(st, &g);
+                if (rc != CPPHF_OK || e != cudaSuccess || !g ||
+                    cudaGraphInstantiate(&gr.exec[cur][lw], g, 0) != cudaSuccess) {
+                    gr.failed[cur][lw] = true;
+                    gr.exec[cur][lw] = nullptr;
+                }
+                if (g) cudaGraphDestroy(g);
+            }
+            (void)cudaGetLastError();
         }
-        // 5. Cayley line search (elimination form of the spectral Cayley factor):
-        // one pass per trial; a pass after the accepted trial returns at once
-        for (int64_t bt = 0; bt < cfg->bt_max; ++bt) {
-            if (small)
-                CPPHF_TRY(dm_small_trial(dQ[cur], F, p, dp[cur], wn, nk, nb, T_r, cfg->bt_shrink,
-                                         bt == cfg->bt_max - 1, fallback, S, st));
-            else
-                CPPHF_TRY(dm_trial_lu(dQ[cur], F, p, dp[cur], wn, nk, nb, T_r, cfg->bt_shrink,
-                                      bt == cfg->bt_max - 1, fallback, S, st));
-        }
-        // 6. retraction and mu (occupations are formed by the next density step)
-        if (small)
-            CPPHF_TRY(dm_small_retract(Q, dQ[cur], F, ew, nk, nb, S, st));
+        if (gr.exec[cur][lw])
+            CPPHF_CUDA(cudaGraphLaunch(gr.exec[cur][lw], st));
         else
-            CPPHF_TRY(dm_retract_lu(Q, dQ[cur], F, ew, nk, nb, S, st));
-        CPPHF_TRY(mu_solve(ew, wn, nk, nb, n_t, &S->mu, T_r, mu_it, 1, &S->mu, mws, L.mu_bytes, st));
-        // 7. record
-        CPPHF_CUDA(cudaMemcpyAsync(hbuf, &S->energy, sizeof(double), cudaMemcpyDeviceToHost, st));
-        CPPHF_CUDA(cudaMemcpyAsync(hbuf + 1, &S->grad_norm, sizeof(double), cudaMemcpyDeviceToHost, st));
-        CPPHF_CUDA(cudaMemcpyAsync(hbuf + 2, &S->mu, sizeof(double), cudaMemcpyDeviceToHost, st));
+            CPPHF_TRY(iteration(cur, prv, low));
+        // 7. record: mu, mu_new, energy, grad_norm are adjacent in DmScalars (one copy)
+        static_assert(offsetof(DmScalars, grad_norm) == offsetof(DmScalars, mu) + 3 * sizeof(double),
+                      "DmScalars read-back layout");
+        CPPHF_CUDA(cudaMemcpyAsync(hbuf, &S->mu, 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
         CPPHF_CUDA(cudaStreamSynchronize(st));
-        if (!std::isfinite(hbuf[2]))
+        if (!std::isfinite(hbuf[0]))
             return fail(CPPHF_ERR_TIMEOUT, "solve_dm: chemical-potential solve failed (device wait timeout or non-finite)");
-        const double E = hbuf[0];
-        grad_norm = hbuf[1];
+        const double E = hbuf[2];
+        grad_norm = hbuf[3];
         hE[k] = E;
         hG[k] = grad_norm;
         dE = std::fabs(E - E_prev);
@@ -546,9 +636,11 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
         else
             k_scf_residuals<false><<<tgrid, kCtaTeamThreadsDense, rsmem, st>>>(F, D, Pn, K->w2d, nk, nb, S);
         CPPHF_LAUNCH_CHECK("scf residuals");
-        CPPHF_CUDA(cudaMemcpyAsync(hbuf, &S->energy, sizeof(double), cudaMemcpyDeviceToHost, st));
-        CPPHF_CUDA(cudaMemcpyAsync(hbuf + 1, &S->grad_norm, sizeof(double), cudaMemcpyDeviceToHost, st));
-        CPPHF_CUDA(cudaMemcpyAsync(hbuf + 2, &S->lam_pc, sizeof(double), cudaMemcpyDeviceToHost, st));
+        // energy, grad_norm (density residual) and lam_pc (commutator residual) are
+        // adjacent in DmScalars: one copy, plus mu
+        static_assert(offsetof(DmScalars, lam_pc) == offsetof(DmScalars, energy) + 2 * sizeof(double),
+                      "DmScalars read-back layout");
+        CPPHF_CUDA(cudaMemcpyAsync(hbuf, &S->energy, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
         CPPHF_CUDA(cudaMemcpyAsync(hbuf + 3, mu_fin, sizeof(double), cudaMemcpyDeviceToHost, st));
         CPPHF_CUDA(cudaStreamSynchronize(st));
         if (!std::isfinite(hbuf[3]))

@@ -221,6 +221,12 @@ typedef struct cpphf_dm_config {
      * never ends the solve during the complex64 phase: it switches instead.
      * 0 = plain solve at K->exchange_precision. */
     double mixed_switch_grad;
+    /* 1: each iteration's launches are captured once as a CUDA graph and replayed
+     * (fewer launch gaps for a single solve); 0: every kernel is launched each
+     * iteration (better when many solves share the GPU from several host
+     * threads, where per-solve graph instantiation contends in the driver). */
+    int32_t graphs;
+    int32_t reserved_dm;
 } cpphf_dm_config;
 
 typedef struct cpphf_dm_result {
