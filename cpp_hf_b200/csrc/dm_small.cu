@@ -333,14 +333,16 @@ __device__ __forceinline__ double row_diag_uhfu(const double2 (&ftj)[NB], const 
 
 // One backtracking trial (solver_dm.hpp:577-589) by elimination.
 // Dynamic shared memory: sD | sF | sU, TILE double2 each.
-// Every trial that runs writes its diag(U^H Ft U) to ew, so after the line
-// search ew holds the accepted trial's values (the retraction reuses them).
+// Every trial that runs writes its U(tau) and diag(U^H Ft U) (to Uout, ew), so
+// after the line search they hold the accepted trial's values and the
+// retraction reuses them.
 template <int NB>
 __global__ void __launch_bounds__(kThreads) k_trial_small(const double2* __restrict__ dQ, const double2* __restrict__ Ft,
                                                           const double* __restrict__ p, const double* __restrict__ d_p,
                                                           const double* __restrict__ w, double* __restrict__ ew,
-                                                          int64_t nk, double T_r, double shrink, int last_trial,
-                                                          double fallback, DmScalars* S) {
+                                                          double2* __restrict__ Uout, int64_t nk, double T_r,
+                                                          double shrink, int last_trial, double fallback,
+                                                          DmScalars* S) {
     if (S->accepted) return;  // grid-uniform
     using G = Geo<NB>;
     extern __shared__ __align__(16) double2 dyn[];
@@ -367,8 +369,12 @@ __global__ void __launch_bounds__(kThreads) k_trial_small(const double2* __restr
             double2 u[NB];
             row_cayley<NB, G::LD>(sD + grp * G::MS, tau, rr, sPiv + grp * 2 * NB, u, mask);
             if (live) {
+                double2* urow = Uout + ((size_t)k * NB + r) * NB;
 #pragma unroll
-                for (int j = 0; j < NB; ++j) sU[grp * G::MS + r * G::LD + j] = u[j];
+                for (int j = 0; j < NB; ++j) {
+                    sU[grp * G::MS + r * G::LD + j] = u[j];
+                    urow[j] = u[j];
+                }
             }
         }
         __syncthreads();
@@ -405,7 +411,8 @@ __global__ void __launch_bounds__(kThreads) k_trial_small(const double2* __restr
 template <int NB>
 __global__ void __launch_bounds__(kThreads) k_retract_small(double2* Q, const double2* __restrict__ dQ,
                                                             const double2* __restrict__ Ft, double* __restrict__ ew,
-                                                            int64_t nk, const DmScalars* S) {
+                                                            const double2* __restrict__ Uacc, int64_t nk,
+                                                            const DmScalars* S) {
     using G = Geo<NB>;
     extern __shared__ __align__(16) double2 dyn[];
     double2* sD = dyn;
@@ -416,21 +423,25 @@ __global__ void __launch_bounds__(kThreads) k_retract_small(double2* Q, const do
     const int grp = threadIdx.x / G::GS, r = threadIdx.x % G::GS;
     const unsigned mask = group_mask<NB>(threadIdx.x & 31);
     const double tau = S->tau_final;
-    // an accepted trial left its diag(U^H Ft U) in ew; only the fallback step
-    // (no trial accepted) needs it here (grid-uniform)
+    // an accepted trial left its U(tau) in Uacc and its diag(U^H Ft U) in ew;
+    // only the fallback step (no trial accepted) computes them here (grid-uniform)
     const bool need_diag = S->accepted == 0;
     const int64_t ntiles = (nk + G::KT - 1) / G::KT;
     for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int64_t k0 = t * G::KT;
         const int nkt = (int)((nk - k0) < G::KT ? (nk - k0) : G::KT);
-        tile_load<NB>(sD, dQ + (size_t)k0 * G::NB2, nkt);
-        if (need_diag) tile_load<NB>(sF, Ft + (size_t)k0 * G::NB2, nkt);
+        if (need_diag) {
+            tile_load<NB>(sD, dQ + (size_t)k0 * G::NB2, nkt);
+            tile_load<NB>(sF, Ft + (size_t)k0 * G::NB2, nkt);
+        } else {
+            tile_load<NB>(sU, Uacc + (size_t)k0 * G::NB2, nkt);
+        }
         tile_load<NB>(sQ, Q + (size_t)k0 * G::NB2, nkt);
         __syncthreads();
         const bool live = grp < nkt && r < NB;
         const int rr = r < NB ? r : 0;
         const int64_t k = k0 + grp;
-        if (grp < nkt) {
+        if (need_diag && grp < nkt) {
             double2 u[NB];
             row_cayley<NB, G::LD>(sD + grp * G::MS, tau, rr, sPiv + grp * 2 * NB, u, mask);
             if (live) {
@@ -660,24 +671,24 @@ int dm_small_direction(const double2* Gc, const double2* dQp, const double* g_p,
 }
 
 int dm_small_trial(const double2* dQ, const double2* Ft, const double* p, const double* d_p, const double* w,
-                   double* ew, int64_t nk, int nb, double T_r, double shrink, int last_trial, double fallback,
-                   DmScalars* S, cudaStream_t st) {
+                   double* ew, double2* U, int64_t nk, int nb, double T_r, double shrink, int last_trial,
+                   double fallback, DmScalars* S, cudaStream_t st) {
 #define X(N)                                                                                                         \
     small_attrs<N>();                                                                                                \
     k_trial_small<N><<<tiles_grid(nk, Geo<N>::KT, kDmMaxPartials), kThreads, 3 * sizeof(double2) * Geo<N>::TILE,    \
-                       st>>>(dQ, Ft, p, d_p, w, ew, nk, T_r, shrink, last_trial, fallback, S);                       \
+                       st>>>(dQ, Ft, p, d_p, w, ew, U, nk, T_r, shrink, last_trial, fallback, S);                    \
     CPPHF_LAUNCH_CHECK("trial");
     SMALL_DISPATCH(nb, X)
 #undef X
     return CPPHF_OK;
 }
 
-int dm_small_retract(double2* Q, const double2* dQ, const double2* Ft, double* ew, int64_t nk, int nb,
-                     const DmScalars* S, cudaStream_t st) {
+int dm_small_retract(double2* Q, const double2* dQ, const double2* Ft, double* ew, const double2* U, int64_t nk,
+                     int nb, const DmScalars* S, cudaStream_t st) {
 #define X(N)                                                                                                      \
     small_attrs<N>();                                                                                             \
     k_retract_small<N><<<tiles_grid(nk, Geo<N>::KT, 16 * num_sms()), kThreads, 4 * sizeof(double2) * Geo<N>::TILE, \
-                         st>>>(Q, dQ, Ft, ew, nk, S);                                                             \
+                         st>>>(Q, dQ, Ft, ew, U, nk, S);                                                          \
     CPPHF_LAUNCH_CHECK("retract");
     SMALL_DISPATCH(nb, X)
 #undef X

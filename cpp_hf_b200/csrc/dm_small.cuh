@@ -18,9 +18,9 @@ int dm_small_direction(const double2* Gc, const double2* dQp, const double* g_p,
                        const double* p, const double* w, double2* dQ, double* d_p, int64_t nk, int nb, double T_r,
                        double max_step, DmScalars* S, cudaStream_t st);
 int dm_small_trial(const double2* dQ, const double2* Ft, const double* p, const double* d_p, const double* w,
-                   double* ew, int64_t nk, int nb, double T_r, double shrink, int last_trial, double fallback,
-                   DmScalars* S, cudaStream_t st);
-int dm_small_retract(double2* Q, const double2* dQ, const double2* Ft, double* ew, int64_t nk, int nb,
-                     const DmScalars* S, cudaStream_t st);
+                   double* ew, double2* U, int64_t nk, int nb, double T_r, double shrink, int last_trial,
+                   double fallback, DmScalars* S, cudaStream_t st);
+int dm_small_retract(double2* Q, const double2* dQ, const double2* Ft, double* ew, const double2* U, int64_t nk,
+                     int nb, const DmScalars* S, cudaStream_t st);
 
 }  // namespace cpphf

@@ -407,7 +407,7 @@ int solve_dm(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* P
         // one pass per trial; a pass after the accepted trial returns at once
         for (int64_t bt = 0; bt < cfg->bt_max; ++bt) {
             if (small)
-                CPPHF_TRY(dm_small_trial(dQ[cur], F, p, dp[cur], wn, ew, nk, nb, T_r, cfg->bt_shrink,
+                CPPHF_TRY(dm_small_trial(dQ[cur], F, p, dp[cur], wn, ew, Vd, nk, nb, T_r, cfg->bt_shrink,
                                          bt == cfg->bt_max - 1, fallback, S, st));
             else
                 CPPHF_TRY(dm_trial_lu(dQ[cur], F, p, dp[cur], wn, nk, nb, T_r, cfg->bt_shrink,
@@ -415,7 +415,7 @@ int solve_dm(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* P
         }
         // 6. retraction and mu (occupations are formed by the next density step)
         if (small)
-            CPPHF_TRY(dm_small_retract(Q, dQ[cur], F, ew, nk, nb, S, st));
+            CPPHF_TRY(dm_small_retract(Q, dQ[cur], F, ew, Vd, nk, nb, S, st));
         else
             CPPHF_TRY(dm_retract_lu(Q, dQ[cur], F, ew, nk, nb, S, st));
         CPPHF_TRY(mu_solve(ew, wn, nk, nb, n_t, &S->mu, T_r, mu_it, 1, &S->mu, mws, L.mu_bytes, st));
@@ -585,9 +585,12 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
     // the occupation mu: mu2[1] after a level shift, else mu2[0]
     double* mu_fin = (cfg->level_shift != 0.0) ? &mu2[1] : &mu2[0];
     // build_and_occupy (solver_scf.hpp:179-197); mu -> mu_fin, E -> S->energy
+    // D is exactly Hermitian after the mixing kernel (it writes h and conj(h)) and
+    // after a copy of P_new; hermitizing it again is a bitwise no-op and is skipped
+    bool d_hermitian = false;
     auto build_and_occupy = [&]() -> int {
         if (project) CPPHF_TRY(call_project(project, puser, D, K, st));
-        CPPHF_TRY(hermitize(D, D, nk, nb, st));
+        if (project || !d_hermitian) CPPHF_TRY(hermitize(D, D, nk, nb, st));
         CPPHF_TRY(build_fock(low ? &K32 : K, D, Sig, F, nullptr, &S->energy, nullptr, fws, L.fock_bytes, st));
         if (project) {
             CPPHF_TRY(call_project(project, puser, F, K, st));
@@ -608,9 +611,13 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
             CPPHF_TRY(mu_solve(e_occ, K->w2d, nk, nb, n_e, nullptr, K->T, 30, 0, mu_fin, mws, L.mu_bytes, st));
         k_fermi<<<grid_for(nk * nb, 256), 256, 0, st>>>(e_occ, mu_fin, K->T, occ, nk * nb);
         CPPHF_LAUNCH_CHECK("fermi");
+        // dm_density writes (X + X^H) / 2, exactly Hermitian: only a projector needs
+        // the hermitisation again
         CPPHF_TRY(dm_density(V, occ, Pn, nk, nb, st));
-        if (project) CPPHF_TRY(call_project(project, puser, Pn, K, st));
-        CPPHF_TRY(hermitize(Pn, Pn, nk, nb, st));
+        if (project) {
+            CPPHF_TRY(call_project(project, puser, Pn, K, st));
+            CPPHF_TRY(hermitize(Pn, Pn, nk, nb, st));
+        }
         return CPPHF_OK;
     };
 
@@ -653,6 +660,7 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
             low = false;
             converged = false;
         }
+        d_hermitian = true;
         if (converged) {
             CPPHF_CUDA(cudaMemcpyAsync(D, Pn, fbytes, cudaMemcpyDeviceToDevice, st));
         } else {

@@ -157,6 +157,43 @@ def test_find_mu_bisection(native, oracle, nk, nb, T):
     assert abs(mu - mu_ref) < 1e-12 * max(1.0, abs(mu_ref))
 
 
+@pytest.mark.parametrize("nk,nb,T,maxiter", [(36864, 8, 0.01, 0), (9216, 4, 0.5, 0), (36864, 8, 0.05, 12),
+                                             (36864, 8, 0.05, 45), (40000, 2, 0.002, 0)])
+def test_find_mu_bisection_root_replay(native, oracle, nk, nb, T, maxiter):
+    """Large multi-block problems, where the GPU runs the first bisection levels
+    as multisection rounds, finds the root of N(mu) = n_e by Newton and replays
+    the remaining levels against it: the result equals the oracle's sequential
+    bisection for short, default and long level counts and cold and hot T."""
+    rng = np.random.default_rng(nk + nb + int(1e3 * T) + maxiter)
+    bands = rng.normal(size=(nk, nb))
+    w = rng.uniform(0.5, 1.5, size=nk)
+    w /= w.sum()
+    n_e = 0.37 * nb
+    mu = native.find_mu_bisection(bands, w, n_e, T, maxiter)
+    mu_ref = oracle.find_mu_bisection(bands, w, n_e, T, maxiter)
+    assert abs(mu - mu_ref) < 1e-12 * max(1.0, abs(mu_ref))
+
+
+def test_find_mu_bisection_gapped_spectrum(native, oracle):
+    """mu inside a band gap with T well below the gap: N(mu) is flat to rounding
+    there, so the GPU keeps exact counts for the levels whose sign is not certain
+    (the reference's own decisions are rounding noise there too); the count
+    reached must equal n_e and mu must lie in the gap."""
+    rng = np.random.default_rng(5)
+    nk, nb = 40000, 4
+    lower = rng.uniform(-2.0, -1.0, size=(nk, nb // 2))
+    upper = rng.uniform(1.0, 2.0, size=(nk, nb // 2))
+    bands = np.concatenate([lower, upper], axis=1)
+    w = np.full(nk, 1.0 / nk)
+    n_e = nb // 2
+    T = 0.02
+    mu = native.find_mu_bisection(bands, w, n_e, T, 0)
+    mu_ref = oracle.find_mu_bisection(bands, w, n_e, T, 0)
+    assert -1.0 < mu < 1.0 and -1.0 < mu_ref < 1.0
+    occ = 0.5 * (1.0 - np.tanh(0.5 * (bands - mu) / (T + 1e-12)))
+    assert abs(float(np.sum(w[:, None] * occ)) - n_e) < 1e-12
+
+
 def test_find_mu_bisection_cold_limit_hits_target(native, oracle):
     """T -> 0 with the target on a plateau of the count: mu is only defined up to
     the plateau (serial, pairwise and tree sums decide count > n_e differently
