@@ -74,6 +74,7 @@ class ScfConfig(C.Structure):
     _fields_ = [
         ("max_iter", i64), ("density_tol", f64), ("comm_tol", f64), ("mixing", f64),
         ("level_shift", f64), ("acceleration", i32), ("reserved", i32), ("mixed_switch_tol", f64),
+        ("diis_size", i32), ("diis_start", i32), ("diis_damping", f64), ("trust_radius", f64),
     ]
 
 
@@ -127,6 +128,7 @@ _SIGS = {
     "cpphf_density_from_fock_backward_workspace_bytes": (sz, []),
     "cpphf_density_from_fock_backward": (C.c_int, [vp, vp, vp, f64, vp, vp, vp, i64, i64, vp, sz, vp]),
     "cpphf_solve_scf_workspace_bytes": (sz, [C.POINTER(Kernel)]),
+    "cpphf_solve_scf_workspace_bytes_cfg": (sz, [C.POINTER(Kernel), C.POINTER(ScfConfig)]),
     "cpphf_solve_scf": (C.c_int, [C.POINTER(Kernel), C.POINTER(ScfConfig), vp, f64, PROJECT_FN, vp,
                                   vp, vp, dp, dp, dp, C.POINTER(ScfResult), vp, sz, vp]),
 }

@@ -488,15 +488,11 @@ def solve_dm(kernel_args, P0, n_e, max_iter, tol_E, tol_grad, max_step, bt_shrin
 def solve_scf(kernel_args, P0, n_e, max_iter, density_tol, comm_tol, mixing, level_shift, project_fn,
               block_sizes, acceleration, diis_size, diis_start, diis_damping, trust_radius,
               return_density, return_fock):
-    """cpp_hf_native.cpp:418-485 (linear mixing)."""
+    """cpp_hf_native.cpp:418-485 (linear mixing, C-DIIS, ODA, trust radius)."""
     lib = _lib_handle()
     acc = str(acceleration)
     if acc not in ("linear", "diis", "oda"):
         raise ValueError("SCFConfig.acceleration must be 'linear', 'diis', or 'oda'")
-    if acc != "linear":
-        raise NotImplementedError(f"SCF acceleration {acc!r} is not built into cpp_hf_b200")
-    if float(trust_radius) > 0.0:
-        raise NotImplementedError("SCF trust_radius is not built into cpp_hf_b200")
     as_np = not _is_torch(P0)
     dk = _DeviceKernel(kernel_args)
     P0_t = _to_dev(P0, "c")
@@ -505,7 +501,9 @@ def solve_scf(kernel_args, P0, n_e, max_iter, density_tol, comm_tol, mixing, lev
     cfg.max_iter = max_iter
     cfg.density_tol, cfg.comm_tol = float(density_tol), float(comm_tol)
     cfg.mixing, cfg.level_shift = float(mixing), float(level_shift)
-    cfg.acceleration = 0
+    cfg.acceleration = {"linear": 0, "diis": 1, "oda": 2}[acc]
+    cfg.diis_size, cfg.diis_start = int(diis_size), int(diis_start)
+    cfg.diis_damping, cfg.trust_radius = float(diis_damping), float(trust_radius)
     cfg.mixed_switch_tol = dk.mixed_switch
     D = torch.empty_like(P0_t) if return_density else None
     F = torch.empty_like(P0_t) if return_fock else None
@@ -515,7 +513,7 @@ def solve_scf(kernel_args, P0, n_e, max_iter, density_tol, comm_tol, mixing, lev
     res = _lib.ScfResult()
     errors = []
     cb = _project_callback(project_fn, errors)
-    ws = _ws(lib.cpphf_solve_scf_workspace_bytes(dk.ref()))
+    ws = _ws(lib.cpphf_solve_scf_workspace_bytes_cfg(dk.ref(), C.byref(cfg)))
     check(lib.cpphf_solve_scf(dk.ref(), C.byref(cfg), _ptr(P0_t), float(n_e), cb, None, _ptr(D), _ptr(F),
                               hE.ctypes.data_as(_lib.dp), hD.ctypes.data_as(_lib.dp),
                               hC.ctypes.data_as(_lib.dp), C.byref(res), _ptr(ws), ws.numel(), _stream()),

@@ -83,7 +83,7 @@ __global__ void k_fermi(const double* __restrict__ e, const double* __restrict__
 template <bool WARP>
 __global__ void k_scf_residuals(const double2* __restrict__ F, const double2* __restrict__ D,
                                 const double2* __restrict__ Pn, const double* __restrict__ w, int64_t nk, int nb,
-                                DmScalars* S) {
+                                DmScalars* S, double2* __restrict__ comm_out) {
     extern __shared__ __align__(16) unsigned char raw[];
     __shared__ double red[64];
     Team<WARP> t;
@@ -108,6 +108,7 @@ __global__ void k_scf_residuals(const double2* __restrict__ F, const double2* __
                 cfma(pf, Ds[i * ld + l], Fs[l * ld + j]);
             }
             const double2 c = csub(fp, pf);
+            if (comm_out) comm_out[(size_t)k * nb * nb + e] = c;
             sc += c.x * c.x + c.y * c.y;
         }
         v[0] += wk * sd;
@@ -122,7 +123,7 @@ __global__ void k_scf_residuals(const double2* __restrict__ F, const double2* __
 }
 
 // density <- herm(density + mixing (P_new - density))  (solver_scf.hpp:395-401)
-__global__ void k_scf_mix(double2* D, const double2* __restrict__ Pn, double mixing, int64_t nk, int nb) {
+__global__ void k_scf_mix(const double2* D, const double2* Pn, double mixing, double2* out, int64_t nk, int nb) {
     const int npair = nb * (nb + 1) / 2;
     const int64_t total = nk * npair;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
@@ -138,9 +139,154 @@ __global__ void k_scf_mix(double2* D, const double2* __restrict__ Pn, double mix
         const double2 a = cadd(dij, cscale(csub(Pn[ij], dij), mixing));
         const double2 b = cadd(dji, cscale(csub(Pn[ji], dji), mixing));
         const double2 h = mk(0.5 * (a.x + b.x), 0.5 * (a.y - b.y));
-        D[ij] = h;
-        D[ji] = cconj(h);
+        out[ij] = h;
+        out[ji] = cconj(h);
     }
+}
+
+// ---------------------------------------------------------------------------
+// SCF acceleration (solver_scf.hpp:253-428)
+// ---------------------------------------------------------------------------
+constexpr int kDiisMax = 16;  // history slots a launch handles
+
+struct FieldSet {
+    const double2* p[kDiisMax];
+};
+
+// out[i] = sum_k w_k Re sum_a conj(H_i[k, a]) Rn[k, a] for the m history
+// residuals H_i (the new row of the C-DIIS matrix B, solver_scf.hpp:273-289)
+__global__ void k_diis_dots(FieldSet H, int m, const double2* __restrict__ Rn, const double* __restrict__ w,
+                            int64_t nk, int nb2, DmScalars* S, double* __restrict__ out) {
+    __shared__ double red[32 * kDiisMax];
+    double v[kDiisMax];
+#pragma unroll
+    for (int i = 0; i < kDiisMax; ++i) v[i] = 0.0;
+    const int64_t n = nk * nb2;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        const double wk = w[e / nb2];
+        const double2 r = Rn[e];
+#pragma unroll
+        for (int i = 0; i < kDiisMax; ++i) {
+            if (i < m) {
+                const double2 a = H.p[i][e];
+                v[i] += wk * (a.x * r.x + a.y * r.y);
+            }
+        }
+    }
+    double o[kDiisMax];
+    if (reduce_last_block<kDiisMax>(v, S->part, &S->counter, o, red) && threadIdx.x == 0)
+        for (int i = 0; i < m; ++i) out[i] = o[i];
+}
+
+// Fex = damp sum_i c_i F_i + (1 - damp) Fcur, summed in history order
+// (solver_scf.hpp:305-320); the caller hermitizes
+struct DiisCoef {
+    double c[kDiisMax];
+};
+__global__ void k_diis_extrapolate(FieldSet Fh, DiisCoef cf, int m, double damp, const double2* __restrict__ Fcur,
+                                   double2* __restrict__ Fex, int64_t n) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        double2 acc = mk(0.0, 0.0);
+#pragma unroll
+        for (int i = 0; i < kDiisMax; ++i) {
+            if (i < m) {
+                const double2 f = Fh.p[i][e];
+                acc = mk(acc.x + cf.c[i] * f.x, acc.y + cf.c[i] * f.y);
+            }
+        }
+        if (damp < 1.0) {
+            const double2 f = Fcur[e];
+            acc = mk(damp * acc.x + (1.0 - damp) * f.x, damp * acc.y + (1.0 - damp) * f.y);
+        }
+        Fex[e] = acc;
+    }
+}
+
+// c1 = sum_k w_k Re tr(F_k (Pn_k - D_k)) (ODA slope, solver_scf.hpp:362-374)
+__global__ void k_oda_c1(const double2* __restrict__ F, const double2* __restrict__ D, const double2* __restrict__ Pn,
+                         const double* __restrict__ w, int64_t nk, int nb, DmScalars* S, double* __restrict__ out) {
+    __shared__ double red[32];
+    double v[1] = {0.0};
+    const int nb2 = nb * nb;
+    const int64_t n = nk * nb2;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = e / nb2;
+        const int r = (int)(e - k * nb2), a = r / nb, b = r - a * nb;
+        const size_t ba = (size_t)k * nb2 + (size_t)b * nb + a;
+        const double2 f = F[e];
+        const double2 d = csub(Pn[ba], D[ba]);
+        v[0] += w[k] * (f.x * d.x - f.y * d.y);
+    }
+    double o[1];
+    if (reduce_last_block<1>(v, S->part, &S->counter, o, red) && threadIdx.x == 0) *out = o[0];
+}
+
+// sum_k w_k ||A_k - B_k||_F^2 (weighted_difference_norm before its division,
+// solver_scf.hpp:77-91)
+__global__ void k_wdiff2(const double2* __restrict__ A, const double2* __restrict__ B, const double* __restrict__ w,
+                         int64_t nk, int nb2, DmScalars* S, double* __restrict__ out) {
+    __shared__ double red[32];
+    double v[1] = {0.0};
+    const int64_t n = nk * nb2;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        const double2 d = csub(A[e], B[e]);
+        v[0] += w[e / nb2] * (d.x * d.x + d.y * d.y);
+    }
+    double o[1];
+    if (reduce_last_block<1>(v, S->part, &S->counter, o, red) && threadIdx.x == 0) *out = o[0];
+}
+
+// Solve [B -1; -1^T 0] [c; l] = [0; -1] (size n = m + 1, row-major A) by
+// Gaussian elimination with complete pivoting.  False when the matrix is
+// rank-deficient at the threshold of Eigen's FullPivLU::isInvertible (a pivot
+// below eps * n * |first pivot|, the reference's check, solver_scf.hpp:291-300)
+// or the solution is not finite.
+bool diis_solve(std::vector<double> A, int n, std::vector<double>& x) {
+    std::vector<double> b((size_t)n, 0.0);
+    b[(size_t)n - 1] = -1.0;
+    std::vector<int> colp((size_t)n);
+    for (int i = 0; i < n; ++i) colp[(size_t)i] = i;
+    double maxpiv = 0.0;
+    const double thr = std::numeric_limits<double>::epsilon() * n;
+    for (int kk = 0; kk < n; ++kk) {
+        int pr = kk, pc = kk;
+        double best = -1.0;
+        for (int i = kk; i < n; ++i)
+            for (int j = kk; j < n; ++j)
+                if (std::fabs(A[(size_t)i * n + j]) > best) {
+                    best = std::fabs(A[(size_t)i * n + j]);
+                    pr = i;
+                    pc = j;
+                }
+        if (kk == 0) maxpiv = best;
+        if (!(best > thr * maxpiv) || best == 0.0) return false;
+        if (pr != kk) {
+            for (int j = 0; j < n; ++j) std::swap(A[(size_t)kk * n + j], A[(size_t)pr * n + j]);
+            std::swap(b[(size_t)kk], b[(size_t)pr]);
+        }
+        if (pc != kk) {
+            for (int i = 0; i < n; ++i) std::swap(A[(size_t)i * n + kk], A[(size_t)i * n + pc]);
+            std::swap(colp[(size_t)kk], colp[(size_t)pc]);
+        }
+        const double piv = A[(size_t)kk * n + kk];
+        for (int i = kk + 1; i < n; ++i) {
+            const double f = A[(size_t)i * n + kk] / piv;
+            if (f == 0.0) continue;
+            for (int j = kk; j < n; ++j) A[(size_t)i * n + j] -= f * A[(size_t)kk * n + j];
+            b[(size_t)i] -= f * b[(size_t)kk];
+        }
+    }
+    std::vector<double> y((size_t)n);
+    for (int i = n - 1; i >= 0; --i) {
+        double acc = b[(size_t)i];
+        for (int j = i + 1; j < n; ++j) acc -= A[(size_t)i * n + j] * y[(size_t)j];
+        y[(size_t)i] = acc / A[(size_t)i * n + i];
+    }
+    x.assign((size_t)n, 0.0);
+    for (int i = 0; i < n; ++i) x[(size_t)colp[(size_t)i]] = y[(size_t)i];
+    for (int i = 0; i < n - 1; ++i)
+        if (!std::isfinite(x[(size_t)i])) return false;
+    return true;
 }
 
 unsigned grid_for(int64_t n, int threads) {
@@ -517,9 +663,12 @@ namespace {
 struct ScfLayout {
     size_t D, Sig, F, Pn, V, eps, sh, occ, S, fock_ws, mu_ws, mu2, total;
     size_t fock_bytes, mu_bytes;
+    size_t R, Fh, Fex, dots, Sn, Fn, Dpre;  // acceleration extras (0 when unused)
+    int nhist;
 };
 
-ScfLayout scf_layout(const cpphf_kernel* K) {
+// cfg == null: linear mixing without a trust radius
+ScfLayout scf_layout(const cpphf_kernel* K, const cpphf_scf_config* cfg = nullptr) {
     const size_t nk = (size_t)K->nk1 * K->nk2, nb = (size_t)K->nb;
     const size_t fld = sizeof(double2) * nk * nb * nb, vec = sizeof(double) * nk * nb;
     SolverWs W;
@@ -538,6 +687,20 @@ ScfLayout scf_layout(const cpphf_kernel* K) {
     L.fock_ws = W.take(L.fock_bytes);
     L.mu_bytes = mu_workspace_bytes((int64_t)nk, (int64_t)nb);
     L.mu_ws = W.take(L.mu_bytes);
+    L.R = L.Fh = L.Fex = L.dots = L.Sn = L.Fn = L.Dpre = 0;
+    L.nhist = 0;
+    if (cfg && cfg->acceleration == 1) {
+        L.nhist = std::max(1, std::min<int>(cfg->diis_size, kDiisMax));
+        L.R = W.take(fld * (size_t)L.nhist);
+        L.Fh = W.take(fld * (size_t)L.nhist);
+        L.Fex = W.take(fld);
+        L.dots = W.take(sizeof(double) * kDiisMax);
+    }
+    if (cfg && cfg->acceleration == 2) {
+        L.Sn = W.take(fld);
+        L.Fn = W.take(fld);
+    }
+    if (cfg && cfg->trust_radius > 0.0) L.Dpre = W.take(fld);
     L.total = W.total;
     return L;
 }
@@ -545,17 +708,23 @@ ScfLayout scf_layout(const cpphf_kernel* K) {
 }  // namespace
 
 size_t solve_scf_workspace_bytes(const cpphf_kernel* K) { return scf_layout(K).total; }
+size_t solve_scf_workspace_bytes_cfg(const cpphf_kernel* K, const cpphf_scf_config* cfg) {
+    return scf_layout(K, cfg).total;
+}
 
 int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2* P0, double n_e,
               cpphf_project_fn project, void* puser, double2* D_out, double2* F_out, double* hist_E, double* hist_D,
               double* hist_C, cpphf_scf_result* res, void* ws, size_t wsb, cudaStream_t st) {
     CPPHF_TRY(validate_kernel(K));
     if (!cfg || !P0 || !res) return fail(CPPHF_ERR_INVALID, "solve_scf: null argument");
-    if (cfg->acceleration != 0)
-        return fail(CPPHF_ERR_UNSUPPORTED, "SCF acceleration 'diis'/'oda' is not built into this library");
+    if (cfg->acceleration < 0 || cfg->acceleration > 2)
+        return fail(CPPHF_ERR_INVALID, "SCFConfig.acceleration must be 'linear', 'diis', or 'oda'");
+    if (cfg->acceleration == 1 && cfg->diis_size < 1) return fail(CPPHF_ERR_INVALID, "SCF diis_size must be positive");
+    if (cfg->acceleration == 1 && cfg->diis_size > kDiisMax)
+        return fail(CPPHF_ERR_UNSUPPORTED, "SCF diis_size above " + std::to_string(kDiisMax) + " is not supported");
     CPPHF_TRY(dm_check_nb(K->nb));
     CPPHF_TRY(check_mixed(K, cfg->mixed_switch_tol));
-    const ScfLayout L = scf_layout(K);
+    const ScfLayout L = scf_layout(K, cfg);
     if (!ws || wsb < L.total)
         return fail(CPPHF_ERR_INVALID, "solve_scf: workspace too small (" + std::to_string(L.total) + " bytes needed)");
     unsigned char* W = static_cast<unsigned char*>(ws);
@@ -588,16 +757,9 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
     // D is exactly Hermitian after the mixing kernel (it writes h and conj(h)) and
     // after a copy of P_new; hermitizing it again is a bitwise no-op and is skipped
     bool d_hermitian = false;
-    auto build_and_occupy = [&]() -> int {
-        if (project) CPPHF_TRY(call_project(project, puser, D, K, st));
-        if (project || !d_hermitian) CPPHF_TRY(hermitize(D, D, nk, nb, st));
-        CPPHF_TRY(build_fock(low ? &K32 : K, D, Sig, F, nullptr, &S->energy, nullptr, fws, L.fock_bytes, st));
-        if (project) {
-            CPPHF_TRY(call_project(project, puser, F, K, st));
-            CPPHF_TRY(hermitize(F, F, nk, nb, st));
-        }
-        // density_from_fock (solver_scf.hpp:96-154)
-        CPPHF_TRY(eigh_batched(F, eps, V, nk, nb, 0, nullptr, st));
+    // density_from_fock (solver_scf.hpp:96-154): P_out = herm(V f V^H) from Fsrc
+    auto occupy = [&](const double2* Fsrc, double2* Pout) -> int {
+        CPPHF_TRY(eigh_batched(Fsrc, eps, V, nk, nb, 0, nullptr, st));
         CPPHF_TRY(mu_solve(eps, K->w2d, nk, nb, n_e, nullptr, K->T, 30, 0, &mu2[0], mws, L.mu_bytes, st));
         const double* e_occ = eps;
         if (cfg->level_shift != 0.0) {
@@ -613,10 +775,30 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
         CPPHF_LAUNCH_CHECK("fermi");
         // dm_density writes (X + X^H) / 2, exactly Hermitian: only a projector needs
         // the hermitisation again
-        CPPHF_TRY(dm_density(V, occ, Pn, nk, nb, st));
+        CPPHF_TRY(dm_density(V, occ, Pout, nk, nb, st));
         if (project) {
-            CPPHF_TRY(call_project(project, puser, Pn, K, st));
-            CPPHF_TRY(hermitize(Pn, Pn, nk, nb, st));
+            CPPHF_TRY(call_project(project, puser, Pout, K, st));
+            CPPHF_TRY(hermitize(Pout, Pout, nk, nb, st));
+        }
+        return CPPHF_OK;
+    };
+    auto build_and_occupy = [&]() -> int {
+        if (project) CPPHF_TRY(call_project(project, puser, D, K, st));
+        if (project || !d_hermitian) CPPHF_TRY(hermitize(D, D, nk, nb, st));
+        CPPHF_TRY(build_fock(low ? &K32 : K, D, Sig, F, nullptr, &S->energy, nullptr, fws, L.fock_bytes, st));
+        if (project) {
+            CPPHF_TRY(call_project(project, puser, F, K, st));
+            CPPHF_TRY(hermitize(F, F, nk, nb, st));
+        }
+        return occupy(F, Pn);
+    };
+    // density <- herm(A + s (B - A)), then the projector
+    auto mix_into_D = [&](const double2* A, const double2* B, double s_) -> int {
+        k_scf_mix<<<grid_for(nk * (int64_t)nb * (nb + 1) / 2, 256), 256, 0, st>>>(A, B, s_, D, nk, nb);
+        CPPHF_LAUNCH_CHECK("scf mix");
+        if (project) {
+            CPPHF_TRY(call_project(project, puser, D, K, st));
+            CPPHF_TRY(hermitize(D, D, nk, nb, st));
         }
         return CPPHF_OK;
     };
@@ -636,13 +818,53 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
         raise_smem(k_scf_residuals<true>);
         raise_smem(k_scf_residuals<false>);
     });
+
+    // acceleration state
+    const int acc = cfg->acceleration;
+    const int64_t nel = nk * (int64_t)nb * nb;
+    const int nb2 = nb * nb;
+    const unsigned egrid = grid_for(nel, 256);
+    // reductions with up to kDiisMax values per block must fit S->part
+    const unsigned rgrid = std::min<unsigned>(egrid, (unsigned)((3 * kDmMaxPartials) / kDiisMax));
+    double2* Rh = acc == 1 ? fld(L.R) : nullptr;
+    double2* Fh = acc == 1 ? fld(L.Fh) : nullptr;
+    double2* Fex = acc == 1 ? fld(L.Fex) : nullptr;
+    double* dots = acc == 1 ? reinterpret_cast<double*>(W + L.dots) : nullptr;
+    double2* Sn = acc == 2 ? fld(L.Sn) : nullptr;
+    double2* Fn = acc == 2 ? fld(L.Fn) : nullptr;
+    double2* Dpre = cfg->trust_radius > 0.0 ? fld(L.Dpre) : nullptr;
+    const int nh = L.nhist;
+    int hcount = 0, hhead = 0;  // DIIS ring: entries held, next slot
+    // Bs[a * kDiisMax + b] = <R_a, R_b>_w for ring slots a, b
+    std::vector<double> Bs((size_t)kDiisMax * kDiisMax, 0.0);
+    double dbuf[kDiisMax];
+
     while (k < max_iter && !converged) {
         CPPHF_TRY(build_and_occupy());
+        // the new C-DIIS residual goes to the slot after the newest entry
+        // (overwriting the oldest when the ring is full)
+        double2* comm_out = acc == 1 ? Rh + (size_t)hhead * nel : nullptr;
         if (warp)
-            k_scf_residuals<true><<<tgrid, 32 * kWarpTeams, rsmem, st>>>(F, D, Pn, K->w2d, nk, nb, S);
+            k_scf_residuals<true><<<tgrid, 32 * kWarpTeams, rsmem, st>>>(F, D, Pn, K->w2d, nk, nb, S, comm_out);
         else
-            k_scf_residuals<false><<<tgrid, kCtaTeamThreadsDense, rsmem, st>>>(F, D, Pn, K->w2d, nk, nb, S);
+            k_scf_residuals<false><<<tgrid, kCtaTeamThreadsDense, rsmem, st>>>(F, D, Pn, K->w2d, nk, nb, S,
+                                                                                comm_out);
         CPPHF_LAUNCH_CHECK("scf residuals");
+        int nslots = 0;
+        int slots[kDiisMax];
+        if (acc == 1) {
+            // the history after this entry is added (oldest first), and the new
+            // row of B: <R_slot, R_new> for each of its slots
+            CPPHF_CUDA(cudaMemcpyAsync(Fh + (size_t)hhead * nel, F, fbytes, cudaMemcpyDeviceToDevice, st));
+            const int m = std::min(hcount + 1, nh);
+            for (int i = 0; i < m; ++i) slots[i] = ((hhead - (m - 1) + i) % nh + nh) % nh;
+            nslots = m;
+            FieldSet Hs;
+            for (int i = 0; i < kDiisMax; ++i) Hs.p[i] = Rh + (size_t)slots[i < m ? i : 0] * nel;
+            k_diis_dots<<<rgrid, 256, 0, st>>>(Hs, m, comm_out, K->w2d, nk, nb2, S, dots);
+            CPPHF_LAUNCH_CHECK("diis dots");
+            CPPHF_CUDA(cudaMemcpyAsync(dbuf, dots, sizeof(double) * m, cudaMemcpyDeviceToHost, st));
+        }
         // energy, grad_norm (density residual) and lam_pc (commutator residual) are
         // adjacent in DmScalars: one copy, plus mu
         static_assert(offsetof(DmScalars, lam_pc) == offsetof(DmScalars, energy) + 2 * sizeof(double),
@@ -652,6 +874,7 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
         CPPHF_CUDA(cudaStreamSynchronize(st));
         if (!std::isfinite(hbuf[3]))
             return fail(CPPHF_ERR_TIMEOUT, "solve_scf: chemical-potential solve failed (device wait timeout or non-finite)");
+        const double E_it = hbuf[0];
         const double d_res = std::sqrt(hbuf[1] / wsum);
         const double c_res = std::sqrt(hbuf[2] / wsum);
         converged = (d_res <= cfg->density_tol) && (c_res <= cfg->comm_tol);
@@ -660,18 +883,79 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
             low = false;
             converged = false;
         }
+        if (Dpre && !converged) CPPHF_CUDA(cudaMemcpyAsync(Dpre, D, fbytes, cudaMemcpyDeviceToDevice, st));
         d_hermitian = true;
         if (converged) {
             CPPHF_CUDA(cudaMemcpyAsync(D, Pn, fbytes, cudaMemcpyDeviceToDevice, st));
-        } else {
-            k_scf_mix<<<grid_for(nk * (int64_t)nb * (nb + 1) / 2, 256), 256, 0, st>>>(D, Pn, cfg->mixing, nk, nb);
-            CPPHF_LAUNCH_CHECK("scf mix");
-            if (project) {
-                CPPHF_TRY(call_project(project, puser, D, K, st));
-                CPPHF_TRY(hermitize(D, D, nk, nb, st));
+        } else if (acc == 1) {
+            // ---- C-DIIS (solver_scf.hpp:253-349) ----
+            const int m = nslots;
+            const int newest = slots[m - 1];
+            for (int i = 0; i < m; ++i) {
+                Bs[(size_t)slots[i] * kDiisMax + newest] = dbuf[i];
+                Bs[(size_t)newest * kDiisMax + slots[i]] = dbuf[i];
             }
+            hcount = m;
+            hhead = (hhead + 1) % nh;
+            bool diis_ok = false;
+            std::vector<double> sol;
+            if (m >= std::max(2, (int)cfg->diis_start)) {
+                const int n = m + 1;
+                std::vector<double> A((size_t)n * n, 0.0);
+                for (int i = 0; i < m; ++i) {
+                    for (int j = 0; j < m; ++j) A[(size_t)i * n + j] = Bs[(size_t)slots[i] * kDiisMax + slots[j]];
+                    A[(size_t)i * n + m] = -1.0;
+                    A[(size_t)m * n + i] = -1.0;
+                }
+                diis_ok = diis_solve(A, n, sol);
+            }
+            if (diis_ok) {
+                FieldSet Fs;
+                DiisCoef cf;
+                for (int i = 0; i < kDiisMax; ++i) {
+                    Fs.p[i] = Fh + (size_t)slots[i < m ? i : 0] * nel;
+                    cf.c[i] = i < m ? sol[(size_t)i] : 0.0;
+                }
+                const double damp = std::min(std::max(cfg->diis_damping, 0.0), 1.0);
+                k_diis_extrapolate<<<egrid, 256, 0, st>>>(Fs, cf, m, damp, F, Fex, nel);
+                CPPHF_LAUNCH_CHECK("diis extrapolate");
+                CPPHF_TRY(hermitize(Fex, Fex, nk, nb, st));
+                CPPHF_TRY(occupy(Fex, D));
+            } else {
+                CPPHF_TRY(mix_into_D(D, Pn, cfg->mixing));
+            }
+        } else if (acc == 2) {
+            // ---- ODA (solver_scf.hpp:350-392): E(lambda) quadratic, one extra build ----
+            CPPHF_TRY(build_fock(low ? &K32 : K, Pn, Sn, Fn, nullptr, &mu2[2], nullptr, fws, L.fock_bytes, st));
+            k_oda_c1<<<rgrid, 256, 0, st>>>(F, D, Pn, K->w2d, nk, nb, S, &mu2[3]);
+            CPPHF_LAUNCH_CHECK("oda slope");
+            double e2[2];
+            CPPHF_CUDA(cudaMemcpyAsync(e2, &mu2[2], 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+            CPPHF_CUDA(cudaStreamSynchronize(st));
+            const double c1 = e2[1];
+            const double c2 = (e2[0] - E_it) - c1;
+            double lam;
+            if (c2 > 1.0e-12)
+                lam = std::min(std::max(-c1 / (2.0 * c2), 0.0), 1.0);
+            else if (c1 < 0.0)
+                lam = 1.0;
+            else
+                lam = 0.0;
+            CPPHF_TRY(mix_into_D(D, Pn, lam));
+        } else {
+            CPPHF_TRY(mix_into_D(D, Pn, cfg->mixing));
         }
-        if (hist_E) hist_E[k] = hbuf[0];
+        if (Dpre && !converged) {
+            // ---- trust-radius clip (solver_scf.hpp:410-428) ----
+            k_wdiff2<<<rgrid, 256, 0, st>>>(D, Dpre, K->w2d, nk, nb2, S, &mu2[2]);
+            CPPHF_LAUNCH_CHECK("trust step norm");
+            double s2 = 0.0;
+            CPPHF_CUDA(cudaMemcpyAsync(&s2, &mu2[2], sizeof(double), cudaMemcpyDeviceToHost, st));
+            CPPHF_CUDA(cudaStreamSynchronize(st));
+            const double step = std::sqrt(s2 / wsum);
+            if (step > cfg->trust_radius) CPPHF_TRY(mix_into_D(Dpre, D, cfg->trust_radius / step));
+        }
+        if (hist_E) hist_E[k] = E_it;
         if (hist_D) hist_D[k] = d_res;
         if (hist_C) hist_C[k] = c_res;
         ++k;
@@ -767,6 +1051,10 @@ int cpphf_solve_dm(const cpphf_kernel* K, const cpphf_dm_config* cfg, const void
 }
 
 size_t cpphf_solve_scf_workspace_bytes(const cpphf_kernel* K) { return K ? cpphf::solve_scf_workspace_bytes(K) : 0; }
+
+size_t cpphf_solve_scf_workspace_bytes_cfg(const cpphf_kernel* K, const cpphf_scf_config* cfg) {
+    return K ? cpphf::solve_scf_workspace_bytes_cfg(K, cfg) : 0;
+}
 
 int cpphf_solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const void* P0, double n_e,
                     cpphf_project_fn project, void* project_user, void* density_out, void* fock_out,

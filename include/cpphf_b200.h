@@ -254,7 +254,7 @@ typedef struct cpphf_scf_config {
     double comm_tol;
     double mixing;
     double level_shift;
-    int32_t acceleration;
+    int32_t acceleration; /* 0 linear mixing, 1 C-DIIS, 2 ODA */
     int32_t reserved;
     /* Switched precision (no counterpart in the reference): > 0 runs the exchange
      * in complex64 until the density residual ||P_new - P||_w and the commutator
@@ -262,6 +262,15 @@ typedef struct cpphf_scf_config {
      * (K->exchange_precision must be 64); convergence is only accepted in the
      * complex128 phase.  0 = plain. */
     double mixed_switch_tol;
+    /* acceleration 1 (C-DIIS): history length, first iteration count at which
+     * extrapolation starts (at least 2), damping of the extrapolated Fock towards
+     * the current one (1 = none); acceleration 2 = ODA (one extra Fock build per
+     * iteration).  trust_radius > 0 clips each density step to that weighted
+     * norm.  (solver_scf.hpp:200-428, SCFConfig in reference_scf.py:18-57) */
+    int32_t diis_size;
+    int32_t diis_start;
+    double diis_damping;
+    double trust_radius;
 } cpphf_scf_config;
 
 typedef struct cpphf_scf_result {
@@ -276,6 +285,11 @@ typedef struct cpphf_scf_result {
  * density_out / fock_out device fields (may be NULL); hist_* HOST arrays of
  * max_iter doubles. */
 size_t cpphf_solve_scf_workspace_bytes(const cpphf_kernel* K);
+/* Workspace of a solve with a given configuration: the DIIS history (2 x
+ * diis_size fields and the extrapolated Fock), the ODA trial build (2 fields)
+ * and the trust-radius snapshot (1 field) come on top of the linear-mixing
+ * size above. */
+size_t cpphf_solve_scf_workspace_bytes_cfg(const cpphf_kernel* K, const cpphf_scf_config* cfg);
 int cpphf_solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const void* P0, double n_e,
                     cpphf_project_fn project, void* project_user, void* density_out,
                     void* fock_out, double* hist_E, double* hist_density, double* hist_comm,

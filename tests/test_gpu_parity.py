@@ -413,6 +413,61 @@ def test_solve_scf_meshgrid_regression_case(native):
     assert abs(out[8][0] - float(d["hist_dC_expected"][0])) < 1e-6
 
 
+def _scf_acc(mod, args, P0, n_e, acc, diis_size=6, diis_start=2, damping=1.0, trust=0.0, max_iter=200, tol=1e-9,
+             project_fn=None):
+    return mod.solve_scf(args, P0, n_e, max_iter, tol, tol, 0.5, 0.0, project_fn, [], acc, diis_size, diis_start,
+                         damping, trust, True, True)
+
+
+@pytest.mark.parametrize("acc,diis_size,diis_start,damping,trust,max_iter", [
+    ("diis", 6, 2, 1.0, 0.0, 200), ("diis", 3, 2, 0.7, 0.0, 200), ("diis", 4, 3, 1.0, 0.05, 200),
+    ("oda", 6, 2, 1.0, 0.0, 15), ("oda", 6, 2, 1.0, 0.02, 15), ("linear", 6, 2, 1.0, 0.03, 30)])
+@pytest.mark.parametrize("case", ["dirac8", "layered6"])
+def test_solve_scf_acceleration_matches_oracle(native, oracle, acc, diis_size, diis_start, damping, trust, max_iter,
+                                                case):
+    """C-DIIS (history ring, B matrix from the new residual's inner products,
+    complete-pivoting solve with the rank test, extrapolated Fock), ODA (extra
+    build at P_new, analytic step) and the trust-radius clip against the oracle's
+    restatement of solver_scf.hpp:253-428.  ODA and the clipped linear runs stall
+    on these models (the reference's ODA takes lambda = 0 once c1, c2 reach the
+    rounding level), so they are compared over their first iterations."""
+    args, P0, n_e = workloads.dirac(8, seed=3) if case == "dirac8" else workloads.layered(6, n_layers=2, seed=1)
+    got = _scf_acc(native, args, P0, n_e, acc, diis_size, diis_start, damping, trust, max_iter=max_iter)
+    ref = _scf_acc(oracle, args, P0, n_e, acc, diis_size, diis_start, damping, trust, max_iter=max_iter)
+    print(f"scf {acc} size {diis_size} start {diis_start} damp {damping} trust {trust}: iterations gpu {got[4]} "
+          f"oracle {ref[4]}, |dE| {abs(got[2] - ref[2]):.2e}")
+    assert got[5] == ref[5]
+    assert abs(got[2] - ref[2]) < 1e-9 * max(1.0, abs(ref[2]))
+    assert rel(got[0], ref[0]) < 1e-7
+    assert abs(got[4] - ref[4]) <= 1
+    n = min(len(got[6]), len(ref[6]))
+    np.testing.assert_allclose(got[6][:n], ref[6][:n], rtol=1e-9, atol=1e-12)
+
+
+def test_solve_scf_diis_meshgrid_regression_case(native, oracle):
+    """The reference's stored SCF case (Hartree, exchange, reference density) with
+    C-DIIS: GPU against the oracle."""
+    from conftest import GOLDEN
+
+    d = np.load(GOLDEN / "meshgrid_scf_v1.npz")
+    args = problem.kernel_args(d["weights"], d["hamiltonian"], d["coulomb_q"], float(d["T"]),
+                               include_hartree=True, include_exchange=True,
+                               reference_density=d["reference_density"], hartree_matrix=d["hartree_matrix"])
+    P0, n_e = np.asarray(d["P0"]), float(d["electrondensity0"])
+    got = _scf_acc(native, args, P0, n_e, "diis", max_iter=60, tol=1e-8)
+    ref = _scf_acc(oracle, args, P0, n_e, "diis", max_iter=60, tol=1e-8)
+    print(f"meshgrid DIIS: iterations gpu {got[4]} oracle {ref[4]}, |dE| {abs(got[2] - ref[2]):.2e}")
+    assert got[5] and ref[5]
+    assert abs(got[2] - ref[2]) < 1e-9 * max(1.0, abs(ref[2]))
+    assert abs(got[4] - ref[4]) <= 1
+
+
+def test_solve_scf_rejects_bad_diis_size(native):
+    args, P0, n_e = workloads.dirac(4, seed=0)
+    with pytest.raises(ValueError, match="diis_size"):
+        _scf_acc(native, args, P0, n_e, "diis", diis_size=0)
+
+
 def test_solve_scf_rejects_unknown_acceleration(native):
     args, P0, n_e = workloads.dirac(4, seed=0)
     with pytest.raises(ValueError, match="acceleration"):
