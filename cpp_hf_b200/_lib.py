@@ -62,7 +62,7 @@ class DmConfig(C.Structure):
         ("denom_scale", f64), ("max_step", f64), ("cg_restart", i64), ("bt_shrink", f64),
         ("bt_max", i64), ("mu_maxiter", i32), ("optimizer", i32),
         ("block_sizes", C.POINTER(i64)), ("n_block_sizes", i64), ("mixed_switch_grad", f64),
-        ("graphs", i32), ("reserved_dm", i32),
+        ("graphs", i32), ("project_device", i32),
     ]
 
 
@@ -83,6 +83,14 @@ class ScfResult(C.Structure):
 
 
 PROJECT_FN = C.CFUNCTYPE(C.c_int, vp, vp, i64, i64, i64, vp)
+
+
+class Symmetry(C.Structure):
+    _fields_ = [
+        ("unitary_group", vp), ("n_unitary", i64), ("spatial_group", vp), ("n_spatial", i64),
+        ("spatial_convention", i32), ("spatial_axes", i32), ("time_reversal_U", vp), ("tr_convention", i32),
+        ("tr_axes", i32), ("scratch", vp),
+    ]
 
 # name -> (restype, argtypes)
 _SIGS = {
@@ -129,6 +137,9 @@ _SIGS = {
     "cpphf_density_from_fock_backward": (C.c_int, [vp, vp, vp, f64, vp, vp, vp, i64, i64, vp, sz, vp]),
     "cpphf_solve_scf_workspace_bytes": (sz, [C.POINTER(Kernel)]),
     "cpphf_solve_scf_workspace_bytes_cfg": (sz, [C.POINTER(Kernel), C.POINTER(ScfConfig)]),
+    "cpphf_resample_kgrid_2d": (C.c_int, [vp, vp, i64, i64, i64, vp]),
+    "cpphf_symmetry_project": (C.c_int, [C.POINTER(Symmetry), vp, i64, i64, i64, vp]),
+    "cpphf_symmetry_project_fn": (C.c_int, [vp, vp, i64, i64, i64, vp]),
     "cpphf_solve_scf": (C.c_int, [C.POINTER(Kernel), C.POINTER(ScfConfig), vp, f64, PROJECT_FN, vp,
                                   vp, vp, dp, dp, dp, C.POINTER(ScfResult), vp, sz, vp]),
 }

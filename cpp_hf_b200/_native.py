@@ -8,8 +8,8 @@ stay on the device as tensors.  Every computation runs in the CUDA library on
 ``torch.cuda.current_stream()``; there is no CPU fallback.
 
 Outside the hot path and not built: the trust-region Newton optimiser
-(``optimizer=1``, ``_rtr_joint_hvp``, ``_deflation_bias``) and SCF DIIS / ODA
-acceleration raise ``NotImplementedError``.
+(``optimizer=1``, ``_rtr_joint_hvp``, ``_deflation_bias``) raises
+``NotImplementedError``.
 """
 
 from __future__ import annotations
@@ -21,6 +21,7 @@ import numpy as np
 import torch
 
 from . import _lib
+from . import symmetry as _symmetry
 from ._lib import check
 
 __all__ = [
@@ -405,13 +406,35 @@ def build_fock_apply(kernel_args, P, project_fn):
     check(lib.cpphf_build_fock(dk.ref(), _ptr(P_t), _ptr(Sigma), _ptr(F), _ptr(hd), _ptr(E), _ptr(H),
                                _ptr(ws), ws.numel(), _stream()), "build_fock_apply")
     if project_fn is not None:
-        F = _host_project(project_fn, F)
+        dproj = _symmetry.device_projector(project_fn)
+        if dproj is None:
+            F = _host_project(project_fn, F)
+        elif not dproj.is_identity:
+            dproj.project_(F)
+            F = 0.5 * (F + F.conj().transpose(-1, -2))
     return _out(Sigma, as_np), _out(H, as_np), _out(F, as_np), float(E.item())
 
 
 # ---------------------------------------------------------------------------
 # solvers
 # ---------------------------------------------------------------------------
+
+def _projector(project_fn, errors, shape):
+    """(callback, user pointer, runs on the device, objects to keep alive) for a
+    solver's project_fn: a symmetry projector (cpp_hf_b200.symmetry or the
+    reference's cpp_hf.symmetry.make_project_fn) runs as the library's device
+    projector; any other callable goes through the host."""
+    if project_fn is None:
+        return _lib.PROJECT_FN(), None, False, None
+    dproj = _symmetry.device_projector(project_fn)
+    if dproj is not None:
+        if dproj.is_identity:
+            return _lib.PROJECT_FN(), None, False, None
+        s = dproj.struct(*shape)
+        fn = C.cast(_lib.load().cpphf_symmetry_project_fn, _lib.PROJECT_FN)
+        return fn, C.cast(C.pointer(s), C.c_void_p), True, (dproj, s)
+    return _project_callback(project_fn, errors), None, False, None
+
 
 def _project_callback(project_fn, errors):
     if project_fn is None:
@@ -472,9 +495,10 @@ def solve_dm(kernel_args, P0, n_e, max_iter, tol_E, tol_grad, max_step, bt_shrin
     hG = np.zeros(max(max_iter, 1))
     res = _lib.DmResult()
     errors = []
-    cb = _project_callback(project_fn, errors)
+    cb, cb_user, cb_device, _keep = _projector(project_fn, errors, (nk1, nk2, nb))
+    cfg.project_device = 1 if cb_device else 0
     ws = _ws(lib.cpphf_solve_dm_workspace_bytes(dk.ref()))
-    st = check(lib.cpphf_solve_dm(dk.ref(), C.byref(cfg), _ptr(P0_t), float(n_e), cb, None, _ptr(Q), _ptr(p),
+    st = check(lib.cpphf_solve_dm(dk.ref(), C.byref(cfg), _ptr(P0_t), float(n_e), cb, cb_user, _ptr(Q), _ptr(p),
                                   _ptr(D), _ptr(F), hE.ctypes.data_as(_lib.dp), hG.ctypes.data_as(_lib.dp),
                                   C.byref(res), _ptr(ws), ws.numel(), _stream()), "solve_dm")
     _raise_callback(errors)
@@ -512,9 +536,10 @@ def solve_scf(kernel_args, P0, n_e, max_iter, density_tol, comm_tol, mixing, lev
     hC = np.zeros(max(max_iter, 1))
     res = _lib.ScfResult()
     errors = []
-    cb = _project_callback(project_fn, errors)
+    nk1, nk2, nb = dk.shape
+    cb, cb_user, _cb_device, _keep = _projector(project_fn, errors, (nk1, nk2, nb))
     ws = _ws(lib.cpphf_solve_scf_workspace_bytes_cfg(dk.ref(), C.byref(cfg)))
-    check(lib.cpphf_solve_scf(dk.ref(), C.byref(cfg), _ptr(P0_t), float(n_e), cb, None, _ptr(D), _ptr(F),
+    check(lib.cpphf_solve_scf(dk.ref(), C.byref(cfg), _ptr(P0_t), float(n_e), cb, cb_user, _ptr(D), _ptr(F),
                               hE.ctypes.data_as(_lib.dp), hD.ctypes.data_as(_lib.dp),
                               hC.ctypes.data_as(_lib.dp), C.byref(res), _ptr(ws), ws.numel(), _stream()),
           "solve_scf")
@@ -642,5 +667,23 @@ def selfenergy_superlattice_streamed(rho, VR_fft, g_a_off, pair_i, pair_j, pair_
 
 
 def resample_kgrid_2d(values, nk_new):
-    """cpp_hf_native.cpp:819-840."""
-    raise NotImplementedError("resample_kgrid_2d is not built into cpp_hf_b200 yet")
+    """cpp_hf_native.cpp:819-840 -> utils.hpp:120-176 (periodic linear resampling of
+    the two leading, square k axes; trailing axes are carried along)."""
+    lib = _lib_handle()
+    as_np = not _is_torch(values)
+    shape = tuple(values.shape)
+    if len(shape) < 2:
+        raise ValueError("need >= 2 dims")
+    nk_old = int(shape[0])
+    if int(shape[1]) != nk_old:
+        raise ValueError("First two axes must be square (nk_old, nk_old)")
+    nk_new = int(nk_new)
+    inner = 1
+    for d in shape[2:]:
+        inner *= int(d)
+    x = _to_dev(values, "c")
+    out = torch.empty((nk_new, nk_new) + shape[2:], dtype=torch.complex128, device=_dev())
+    if out.numel() > 0 and x.numel() > 0:
+        check(lib.cpphf_resample_kgrid_2d(_ptr(x), _ptr(out), nk_old, nk_new, inner, _stream()), "resample_kgrid_2d")
+    _sync()
+    return _out(out, as_np)

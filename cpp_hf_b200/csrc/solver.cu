@@ -452,11 +452,12 @@ int solve_dm(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* P
         return fail(CPPHF_ERR_INVALID, "solve_dm: workspace too small (" + std::to_string(L.total) + " bytes needed)");
     const SolveStream guard(st);
     st = guard.stream();
-    // Not captured: projector callbacks (host round trips) and the superlattice
+    // Not captured: host projector callbacks (host round trips) and the superlattice
     // exchange, whose per-call channel tables are copied from host buffers that
     // a replayed graph would read after they are gone.
     const bool sl_path = K->sl && (K->sl->fock_active || K->sl->hartree_active);
-    const bool use_graphs = cfg->graphs != 0 && guard.capturable && !project && !sl_path && solve_graphs_enabled();
+    const bool use_graphs = cfg->graphs != 0 && guard.capturable && (!project || cfg->project_device != 0) &&
+                            !sl_path && solve_graphs_enabled();
     IterGraphs graphs;
     unsigned char* W = static_cast<unsigned char*>(ws);
     auto fld = [&](size_t off) { return reinterpret_cast<double2*>(W + off); };

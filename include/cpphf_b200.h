@@ -226,7 +226,9 @@ typedef struct cpphf_dm_config {
      * iteration (better when many solves share the GPU from several host
      * threads, where per-solve graph instantiation contends in the driver). */
     int32_t graphs;
-    int32_t reserved_dm;
+    /* 1: the projector only enqueues device work on the stream (e.g.
+     * cpphf_symmetry_project_fn), so iterations with it may still be captured. */
+    int32_t project_device;
 } cpphf_dm_config;
 
 typedef struct cpphf_dm_result {
@@ -376,6 +378,39 @@ int cpphf_density_from_fock_backward(const void* V, const double* eps, const dou
                                      const double* w, const void* G, void* gF, int64_t nk,
                                      int64_t nb, void* workspace, size_t workspace_bytes,
                                      void* stream);
+
+/* Symmetry-averaging projector (cpp_hf src/cpp_hf/symmetry.py:18-117, make_project_fn)
+ * on device fields: group average (1/N)(sum_g g A(k) g^H + sum_s s A(-k) s^H)
+ * followed by the time-reversal average (A + U conj(A(-k)) U^H)/2.  All arrays
+ * are DEVICE complex128: unitary_group (n_unitary, nb, nb) -- pass the identity
+ * as a one-element unitary group when only a spatial group is given, as the
+ * reference does --, spatial_group (n_spatial, nb, nb), time_reversal_U (nb, nb)
+ * or null, scratch one (nk1, nk2, nb, nb) field.  Conventions: 0 "mod" (-i mod
+ * n), 1 "flip" (n - 1 - i); axes: bit 0 = axis 0, bit 1 = axis 1.  nb <= 64. */
+typedef struct cpphf_symmetry {
+    const void* unitary_group;
+    int64_t n_unitary;
+    const void* spatial_group;
+    int64_t n_spatial;
+    int32_t spatial_convention;
+    int32_t spatial_axes;
+    const void* time_reversal_U;
+    int32_t tr_convention;
+    int32_t tr_axes;
+    void* scratch;
+} cpphf_symmetry;
+
+/* Projects M in place on `stream`. */
+int cpphf_symmetry_project(const cpphf_symmetry* sym, void* M, int64_t nk1, int64_t nk2, int64_t nb, void* stream);
+/* The same with the cpphf_project_fn signature (user = const cpphf_symmetry*):
+ * pass it as a solver's projector and the solve projects on the device. */
+int cpphf_symmetry_project_fn(void* user, void* M, int64_t nk1, int64_t nk2, int64_t nb, void* stream);
+
+/* Replaces _native.resample_kgrid_2d (cpp_hf_native.cpp:819-840 -> utils.hpp:120-176):
+ * periodic linear resampling of a complex128 field (nk_old, nk_old, inner) to
+ * (nk_new, nk_new, inner) on centred grids (k = 0 at index n/2); device
+ * pointers, bitwise the reference's two-pass result. */
+int cpphf_resample_kgrid_2d(const void* values, void* out, int64_t nk_old, int64_t nk_new, int64_t inner, void* stream);
 
 #ifdef __cplusplus
 }

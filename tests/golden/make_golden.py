@@ -119,6 +119,37 @@ def _superlattice_case():
     return arrays
 
 
+def _symmetry_cases():
+    """Inputs and outputs of the reference's make_project_fn (src/cpp_hf/symmetry.py)
+    for the group / spatial / time-reversal combinations and both k conventions."""
+    from cpp_hf.symmetry import make_project_fn
+
+    rng = np.random.default_rng(11)
+    n1, n2, nb = 6, 5, 4
+    A = rng.normal(size=(n1, n2, nb, nb)) + 1j * rng.normal(size=(n1, n2, nb, nb))
+
+    def unitary(m):
+        q, _ = np.linalg.qr(rng.normal(size=(m, m)) + 1j * rng.normal(size=(m, m)))
+        return q
+
+    G = np.stack([np.eye(nb), unitary(nb), unitary(nb)])
+    S = np.stack([unitary(nb), unitary(nb)])
+    U = unitary(nb)
+    cases = {
+        "unitary": dict(unitary_group=G),
+        "spatial_mod": dict(spatial_group=S),
+        "spatial_flip_axis0": dict(spatial_group=S, spatial_k_convention="flip", spatial_k_flip_axes=(0,)),
+        "combined": dict(unitary_group=G, spatial_group=S),
+        "tr_mod": dict(time_reversal_U=U),
+        "tr_flip_axis1": dict(time_reversal_U=U, time_reversal_k_convention="flip", time_reversal_k_flip_axes=(1,)),
+        "all": dict(unitary_group=G, spatial_group=S, time_reversal_U=U, spatial_k_flip_axes=(1,)),
+    }
+    arrays = {"in.A": A, "in.G": G, "in.S": S, "in.U": U}
+    for name, kw in cases.items():
+        arrays[f"{name}.out"] = make_project_fn(**kw)(A)
+    return arrays
+
+
 def main():
     sys.path.insert(0, str(REPO))
     sys.path.insert(0, str(REF / "src"))
@@ -134,7 +165,9 @@ def main():
     np.savez_compressed(HERE / "meshgrid_scf_v1.npz", **{k: d[k] for k in keep})
     np.savez_compressed(HERE / "kernel_args_ref.npz", **_ref_cases())
     np.savez_compressed(HERE / "superlattice_ref.npz", **_superlattice_case())
-    print("wrote", HERE / "meshgrid_scf_v1.npz", HERE / "kernel_args_ref.npz", HERE / "superlattice_ref.npz")
+    np.savez_compressed(HERE / "symmetry_ref.npz", **_symmetry_cases())
+    print("wrote", HERE / "meshgrid_scf_v1.npz", HERE / "kernel_args_ref.npz", HERE / "superlattice_ref.npz",
+          HERE / "symmetry_ref.npz")
 
 
 if __name__ == "__main__":

@@ -143,3 +143,27 @@ def test_superlattice_layout_and_kernel_args_match_reference_fixture():
             continue
         assert got.shape == ref.shape, k
         np.testing.assert_allclose(got, ref, rtol=0, atol=1e-13, err_msg=k)
+
+
+def _symmetry_kwargs(G, S, U):
+    """The projector configurations of tests/golden/make_golden.py:_symmetry_cases."""
+    return {
+        "unitary": dict(unitary_group=G),
+        "spatial_mod": dict(spatial_group=S),
+        "spatial_flip_axis0": dict(spatial_group=S, spatial_k_convention="flip", spatial_k_flip_axes=(0,)),
+        "combined": dict(unitary_group=G, spatial_group=S),
+        "tr_mod": dict(time_reversal_U=U),
+        "tr_flip_axis1": dict(time_reversal_U=U, time_reversal_k_convention="flip", time_reversal_k_flip_axes=(1,)),
+        "all": dict(unitary_group=G, spatial_group=S, time_reversal_U=U, spatial_k_flip_axes=(1,)),
+    }
+
+
+def test_symmetry_projector_restatement_matches_reference_vectors():
+    """oracle/symmetry_np.py against outputs of the reference's
+    cpp_hf.symmetry.make_project_fn (tests/golden/symmetry_ref.npz)."""
+    from oracle import symmetry_np
+
+    d = np.load(GOLDEN / "symmetry_ref.npz")
+    for name, kw in _symmetry_kwargs(d["in.G"], d["in.S"], d["in.U"]).items():
+        got = symmetry_np.make_project_fn(**kw)(d["in.A"])
+        np.testing.assert_allclose(got, d[f"{name}.out"], rtol=0, atol=1e-14, err_msg=name)
