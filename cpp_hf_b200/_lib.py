@@ -63,6 +63,8 @@ class DmConfig(C.Structure):
         ("bt_max", i64), ("mu_maxiter", i32), ("optimizer", i32),
         ("block_sizes", C.POINTER(i64)), ("n_block_sizes", i64), ("mixed_switch_grad", f64),
         ("graphs", i32), ("project_device", i32),
+        ("tr_delta0", f64), ("tr_cg_max", i64), ("deflation_targets", C.c_void_p), ("n_deflation", i64),
+        ("deflation_sigma", f64), ("deflation_length", f64),
     ]
 
 
@@ -115,6 +117,11 @@ _SIGS = {
     "cpphf_cayley_unitary": (C.c_int, [vp, vp, f64, vp, i64, i64, vp]),
     "cpphf_diag_ufu": (C.c_int, [vp, vp, vp, f64, vp, i64, i64, vp]),
     "cpphf_solve_dm_workspace_bytes": (sz, [C.POINTER(Kernel)]),
+    "cpphf_solve_dm_workspace_bytes_cfg": (sz, [C.POINTER(Kernel), C.POINTER(DmConfig)]),
+    "cpphf_rtr_joint_hvp_workspace_bytes": (sz, [C.POINTER(Kernel)]),
+    "cpphf_rtr_joint_hvp": (C.c_int, [C.POINTER(Kernel), vp, vp, vp, vp, vp, vp, vp, vp, sz, vp]),
+    "cpphf_deflation_bias_workspace_bytes": (sz, [i64]),
+    "cpphf_deflation_bias": (C.c_int, [vp, vp, i64, vp, i64, i64, i64, f64, f64, vp, dp, vp, sz, vp]),
     "cpphf_solve_dm": (C.c_int, [C.POINTER(Kernel), C.POINTER(DmConfig), vp, f64, PROJECT_FN, vp,
                                  vp, vp, vp, vp, dp, dp, C.POINTER(DmResult), vp, sz, vp]),
     "cpphf_superlattice_workspace_bytes": (sz, [i64, i64, i64, i64, i64, C.c_int]),

@@ -7,9 +7,9 @@ come back as NumPy arrays; ``torch`` CUDA tensors are used in place and results
 stay on the device as tensors.  Every computation runs in the CUDA library on
 ``torch.cuda.current_stream()``; there is no CPU fallback.
 
-Outside the hot path and not built: the trust-region Newton optimiser
-(``optimizer=1``, ``_rtr_joint_hvp``, ``_deflation_bias``) raises
-``NotImplementedError``.
+``solve_dm`` runs the preconditioned Riemannian CG (``optimizer=0``) or the
+trust-region Newton solver with optional deflation (``optimizer=1``); the
+Newton hooks ``_rtr_joint_hvp`` and ``_deflation_bias`` run on the device too.
 """
 
 from __future__ import annotations
@@ -466,10 +466,8 @@ def solve_dm(kernel_args, P0, n_e, max_iter, tol_E, tol_grad, max_step, bt_shrin
              cg_restart, plateau_window, mu_maxiter, optimizer, tr_delta0, tr_cg_max, deflation_targets,
              deflation_sigma, deflation_length, block_sizes, project_fn, return_Q, return_density,
              return_fock):
-    """cpp_hf_native.cpp:488-582 (optimizer 0)."""
+    """cpp_hf_native.cpp:488-582 (optimizer 0: solver_dm.hpp, 1: solver_rtr.hpp)."""
     lib = _lib_handle()
-    if int(optimizer) == 1:
-        raise NotImplementedError("optimizer='newton' (trust-region Newton) is not built into cpp_hf_b200")
     as_np = not _is_torch(P0)
     dk = _DeviceKernel(kernel_args)
     P0_t = _to_dev(P0, "c")
@@ -487,6 +485,20 @@ def solve_dm(kernel_args, P0, n_e, max_iter, tol_E, tol_grad, max_step, bt_shrin
     cfg.n_block_sizes = n_bs
     cfg.mixed_switch_grad = dk.mixed_switch
     cfg.graphs = 1 if kernel_args.get("solve_graphs", True) else 0
+    cfg.tr_delta0, cfg.tr_cg_max = float(tr_delta0), int(tr_cg_max)
+    cfg.deflation_sigma, cfg.deflation_length = float(deflation_sigma), float(deflation_length)
+    defl_t = None
+    if int(optimizer) == 1 and deflation_targets is not None and float(deflation_sigma) > 0.0:
+        # cpp_hf_native.cpp:533-544 and solver_rtr.hpp:196-205: n_deflation from
+        # shape[0] of a 5-d array; the flat buffer must hold n * nk * nb * nb values
+        t = _to_dev(deflation_targets, "c")
+        if t.dim() == 5 and t.shape[0] > 0:
+            n_defl = int(t.shape[0])
+            if t.numel() < n_defl * P0_t.numel():
+                raise ValueError("deflation_targets buffer smaller than n_deflation * nk * nb * nb.")
+            defl_t = t.reshape(-1)[: n_defl * P0_t.numel()].contiguous()
+            cfg.deflation_targets = defl_t.data_ptr()
+            cfg.n_deflation = n_defl
     Q = torch.empty_like(P0_t) if return_Q else None
     D = torch.empty_like(P0_t) if return_density else None
     F = torch.empty_like(P0_t) if return_fock else None
@@ -497,7 +509,7 @@ def solve_dm(kernel_args, P0, n_e, max_iter, tol_E, tol_grad, max_step, bt_shrin
     errors = []
     cb, cb_user, cb_device, _keep = _projector(project_fn, errors, (nk1, nk2, nb))
     cfg.project_device = 1 if cb_device else 0
-    ws = _ws(lib.cpphf_solve_dm_workspace_bytes(dk.ref()))
+    ws = _ws(lib.cpphf_solve_dm_workspace_bytes_cfg(dk.ref(), C.byref(cfg)))
     st = check(lib.cpphf_solve_dm(dk.ref(), C.byref(cfg), _ptr(P0_t), float(n_e), cb, cb_user, _ptr(Q), _ptr(p),
                                   _ptr(D), _ptr(F), hE.ctypes.data_as(_lib.dp), hG.ctypes.data_as(_lib.dp),
                                   C.byref(res), _ptr(ws), ws.numel(), _stream()), "solve_dm")
@@ -606,17 +618,54 @@ def _diag_UFU_from_spectrum(V, Ft_eig, lam, tau):
 
 
 # ---------------------------------------------------------------------------
-# outside the hot path
+# trust-region Newton hooks
 # ---------------------------------------------------------------------------
 
 def _rtr_joint_hvp(kernel_args, X, dp, Q, p, Ft):
-    """cpp_hf_native.cpp:654-694: trust-region Newton HVP (not built)."""
-    raise NotImplementedError("_rtr_joint_hvp (trust-region Newton) is not built into cpp_hf_b200")
+    """cpp_hf_native.cpp:654-694: joint (Q, p) Hessian-vector product -> (HX, Hp)."""
+    lib = _lib_handle()
+    as_np = not _is_torch(X)
+    dk = _DeviceKernel(kernel_args)
+    nk1, nk2, nb = dk.shape
+    fshape, vshape = (nk1, nk2, nb, nb), (nk1, nk2, nb)
+    ins = []
+    for name, x, kind, shape in (("X", X, "c", fshape), ("dp", dp, "f", vshape), ("Q", Q, "c", fshape),
+                                 ("p", p, "f", vshape), ("Ft", Ft, "c", fshape)):
+        t = _to_dev(x, kind)
+        if t.numel() != int(np.prod(shape)):
+            raise ValueError(f"{name} must have {int(np.prod(shape))} elements (shape {shape})")
+        ins.append(t.reshape(shape))
+    X_t, dp_t, Q_t, p_t, Ft_t = ins
+    HX = torch.empty(fshape, dtype=torch.complex128, device=_dev())
+    Hp = torch.empty(vshape, dtype=torch.float64, device=_dev())
+    ws = _ws(lib.cpphf_rtr_joint_hvp_workspace_bytes(dk.ref()))
+    check(lib.cpphf_rtr_joint_hvp(dk.ref(), _ptr(X_t), _ptr(dp_t), _ptr(Q_t), _ptr(p_t), _ptr(Ft_t), _ptr(HX),
+                                  _ptr(Hp), _ptr(ws), ws.numel(), _stream()), "_rtr_joint_hvp")
+    return _out(HX, as_np), _out(Hp, as_np)
 
 
 def _deflation_bias(P, targets, w2d, sigma, length):
-    """cpp_hf_native.cpp:697-716: deflation bias (not built)."""
-    raise NotImplementedError("_deflation_bias (trust-region Newton deflation) is not built into cpp_hf_b200")
+    """cpp_hf_native.cpp:697-716 -> (Phi, S_pen, diag_coeff)."""
+    lib = _lib_handle()
+    as_np = not _is_torch(P)
+    P_t = _to_dev(P, "c")
+    if P_t.dim() != 4 or P_t.shape[2] != P_t.shape[3]:
+        raise ValueError("P must be (nk1, nk2, nb, nb)")
+    nk1, nk2, nb = (int(v) for v in P_t.shape[:3])
+    T_t = _to_dev(targets, "c")
+    n_defl = int(T_t.shape[0]) if T_t.dim() == 5 else 0
+    if n_defl and T_t.numel() < n_defl * P_t.numel():
+        raise ValueError("targets must have shape (n, nk1, nk2, nb, nb)")
+    w_t = _to_dev(w2d, "f").reshape(-1)
+    if w_t.numel() < nk1 * nk2:
+        raise ValueError("w2d must have nk1 * nk2 entries")
+    S_pen = torch.empty_like(P_t)
+    out = np.zeros(2)
+    ws = _ws(lib.cpphf_deflation_bias_workspace_bytes(n_defl))
+    check(lib.cpphf_deflation_bias(_ptr(P_t), _ptr(T_t) if n_defl else C.c_void_p(0), n_defl, _ptr(w_t), nk1, nk2,
+                                   nb, float(sigma), float(length), _ptr(S_pen), out.ctypes.data_as(_lib.dp),
+                                   _ptr(ws), ws.numel(), _stream()), "_deflation_bias")
+    return float(out[0]), _out(S_pen, as_np), float(out[1])
 
 
 def selfenergy_superlattice_streamed(rho, VR_fft, g_a_off, pair_i, pair_j, pair_start, nkx, nky, n_G,

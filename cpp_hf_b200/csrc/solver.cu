@@ -10,6 +10,8 @@
 #include "eigh.cuh"
 #include "fock.cuh"
 #include "mu.cuh"
+#include "rtr.cuh"
+#include "solve_util.cuh"
 #include "team.cuh"
 
 #include <algorithm>
@@ -289,6 +291,8 @@ bool diis_solve(std::vector<double> A, int n, std::vector<double>& x) {
     return true;
 }
 
+}  // namespace
+
 unsigned grid_for(int64_t n, int threads) {
     const int64_t want = (n + threads - 1) / threads;
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)num_sms() * 8));
@@ -307,6 +311,14 @@ int call_project(cpphf_project_fn fn, void* user, double2* M, const cpphf_kernel
     if (rc != 0) return fail(CPPHF_ERR_INVALID, std::string("project_fn failed: ") + cpphf_last_error());
     return CPPHF_OK;
 }
+
+int scale_weights(const double* w, double wsum, double* out, int64_t n, cudaStream_t st) {
+    k_scale_weights<<<grid_for(n, 256), 256, 0, st>>>(w, wsum, out, n);
+    CPPHF_LAUNCH_CHECK("scale weights");
+    return CPPHF_OK;
+}
+
+namespace {
 
 // Workspace carve-up shared by both solvers.
 struct SolverWs {
@@ -442,8 +454,9 @@ int solve_dm(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* P
              double* hist_E, double* hist_G, cpphf_dm_result* res, void* ws, size_t wsb, cudaStream_t st) {
     CPPHF_TRY(validate_kernel(K));
     if (!cfg || !P0 || !res) return fail(CPPHF_ERR_INVALID, "solve_dm: null argument");
-    if (cfg->optimizer != 0)
-        return fail(CPPHF_ERR_UNSUPPORTED, "optimizer='newton' (trust-region Newton) is not built into this library");
+    if (cfg->optimizer == 1)  // cpp_hf_native.cpp:557-559: 1 is Newton, any other code the CG solver
+        return solve_rtr(K, cfg, P0, n_e, project, puser, Q_out, p_out, D_out, F_out, hist_E, hist_G, res, ws, wsb,
+                         st);
     CPPHF_TRY(check_block_sizes(cfg->block_sizes, cfg->n_block_sizes, K->nb));
     CPPHF_TRY(dm_check_nb(K->nb));
     CPPHF_TRY(check_mixed(K, cfg->mixed_switch_grad));
@@ -1040,6 +1053,12 @@ int cpphf_density_from_fock(const void* F, const double* w, int64_t nk1, int64_t
 }
 
 size_t cpphf_solve_dm_workspace_bytes(const cpphf_kernel* K) { return K ? cpphf::solve_dm_workspace_bytes(K) : 0; }
+
+size_t cpphf_solve_dm_workspace_bytes_cfg(const cpphf_kernel* K, const cpphf_dm_config* cfg) {
+    if (!K) return 0;
+    if (cfg && cfg->optimizer == 1) return cpphf::solve_rtr_workspace_bytes(K, cfg);
+    return cpphf::solve_dm_workspace_bytes(K);
+}
 
 int cpphf_solve_dm(const cpphf_kernel* K, const cpphf_dm_config* cfg, const void* P0, double n_e,
                    cpphf_project_fn project, void* project_user, void* Q_out, double* p_out, void* density_out,

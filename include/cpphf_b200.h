@@ -229,6 +229,18 @@ typedef struct cpphf_dm_config {
     /* 1: the projector only enqueues device work on the stream (e.g.
      * cpphf_symmetry_project_fn), so iterations with it may still be captured. */
     int32_t project_device;
+    /* optimizer 1, trust-region Newton (SolverConfig.tr_delta0 / tr_cg_max /
+     * deflation_* of src/cpp_hf/solver.py:48-59, solver_rtr.hpp:163-205):
+     * initial trust radius, Steihaug CG iterations per outer step, and the
+     * deflation bias (deflation_targets: device complex128
+     * (n_deflation, nk1, nk2, nb, nb) or NULL; off unless n_deflation > 0 and
+     * deflation_sigma > 0). */
+    double tr_delta0;
+    int64_t tr_cg_max;
+    const void* deflation_targets;
+    int64_t n_deflation;
+    double deflation_sigma;
+    double deflation_length;
 } cpphf_dm_config;
 
 typedef struct cpphf_dm_result {
@@ -239,15 +251,40 @@ typedef struct cpphf_dm_result {
     int32_t reserved;
 } cpphf_dm_result;
 
-/* Replaces _native.solve_dm (cpp_hf_native.cpp:488-582 -> solver_dm.hpp:392-653).
+/* Replaces _native.solve_dm (cpp_hf_native.cpp:488-582 -> solver_dm.hpp:392-653
+ * for optimizer 0, solver_rtr.hpp:163-459 for optimizer 1).
  * Q_out, density_out, fock_out (device fields) may be NULL; p_out (device,
- * (nk1, nk2, nb)); hist_E / hist_grad are HOST arrays of max_iter doubles. */
+ * (nk1, nk2, nb)); hist_E / hist_grad are HOST arrays of max_iter doubles.
+ * cpphf_solve_dm_workspace_bytes covers optimizer 0 only; the _cfg form covers
+ * the optimizer and deflation settings of *cfg. */
 size_t cpphf_solve_dm_workspace_bytes(const cpphf_kernel* K);
+size_t cpphf_solve_dm_workspace_bytes_cfg(const cpphf_kernel* K, const cpphf_dm_config* cfg);
 int cpphf_solve_dm(const cpphf_kernel* K, const cpphf_dm_config* cfg, const void* P0, double n_e,
                    cpphf_project_fn project, void* project_user, void* Q_out, double* p_out,
                    void* density_out, void* fock_out, double* hist_E, double* hist_grad,
                    cpphf_dm_result* result, void* workspace, size_t workspace_bytes,
                    void* stream);
+
+/* Replaces _native._rtr_joint_hvp (cpp_hf_native.cpp:654-694 ->
+ * solver_rtr.hpp:55-111): the joint (Q, p) Hessian-vector product of the
+ * trust-region Newton solver, one Fock build of the linear response.  X, Q, Ft,
+ * HX: device complex128 (nk1, nk2, nb, nb); dp, p, Hp: device float64
+ * (nk1, nk2, nb).  Hp is projected onto sum_k w_k sum_b Hp = 0. */
+size_t cpphf_rtr_joint_hvp_workspace_bytes(const cpphf_kernel* K);
+int cpphf_rtr_joint_hvp(const cpphf_kernel* K, const void* X, const double* dp, const void* Q, const double* p,
+                        const void* Ft, void* HX, double* Hp, void* workspace, size_t workspace_bytes,
+                        void* stream);
+
+/* Replaces _native._deflation_bias (cpp_hf_native.cpp:697-716 ->
+ * solver_rtr.hpp:124-157): Phi = sigma sum_i exp(-d_i^2 / (2 length^2)) with
+ * d_i^2 = sum_k w2d_k |P_k - targets_i,k|_F^2, S_pen = 2 sum_i phi'(d_i^2)
+ * (P - targets_i) and diag = 2 sum_i phi'(d_i^2).  P, targets, S_pen: device
+ * complex128; w2d: device (nk1, nk2); phi_diag: HOST double[2] <- (Phi, diag).
+ * targets NULL, n_deflation 0 or sigma 0 give zeros. */
+size_t cpphf_deflation_bias_workspace_bytes(int64_t n_deflation);
+int cpphf_deflation_bias(const void* P, const void* targets, int64_t n_deflation, const double* w2d, int64_t nk1,
+                         int64_t nk2, int64_t nb, double sigma, double length, void* S_pen, double* phi_diag,
+                         void* workspace, size_t workspace_bytes, void* stream);
 
 /* SCFConfig of solver_scf.hpp:20-50; acceleration 0 = linear mixing. */
 typedef struct cpphf_scf_config {

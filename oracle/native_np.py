@@ -28,6 +28,7 @@ meshgrid regression case against it.
 
 from __future__ import annotations
 
+import copy
 import math
 import os
 
@@ -880,22 +881,259 @@ def _solve_dm(K, P0, n_e, cfg, project_fn=None):
                 converged=k < max_iter, hist_E=hist_E[:k].copy(), hist_grad=hist_g[:k].copy())
 
 
+# ---------------------------------------------------------------------------
+# Trust-region Newton (optimizer == 1) and the deflation bias
+# ---------------------------------------------------------------------------
+
+
+def _fock_response(K, dP):
+    """solver_rtr.hpp:31-39: Sigma[dP] = F[dP] - h with the reference density off."""
+    Kr = copy.copy(K)
+    Kr.has_refP = False
+    Kr.refP = None
+    _S, F, _hd = _build_fock_compact(Kr, dP, None)
+    return F - K.h
+
+
+def _project_occ(dp, w2d):
+    """solver_rtr.hpp:42-50: remove the w2d-weighted mean so sum_k w_k sum_b dp = 0."""
+    nb = dp.shape[-1]
+    num = float(np.sum(w2d[..., None] * dp))
+    den = float(np.sum(w2d)) * nb
+    shift = num / den if den > 0.0 else 0.0
+    return dp - shift
+
+
+def _joint_hvp(K, X, dp, Q, p, Ft, T_r, pen_diag=0.0):
+    """solver_rtr.hpp:55-111: joint (Q, p) Hessian-vector product (one Fock build)."""
+    nb = K.nb
+    idx = np.arange(nb)
+    pdiff = p[..., None, :] - p[..., :, None]  # p_j - p_i
+    M = X * pdiff
+    M[..., idx, idx] = dp
+    dP = hermitize(Q @ M @ _adj(Q))
+    R = _fock_response(K, dP)
+    if pen_diag != 0.0:
+        R = R + pen_diag * dP
+    St = _adj(Q) @ R @ Q
+    A = Ft @ X - X @ Ft + St
+    ddiff = dp[..., None, :] - dp[..., :, None]
+    C = ddiff * Ft + pdiff * A
+    HX = 0.5 * (C - _adj(C))
+    HX[..., idx, idx] = 0.0
+    pc = np.clip(p, OCC_CLIP, 1.0 - OCC_CLIP)
+    Hp = np.real(np.diagonal(A, axis1=-2, axis2=-1)) + T_r / (pc * (1.0 - pc)) * dp
+    return HX, _project_occ(Hp, K.w2d)
+
+
+def _deflation_terms(P, targets, w2d, sigma, length):
+    """solver_rtr.hpp:124-157 -> (Phi, S_pen, diag_coeff); a no-op without targets or sigma."""
+    S_pen = np.zeros_like(P)
+    if targets is None or len(targets) == 0 or sigma == 0.0:
+        return 0.0, S_pen, 0.0
+    inv2L2 = 1.0 / (2.0 * float(length) * float(length))
+    Phi = 0.0
+    diag = 0.0
+    for T in targets:
+        D = P - T
+        d2 = float(np.sum(w2d * np.sum(np.abs(D) ** 2, axis=(-2, -1))))
+        phi = float(sigma) * math.exp(-d2 * inv2L2)
+        phip = -phi * inv2L2
+        Phi += phi
+        diag += phip
+        S_pen = S_pen + (2.0 * phip) * D
+    return Phi, S_pen, 2.0 * diag
+
+
+def _solve_rtr(K, P0, n_e, cfg, project_fn=None):
+    """solver_rtr.hpp:163-459 (optimizer == 1): Steihaug truncated CG on the joint
+    (Q, p) quadratic model inside a trust region, Cayley retraction with tau = -1."""
+    nk1, nk2, nb = K.nk1, K.nk2, K.nb
+    T_r = max(K.T, 1.0e-12)
+    tol_g = cfg["tol_grad"] if cfg["tol_grad"] > 0.0 else 1.0e-6
+    ws = max(K.weight_sum, TINY_REAL)
+    w_norm = K.w2d / ws
+    n_t = n_e / ws
+    w2d = K.w2d
+    max_iter = int(cfg["max_iter"])
+    mu_maxiter = int(cfg["mu_maxiter"])
+    idx = np.arange(nb)
+    targets = cfg["deflation_targets"]
+    n_defl = 0 if targets is None else int(targets.shape[0])
+    d_sigma = float(cfg["deflation_sigma"])
+    d_len = max(float(cfg["deflation_length"]), 1.0e-12)
+    defl_on = n_defl > 0 and d_sigma > 0.0
+
+    def jip(aX, ap, bX, bp):
+        return _ip_matrix(aX, bX, 1.0) + _ip_vec(ap, bp, w2d)
+
+    def jfro(aX, ap):
+        return math.sqrt(max(0.0, jip(aX, ap, aX, ap)))
+
+    def prec(aX, ap, lam, eps, p):
+        gap = eps[..., :, None] - eps[..., None, :]
+        oX = aX / np.sqrt(gap * gap + lam * lam)
+        pc = np.clip(p, OCC_CLIP, 1.0 - OCC_CLIP)
+        return oX, _project_occ(ap * pc * (1.0 - pc) / T_r, w2d)
+
+    def project(M):
+        return _call_project(project_fn, M) if project_fn is not None else M
+
+    # init (solver_rtr.hpp:251-262)
+    P_cur = hermitize(P0)
+    _S, F, _hd = _build_fock_compact(K, P_cur, None)
+    eps, Q = _eigh(F)
+    mu = _solve_mu_inloop(eps, w_norm, n_t, 0.0, T_r, mu_maxiter)
+    p = expit((mu - eps) / T_r)
+
+    def eval_state(Qs, ps):
+        # solver_rtr.hpp:264-285
+        P = hermitize(project((Qs * ps[..., None, :]) @ _adj(Qs)))
+        Sigma, F, hd = _build_fock_compact(K, P, None)
+        E = _hf_energy_hd(K, P, Sigma, hd)
+        pen = 0.0
+        if defl_on:
+            Phi, S_pen, pen = _deflation_terms(P, targets, w2d, d_sigma, d_len)
+            E += Phi
+            F = F + S_pen
+        Ft = _adj(Qs) @ F @ Qs
+        eps = np.real(np.diagonal(Ft, axis1=-2, axis2=-1)).copy()
+        A = (ps[..., None, :] - ps[..., :, None]) * Ft
+        G = 0.5 * (A - _adj(A))
+        G[..., idx, idx] = 0.0
+        return E, Ft, eps, G, pen
+
+    E, Ft, eps, G, pen = eval_state(Q, p)
+    Delta = float(cfg["tr_delta0"])
+    hist_E = np.zeros(max_iter, dtype=np.float64)
+    hist_g = np.zeros(max_iter, dtype=np.float64)
+    k = 0
+    converged = False
+    while k < max_iter:
+        grad_norm = math.sqrt(max(0.0, _ip_matrix(G, G, w_norm)))
+        hist_E[k] = E
+        hist_g[k] = grad_norm
+        if grad_norm < tol_g:
+            converged = True
+            k += 1
+            break
+        eps_sq = float(np.sum(eps * eps))
+        lam = max(T_r, float(cfg["denom_scale"]) * math.sqrt(eps_sq / max(eps.size, 1) + TINY_REAL))
+        # Steihaug truncated CG (solver_rtr.hpp:304-364)
+        vX = np.zeros_like(G)
+        vp = np.zeros_like(p)
+        HvX = np.zeros_like(G)
+        Hvp = np.zeros_like(p)
+        rX = -G
+        rp = np.zeros_like(p)
+        zX, zp = prec(rX, rp, lam, eps, p)
+        dX, dp = zX, zp
+        rz = jip(rX, rp, zX, zp)
+        for _cg in range(int(cfg["tr_cg_max"])):
+            HDX, HDp = _joint_hvp(K, dX, dp, Q, p, Ft, T_r, pen)
+            dHd = jip(dX, dp, HDX, HDp)
+            dd = jip(dX, dp, dX, dp)
+
+            def to_boundary(vX, vp, HvX, Hvp):
+                a = dd
+                b = 2.0 * jip(vX, vp, dX, dp)
+                c = jfro(vX, vp)
+                cc = c * c - Delta * Delta
+                t = (-b + math.sqrt(max(b * b - 4.0 * a * cc, 0.0))) / (2.0 * a + 1e-30)
+                return vX + t * dX, vp + t * dp, HvX + t * HDX, Hvp + t * HDp
+
+            if dHd <= 1e-14 * dd:
+                vX, vp, HvX, Hvp = to_boundary(vX, vp, HvX, Hvp)
+                break
+            alpha = rz / dHd
+            s2 = float(np.sum(np.abs(vX + alpha * dX) ** 2))
+            s2 += float(np.sum(w2d * np.sum((vp + alpha * dp) ** 2, axis=-1)))
+            if math.sqrt(max(0.0, s2)) >= Delta:
+                vX, vp, HvX, Hvp = to_boundary(vX, vp, HvX, Hvp)
+                break
+            vX = vX + alpha * dX
+            HvX = HvX + alpha * HDX
+            rX = rX - alpha * HDX
+            vp = vp + alpha * dp
+            Hvp = Hvp + alpha * HDp
+            rp = rp - alpha * HDp
+            rn = math.sqrt(max(0.0, jip(rX, rp, rX, rp)))
+            if rn < 0.05 * grad_norm:
+                break
+            zX, zp = prec(rX, rp, lam, eps, p)
+            rz_new = jip(rX, rp, zX, zp)
+            beta = rz_new / rz
+            dX = zX + beta * dX
+            dp = zp + beta * dp
+            rz = rz_new
+        # predicted reduction in energy units (solver_rtr.hpp:366-378)
+        gv = _ip_matrix(G, vX, w2d)
+        vHv = _ip_matrix(vX, HvX, w2d) + _ip_vec(vp, Hvp, w2d)
+        pred = -(gv + 0.5 * vHv)
+        if Delta < 1e-10:
+            break
+        # retraction Q <- Q Cayley(tau = -1, vX), trial occupations (solver_rtr.hpp:380-396)
+        Vd, lamd = _cayley_setup(vX)
+        U = _cayley_unitary(Vd, lamd, -1.0)
+        Qt = Q @ U
+        eps_t = np.real(np.diagonal(_adj(U) @ Ft @ U, axis1=-2, axis2=-1)).copy()
+        mu_t = _solve_mu_inloop(eps_t, w_norm, n_t, mu, T_r, mu_maxiter)
+        p_t = expit((mu_t - eps_t) / T_r)
+        E_t, Ft_t, eps_tr, G_t, pen_t = eval_state(Qt, p_t)
+        grad_t = math.sqrt(max(0.0, _ip_matrix(G_t, G_t, w_norm)))
+        # acceptance and radius update (solver_rtr.hpp:406-420)
+        noise = 1e-12 * max(abs(E), 1.0)
+        if pred <= noise:
+            accept = (grad_t <= grad_norm) and (E_t <= E + noise)
+            if not accept:
+                Delta *= 0.5
+        else:
+            ratio = (E - E_t) / pred
+            if ratio < 0.25:
+                Delta *= 0.25
+            elif ratio > 0.75 and jfro(vX, vp) > 0.9 * Delta:
+                Delta = min(2.0 * Delta, 5.0)
+            accept = ratio > 0.1
+        if accept:
+            Q, p, E, mu = Qt, p_t, E_t, mu_t
+            Ft, eps, G, pen = Ft_t, eps_tr, G_t, pen_t
+        k += 1
+
+    # finalize (solver_rtr.hpp:437-443)
+    P_cur = hermitize(project((Q * p[..., None, :]) @ _adj(Q)))
+    Sigma, F, hd = _build_fock_compact(K, P_cur, None)
+    E_fin = _hf_energy_hd(K, P_cur, Sigma, hd)
+    return dict(Q=Q, p=p, density=P_cur, fock=F, mu=mu, energy=E_fin, n_iter=k,
+                converged=converged, hist_E=hist_E[:k].copy(), hist_grad=hist_g[:k].copy())
+
+
 def solve_dm(kernel_args, P0, n_e, max_iter, tol_E, tol_grad, max_step, bt_shrink,
              denom_scale, bt_max, cg_restart, plateau_window, mu_maxiter, optimizer,
              tr_delta0, tr_cg_max, deflation_targets, deflation_sigma, deflation_length,
              block_sizes, project_fn, return_Q, return_density, return_fock):
-    """cpp_hf_native.cpp:488-582 (optimizer 0 only)."""
+    """cpp_hf_native.cpp:488-582 (optimizer 0: solver_dm.hpp, 1: solver_rtr.hpp)."""
     K = _Kernel(kernel_args)
     P0 = _c128(P0)
-    if int(optimizer) == 1:
-        raise NotImplementedError(
-            "optimizer='newton' (solver_rtr.hpp) is outside this build's scope")
     cfg = dict(max_iter=int(max_iter), tol_E=float(tol_E), tol_grad=float(tol_grad),
                max_step=float(max_step), bt_shrink=float(bt_shrink),
                denom_scale=float(denom_scale), bt_max=int(bt_max),
                cg_restart=int(cg_restart), plateau_window=int(plateau_window),
                mu_maxiter=int(mu_maxiter), block_sizes=[int(s) for s in block_sizes])
-    r = _solve_dm(K, P0, float(n_e), cfg, project_fn)
+    if int(optimizer) == 1:
+        # cpp_hf_native.cpp:533-547: targets of shape (n, nk1, nk2, nb, nb), n > 0
+        # solver_rtr.hpp:196-205: the size is checked only when deflation is on
+        targets = None
+        if deflation_targets is not None and float(deflation_sigma) > 0.0:
+            t = _c128(deflation_targets)
+            if t.ndim == 5 and t.shape[0] > 0:
+                if t.size < t.shape[0] * P0.size:
+                    raise ValueError("deflation_targets buffer smaller than n_deflation * nk * nb * nb.")
+                targets = t.reshape((t.shape[0],) + P0.shape)
+        cfg.update(tr_delta0=float(tr_delta0), tr_cg_max=int(tr_cg_max), deflation_targets=targets,
+                   deflation_sigma=float(deflation_sigma), deflation_length=float(deflation_length))
+        r = _solve_rtr(K, P0, float(n_e), cfg, project_fn)
+    else:
+        r = _solve_dm(K, P0, float(n_e), cfg, project_fn)
     shape = P0.shape
     return (
         np.ascontiguousarray(r["Q"]).reshape(shape) if return_Q else None,
@@ -938,13 +1176,26 @@ def _diag_UFU_from_spectrum(V, Ft_eig, lam, tau):
 
 
 def _rtr_joint_hvp(kernel_args, X, dp, Q, p, Ft):
-    """cpp_hf_native.cpp:654-694 (trust-region Newton HVP): outside this build's scope."""
-    raise NotImplementedError("_rtr_joint_hvp (solver_rtr.hpp) is outside this build's scope")
+    """cpp_hf_native.cpp:654-694: joint (Q, p) Hessian-vector product -> (HX, Hp)."""
+    K = _Kernel(kernel_args)
+    shape = (K.nk1, K.nk2, K.nb, K.nb)
+    X = _c128(X).reshape(shape)
+    Q = _c128(Q).reshape(shape)
+    Ft = _c128(Ft).reshape(shape)
+    dp = _f64(dp).reshape(shape[:3])
+    p = _f64(p).reshape(shape[:3])
+    HX, Hp = _joint_hvp(K, X, dp, Q, p, Ft, max(K.T, 1.0e-12))
+    return np.ascontiguousarray(HX), np.ascontiguousarray(Hp)
 
 
 def _deflation_bias(P, targets, w2d, sigma, length):
-    """cpp_hf_native.cpp:697-716 (deflation bias): outside this build's scope."""
-    raise NotImplementedError("_deflation_bias (solver_rtr.hpp) is outside this build's scope")
+    """cpp_hf_native.cpp:697-716 -> (Phi, S_pen, diag_coeff)."""
+    P = _c128(P)
+    t = _c128(targets)
+    w2d = _f64(w2d).reshape(P.shape[:2])
+    tl = t.reshape((t.shape[0],) + P.shape) if (t.ndim == 5 and t.shape[0] > 0) else None
+    Phi, S_pen, diag = _deflation_terms(P, tl, w2d, float(sigma), float(length))
+    return float(Phi), np.ascontiguousarray(S_pen), float(diag)
 
 
 # ---------------------------------------------------------------------------

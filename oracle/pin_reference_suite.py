@@ -4,9 +4,9 @@ Test infrastructure.  Runs in a container where the reference checkout is
 present (default ``/root/reference``; override with ``CPPHF_REFERENCE``):
 
 1. the reference's pytest suite (``tests/``) with ``oracle.native_np`` installed
-   as ``cpp_hf._native`` (tests of the trust-region Newton / deflation
-   optimiser and the ``contimod``-gated regression are outside this build's
-   scope and are deselected by name);
+   as ``cpp_hf._native``, the trust-region Newton and deflation tests
+   (``test_solver_rtr.py``, ``test_deflation.py``) included (the
+   ``contimod``-gated regression skips itself without that package);
 2. the stored SCF regression case ``tests/data/meshgrid_regression_case_v1.npz``
    through the reference's own ``cpp_hf.solve_scf`` with the same settings as
    ``examples/contimod_example_meshgrid_offline.py:36-60``, checked at 1e-6.
@@ -24,9 +24,8 @@ from pathlib import Path
 REPO = Path(__file__).resolve().parents[1]
 REF = Path(os.environ.get("CPPHF_REFERENCE", "/root/reference"))
 
-# Outside the hot-path scope: optimizer="newton" (solver_rtr.hpp) and the
-# deflation driver built on it.
-DESELECT = ["test_solver_rtr.py", "test_deflation.py"]
+# Every reference test file runs.
+DESELECT: list[str] = []
 
 
 def run_suite() -> int:

@@ -358,11 +358,8 @@ def test_solve_dm_result_shapes_and_omission(native):
     assert len(out[8]) == out[6]
 
 
-def test_solve_dm_rejects_newton_and_bad_blocks(native):
+def test_solve_dm_rejects_bad_blocks(native):
     args, P0, n_e = workloads.dirac(4, seed=0)
-    with pytest.raises(NotImplementedError):
-        native.solve_dm(args, P0, n_e, 5, 1e-8, 0.0, 0.6, 0.5, 1e-3, 8, 10, 5, 25, 1, 0.5, 20,
-                        np.empty((0, 4, 4, 2, 2), np.complex128), 0.0, 1.0, [], None, True, True, True)
     with pytest.raises(ValueError, match="block_sizes must sum to nb"):
         _dm(native, args, P0, n_e, 5, block_sizes=(1, 2))
 
