@@ -230,6 +230,33 @@ def time_solves(torch, native, args_dev, P0_dev, n_e, reps):
     return out
 
 
+def time_newton(torch, native, args_dev, P0_dev, n_e, reps=2, max_iter=60):
+    """The trust-region Newton solve (optimizer=1, tol_grad=1e-6) of the same
+    instance, FP64, device resident: time, outer iterations, final gradient norm."""
+    nk1, nk2, nb = P0_dev.shape[0], P0_dev.shape[1], P0_dev.shape[2]
+    empty = torch.empty((0, nk1, nk2, nb, nb), dtype=torch.complex128, device=P0_dev.device)
+
+    def call():
+        return native.solve_dm(args_dev, P0_dev, n_e, max_iter, 1e-7, 1e-6, 0.6, 0.5, 1e-3, 8, 10, 5, 25, 1, 0.5,
+                               20, empty, 0.0, 1.0, [], None, False, True, False)
+
+    r = call()
+    stream = torch.cuda.current_stream()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        r = call()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3 / reps
+    it = int(r[6])
+    return {"solves_per_s": 1.0 / t, "ms_per_solve": 1e3 * t, "iterations": it, "converged": bool(r[7]),
+            "energy": float(r[5]), "final_grad_norm": float(r[9][-1]) if it else None,
+            "ms_per_iteration": 1e3 * t / max(it, 1),
+            "config": f"optimizer=newton, tol_grad=1e-6, max_iter={max_iter}, tr_delta0=0.5, tr_cg_max=20"}
+
+
 def oracle_solve_estimate(args, P0_np, n_e, n_iter_gpu):
     """Oracle DM solve time from a bounded sample: init + 2 iterations, extrapolated to the
     iteration count of the FP64 GPU solve (the trajectories agree to ~1e-8)."""
@@ -364,6 +391,7 @@ def main():
         P0_dev = torch.from_numpy(np.ascontiguousarray(_P0)).to(dev)
         barrier()
         solves = time_solves(torch, native, args_dev, P0_dev, _ne, a.solve_reps)
+        solves["newton_fp64"] = time_newton(torch, native, args_dev, P0_dev, _ne)
         barrier()
 
     # ---- batched sweep: concurrent streams (mixed and FP64) vs one by one in FP64 ----

@@ -40,35 +40,9 @@ namespace cpphf {
 
 namespace {
 
-constexpr int kRtrMaxBlocks = 1024;
 constexpr int kRtrMaxNb = 48;    // five team matrices per k-point in shared memory
 constexpr int kMaxDeflation = 256;
-constexpr double kOccClip = 1.0e-8;  // OCC_CLIP (solver_dm.hpp)
 constexpr double kTinyReal = 1.0e-30;
-
-// reduction result slots
-enum : int {
-    kSumDD = 0, kSumVD, kSumVV,                           // direction pass: <d,d>, <v,d>, <v,v> (joint metric)
-    kSumB1, kSumB2, kSumB3, kSumB4,                       // HVP pass: Re<dX,HX>, sum w dp Hp, sum w dp, sum w Hp
-    kSumRR, kSumA1, kSumA2, kSumA3, kSumA4,               // update pass: <r,r>, Re<rX,zX>, sum w rp z, sum w z, sum w rp
-    kSumGV, kSumVHX, kSumVHP, kSumVVX, kSumVVP,           // model pass
-    kSumW,                                                // sum_k w2d
-    kNumSums
-};
-
-struct RtrScalars {
-    double mu[2];      // chemical potential of each state slot
-    double energy[2];  // free energy (+ deflation bias) of each state slot
-    double pen[2];     // deflation curvature 2 sum_i phi'(d_i^2) of each state slot
-    double phi;        // deflation bias of the last evaluation
-    double efin;       // energy of the final density
-    double sums[kNumSums];
-    unsigned counter;
-    unsigned pad;
-    double part[8 * kRtrMaxBlocks];
-};
-
-__device__ __forceinline__ double occ_clip(double p) { return fmin(fmax(p, kOccClip), 1.0 - kOccClip); }
 
 unsigned flat_blocks(int64_t n, int threads) {
     const int64_t want = (n + threads - 1) / threads;
@@ -93,7 +67,8 @@ __global__ void k_rtr_wsum(const double* __restrict__ w, int64_t nk, RtrScalars*
 
 // ---------------------------------------------------------------------------
 // Direction and its density variation (solver_rtr.hpp:61-75, 218-231, 356-362).
-// mode 0: d = z(r); mode 1: d = z(r) + beta d; mode 2: d given.  z(r) is the
+// mode 0: d = z(r); mode 1: d = z(r) + beta d; mode 2: d given; mode 3: as 1
+// with beta and shift_z formed here from the update pass's sums.  z(r) is the
 // block preconditioner: rX / sqrt(gap^2 + lam^2) and rp p(1-p) / T minus the
 // weighted mean shift_z.  Then dP = herm(Q M Q^H) with M = [X, diag p]
 // off the diagonal and dp on it.  Sums <d,d>, <v,d>, <v,v> in the joint metric
@@ -105,7 +80,7 @@ __global__ void k_rtr_direction(const double2* __restrict__ rX, const double* __
                                 const double* __restrict__ w, const double2* __restrict__ Q,
                                 const double2* __restrict__ vX, const double* __restrict__ vp, double2* dX,
                                 double* dp, double2* __restrict__ dP, int64_t nk, int nb, double T_r, double lam,
-                                double beta, double shift_z, int mode, RtrScalars* R) {
+                                double beta, double shift_z, double rz_old, int mode, RtrScalars* R) {
     extern __shared__ __align__(16) unsigned char raw[];
     __shared__ double red[32 * 3];
     Team<WARP> t;
@@ -115,6 +90,12 @@ __global__ void k_rtr_direction(const double2* __restrict__ rX, const double* __
     double2* sT = sM + team_mat_elems(nb);
     double* sdp = reinterpret_cast<double*>(sT + team_mat_elems(nb));
     const double lam2 = lam * lam;
+    if (mode == 3) {  // beta and shift_z from the preceding update pass (same arithmetic as the host)
+        const double den = R->sums[kSumW] * (double)nb;
+        shift_z = den > 0.0 ? R->sums[kSumA3] / den : 0.0;
+        beta = (R->sums[kSumA1] + R->sums[kSumA2] - shift_z * R->sums[kSumA4]) / rz_old;
+        mode = 1;
+    }
     double acc[3] = {0.0, 0.0, 0.0};
     for (int64_t k = (int64_t)blockIdx.x * t.nteams + t.team; k < nk; k += (int64_t)gridDim.x * t.nteams) {
         tload<WARP>(sQ, Q + (size_t)k * nb2, nb, t);
@@ -532,17 +513,21 @@ int rtr_check_nb(int64_t nb) {
 
 int launch_direction(const double2* rX, const double* rp, const double* eps, const double* p, const double* w,
                      const double2* Q, const double2* vX, const double* vp, double2* dX, double* dp, double2* dP,
-                     int64_t nk, int nb, double T_r, double lam, double beta, double shift_z, int mode,
-                     RtrScalars* R, cudaStream_t st) {
+                     int64_t nk, int nb, double T_r, double lam, double beta, double shift_z, double rz_old,
+                     int mode, RtrScalars* R, cudaStream_t st) {
+    if (rtr_small_supported(nb))
+        return rtr_small_direction(rX, rp, eps, p, w, Q, vX, vp, dX, dp, dP, nk, nb, T_r, lam, beta, shift_z, rz_old,
+                                   mode, R, st);
     const TeamLaunch L = rtr_team_launch(nk, nb);
     TEAM_DISPATCH(L, k_rtr_direction, 3, nb, rX, rp, eps, p, w, Q, vX, vp, dX, dp, dP, nk, nb, T_r, lam, beta,
-                  shift_z, mode, R);
+                  shift_z, rz_old, mode, R);
     return CPPHF_OK;
 }
 
 int launch_hvp(const double2* X, const double* dp, const double2* Q, const double* p, const double2* Ft,
                const double2* Fr, const double2* h, const double2* dP, const double* pen, const double* w,
                double2* HX, double* Hp, int64_t nk, int nb, double T_r, RtrScalars* R, cudaStream_t st) {
+    if (rtr_small_supported(nb)) return rtr_small_hvp(X, dp, Q, p, Ft, Fr, h, dP, pen, w, HX, Hp, nk, nb, T_r, R, st);
     const TeamLaunch L = rtr_team_launch(nk, nb);
     TEAM_DISPATCH(L, k_rtr_hvp, 5, 2 * nb, X, dp, Q, p, Ft, Fr, h, dP, pen, w, HX, Hp, nk, nb, T_r, R);
     return CPPHF_OK;
@@ -716,7 +701,8 @@ int solve_rtr(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* 
     // norm, and the preconditioner scale lam_pc (solver_rtr.hpp:300-302)
     double hE[2] = {0.0, 0.0}, hg[2] = {0.0, 0.0}, hlam[2] = {0.0, 0.0};
     double hb[4];
-    auto eval = [&](int s) -> int {
+    double sums[kNumSums];
+    auto eval = [&](int s, bool with_model) -> int {
         CPPHF_TRY(finish_density());
         CPPHF_TRY(build_fock(K, P, Sig, Ft[s], nullptr, &R->energy[s], nullptr, fws, L.fock_bytes, st));
         if (defl)
@@ -734,6 +720,9 @@ int solve_rtr(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* 
         static_assert(offsetof(DmScalars, lam_pc) == offsetof(DmScalars, grad_norm) + sizeof(double),
                       "DmScalars read-back layout");
         CPPHF_CUDA(cudaMemcpyAsync(hb + 2, &S->grad_norm, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+        if (with_model)
+            CPPHF_CUDA(cudaMemcpyAsync(sums + kSumGV, &R->sums[kSumGV], 5 * sizeof(double), cudaMemcpyDeviceToHost,
+                                       st));
         CPPHF_CUDA(cudaStreamSynchronize(st));
         if (!std::isfinite(hb[0]))
             return fail(CPPHF_ERR_TIMEOUT,
@@ -743,7 +732,6 @@ int solve_rtr(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* 
         hlam[s] = hb[3];
         return CPPHF_OK;
     };
-    double sums[kNumSums];
     auto read_sums = [&](int first, int count) -> int {
         CPPHF_CUDA(cudaMemcpyAsync(sums + first, &R->sums[first], sizeof(double) * count, cudaMemcpyDeviceToHost,
                                    st));
@@ -757,7 +745,7 @@ int solve_rtr(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* 
     CPPHF_TRY(eigh_batched(F, eps[0], Q[0], nk, nb, 0, nullptr, st));
     CPPHF_TRY(mu_solve(eps[0], wn, nk, nb, n_t, &R->mu[0], T_r, mu_it, 1, &R->mu[0], mws, L.mu_bytes, st));
     CPPHF_TRY(occupy(0, eps[0]));
-    CPPHF_TRY(eval(0));
+    CPPHF_TRY(eval(0, false));
     CPPHF_TRY(read_sums(kSumW, 1));
     const double wtot = sums[kSumW];
     const double occ_den = wtot * (double)nb;  // project_occ's denominator
@@ -778,77 +766,78 @@ int solve_rtr(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* 
             ++k;
             break;
         }
+        if (Delta < 1e-10) break;  // solver_rtr.hpp:379 (Delta does not change before that test)
         const double lam = hlam[s];
         const double* ek = eps[s];
         const double* pk = p[s];
-        // ---- Steihaug truncated CG (solver_rtr.hpp:304-364) ----
-        k_rtr_update<<<flat_blocks(nk * nb * nb, 256), 256, 0, st>>>(2, 0.0, 0.0, G[s], vX, HvX, rX, dX, HDX, vp,
-                                                                     Hvp, rp, dp, HDp, ek, pk, K->w2d, nk, nb, T_r,
-                                                                     lam, R);
-        CPPHF_LAUNCH_CHECK("rtr cg start");
-        CPPHF_TRY(read_sums(kSumRR, 5));
-        double rz = sums[kSumA1] + sums[kSumA2] - occ_shift(sums[kSumA3]) * sums[kSumA4];
-        double beta = 0.0, shift_z = occ_shift(sums[kSumA3]);
-        int dmode = 0;
-        for (int64_t cg = 0; cg < cg_max; ++cg) {
-            CPPHF_TRY(launch_direction(rX, rp, ek, pk, K->w2d, Q[s], vX, vp, dX, dp, dP, nk, nb, T_r, lam, beta,
-                                       shift_z, dmode, R, st));
+        const double* pen = defl ? &R->pen[s] : nullptr;
+        const double2* hmat = static_cast<const double2*>(K->h);
+        // one Hessian-vector product of direction mode `mode` (its sums land in R)
+        auto hvp_step = [&](int mode, double beta, double rz_old) -> int {
+            CPPHF_TRY(launch_direction(rX, rp, ek, pk, K->w2d, Q[s], vX, vp, dX, dp, dP, nk, nb, T_r, lam, beta, 0.0,
+                                       rz_old, mode, R, st));
             CPPHF_TRY(build_fock(&Kr, dP, Sig, F, nullptr, nullptr, nullptr, fws, L.fock_bytes, st));
-            CPPHF_TRY(launch_hvp(dX, dp, Q[s], pk, Ft[s], F, static_cast<const double2*>(K->h), dP, defl ? &R->pen[s] : nullptr, K->w2d, HDX,
-                                 HDp, nk, nb, T_r, R, st));
-            CPPHF_TRY(read_sums(kSumDD, 7));
+            return launch_hvp(dX, dp, Q[s], pk, Ft[s], F, hmat, dP, pen, K->w2d, HDX, HDp, nk, nb, T_r, R, st);
+        };
+        auto update = [&](int mode, double a, double shift_h) -> int {
+            k_rtr_update<<<flat_blocks(nk * nb * nb, 256), 256, 0, st>>>(mode, a, shift_h, G[s], vX, HvX, rX, dX, HDX,
+                                                                         vp, Hvp, rp, dp, HDp, ek, pk, K->w2d, nk, nb,
+                                                                         T_r, lam, R);
+            CPPHF_LAUNCH_CHECK("rtr cg update");
+            return CPPHF_OK;
+        };
+        // ---- Steihaug truncated CG (solver_rtr.hpp:304-364) ----
+        // r = -G, v = Hv = 0 and the first direction d = z(r) with its product
+        // are queued together; every later step queues the next direction and
+        // product behind the vector update before reading the sums of both
+        // (one synchronisation per step).  A product queued for a step the host
+        // then does not take only overwrote d, which the solve no longer needs.
+        CPPHF_TRY(update(2, 0.0, 0.0));
+        if (cg_max > 0) CPPHF_TRY(hvp_step(0, 0.0, 1.0));
+        CPPHF_TRY(read_sums(kSumDD, kSumA4 + 1));
+        double rz = sums[kSumA1] + sums[kSumA2] - occ_shift(sums[kSumA3]) * sums[kSumA4];
+        for (int64_t cg = 0; cg < cg_max; ++cg) {
             const double shift_h = occ_shift(sums[kSumB4]);
             const double dHd = sums[kSumB1] + sums[kSumB2] - shift_h * sums[kSumB3];
             const double dd = sums[kSumDD], vd = sums[kSumVD], vv = sums[kSumVV];
-            auto to_boundary = [&]() -> int {
-                // the positive root of |v + t d|^2 = Delta^2
+            bool boundary = dHd <= 1e-14 * dd;  // negative curvature
+            if (!boundary) {
+                const double alpha = rz / dHd;
+                const double s2 = vv + 2.0 * alpha * vd + alpha * alpha * dd;  // |v + alpha d|^2
+                boundary = std::sqrt(std::max(0.0, s2)) >= Delta;
+            }
+            if (boundary) {  // to the positive root of |v + t d|^2 = Delta^2
                 const double a = dd, b = 2.0 * vd, c = std::sqrt(std::max(0.0, vv));
                 const double cc = c * c - Delta * Delta;
                 const double tt = (-b + std::sqrt(std::max(b * b - 4.0 * a * cc, 0.0))) / (2.0 * a + 1e-30);
-                k_rtr_update<<<flat_blocks(nk * nb * nb, 256), 256, 0, st>>>(1, tt, shift_h, G[s], vX, HvX, rX, dX,
-                                                                             HDX, vp, Hvp, rp, dp, HDp, ek, pk,
-                                                                             K->w2d, nk, nb, T_r, lam, R);
-                CPPHF_LAUNCH_CHECK("rtr boundary step");
-                return CPPHF_OK;
-            };
-            if (dHd <= 1e-14 * dd) {  // negative curvature
-                CPPHF_TRY(to_boundary());
+                CPPHF_TRY(update(1, tt, shift_h));
                 break;
             }
-            const double alpha = rz / dHd;
-            const double s2 = vv + 2.0 * alpha * vd + alpha * alpha * dd;  // |v + alpha d|^2
-            if (std::sqrt(std::max(0.0, s2)) >= Delta) {
-                CPPHF_TRY(to_boundary());
-                break;
-            }
-            k_rtr_update<<<flat_blocks(nk * nb * nb, 256), 256, 0, st>>>(0, alpha, shift_h, G[s], vX, HvX, rX, dX,
-                                                                         HDX, vp, Hvp, rp, dp, HDp, ek, pk, K->w2d,
-                                                                         nk, nb, T_r, lam, R);
-            CPPHF_LAUNCH_CHECK("rtr cg step");
-            CPPHF_TRY(read_sums(kSumRR, 5));
-            const double rn = std::sqrt(std::max(0.0, sums[kSumRR]));
-            if (rn < 0.05 * grad_norm) break;
-            shift_z = occ_shift(sums[kSumA3]);
-            const double rz_new = sums[kSumA1] + sums[kSumA2] - shift_z * sums[kSumA4];
-            beta = rz_new / rz;
-            rz = rz_new;
-            dmode = 1;
+            CPPHF_TRY(update(0, rz / dHd, shift_h));
+            const bool more = cg + 1 < cg_max;
+            if (more) CPPHF_TRY(hvp_step(3, 0.0, rz));
+            CPPHF_TRY(read_sums(kSumDD, kSumA4 + 1));
+            if (std::sqrt(std::max(0.0, sums[kSumRR])) < 0.05 * grad_norm || !more) break;
+            const double shift_z = occ_shift(sums[kSumA3]);
+            rz = sums[kSumA1] + sums[kSumA2] - shift_z * sums[kSumA4];
         }
-        // ---- predicted reduction in energy units (solver_rtr.hpp:366-378) ----
+        // ---- predicted reduction in energy units (solver_rtr.hpp:366-378), read with the trial state ----
         k_rtr_model<<<flat_blocks(nk * nb * nb, 256), 256, 0, st>>>(G[s], vX, HvX, vp, Hvp, K->w2d, nk, nb, R);
         CPPHF_LAUNCH_CHECK("rtr model");
-        CPPHF_TRY(read_sums(kSumGV, 5));
-        const double pred = -(sums[kSumGV] + 0.5 * (sums[kSumVHX] + sums[kSumVHP]));
-        const double vnorm = std::sqrt(std::max(0.0, sums[kSumVVX] + sums[kSumVVP]));
-        if (Delta < 1e-10) break;
 
         // ---- retraction Q <- Q Cayley(tau = -1, vX), trial mu and occupations ----
         const int t = s ^ 1;
-        CPPHF_TRY(eigh_batched(vX, lamd, Vd, nk, nb, 1, nullptr, st));
-        CPPHF_TRY(launch_retract(Vd, lamd, Q[s], Ft[s], Q[t], ew, nk, nb, st));
+        if (rtr_small_supported(nb)) {  // Cayley factor by elimination
+            CPPHF_TRY(rtr_small_retract(vX, Q[s], Ft[s], Q[t], ew, nk, nb, st));
+        } else {  // spectral Cayley factor (solver_rtr.hpp:386-387)
+            CPPHF_TRY(eigh_batched(vX, lamd, Vd, nk, nb, 1, nullptr, st));
+            CPPHF_TRY(launch_retract(Vd, lamd, Q[s], Ft[s], Q[t], ew, nk, nb, st));
+        }
         CPPHF_TRY(mu_solve(ew, wn, nk, nb, n_t, &R->mu[s], T_r, mu_it, 1, &R->mu[t], mws, L.mu_bytes, st));
         CPPHF_TRY(occupy(t, ew));
-        CPPHF_TRY(eval(t));  // the one Fock build at the trial point
+        CPPHF_TRY(eval(t, true));  // the one Fock build at the trial point
+        const double pred = -(sums[kSumGV] + 0.5 * (sums[kSumVHX] + sums[kSumVHP]));
+        const double vnorm = std::sqrt(std::max(0.0, sums[kSumVVX] + sums[kSumVVP]));
         const double E = hE[s], E_t = hE[t], grad_t = hg[t];
 
         // ---- acceptance and trust radius (solver_rtr.hpp:398-420) ----
@@ -933,7 +922,7 @@ int cpphf_rtr_joint_hvp(const cpphf_kernel* K, const void* X, const double* dp, 
     // dP from the given direction (X, dp): mode 2 reads it unchanged
     CPPHF_TRY(launch_direction(nullptr, nullptr, nullptr, p, K->w2d, static_cast<const double2*>(Q), nullptr,
                                nullptr, const_cast<double2*>(static_cast<const double2*>(X)),
-                               const_cast<double*>(dp), dP, nk, nb, T_r, 0.0, 0.0, 0.0, 2, R, st));
+                               const_cast<double*>(dp), dP, nk, nb, T_r, 0.0, 0.0, 0.0, 1.0, 2, R, st));
     CPPHF_TRY(build_fock(&Kr, dP, Sig, F, nullptr, nullptr, nullptr, fws, fb, st));
     CPPHF_TRY(launch_hvp(static_cast<const double2*>(X), dp, static_cast<const double2*>(Q), p,
                          static_cast<const double2*>(Ft), F, static_cast<const double2*>(K->h), dP, nullptr, K->w2d,

@@ -1,0 +1,182 @@
+// Tile helpers of the small-nb (2, 4, 6, 8) per-k kernels: a group of GS
+// threads (nb rounded up to a power of two) owns one k-point, thread r owns row
+// r of every matrix, and a CTA of kThreads threads stages KT = kThreads / GS
+// k-points per tile through shared memory (coalesced loads and stores into a
+// padded layout).  Used by the direct-minimisation (dm_small.cu) and
+// trust-region Newton (rtr_small.cu) kernels.
+#pragma once
+
+#include "common.cuh"
+
+#include <algorithm>
+
+namespace cpphf {
+namespace tile {
+
+constexpr int kThreads = 128;
+
+// Matrix stride in double2 units: >= nb * ld and, with 4 groups per warp
+// (gs = 8), congruent to 2 or 6 mod 8 so the groups' broadcast reads use
+// different banks; odd for smaller groups.
+constexpr int pad_ms(int nb, int ld, int gs) {
+    int m = nb * ld;
+    if (gs == 8) {
+        while (m % 8 != 2 && m % 8 != 6) ++m;
+    } else if (m % 2 == 0) {
+        ++m;
+    }
+    return m;
+}
+
+template <int NB>
+struct Geo {
+    static constexpr int GS = NB <= 2 ? 2 : (NB <= 4 ? 4 : 8);        // group size
+    static constexpr int KT = kThreads / GS;                           // k-points per CTA tile
+    static constexpr int NB2 = NB * NB;
+    static constexpr int LD = NB + 1;                                  // padded row stride
+    static constexpr int MS = pad_ms(NB, LD, GS);                      // padded matrix stride
+    static constexpr int TILE = KT * MS;                               // shared double2 per staged tile
+    static constexpr int PER = (KT * NB2 + kThreads - 1) / kThreads;  // elements per thread per tile
+};
+
+// coalesced global (dense k-blocks) -> shared (padded) copy of one tile; all
+// loads are issued before the first shared store
+template <int NB>
+__device__ __forceinline__ void tile_load(double2* s, const double2* __restrict__ g, int nkt) {
+    using G = Geo<NB>;
+    const int n = nkt * G::NB2;
+    double2 v[G::PER];
+#pragma unroll
+    for (int u = 0; u < G::PER; ++u) {
+        const int e = threadIdx.x + u * kThreads;
+        v[u] = (e < n) ? g[e] : mk(0.0, 0.0);
+    }
+#pragma unroll
+    for (int u = 0; u < G::PER; ++u) {
+        const int e = threadIdx.x + u * kThreads;
+        if (e < n) {
+            const int kl = e / G::NB2, rem = e - kl * G::NB2, i = rem / NB, j = rem - i * NB;
+            s[kl * G::MS + i * G::LD + j] = v[u];
+        }
+    }
+}
+
+template <int NB>
+__device__ __forceinline__ void tile_store(double2* g, const double2* s, int nkt) {
+    using G = Geo<NB>;
+    const int n = nkt * G::NB2;
+#pragma unroll
+    for (int u = 0; u < G::PER; ++u) {
+        const int e = threadIdx.x + u * kThreads;
+        if (e < n) {
+            const int kl = e / G::NB2, rem = e - kl * G::NB2, i = rem / NB, j = rem - i * NB;
+            g[e] = s[kl * G::MS + i * G::LD + j];
+        }
+    }
+}
+
+template <int NB>
+__device__ __forceinline__ unsigned group_mask(int lane) {
+    using G = Geo<NB>;
+    const unsigned base = (1u << G::GS) - 1u;
+    return G::GS == 32 ? 0xffffffffu : (base << ((lane / G::GS) * G::GS));
+}
+
+
+// ---------------------------------------------------------------------------
+// Cayley unitary U(tau) = (I + tau d/2)^{-1} (I - tau d/2) of one k-point by
+// Gauss-Jordan elimination, one row per thread (row r of the result in u[]).
+// At step pp the owner of row pp divides its row by the pivot (one reciprocal
+// per step) and broadcasts it through the group's shared slot `piv`; the other
+// rows eliminate column pp, touching only the columns right of the pivot in
+// the left block (the ones left of it are already zero).  The rows end
+// normalised, so u[] is row r of U.
+// ---------------------------------------------------------------------------
+template <int NB, int LD>
+__device__ __forceinline__ void row_cayley(const double2* d, double tau, int r, double2* piv, double2 (&u)[NB],
+                                           unsigned mask) {
+    double2 mrow[NB];
+    const double h = 0.5 * tau;
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+        const double2 a = cscale(d[r * LD + j], h);
+        const double one = (j == r) ? 1.0 : 0.0;
+        mrow[j] = mk(one + a.x, a.y);
+        u[j] = mk(one - a.x, -a.y);
+    }
+#pragma unroll
+    for (int pp = 0; pp < NB; ++pp) {
+        if (r == pp) {
+            const double2 pv = mrow[pp];
+            const double inv = 1.0 / (pv.x * pv.x + pv.y * pv.y);
+            const double2 rp = mk(pv.x * inv, -pv.y * inv);
+#pragma unroll
+            for (int j = pp + 1; j < NB; ++j) {
+                mrow[j] = cmul(mrow[j], rp);
+                piv[j] = mrow[j];
+            }
+#pragma unroll
+            for (int j = 0; j < NB; ++j) {
+                u[j] = cmul(u[j], rp);
+                piv[NB + j] = u[j];
+            }
+        }
+        __syncwarp(mask);
+        if (r != pp) {
+            const double2 f = mrow[pp];
+#pragma unroll
+            for (int j = pp + 1; j < NB; ++j) mrow[j] = csub(mrow[j], cmul(f, piv[j]));
+#pragma unroll
+            for (int j = 0; j < NB; ++j) u[j] = csub(u[j], cmul(f, piv[NB + j]));
+        }
+        __syncwarp(mask);
+    }
+}
+
+// diag(U^H Ft U) for the group: thread j holds Ft row j (ftj); it forms
+// c_jq = conj(U_jq) (Ft U)_jq for every q from the group's padded U in shared
+// memory `su`, and the group sums c_jq over j with xor-shuffles (fixed tree).
+// Thread r returns diag_r.
+template <int NB, int GS, int LD>
+__device__ __forceinline__ double row_diag_uhfu(const double2 (&ftj)[NB], const double2* su, int r, unsigned mask,
+                                                bool live) {
+    double c[NB];
+    const int rr = live ? r : 0;
+#pragma unroll
+    for (int q = 0; q < NB; ++q) {
+        double2 wjq = mk(0.0, 0.0);
+#pragma unroll
+        for (int l = 0; l < NB; ++l) cfma(wjq, ftj[l], su[l * LD + q]);
+        const double2 ujq = su[rr * LD + q];
+        c[q] = live ? (ujq.x * wjq.x + ujq.y * wjq.y) : 0.0;
+    }
+#pragma unroll
+    for (int o = GS / 2; o > 0; o >>= 1)
+#pragma unroll
+        for (int q = 0; q < NB; ++q) c[q] += __shfl_xor_sync(mask, c[q], o);
+    double out = 0.0;
+#pragma unroll
+    for (int q = 0; q < NB; ++q)
+        if (q == r) out = c[q];
+    return out;
+}
+
+
+inline unsigned tiles_grid(int64_t nk, int KT, int cap) {
+    const int64_t nt = (nk + KT - 1) / KT;
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>(nt, cap));
+}
+
+
+#define SMALL_DISPATCH(nb, X) \
+    switch (nb) {             \
+        case 2: X(2); break;  \
+        case 4: X(4); break;  \
+        case 6: X(6); break;  \
+        case 8: X(8); break;  \
+        default: return fail(CPPHF_ERR_UNSUPPORTED, "small-nb kernel called with unsupported nb"); \
+    }
+
+
+}  // namespace tile
+}  // namespace cpphf
