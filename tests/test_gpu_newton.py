@@ -169,3 +169,20 @@ def test_newton_deflation_noop_and_errors(native):
     r_2 = native.solve_dm(args, P0, 4.0, 50, 1e-7, 0.0, 0.6, 0.5, 1e-3, 8, 10, 5, 25, 2, 0.5, 20,
                           np.empty((0, 2, 2, 2, 2), np.complex128), 0.0, 1.0, [], None, True, True, True)
     assert r_2[5] == r_cg["energy"] and r_2[6] == r_cg["n_iter"]
+
+
+def test_newton_full_size_history_matches_oracle(native):
+    """The 192x192, nb = 8 layered workload: the GPU solve against the oracle's
+    history (tests/golden/newton_layered192.npz, made by make_oracle_golden.py)."""
+    from conftest import GOLDEN
+
+    g = np.load(GOLDEN / "newton_layered192.npz")
+    args, P0, ne = workloads.layered(192, seed=0)
+    r = nc.solve(native, args, P0, ne, optimizer="newton", tol_grad=1e-6, max_iter=60)
+    print(f"  newton 192^2: iterations gpu {r['n_iter']} oracle {int(g['n_iter'])}, "
+          f"|dE| {abs(r['energy'] - float(g['energy'])):.2e}")
+    assert r["n_iter"] == int(g["n_iter"]) and r["converged"] == bool(g["converged"])
+    assert abs(r["energy"] - float(g["energy"])) < 1e-10 * abs(float(g["energy"]))
+    np.testing.assert_allclose(r["hist_E"], g["hist_E"], rtol=1e-11, atol=0)
+    np.testing.assert_allclose(r["hist_grad"], g["hist_grad"], rtol=1e-7, atol=0)
+    assert abs(float(np.sum(r["p"])) - float(g["p_sum"])) < 1e-8 * abs(float(g["p_sum"]))
