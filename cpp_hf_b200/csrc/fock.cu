@@ -257,14 +257,14 @@ __global__ void __launch_bounds__(kAsmThreads) k_assemble_tiled(AsmArgs a, int K
 // shared-memory stage with three (four) bulk copies while the CTA assembles the
 // current one, so each SM keeps two tiles of loads in flight.  The energy is
 // reduced in the same launch (last-block sum in a fixed order).
-template <bool REF>
+template <bool REF, int NBC>
 __global__ void __launch_bounds__(kAsmThreads) k_assemble_bulk(AsmArgs a, int KT, int64_t ntiles,
                                                                unsigned* counter, double* energy_out, int nst) {
     constexpr int NARR = REF ? 4 : 3;
     extern __shared__ __align__(16) unsigned char smem_dyn[];
     __shared__ double red[32];
     __shared__ __align__(8) unsigned long long bar[kAsmMaxStages];
-    const int nb = a.nb, nb2 = nb * nb;
+    const int nb = NBC > 0 ? NBC : a.nb, nb2 = nb * nb;
     const int tile = KT * nb2;
     double2* stg = reinterpret_cast<double2*>(
         (reinterpret_cast<uintptr_t>(smem_dyn) + 127) & ~(uintptr_t)127);
@@ -303,9 +303,16 @@ __global__ void __launch_bounds__(kAsmThreads) k_assemble_bulk(AsmArgs a, int KT
         const int nkt = (int)((a.nk - k0) < (int64_t)KT ? (a.nk - k0) : (int64_t)KT);
         const int n = nkt * nb2;
         const size_t base = (size_t)k0 * nb2;
-        for (int e = threadIdx.x; e < n; e += blockDim.x) {
-            const int kl = e / nb2, r = e - kl * nb2;
-            const int ii = r / nb, j = r - ii * nb;
+        for (int es = threadIdx.x; es < n; es += blockDim.x) {
+            // skewed order inside each k-block: slot (q, j) is element (q + j mod nb, j),
+            // so 8 consecutive threads touch 8 different 16-byte bank groups both in
+            // the element and in its transpose (row-major order puts the transposed
+            // reads 128 bytes apart: an 8-way bank conflict)
+            const int kl = es / nb2, sl = es - kl * nb2;
+            const int q = sl / nb, j = sl - q * nb;
+            const int ii = (q + j) < nb ? q + j : q + j - nb;
+            const int r = ii * nb + j;
+            const int e = kl * nb2 + r;
             const int eT = kl * nb2 + j * nb + ii;
             const double hdi = a.hd ? a.hd[ii] : 0.0;
             double2 se = sS[e], sT = sS[eT];
@@ -529,23 +536,29 @@ int build_fock(const cpphf_kernel* K, const double2* P, double2* Sigma, double2*
         const size_t smem = sizeof(double2) * (size_t)KT * nb2 * narr * cfg.nst + 128;
         static std::once_flag once_b;
         std::call_once(once_b, [] {
-            raise_smem(k_assemble_bulk<false>);
-            raise_smem(k_assemble_bulk<true>);
+            raise_smem(k_assemble_bulk<false, 0>);
+            raise_smem(k_assemble_bulk<true, 0>);
+            raise_smem(k_assemble_bulk<false, 8>);
+            raise_smem(k_assemble_bulk<true, 8>);
         });
         int per = 0;
         if (refP)
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_assemble_bulk<true>, kAsmThreads, smem);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_assemble_bulk<true, 0>, kAsmThreads, smem);
         else
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_assemble_bulk<false>, kAsmThreads, smem);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_assemble_bulk<false, 0>, kAsmThreads, smem);
         (void)cudaGetLastError();
         per = std::max(1, per);
         const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(ntiles, std::min<int64_t>(kMaxPartials, (int64_t)per * num_sms())));
         unsigned* counter = reinterpret_cast<unsigned*>(W + L.off_counter);
         if (energy) CPPHF_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned), st));
-        if (refP)
-            k_assemble_bulk<true><<<grid, kAsmThreads, smem, st>>>(a, KT, ntiles, counter, energy, cfg.nst);
+        if (refP && nb == 8)
+            k_assemble_bulk<true, 8><<<grid, kAsmThreads, smem, st>>>(a, KT, ntiles, counter, energy, cfg.nst);
+        else if (refP)
+            k_assemble_bulk<true, 0><<<grid, kAsmThreads, smem, st>>>(a, KT, ntiles, counter, energy, cfg.nst);
+        else if (nb == 8)
+            k_assemble_bulk<false, 8><<<grid, kAsmThreads, smem, st>>>(a, KT, ntiles, counter, energy, cfg.nst);
         else
-            k_assemble_bulk<false><<<grid, kAsmThreads, smem, st>>>(a, KT, ntiles, counter, energy, cfg.nst);
+            k_assemble_bulk<false, 0><<<grid, kAsmThreads, smem, st>>>(a, KT, ntiles, counter, energy, cfg.nst);
         CPPHF_LAUNCH_CHECK("assemble (bulk pipelined)");
         return CPPHF_OK;
     }
