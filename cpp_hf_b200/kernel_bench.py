@@ -24,7 +24,7 @@ from ._native import _DeviceKernel, _ptr, _stream, _ws
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--op", default="exchange",
-                    choices=["exchange", "exchange32", "exchange_hcp", "build", "eigh", "mu", "solve_dm", "solve_scf",
+                    choices=["exchange", "exchange32", "exchange_hcp", "build", "eigh", "mu", "solve_dm", "solve_scf", "solve_newton",
                              "sl_build", "sl_mesh_build", "sl_dm"])
     ap.add_argument("--pw", type=int, default=32, help="plane waves of the Dirac superlattice (sl_* ops)")
     ap.add_argument("--iters", type=int, default=10, help="solver iterations per call (solve_* ops)")
@@ -77,13 +77,16 @@ def main():
         def op():
             _lib.check(lib.cpphf_find_mu_bisection(_ptr(bands), _ptr(wt), a.n * a.n, nb, nb / 2.0, 0.05, 0,
                                                    _ptr(mu), _ptr(ws), ws.numel(), st), "mu")
-    elif a.op in ("solve_dm", "solve_scf"):
+    elif a.op in ("solve_dm", "solve_scf", "solve_newton"):
         from . import _native
 
         P0 = torch.zeros_like(P)
 
         def op():
-            if a.op == "solve_dm":
+            if a.op == "solve_newton":  # trust-region Newton, tol_grad 1e-6, at most --iters outer steps
+                _native.solve_dm(args, P0, float(a.layers), a.iters, 1e-7, 1e-6, 0.6, 0.5, 1e-3, 8, 10, 5, 25, 1,
+                                 0.5, 20, None, 0.0, 1.0, [], None, True, True, True)
+            elif a.op == "solve_dm":
                 _native.solve_dm(args, P0, float(a.layers), a.iters, 0.0, 0.0, 0.6, 0.5, 1e-3, 8, 10, 5, 25, 0,
                                  0.5, 20, None, 0.0, 1.0, [], None, True, True, True)
             else:
