@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(kThreads) k_rot_grad(const double2* __restrict
 // after the line search they hold the accepted trial's values and the
 // retraction reuses them.
 template <int NB>
-__global__ void __launch_bounds__(kThreads) k_trial_small(const double2* __restrict__ dQ, const double2* __restrict__ Ft,
+__global__ void __launch_bounds__(kThreads, 4) k_trial_small(const double2* __restrict__ dQ, const double2* __restrict__ Ft,
                                                           const double* __restrict__ p, const double* __restrict__ d_p,
                                                           const double* __restrict__ w, double* __restrict__ ew,
                                                           double2* __restrict__ Uout, int64_t nk, double T_r,
@@ -205,7 +205,7 @@ __global__ void __launch_bounds__(kThreads) k_trial_small(const double2* __restr
     extern __shared__ __align__(16) double2 dyn[];
     double2* sD = dyn;
     double2* sF = dyn + G::TILE;
-    double2* sU = dyn + 2 * G::TILE;
+    double2* sU = sD;  // U replaces d row by row once the elimination has read d
     __shared__ double2 sPiv[G::KT * 2 * NB];
     __shared__ double red[64];
     const int grp = threadIdx.x / G::GS, r = threadIdx.x % G::GS;
@@ -225,6 +225,7 @@ __global__ void __launch_bounds__(kThreads) k_trial_small(const double2* __restr
         if (grp < nkt) {
             double2 u[NB];
             row_cayley<NB, G::LD>(sD + grp * G::MS, tau, rr, sPiv + grp * 2 * NB, u, mask);
+            // (the elimination ends with a group barrier after its last read of d)
             if (live) {
                 double2* urow = Uout + ((size_t)k * NB + r) * NB;
 #pragma unroll
@@ -301,6 +302,7 @@ __global__ void __launch_bounds__(kThreads) k_retract_small(double2* Q, const do
         if (need_diag && grp < nkt) {
             double2 u[NB];
             row_cayley<NB, G::LD>(sD + grp * G::MS, tau, rr, sPiv + grp * 2 * NB, u, mask);
+            // (the elimination ends with a group barrier after its last read of d)
             if (live) {
 #pragma unroll
                 for (int j = 0; j < NB; ++j) sU[grp * G::MS + r * G::LD + j] = u[j];
@@ -518,7 +520,7 @@ int dm_small_trial(const double2* dQ, const double2* Ft, const double* p, const 
                    double fallback, DmScalars* S, cudaStream_t st) {
 #define X(N)                                                                                                         \
     small_attrs<N>();                                                                                                \
-    k_trial_small<N><<<tiles_grid(nk, Geo<N>::KT, kDmMaxPartials), kThreads, 3 * sizeof(double2) * Geo<N>::TILE,    \
+    k_trial_small<N><<<tiles_grid(nk, Geo<N>::KT, kDmMaxPartials), kThreads, 2 * sizeof(double2) * Geo<N>::TILE,    \
                        st>>>(dQ, Ft, p, d_p, w, ew, U, nk, T_r, shrink, last_trial, fallback, S);                    \
     CPPHF_LAUNCH_CHECK("trial");
     SMALL_DISPATCH(nb, X)
