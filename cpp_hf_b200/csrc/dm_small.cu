@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_trial_small(const double2* __re
     double2* sD = dyn;
     double2* sF = dyn + G::TILE;
     double2* sU = sD;  // U replaces d row by row once the elimination has read d
-    __shared__ double2 sPiv[G::KT * 2 * NB];
+    __shared__ double2 sPiv[G::KT * 4 * NB];
     __shared__ double red[64];
     const int grp = threadIdx.x / G::GS, r = threadIdx.x % G::GS;
     const unsigned mask = group_mask<NB>(threadIdx.x & 31);
@@ -224,18 +224,15 @@ __global__ void __launch_bounds__(kThreads, 4) k_trial_small(const double2* __re
         const int64_t k = k0 + grp;
         if (grp < nkt) {
             double2 u[NB];
-            row_cayley<NB, G::LD>(sD + grp * G::MS, tau, rr, sPiv + grp * 2 * NB, u, mask);
+            row_cayley<NB, G::LD>(sD + grp * G::MS, tau, rr, sPiv + grp * 4 * NB, u, mask);
             // (the elimination ends with a group barrier after its last read of d)
             if (live) {
-                double2* urow = Uout + ((size_t)k * NB + r) * NB;
 #pragma unroll
-                for (int j = 0; j < NB; ++j) {
-                    sU[grp * G::MS + r * G::LD + j] = u[j];
-                    urow[j] = u[j];
-                }
+                for (int j = 0; j < NB; ++j) sU[grp * G::MS + r * G::LD + j] = u[j];
             }
         }
         __syncthreads();
+        tile_store<NB>(Uout + (size_t)k0 * G::NB2, sU, nkt);  // coalesced
         if (grp < nkt) {
             double2 ftj[NB];
 #pragma unroll
@@ -277,7 +274,7 @@ __global__ void __launch_bounds__(kThreads) k_retract_small(double2* Q, const do
     double2* sF = dyn + G::TILE;
     double2* sU = dyn + 2 * G::TILE;
     double2* sQ = dyn + 3 * G::TILE;
-    __shared__ double2 sPiv[G::KT * 2 * NB];
+    __shared__ double2 sPiv[G::KT * 4 * NB];
     const int grp = threadIdx.x / G::GS, r = threadIdx.x % G::GS;
     const unsigned mask = group_mask<NB>(threadIdx.x & 31);
     const double tau = S->tau_final;
@@ -301,7 +298,7 @@ __global__ void __launch_bounds__(kThreads) k_retract_small(double2* Q, const do
         const int64_t k = k0 + grp;
         if (need_diag && grp < nkt) {
             double2 u[NB];
-            row_cayley<NB, G::LD>(sD + grp * G::MS, tau, rr, sPiv + grp * 2 * NB, u, mask);
+            row_cayley<NB, G::LD>(sD + grp * G::MS, tau, rr, sPiv + grp * 4 * NB, u, mask);
             // (the elimination ends with a group barrier after its last read of d)
             if (live) {
 #pragma unroll

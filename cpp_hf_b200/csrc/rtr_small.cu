@@ -321,7 +321,7 @@ __global__ void __launch_bounds__(kThreads) k_rtr_retract_small(const double2* _
     double2* sD = dyn;
     double2* sQ = dyn + G::TILE;
     double2* sF = dyn + 2 * G::TILE;
-    __shared__ double2 sPiv[G::KT * 2 * NB];
+    __shared__ double2 sPiv[G::KT * 4 * NB];
     const int grp = threadIdx.x / G::GS, r = threadIdx.x % G::GS;
     const unsigned mask = group_mask<NB>(threadIdx.x & 31);
     const int64_t ntiles = (nk + G::KT - 1) / G::KT;
@@ -339,7 +339,7 @@ __global__ void __launch_bounds__(kThreads) k_rtr_retract_small(const double2* _
             double2* q = sQ + grp * G::MS;
             {
                 double2 ur[NB];
-                row_cayley<NB, G::LD>(u, -1.0, rr, sPiv + grp * 2 * NB, ur, mask);
+                row_cayley<NB, G::LD>(u, -1.0, rr, sPiv + grp * 4 * NB, ur, mask);
                 if (live) {
 #pragma unroll
                     for (int j = 0; j < NB; ++j) u[rr * G::LD + j] = ur[j];

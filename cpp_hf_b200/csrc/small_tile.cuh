@@ -86,11 +86,13 @@ __device__ __forceinline__ unsigned group_mask(int lane) {
 // ---------------------------------------------------------------------------
 // Cayley unitary U(tau) = (I + tau d/2)^{-1} (I - tau d/2) of one k-point by
 // Gauss-Jordan elimination, one row per thread (row r of the result in u[]).
-// At step pp the owner of row pp divides its row by the pivot (one reciprocal
-// per step) and broadcasts it through the group's shared slot `piv`; the other
-// rows eliminate column pp, touching only the columns right of the pivot in
-// the left block (the ones left of it are already zero).  The rows end
-// normalised, so u[] is row r of U.
+// At step pp the owner of row pp publishes its unscaled row through the
+// group's shared slot `piv` (two slots, used alternately, so one group barrier
+// per step suffices); every thread then forms the reciprocal pivot itself:
+// the owner scales its row, the others subtract (f / pivot) times the
+// published row, touching only the columns right of the pivot in the left
+// block (the ones left of it are already zero).  The rows end normalised, so
+// u[] is row r of U.  `piv` holds 2 * 2 * NB values per group.
 // ---------------------------------------------------------------------------
 template <int NB, int LD>
 __device__ __forceinline__ void row_cayley(const double2* d, double tau, int r, double2* piv, double2 (&u)[NB],
@@ -106,31 +108,31 @@ __device__ __forceinline__ void row_cayley(const double2* d, double tau, int r, 
     }
 #pragma unroll
     for (int pp = 0; pp < NB; ++pp) {
+        double2* slot = piv + (pp & 1) * 2 * NB;
         if (r == pp) {
-            const double2 pv = mrow[pp];
-            const double inv = 1.0 / (pv.x * pv.x + pv.y * pv.y);
-            const double2 rp = mk(pv.x * inv, -pv.y * inv);
 #pragma unroll
-            for (int j = pp + 1; j < NB; ++j) {
-                mrow[j] = cmul(mrow[j], rp);
-                piv[j] = mrow[j];
-            }
+            for (int j = pp; j < NB; ++j) slot[j] = mrow[j];
 #pragma unroll
-            for (int j = 0; j < NB; ++j) {
-                u[j] = cmul(u[j], rp);
-                piv[NB + j] = u[j];
-            }
+            for (int j = 0; j < NB; ++j) slot[NB + j] = u[j];
         }
         __syncwarp(mask);
-        if (r != pp) {
-            const double2 f = mrow[pp];
+        const double2 pv = slot[pp];
+        const double inv = 1.0 / (pv.x * pv.x + pv.y * pv.y);
+        const double2 rp = mk(pv.x * inv, -pv.y * inv);
+        if (r == pp) {
 #pragma unroll
-            for (int j = pp + 1; j < NB; ++j) mrow[j] = csub(mrow[j], cmul(f, piv[j]));
+            for (int j = pp + 1; j < NB; ++j) mrow[j] = cmul(mrow[j], rp);
 #pragma unroll
-            for (int j = 0; j < NB; ++j) u[j] = csub(u[j], cmul(f, piv[NB + j]));
+            for (int j = 0; j < NB; ++j) u[j] = cmul(u[j], rp);
+        } else {
+            const double2 f = cmul(mrow[pp], rp);
+#pragma unroll
+            for (int j = pp + 1; j < NB; ++j) mrow[j] = csub(mrow[j], cmul(f, slot[j]));
+#pragma unroll
+            for (int j = 0; j < NB; ++j) u[j] = csub(u[j], cmul(f, slot[NB + j]));
         }
-        __syncwarp(mask);
     }
+    __syncwarp(mask);  // the last step's readers are done before `piv` is reused
 }
 
 // diag(U^H Ft U) for the group: thread j holds Ft row j (ftj); it forms
