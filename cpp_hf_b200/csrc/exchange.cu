@@ -270,6 +270,7 @@ struct PipeLayout {
 // 128-byte aligned shared-memory destinations); `total` includes the slack
 // for aligning the dynamic shared-memory base.
 constexpr int kMaxPipeStages = 4;
+constexpr int kColsMaxThreads = 128;  // launch bound of the pipelined columns pass
 
 __host__ __device__ inline PipeLayout pipe_layout(int N, int CB, size_t in_elem, bool second, int nst) {
     PipeLayout L;
@@ -280,6 +281,25 @@ __host__ __device__ inline PipeLayout pipe_layout(int N, int CB, size_t in_elem,
     L.stage_bytes = L.in_bytes + (second ? sizeof(double2) * (size_t)N * CB : 0);
     L.stage_bytes = (L.stage_bytes + 127) & ~(size_t)127;
     L.total = L.stage0 + (size_t)nst * L.stage_bytes + 128;
+    return L;
+}
+
+// Columns pass: the T tiles keep the ring of nst stages, VR has one buffer that
+// is refilled for the next tile as soon as the current tile's multiply has read
+// it (VR is read once per tile, in the middle of the transform).
+// smem: tw[N] | mbar[kMaxPipeStages + 1] | T stage[nst] | VR [N][CB] double2
+struct ColsLayout {
+    size_t tw, bar, stage0, stage_bytes, vr, total;
+};
+
+__host__ __device__ inline ColsLayout cols_layout(int N, int CB, size_t in_elem, int nst) {
+    ColsLayout L;
+    L.tw = 0;
+    L.bar = (sizeof(double2) * (size_t)N + 15) & ~(size_t)15;
+    L.stage0 = (L.bar + 8 * (kMaxPipeStages + 1) + 127) & ~(size_t)127;
+    L.stage_bytes = ((in_elem * (size_t)N * CB) + 127) & ~(size_t)127;
+    L.vr = L.stage0 + (size_t)nst * L.stage_bytes;
+    L.total = L.vr + ((sizeof(double2) * (size_t)N * CB + 127) & ~(size_t)127) + 128;
     return L;
 }
 
@@ -367,21 +387,25 @@ __global__ void __launch_bounds__(256, 2) k_rows_fwd_p(const __grid_constant__ C
     }
 }
 
-// pass B: columns forward, * VR, inverse.  Tile t -> (ky, chunk).
+// pass B: columns forward, * VR, inverse.  Tile t -> (ky, chunk).  At most 128
+// threads per CTA; three CTAs per SM for lines of up to 192 points.
 template <class Cx, int N1, int N2>
-__global__ void __launch_bounds__(256) k_cols_conv_p(const __grid_constant__ CUtensorMap mT,
-                                                     const __grid_constant__ CUtensorMap mV, Cx* T, ExchangeGeom g,
-                                                     int CB, int nchunk, int ntiles, int conjv, int nst) {
+__global__ void __launch_bounds__(kColsMaxThreads, (N1 * N2 <= 192 ? 3 : 1))
+    k_cols_conv_p(const __grid_constant__ CUtensorMap mT, const __grid_constant__ CUtensorMap mV, Cx* T,
+                  ExchangeGeom g, int CB, int nchunk, int ntiles, int conjv, int nst) {
     constexpr int N = N1 * N2;
     extern __shared__ __align__(16) unsigned char smem_dyn[];
     unsigned char* smem_raw = align128(smem_dyn);
-    const PipeLayout L = pipe_layout(N, CB, sizeof(Cx), true, nst);
+    const ColsLayout L = cols_layout(N, CB, sizeof(Cx), nst);
     Cx* tw = reinterpret_cast<Cx*>(smem_raw + L.tw);
     unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem_raw + L.bar);
+    unsigned long long* barV = bar + kMaxPipeStages;
+    const double2* Vt = reinterpret_cast<const double2*>(smem_raw + L.vr);
     const int c = threadIdx.x % CB, a = threadIdx.x / CB;
     build_line_twiddles(tw, N);
     if (threadIdx.x == 0) {
         for (int b = 0; b < nst; ++b) mbar_init(&bar[b], 1);
+        mbar_init(barV, 1);
         fence_mbar_init();
     }
     __syncthreads();
@@ -389,17 +413,24 @@ __global__ void __launch_bounds__(256) k_cols_conv_p(const __grid_constant__ CUt
         if (threadIdx.x != 0) return;
         const int ky = t / nchunk, c0 = (t - ky * nchunk) * CB;
         const unsigned boxT = (unsigned)(N * CB * sizeof(Cx));
-        const unsigned boxV = (unsigned)(N * (g.dv == 1 ? 1 : CB) * sizeof(double2));
         unsigned char* st = smem_raw + L.stage0 + (size_t)stage * L.stage_bytes;
         fence_proxy_async_smem();
-        mbar_arrive_expect_tx(&bar[stage], boxT + boxV);
+        mbar_arrive_expect_tx(&bar[stage], boxT);
         tma_load_3d(st, &mT, 2 * c0, ky, 0, &bar[stage]);
-        tma_load_3d(st + L.in_bytes, &mV, g.dv == 1 ? 0 : 2 * c0, ky, 0, &bar[stage]);
+    };
+    auto issue_vr = [&](int t) {
+        if (threadIdx.x != 0) return;
+        const int ky = t / nchunk, c0 = (t - ky * nchunk) * CB;
+        const unsigned boxV = (unsigned)(N * (g.dv == 1 ? 1 : CB) * sizeof(double2));
+        fence_proxy_async_smem();
+        mbar_arrive_expect_tx(barV, boxV);
+        tma_load_3d(smem_raw + L.vr, &mV, g.dv == 1 ? 0 : 2 * c0, ky, 0, barV);
     };
     const int s0 = g.shift ? g.n0 / 2 : 0;
     int i = 0;
     for (int j = 0; j < nst - 1; ++j)
         if ((int)blockIdx.x + j * (int)gridDim.x < ntiles) issue(blockIdx.x + j * gridDim.x, j);
+    if ((int)blockIdx.x < ntiles) issue_vr(blockIdx.x);
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
         const int stage = i % nst;
         {
@@ -409,7 +440,6 @@ __global__ void __launch_bounds__(256) k_cols_conv_p(const __grid_constant__ CUt
         if (!mbar_wait(&bar[stage], (unsigned)((i / nst) & 1))) return;
         unsigned char* st = smem_raw + L.stage0 + (size_t)stage * L.stage_bytes;
         Cx* S = reinterpret_cast<Cx*>(st);
-        const double2* Vt = reinterpret_cast<const double2*>(st + L.in_bytes);
         const int ky = t / nchunk, c0 = (t - ky * nchunk) * CB;
         const int ch = c0 + c;
         Cx v[N1];
@@ -429,6 +459,9 @@ __global__ void __launch_bounds__(256) k_cols_conv_p(const __grid_constant__ CUt
 #pragma unroll
             for (int n2 = 0; n2 < N2; ++n2) u[n2] = S[(a * N2 + n2) * CB + c];
             dft<N2, false>(u);
+        }
+        if (!mbar_wait(barV, (unsigned)(i & 1))) return;  // this tile's VR
+        if (a < N1) {
 #pragma unroll
             for (int k2 = 0; k2 < N2; ++k2) {
                 double2 w = g.dv == 1 ? Vt[a + N1 * k2] : Vt[(a + N1 * k2) * CB + c];
@@ -438,6 +471,7 @@ __global__ void __launch_bounds__(256) k_cols_conv_p(const __grid_constant__ CUt
             dft<N2, true>(u);
         }
         __syncthreads();
+        if (t + (int)gridDim.x < ntiles) issue_vr(t + gridDim.x);  // every read of VR is done
         if (a < N1) {
 #pragma unroll
             for (int na = 0; na < N2; ++na) S[(a * N2 + na) * CB + c] = cmulc(u[na], tw[na * a]);
@@ -1181,9 +1215,9 @@ struct Spec {
     static int cols(Cx* T, const double2* VR, const ExchangeGeom& g, int vmode, cudaStream_t st) {
         attrs();
         const PipeCfg cfg = cols_cfg();
-        if (pipelined(g, cfg) && vmode != kColsForwardOnly) {
+        if (pipelined(g, cfg) && vmode != kColsForwardOnly && pipe_launch(g, cfg).threads <= kColsMaxThreads) {
             const Launch L = pipe_launch(g, cfg);
-            const PipeLayout PL = pipe_layout(N1 * N2, L.CB, sizeof(Cx), true, cfg.nst);
+            const ColsLayout PL = cols_layout(N1 * N2, L.CB, sizeof(Cx), cfg.nst);
             if (PL.total <= kSmemMax) {
                 CUtensorMap mT, mV;
                 bool ok = field_map(&mT, T, tdt(), sizeof(Cx) / 2, g.Ct, g, 2 * L.CB, 1, N1 * N2);
