@@ -287,15 +287,19 @@ __host__ __device__ inline PipeLayout pipe_layout(int N, int CB, size_t in_elem,
 // Columns pass: the T tiles keep the ring of nst stages, VR has one buffer that
 // is refilled for the next tile as soon as the current tile's multiply has read
 // it (VR is read once per tile, in the middle of the transform).
-// smem: tw[N] | mbar[kMaxPipeStages + 1] | T stage[nst] | VR [N][CB] double2
+// The twiddle table holds w^m for m < N/2 when N is even (w^(m + N/2) = -w^m),
+// which keeps a 192-point line at three CTAs per SM.
+// smem: tw[N/2 or N] | mbar[kMaxPipeStages + 1] | T stage[nst] | VR [N][CB] double2
 struct ColsLayout {
     size_t tw, bar, stage0, stage_bytes, vr, total;
 };
 
+__host__ __device__ constexpr int cols_twiddles(int N) { return (N % 2 == 0) ? N / 2 : N; }
+
 __host__ __device__ inline ColsLayout cols_layout(int N, int CB, size_t in_elem, int nst) {
     ColsLayout L;
     L.tw = 0;
-    L.bar = (sizeof(double2) * (size_t)N + 15) & ~(size_t)15;
+    L.bar = (sizeof(double2) * (size_t)cols_twiddles(N) + 15) & ~(size_t)15;
     L.stage0 = (L.bar + 8 * (kMaxPipeStages + 1) + 127) & ~(size_t)127;
     L.stage_bytes = ((in_elem * (size_t)N * CB) + 127) & ~(size_t)127;
     L.vr = L.stage0 + (size_t)nst * L.stage_bytes;
@@ -402,7 +406,18 @@ __global__ void __launch_bounds__(kColsMaxThreads, (N1 * N2 <= 192 ? 3 : 1))
     unsigned long long* barV = bar + kMaxPipeStages;
     const double2* Vt = reinterpret_cast<const double2*>(smem_raw + L.vr);
     const int c = threadIdx.x % CB, a = threadIdx.x / CB;
-    build_line_twiddles(tw, N);
+    constexpr int NTW = cols_twiddles(N);
+    using R = decltype(Cx{}.x);
+    for (int m = threadIdx.x; m < NTW; m += blockDim.x) {
+        double sn, cs;
+        sincospi(-2.0 * (double)m / (double)N, &sn, &cs);
+        tw[m] = mk((R)cs, (R)sn);
+    }
+    auto twv = [&](int j) -> Cx {
+        if (NTW == N || j < NTW) return tw[j];
+        const Cx v = tw[j - NTW];
+        return mk(-v.x, -v.y);
+    };
     if (threadIdx.x == 0) {
         for (int b = 0; b < nst; ++b) mbar_init(&bar[b], 1);
         mbar_init(barV, 1);
@@ -451,7 +466,7 @@ __global__ void __launch_bounds__(kColsMaxThreads, (N1 * N2 <= 192 ? 3 : 1))
         __syncthreads();
         if (a < N2) {
 #pragma unroll
-            for (int k1 = 0; k1 < N1; ++k1) S[(k1 * N2 + a) * CB + c] = cmul(v[k1], tw[a * k1]);
+            for (int k1 = 0; k1 < N1; ++k1) S[(k1 * N2 + a) * CB + c] = cmul(v[k1], twv(a * k1));
         }
         __syncthreads();
         Cx u[N2];
@@ -474,7 +489,7 @@ __global__ void __launch_bounds__(kColsMaxThreads, (N1 * N2 <= 192 ? 3 : 1))
         if (t + (int)gridDim.x < ntiles) issue_vr(t + gridDim.x);  // every read of VR is done
         if (a < N1) {
 #pragma unroll
-            for (int na = 0; na < N2; ++na) S[(a * N2 + na) * CB + c] = cmulc(u[na], tw[na * a]);
+            for (int na = 0; na < N2; ++na) S[(a * N2 + na) * CB + c] = cmulc(u[na], twv(na * a));
         }
         __syncthreads();
         if (a < N2) {
