@@ -11,7 +11,8 @@
 // ordering uses __syncwarp().
 //
 // Element kernels (PR+ beta, direction): one thread per matrix element, so
-// every field access is coalesced; per-row terms are added by the j = 0 thread.
+// every field access is coalesced; the per-row occupation terms run in a
+// second loop, one row per thread (no divergent branch in the element loop).
 #include "common.cuh"
 #include "dm.cuh"
 #include "dm_small.cuh"
@@ -353,28 +354,24 @@ __global__ void __launch_bounds__(kThreadsE) k_pr_beta_small(const double2* __re
     __shared__ double red[96];
     const double lam = S->lam_pc, lam2 = lam * lam;
     double v[3] = {0.0, 0.0, 0.0};
-    const int64_t nrow = nk * NB;
+    const int64_t nrow = nk * NB, nel = nrow * NB;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < nrow; row += stride) {
-        const int64_t k = row / NB;
-        double2 g[NB], gp[NB];
-#pragma unroll
-        for (int j = 0; j < NB; ++j) {
-            g[j] = Gc[row * NB + j];
-            gp[j] = Gp[row * NB + j];
-        }
-        const double wk = w[k], ei = eps[row];
-        double a0 = 0.0, a1 = 0.0;
-#pragma unroll
-        for (int j = 0; j < NB; ++j) {
-            const double gap = ei - eps[k * NB + j];
-            const double rb = rsqrt(gap * gap + lam2);
-            const double2 d = mk(g[j].x * rb, g[j].y * rb);
-            a0 += (g[j].x * d.x + g[j].y * d.y) - (gp[j].x * d.x + gp[j].y * d.y);
-            a1 += gp[j].x * gp[j].x + gp[j].y * gp[j].y;
-        }
-        v[0] += wk * a0;
-        v[1] += wk * a1;
+    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    // matrix terms, one element per thread (coalesced)
+    for (int64_t e = tid; e < nel; e += stride) {
+        const int64_t row = e / NB, k = row / NB;
+        const int j = (int)(e - row * NB);
+        const double2 g = Gc[e], gp = Gp[e];
+        const double gap = eps[row] - eps[k * NB + j];
+        const double rb = rsqrt(gap * gap + lam2);
+        const double2 d = mk(g.x * rb, g.y * rb);
+        const double wk = w[k];
+        v[0] += wk * ((g.x * d.x + g.y * d.y) - (gp.x * d.x + gp.y * d.y));
+        v[1] += wk * (gp.x * gp.x + gp.y * gp.y);
+    }
+    // occupation terms, one row per thread
+    for (int64_t row = tid; row < nrow; row += stride) {
+        const double wk = w[row / NB];
         const double ps = fmin(fmax(p[row], OCC_CLIP), 1.0 - OCC_CLIP);
         const double gr = g_p[row], gq = g_pp[row];
         const double h = gr / (T_r / (ps * (1.0 - ps)));
@@ -410,31 +407,28 @@ __global__ void __launch_bounds__(kThreadsE) k_direction_small(const double2* __
     __shared__ double red[96];
     const double lam = S->lam_pc, lam2 = lam * lam, beta = S->beta;
     double v[3] = {0.0, 0.0, 0.0};
-    const int64_t nrow = nk * NB;
+    const int64_t nrow = nk * NB, nel = nrow * NB;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < nrow; row += stride) {
-        const int64_t k = row / NB;
-        double2 g[NB], q[NB];
-#pragma unroll
-        for (int j = 0; j < NB; ++j) {
-            g[j] = Gc[row * NB + j];
-            q[j] = beta != 0.0 ? dQp[row * NB + j] : mk(0.0, 0.0);
-        }
-        const double wk = w[k], ei = eps[row];
-        double a0 = 0.0;
-#pragma unroll
-        for (int j = 0; j < NB; ++j) {
-            const double gap = ei - eps[k * NB + j];
-            const double rb = rsqrt(gap * gap + lam2);
-            const double2 d = mk(g[j].x * rb + beta * q[j].x, g[j].y * rb + beta * q[j].y);
-            dQ[row * NB + j] = d;
-            a0 += d.x * d.x + d.y * d.y;
-        }
-        v[0] += wk * a0;
+    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    // matrix terms, one element per thread (coalesced)
+    for (int64_t e = tid; e < nel; e += stride) {
+        const int64_t row = e / NB, k = row / NB;
+        const int j = (int)(e - row * NB);
+        const double2 g = Gc[e];
+        const double2 q = beta != 0.0 ? dQp[e] : mk(0.0, 0.0);
+        const double gap = eps[row] - eps[k * NB + j];
+        const double rb = rsqrt(gap * gap + lam2);
+        const double2 d = mk(g.x * rb + beta * q.x, g.y * rb + beta * q.y);
+        dQ[e] = d;
+        v[0] += w[k] * (d.x * d.x + d.y * d.y);
+    }
+    // occupation terms, one row per thread
+    for (int64_t row = tid; row < nrow; row += stride) {
+        const double wk = w[row / NB];
         const double ps = fmin(fmax(p[row], OCC_CLIP), 1.0 - OCC_CLIP);
         const double h = g_p[row] / (T_r / (ps * (1.0 - ps)));
         d_p[row] = h + beta * dpp[row];
-        v[1] += wk * ps * ei;
+        v[1] += wk * ps * eps[row];
         v[2] -= wk * (ps * log(ps) + (1.0 - ps) * log1p(-ps));
     }
     double out[3];
