@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(kThreads) k_rot_grad(const double2* __restrict
 }
 
 // One backtracking trial (solver_dm.hpp:577-589) by elimination.
-// Dynamic shared memory: sD | sF | sU, TILE double2 each.
+// Dynamic shared memory: sD (d, then U) | sF, TILE double2 each.
 // Every trial that runs writes its U(tau) and diag(U^H Ft U) (to Uout, ew), so
 // after the line search they hold the accepted trial's values and the
 // retraction reuses them.
@@ -263,7 +263,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_trial_small(const double2* __re
 }
 
 // Retraction Q <- Q U(tau_final) and eps_work = diag(U^H Ft U).
-// Dynamic shared memory: sD | sF | sU | sQ, TILE double2 each.
+// Dynamic shared memory: sD (d, then U) | sF | sQ, TILE double2 each.
 template <int NB>
 __global__ void __launch_bounds__(kThreads) k_retract_small(double2* Q, const double2* __restrict__ dQ,
                                                             const double2* __restrict__ Ft, double* __restrict__ ew,
@@ -273,8 +273,8 @@ __global__ void __launch_bounds__(kThreads) k_retract_small(double2* Q, const do
     extern __shared__ __align__(16) double2 dyn[];
     double2* sD = dyn;
     double2* sF = dyn + G::TILE;
-    double2* sU = dyn + 2 * G::TILE;
-    double2* sQ = dyn + 3 * G::TILE;
+    double2* sU = sD;  // U: the accepted trial's, or the elimination's replacing d row by row
+    double2* sQ = dyn + 2 * G::TILE;
     __shared__ double2 sPiv[G::KT * 4 * NB];
     const int grp = threadIdx.x / G::GS, r = threadIdx.x % G::GS;
     const unsigned mask = group_mask<NB>(threadIdx.x & 31);
@@ -523,7 +523,7 @@ int dm_small_retract(double2* Q, const double2* dQ, const double2* Ft, double* e
                      int nb, const DmScalars* S, cudaStream_t st) {
 #define X(N)                                                                                                      \
     small_attrs<N>();                                                                                             \
-    k_retract_small<N><<<tiles_grid(nk, Geo<N>::KT, 16 * num_sms()), kThreads, 4 * sizeof(double2) * Geo<N>::TILE, \
+    k_retract_small<N><<<tiles_grid(nk, Geo<N>::KT, 16 * num_sms()), kThreads, 3 * sizeof(double2) * Geo<N>::TILE, \
                          st>>>(Q, dQ, Ft, ew, U, nk, S);                                                          \
     CPPHF_LAUNCH_CHECK("retract");
     SMALL_DISPATCH(nb, X)
