@@ -8,6 +8,7 @@
 // test.
 #include "common.cuh"
 #include "dm.cuh"
+#include "dm_small.cuh"
 #include "team.cuh"
 
 #include <algorithm>
@@ -580,6 +581,7 @@ int dm_check_nb(int64_t nb) {
 }
 
 int dm_density(const double2* Q, const double* p, double2* P, int64_t nk, int nb, cudaStream_t st) {
+    if (dm_small_supported(nb)) return dm_small_density(Q, p, P, nk, nb, st);
     init_attrs();
     const TeamLaunch L = team_launch(nk, nb);
     TEAM_DISPATCH(L, k_density, 2, nb, Q, p, P, nk, nb);

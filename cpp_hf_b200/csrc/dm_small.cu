@@ -42,7 +42,8 @@ __device__ __forceinline__ double expit(double x) {
 // P = herm(Q diag(p) Q^H) with p = expit((mu - ew) / T_r) computed here
 // (solver_dm.hpp:117-128 + 456-457/598-599); p written out.
 // ---------------------------------------------------------------------------
-template <int NB>
+// FROM_EW = false: the occupations are given in p (read, not written).
+template <int NB, bool FROM_EW>
 __global__ void __launch_bounds__(kThreads) k_dens_occ(const double2* __restrict__ Q, const double* __restrict__ ew,
                                                        const double* __restrict__ mu, double T_r, double* __restrict__ p,
                                                        double2* __restrict__ P, int64_t nk) {
@@ -51,16 +52,20 @@ __global__ void __launch_bounds__(kThreads) k_dens_occ(const double2* __restrict
     __shared__ double2 sX[G::TILE];
     __shared__ double sp[G::KT * NB];
     const int grp = threadIdx.x / G::GS, r = threadIdx.x % G::GS;
-    const double m = *mu;
+    const double m = FROM_EW ? *mu : 0.0;
     const int64_t ntiles = (nk + G::KT - 1) / G::KT;
     for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int64_t k0 = t * G::KT;
         const int nkt = (int)((nk - k0) < G::KT ? (nk - k0) : G::KT);
         tile_load<NB>(sQ, Q + (size_t)k0 * G::NB2, nkt);
         for (int e = threadIdx.x; e < nkt * NB; e += blockDim.x) {
-            const double pv = expit((m - ew[k0 * NB + e]) / T_r);
-            sp[e] = pv;
-            p[k0 * NB + e] = pv;
+            if (FROM_EW) {
+                const double pv = expit((m - ew[k0 * NB + e]) / T_r);
+                sp[e] = pv;
+                p[k0 * NB + e] = pv;
+            } else {
+                sp[e] = p[k0 * NB + e];
+            }
         }
         __syncthreads();
         if (grp < nkt && r < NB) {
@@ -448,6 +453,83 @@ unsigned rows_grid(int64_t nrow) {
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, std::min<int64_t>(kDmMaxPartials, 8 * num_sms())));
 }
 
+// ---------------------------------------------------------------------------
+// SCF residuals (solver_scf.hpp:64-75, 224-242): sum_k w_k |Pn - D|_F^2 and
+// sum_k w_k |F D - D F|_F^2 into S->grad_norm and S->lam_pc; the commutator
+// itself goes to comm_out when given (the C-DIIS residual).
+// ---------------------------------------------------------------------------
+template <int NB>
+__global__ void __launch_bounds__(kThreads) k_scf_residuals_small(const double2* __restrict__ F,
+                                                                  const double2* __restrict__ D,
+                                                                  const double2* __restrict__ Pn,
+                                                                  const double* __restrict__ w, int64_t nk,
+                                                                  DmScalars* S, double2* __restrict__ comm_out) {
+    using G = Geo<NB>;
+    __shared__ double2 sF[G::TILE];
+    __shared__ double2 sD[G::TILE];
+    __shared__ double red[64];
+    const int grp = threadIdx.x / G::GS, r = threadIdx.x % G::GS;
+    const int64_t ntiles = (nk + G::KT - 1) / G::KT;
+    double v[2] = {0.0, 0.0};
+    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int64_t k0 = t * G::KT;
+        const int nkt = (int)((nk - k0) < G::KT ? (nk - k0) : G::KT);
+        const int n = nkt * G::NB2;
+        tile_load<NB>(sF, F + (size_t)k0 * G::NB2, nkt);
+        tile_load<NB>(sD, D + (size_t)k0 * G::NB2, nkt);
+        double2 pv[G::PER];
+#pragma unroll
+        for (int u = 0; u < G::PER; ++u) {
+            const int e = threadIdx.x + u * kThreads;
+            pv[u] = e < n ? Pn[(size_t)k0 * G::NB2 + e] : mk(0.0, 0.0);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < G::PER; ++u) {
+            const int e = threadIdx.x + u * kThreads;
+            if (e < n) {
+                const int kl = e / G::NB2, rem = e - kl * G::NB2, i = rem / NB, j = rem - i * NB;
+                const double2 d = csub(pv[u], sD[kl * G::MS + i * G::LD + j]);
+                v[0] += w[k0 + kl] * (d.x * d.x + d.y * d.y);
+            }
+        }
+        const bool live = grp < nkt && r < NB;
+        double2 c[NB];
+        if (live) {
+            const double2* f = sF + grp * G::MS;
+            const double2* dd = sD + grp * G::MS;
+            double sc = 0.0;
+#pragma unroll
+            for (int j = 0; j < NB; ++j) {
+                double2 fp = mk(0.0, 0.0), pf = mk(0.0, 0.0);
+#pragma unroll
+                for (int l = 0; l < NB; ++l) {
+                    cfma(fp, f[r * G::LD + l], dd[l * G::LD + j]);
+                    cfma(pf, dd[r * G::LD + l], f[l * G::LD + j]);
+                }
+                c[j] = csub(fp, pf);
+                sc += c[j].x * c[j].x + c[j].y * c[j].y;
+            }
+            v[1] += w[k0 + grp] * sc;
+        }
+        if (comm_out) {  // grid-uniform
+            __syncthreads();  // every read of F is done
+            if (live) {
+#pragma unroll
+                for (int j = 0; j < NB; ++j) sF[grp * G::MS + r * G::LD + j] = c[j];
+            }
+            __syncthreads();
+            tile_store<NB>(comm_out + (size_t)k0 * G::NB2, sF, nkt);
+        }
+        __syncthreads();
+    }
+    double out[2];
+    if (reduce_last_block<2>(v, S->part, &S->counter, out, red) && threadIdx.x == 0) {
+        S->grad_norm = out[0];  // density residual^2 * weight_sum
+        S->lam_pc = out[1];     // commutator residual^2 * weight_sum
+    }
+}
+
 template <int NB>
 void small_attrs() {
     static std::once_flag once;
@@ -464,8 +546,29 @@ bool dm_small_supported(int nb) { return nb == 2 || nb == 4 || nb == 6 || nb == 
 int dm_small_dens_occ(const double2* Q, const double* ew, const double* mu, double T_r, double* p, double2* P,
                       int64_t nk, int nb, cudaStream_t st) {
 #define X(N)                                                                                                     \
-    k_dens_occ<N><<<tiles_grid(nk, Geo<N>::KT, 16 * num_sms()), kThreads, 0, st>>>(Q, ew, mu, T_r, p, P, nk); \
+    k_dens_occ<N, true><<<tiles_grid(nk, Geo<N>::KT, 16 * num_sms()), kThreads, 0, st>>>(Q, ew, mu, T_r, p, P, nk); \
     CPPHF_LAUNCH_CHECK("dens_occ");
+    SMALL_DISPATCH(nb, X)
+#undef X
+    return CPPHF_OK;
+}
+
+int dm_small_density(const double2* Q, const double* p, double2* P, int64_t nk, int nb, cudaStream_t st) {
+#define X(N)                                                                                                        \
+    k_dens_occ<N, false><<<tiles_grid(nk, Geo<N>::KT, 16 * num_sms()), kThreads, 0, st>>>(                          \
+        Q, nullptr, nullptr, 1.0, const_cast<double*>(p), P, nk);                                                   \
+    CPPHF_LAUNCH_CHECK("density");
+    SMALL_DISPATCH(nb, X)
+#undef X
+    return CPPHF_OK;
+}
+
+int scf_small_residuals(const double2* F, const double2* D, const double2* Pn, const double* w, int64_t nk, int nb,
+                        DmScalars* S, double2* comm_out, cudaStream_t st) {
+#define X(N)                                                                                                      \
+    k_scf_residuals_small<N><<<tiles_grid(nk, Geo<N>::KT, kDmMaxPartials), kThreads, 0, st>>>(F, D, Pn, w, nk, S, \
+                                                                                             comm_out);            \
+    CPPHF_LAUNCH_CHECK("scf residuals");
     SMALL_DISPATCH(nb, X)
 #undef X
     return CPPHF_OK;

@@ -7,6 +7,11 @@
 namespace cpphf {
 
 bool dm_small_supported(int nb);
+// SCF density and commutator residuals (S->grad_norm, S->lam_pc), commutator to comm_out if given
+int scf_small_residuals(const double2* F, const double2* D, const double2* Pn, const double* w, int64_t nk, int nb,
+                        DmScalars* S, double2* comm_out, cudaStream_t st);
+// P = herm(Q diag(p) Q^H) from given occupations p
+int dm_small_density(const double2* Q, const double* p, double2* P, int64_t nk, int nb, cudaStream_t st);
 int dm_small_dens_occ(const double2* Q, const double* ew, const double* mu, double T_r, double* p, double2* P,
                       int64_t nk, int nb, cudaStream_t st);
 int dm_small_rot_grad(const double2* Q, double2* F, const double* p, const double* w, double* eps, double2* Gout,

@@ -858,7 +858,9 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
         // the new C-DIIS residual goes to the slot after the newest entry
         // (overwriting the oldest when the ring is full)
         double2* comm_out = acc == 1 ? Rh + (size_t)hhead * nel : nullptr;
-        if (warp)
+        if (dm_small_supported(nb))
+            CPPHF_TRY(scf_small_residuals(F, D, Pn, K->w2d, nk, nb, S, comm_out, st));
+        else if (warp)
             k_scf_residuals<true><<<tgrid, 32 * kWarpTeams, rsmem, st>>>(F, D, Pn, K->w2d, nk, nb, S, comm_out);
         else
             k_scf_residuals<false><<<tgrid, kCtaTeamThreadsDense, rsmem, st>>>(F, D, Pn, K->w2d, nk, nb, S,
