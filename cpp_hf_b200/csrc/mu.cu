@@ -30,6 +30,7 @@ constexpr int64_t kMuOneBlockMax = 32768;             // eigenvalues handled by 
 constexpr int kBisectLevels = 3;                      // bisection steps per grid barrier
 constexpr int kMuNV = (1 << kBisectLevels) - 1;       // midpoints evaluated per barrier
 constexpr double kMuWide = 64.0;                      // exact multisection while the bracket exceeds 64 T
+constexpr int kMuWarmMaxIter = 8;                     // Newton rounds from a warm start before the cold path
 constexpr int kMuRootMaxIter = 80;                    // safeguarded Newton rounds (bisection fallback)
 
 __device__ __forceinline__ double expit(double x) {
@@ -53,7 +54,7 @@ struct MuArgs {
     int64_t n;        // nk * nb
     int nb;
     double target;
-    const double* mu0;  // device warm start (newton) or null
+    const double* mu0;  // device warm start (in-loop Newton; optional for the bisection's root) or null
     double T;
     int maxiter;
     int mode;  // 0 bisection (utils.hpp:49-75), 1 in-loop newton (utils.hpp:79-116)
@@ -272,55 +273,80 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
             Z = bc_tot[1];
             __syncthreads();
         };
-        while (ok && it < a.maxiter && (it == 0 || hi - lo > kMuWide * Tj)) msec_round();
-        if (ok && it < a.maxiter) {
-            // 2. root: secant start inside the bracket, then safeguarded Newton
-            double m = 0.5 * (lo + hi);
-            if (isfinite(Nlo) && isfinite(Nhi) && Nhi > Nlo) {
-                const double ms = lo + (a.target - Nlo) * (hi - lo) / (Nhi - Nlo);
-                if (ms > lo && ms < hi) m = ms;
-            }
-            double ra = lo, rb = hi, g = INFINITY, slope = 0.0;
-            bool conv = false;
-            for (int r = 0; ok && r < kMuRootMaxIter; ++r) {
+        // safeguarded Newton for the root of N(mu) = target inside [ra, rb]
+        struct Root {
+            double m, g, slope;
+            bool conv;
+        };
+        auto newton = [&](double m, double ra, double rb, int maxit) {
+            Root R{m, INFINITY, 0.0, false};
+            for (int r = 0; ok && r < maxit; ++r) {
                 double N = 0.0, Z = 0.0;
-                count_round(m, N, Z);
+                count_round(R.m, N, Z);
                 if (!ok) break;
-                g = N - a.target;
-                slope = Z;
-                if (fabs(g) <= epsN) {
-                    conv = true;
+                R.g = N - a.target;
+                R.slope = Z;
+                if (fabs(R.g) <= epsN) {
+                    R.conv = true;
                     break;
                 }
-                if (g > 0.0)
-                    rb = m;
+                if (R.g > 0.0)
+                    rb = R.m;
                 else
-                    ra = m;
-                double mn = (Z > 0.0) ? m - g / Z : NAN;
+                    ra = R.m;
+                double mn = (Z > 0.0) ? R.m - R.g / Z : NAN;
                 if (!(mn > ra && mn < rb)) mn = 0.5 * (ra + rb);
-                if (mn == m) break;
-                m = mn;
+                if (mn == R.m) break;
+                R.m = mn;
             }
-            const double thr = (conv && slope > 0.0) ? 8.0 * (fabs(g) + epsN) / slope : INFINITY;
-            if (ok && thr <= 0.125 * Tj) {
-                // 3. replay of the remaining levels
-                for (; ok && it < a.maxiter; ++it) {
-                    const double md = 0.5 * (lo + hi);
-                    bool up;
-                    if (fabs(md - m) > thr) {
-                        up = md > m;
-                    } else {
-                        double N = 0.0, Z = 0.0;
-                        count_round(md, N, Z);
-                        up = N > a.target;
-                    }
-                    if (up)
-                        hi = md;
-                    else
-                        lo = md;
+            return R;
+        };
+        // replay the levels left against the root when its threshold allows
+        auto replay = [&](const Root& R) {
+            const double thr = (R.conv && R.slope > 0.0) ? 8.0 * (fabs(R.g) + epsN) / R.slope : INFINITY;
+            if (!(ok && thr <= 0.125 * Tj)) return false;
+            for (; ok && it < a.maxiter; ++it) {
+                const double md = 0.5 * (lo + hi);
+                bool up;
+                if (fabs(md - R.m) > thr) {
+                    up = md > R.m;
+                } else {
+                    double N = 0.0, Z = 0.0;
+                    count_round(md, N, Z);
+                    up = N > a.target;
                 }
-            } else {
-                while (ok && it < a.maxiter) msec_round();
+                if (up)
+                    hi = md;
+                else
+                    lo = md;
+            }
+            return true;
+        };
+        // A warm start (the caller's previous mu, e.g. the last SCF iteration's)
+        // inside the initial bracket: Newton from there over the whole bracket and,
+        // if it converges, every level replayed from the top.  The levels depend
+        // only on the root, so the result is the same as from a cold start.
+        bool done = false;
+        if (a.mu0 && a.maxiter > 0) {
+            const double warm = *a.mu0;
+            if (isfinite(warm) && warm > lo && warm < hi) {
+                const Root R = newton(warm, lo, hi, kMuWarmMaxIter);
+                done = ok && replay(R);
+            }
+        }
+        if (!done && ok) {
+            while (ok && it < a.maxiter && (it == 0 || hi - lo > kMuWide * Tj)) msec_round();
+            if (ok && it < a.maxiter) {
+                // 2. root: secant start inside the bracket, then safeguarded Newton
+                double m = 0.5 * (lo + hi);
+                if (isfinite(Nlo) && isfinite(Nhi) && Nhi > Nlo) {
+                    const double ms = lo + (a.target - Nlo) * (hi - lo) / (Nhi - Nlo);
+                    if (ms > lo && ms < hi) m = ms;
+                }
+                const Root R = newton(m, lo, hi, kMuRootMaxIter);
+                // 3. replay, or exact multisection for a flat N
+                if (!replay(R))
+                    while (ok && it < a.maxiter) msec_round();
             }
         }
         if (!ok) {

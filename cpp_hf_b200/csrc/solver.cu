@@ -767,6 +767,7 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
 
     // the occupation mu: mu2[1] after a level shift, else mu2[0]
     double* mu_fin = (cfg->level_shift != 0.0) ? &mu2[1] : &mu2[0];
+    CPPHF_CUDA(cudaMemsetAsync(mu2, 0xFF, 2 * sizeof(double), st));  // NaN: no warm start yet
     // build_and_occupy (solver_scf.hpp:179-197); mu -> mu_fin, E -> S->energy
     // D is exactly Hermitian after the mixing kernel (it writes h and conj(h)) and
     // after a copy of P_new; hermitizing it again is a bitwise no-op and is skipped
@@ -774,7 +775,8 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
     // density_from_fock (solver_scf.hpp:96-154): P_out = herm(V f V^H) from Fsrc
     auto occupy = [&](const double2* Fsrc, double2* Pout) -> int {
         CPPHF_TRY(eigh_batched(Fsrc, eps, V, nk, nb, 0, nullptr, st));
-        CPPHF_TRY(mu_solve(eps, K->w2d, nk, nb, n_e, nullptr, K->T, 30, 0, &mu2[0], mws, L.mu_bytes, st));
+        // the previous iteration's mu warm-starts the bisection's root (same result)
+        CPPHF_TRY(mu_solve(eps, K->w2d, nk, nb, n_e, &mu2[0], K->T, 30, 0, &mu2[0], mws, L.mu_bytes, st));
         const double* e_occ = eps;
         if (cfg->level_shift != 0.0) {
             k_level_shift<<<grid_for(nk * nb, 256), 256, 0, st>>>(eps, &mu2[0], K->T, cfg->level_shift, sh, nk * nb);
@@ -784,7 +786,7 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
         // without a level shift the second bisection (solver_scf.hpp:136) runs on an
         // unchanged copy of eps and returns mu_raw itself
         if (cfg->level_shift != 0.0)
-            CPPHF_TRY(mu_solve(e_occ, K->w2d, nk, nb, n_e, nullptr, K->T, 30, 0, mu_fin, mws, L.mu_bytes, st));
+            CPPHF_TRY(mu_solve(e_occ, K->w2d, nk, nb, n_e, mu_fin, K->T, 30, 0, mu_fin, mws, L.mu_bytes, st));
         k_fermi<<<grid_for(nk * nb, 256), 256, 0, st>>>(e_occ, mu_fin, K->T, occ, nk * nb);
         CPPHF_LAUNCH_CHECK("fermi");
         // dm_density writes (X + X^H) / 2, exactly Hermitian: only a projector needs
