@@ -161,7 +161,8 @@ __global__ void __launch_bounds__(kThreads) k_rtr_dir_small(
 // A = (Ft X - X Ft) + St, HX = (C - C^H)/2 off the diagonal with
 // C_ij = (dp_j - dp_i) Ft_ij + (p_j - p_i) A_ij, Hp = Re A_bb + T dp_b /
 // (pc (1 - pc)) before the projection; sums Re<X,HX>, sum w dp Hp, sum w dp,
-// sum w Hp.  Dynamic shared memory: sQ | sR | sF | sX.
+// sum w Hp.  Dynamic shared memory: sQ (Q, then X) | sR | sF; X is loaded once
+// Q^H (R Q) is formed, so three tiles suffice (three CTAs per SM).
 // ---------------------------------------------------------------------------
 template <int NB>
 __global__ void __launch_bounds__(kThreads) k_rtr_hvp_small(
@@ -175,7 +176,7 @@ __global__ void __launch_bounds__(kThreads) k_rtr_hvp_small(
     double2* sQ = dyn;
     double2* sR = dyn + G::TILE;
     double2* sF = dyn + 2 * G::TILE;
-    double2* sX = dyn + 3 * G::TILE;
+    double2* sX = sQ;
     __shared__ double sdp[G::KT * NB];
     __shared__ double sp[G::KT * NB];
     __shared__ double red[32 * 4];
@@ -190,7 +191,6 @@ __global__ void __launch_bounds__(kThreads) k_rtr_hvp_small(
         const int n = nkt * G::NB2;
         tile_load<NB>(sQ, Q + (size_t)k0 * G::NB2, nkt);
         tile_load<NB>(sF, Ft + (size_t)k0 * G::NB2, nkt);
-        tile_load<NB>(sX, X + (size_t)k0 * G::NB2, nkt);
         {
             double2 fv[G::PER], hv[G::PER], pv[G::PER];
 #pragma unroll
@@ -220,14 +220,12 @@ __global__ void __launch_bounds__(kThreads) k_rtr_hvp_small(
             sp[e] = p[(size_t)k0 * NB + e];
         }
         __syncthreads();
+        double2 v[NB];
         if (grp < nkt) {
             const int rr = r < NB ? r : 0;
             const bool live = r < NB;
             const double2* q = sQ + grp * G::MS;
-            const double2* f = sF + grp * G::MS;
             double2* rm = sR + grp * G::MS;
-            double2* x = sX + grp * G::MS;
-            double2 v[NB];
 #pragma unroll
             for (int j = 0; j < NB; ++j) {  // (R Q)_rj
                 double2 a = mk(0.0, 0.0);
@@ -242,15 +240,31 @@ __global__ void __launch_bounds__(kThreads) k_rtr_hvp_small(
             }
             __syncwarp(mask);
 #pragma unroll
-            for (int j = 0; j < NB; ++j) {  // A_rj = ((Ft X)_rj - (X Ft)_rj) + (Q^H (R Q))_rj
-                double2 s1 = mk(0.0, 0.0), s2 = mk(0.0, 0.0), s3 = mk(0.0, 0.0);
+            for (int j = 0; j < NB; ++j) {  // St_rj = (Q^H (R Q))_rj
+                double2 s1 = mk(0.0, 0.0);
+#pragma unroll
+                for (int l = 0; l < NB; ++l) cfma(s1, cconj(q[l * G::LD + rr]), rm[l * G::LD + j]);
+                v[j] = s1;
+            }
+        }
+        __syncthreads();  // every read of Q is done: X takes its tile
+        tile_load<NB>(sX, X + (size_t)k0 * G::NB2, nkt);
+        __syncthreads();
+        if (grp < nkt) {
+            const int rr = r < NB ? r : 0;
+            const bool live = r < NB;
+            const double2* f = sF + grp * G::MS;
+            double2* rm = sR + grp * G::MS;
+            double2* x = sX + grp * G::MS;
+#pragma unroll
+            for (int j = 0; j < NB; ++j) {  // A_rj = ((Ft X)_rj - (X Ft)_rj) + St_rj
+                double2 s2 = mk(0.0, 0.0), s3 = mk(0.0, 0.0);
 #pragma unroll
                 for (int l = 0; l < NB; ++l) {
-                    cfma(s1, cconj(q[l * G::LD + rr]), rm[l * G::LD + j]);
                     cfma(s2, f[rr * G::LD + l], x[l * G::LD + j]);
                     cfma(s3, x[rr * G::LD + l], f[l * G::LD + j]);
                 }
-                v[j] = cadd(csub(s2, s3), s1);
+                v[j] = cadd(csub(s2, s3), v[j]);
             }
             __syncwarp(mask);
             const size_t kq = (size_t)(k0 + grp) * NB;
@@ -378,7 +392,7 @@ void rtr_small_attrs() {
     static std::once_flag once;
     std::call_once(once, [] {
         cudaFuncSetAttribute(k_rtr_hvp_small<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)(4 * sizeof(double2) * Geo<NB>::TILE));
+                             (int)(3 * sizeof(double2) * Geo<NB>::TILE));
         cudaFuncSetAttribute(k_rtr_retract_small<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(3 * sizeof(double2) * Geo<NB>::TILE));
         (void)cudaGetLastError();
@@ -408,7 +422,7 @@ int rtr_small_hvp(const double2* Xd, const double* dp, const double2* Q, const d
 #define X(N)                                                                                                     \
     rtr_small_attrs<N>();                                                                                        \
     k_rtr_hvp_small<N><<<tiles_grid(nk, Geo<N>::KT, kRtrMaxBlocks), kThreads,                                   \
-                         4 * sizeof(double2) * Geo<N>::TILE, st>>>(Xd, dp, Q, p, Ft, Fr, h, dP, pen, w, HX, Hp, \
+                         3 * sizeof(double2) * Geo<N>::TILE, st>>>(Xd, dp, Q, p, Ft, Fr, h, dP, pen, w, HX, Hp, \
                                                                    nk, T_r, R);                                  \
     CPPHF_LAUNCH_CHECK("rtr hvp");
     SMALL_DISPATCH(nb, X)
