@@ -9,6 +9,15 @@ the kernel on the device instead:
     Sigma, F, E = fb.build(P)                  # P: CUDA tensor (no copies) ...
     F_host, E = fb.build_host(P_pinned)        # ... or pinned host memory
 
+A stream of builds from host memory (many densities, results read back each
+time) pipelines the copies: ``begin_host_pipeline()``, then
+``build_host_async(P_host, F_host, E_host)`` per density (it returns the event
+after which F_host and E_host hold that result), then ``end_host_pipeline()``.  Two device buffer sets alternate; the upload of one
+density runs while the previous result is downloaded (PCIe is full duplex) and
+the build runs between them, each ordered by events.  A host buffer handed to
+``build_host_async`` must stay untouched until ``end_host_pipeline()`` (or a
+later synchronisation) returns.
+
 Each ``build`` is one call of ``cpphf_build_fock`` on the current stream
 (three exchange passes, the assembly kernel and the energy sum).
 """
@@ -55,6 +64,63 @@ class FockBuilder:
                                         _ptr(self.hd), _ptr(self.E), None, _ptr(self.ws), self.ws.numel(),
                                         _stream()), "build_fock")
         return self.Sigma, self.F, self.E
+
+    def _build_into(self, P: torch.Tensor, F: torch.Tensor, E: torch.Tensor):
+        check(self.lib.cpphf_build_fock(C.byref(self.dk.K), _ptr(P), _ptr(self.Sigma), _ptr(F), _ptr(self.hd),
+                                        _ptr(E), None, _ptr(self.ws), self.ws.numel(), _stream()), "build_fock")
+
+    def begin_host_pipeline(self):
+        """Start a pipelined sequence of host builds after the work already on the current stream."""
+        if getattr(self, "_pipe", None) is None:
+            dev = self.F.device
+            self._pipe = {
+                "s_in": torch.cuda.Stream(device=dev), "s_out": torch.cuda.Stream(device=dev),
+                "P": [self.P_dev, torch.empty_like(self.P_dev)], "F": [self.F, torch.empty_like(self.F)],
+                "E": [self.E, torch.zeros_like(self.E)],
+            }
+        pp = self._pipe
+        pp["built"], pp["out"], pp["i"] = [None, None], [None, None], 0
+        start = torch.cuda.Event()
+        start.record(torch.cuda.current_stream())
+        pp["s_in"].wait_event(start)
+
+    def build_host_async(self, P_host: torch.Tensor, F_host: torch.Tensor, E_host: torch.Tensor):
+        """One pipelined build: H2D of P on the copy-in stream, the build on the current
+        stream, D2H of F and E on the copy-out stream (see the module docstring).
+        Returns the CUDA event after which F_host and E_host hold the result."""
+        pp = self._pipe
+        b = pp["i"] & 1
+        pp["i"] += 1
+        cur = torch.cuda.current_stream()
+        s_in, s_out = pp["s_in"], pp["s_out"]
+        if pp["built"][b] is not None:
+            s_in.wait_event(pp["built"][b])  # the build two steps back no longer reads P[b]
+        with torch.cuda.stream(s_in):
+            pp["P"][b].copy_(P_host, non_blocking=True)
+        loaded = torch.cuda.Event()
+        loaded.record(s_in)
+        cur.wait_event(loaded)
+        if pp["out"][b] is not None:
+            cur.wait_event(pp["out"][b])  # F[b] and E[b] of two steps back are copied out
+        self._build_into(pp["P"][b], pp["F"][b], pp["E"][b])
+        built = torch.cuda.Event()
+        built.record(cur)
+        pp["built"][b] = built
+        s_out.wait_event(built)
+        with torch.cuda.stream(s_out):
+            F_host.copy_(pp["F"][b], non_blocking=True)
+            E_host.copy_(pp["E"][b], non_blocking=True)
+        out = torch.cuda.Event()
+        out.record(s_out)
+        pp["out"][b] = out
+        return out  # done once F_host and E_host hold this build's result
+
+    def end_host_pipeline(self):
+        """Order the current stream after every copy of the pipelined builds."""
+        cur = torch.cuda.current_stream()
+        for ev in self._pipe["out"]:
+            if ev is not None:
+                cur.wait_event(ev)
 
     def build_host(self, P_host: torch.Tensor, F_host: torch.Tensor, E_host: torch.Tensor):
         """End-to-end build from host memory: H2D of P, build, D2H of F and E (async on the stream)."""
