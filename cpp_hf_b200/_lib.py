@@ -77,6 +77,7 @@ class ScfConfig(C.Structure):
         ("max_iter", i64), ("density_tol", f64), ("comm_tol", f64), ("mixing", f64),
         ("level_shift", f64), ("acceleration", i32), ("reserved", i32), ("mixed_switch_tol", f64),
         ("diis_size", i32), ("diis_start", i32), ("diis_damping", f64), ("trust_radius", f64),
+        ("graphs", i32), ("reserved1", i32),
     ]
 
 

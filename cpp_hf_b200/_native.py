@@ -51,8 +51,9 @@ __all__ = [
 # and the commutator residuals (SCF), fall below "mixed_switch" (default 1e-5),
 # then complex128
 # to convergence; a single build_fock_apply under "mixed" is complex128.
-# "solve_graphs" (default True): solve_dm replays each iteration as a captured
-# CUDA graph; False launches every kernel (better for many concurrent solves).
+# "solve_graphs" (default True): solve_dm (and solve_scf with linear mixing)
+# replay each iteration as a captured CUDA graph; False launches every kernel
+# (better for many concurrent solves).
 DEFAULT_EXCHANGE_PRECISION = 64
 DEFAULT_MIXED_SWITCH = 1.0e-5
 
@@ -541,6 +542,7 @@ def solve_scf(kernel_args, P0, n_e, max_iter, density_tol, comm_tol, mixing, lev
     cfg.diis_size, cfg.diis_start = int(diis_size), int(diis_start)
     cfg.diis_damping, cfg.trust_radius = float(diis_damping), float(trust_radius)
     cfg.mixed_switch_tol = dk.mixed_switch
+    cfg.graphs = 1 if kernel_args.get("solve_graphs", True) else 0
     D = torch.empty_like(P0_t) if return_density else None
     F = torch.empty_like(P0_t) if return_fock else None
     hE = np.zeros(max(max_iter, 1))

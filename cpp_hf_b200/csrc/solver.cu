@@ -741,6 +741,8 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
     const ScfLayout L = scf_layout(K, cfg);
     if (!ws || wsb < L.total)
         return fail(CPPHF_ERR_INVALID, "solve_scf: workspace too small (" + std::to_string(L.total) + " bytes needed)");
+    const SolveStream guard(st);
+    st = guard.stream();
     unsigned char* W = static_cast<unsigned char*>(ws);
     auto fld = [&](size_t off) { return reinterpret_cast<double2*>(W + off); };
     auto vec = [&](size_t off) { return reinterpret_cast<double*>(W + off); };
@@ -855,19 +857,58 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
     std::vector<double> Bs((size_t)kDiisMax * kDiisMax, 0.0);
     double dbuf[kDiisMax];
 
+    // Linear mixing without a projector, trust radius or superlattice terms: the
+    // mix decided at the end of an iteration is deferred to the start of the next
+    // one, so every iteration after the first is the same launch sequence (mix,
+    // Fock build, occupations, residuals), captured once per precision.
+    const bool sl_path = K->sl && (K->sl->fock_active || K->sl->hartree_active);
+    const bool scf_graphs = cfg->graphs != 0 && guard.capturable && acc == 0 && !project && !Dpre && !sl_path &&
+                            solve_graphs_enabled();
+    IterGraphs sgr;
+    bool pending_mix = false;
     while (k < max_iter && !converged) {
-        CPPHF_TRY(build_and_occupy());
-        // the new C-DIIS residual goes to the slot after the newest entry
-        // (overwriting the oldest when the ring is full)
         double2* comm_out = acc == 1 ? Rh + (size_t)hhead * nel : nullptr;
-        if (dm_small_supported(nb))
-            CPPHF_TRY(scf_small_residuals(F, D, Pn, K->w2d, nk, nb, S, comm_out, st));
-        else if (warp)
-            k_scf_residuals<true><<<tgrid, 32 * kWarpTeams, rsmem, st>>>(F, D, Pn, K->w2d, nk, nb, S, comm_out);
-        else
-            k_scf_residuals<false><<<tgrid, kCtaTeamThreadsDense, rsmem, st>>>(F, D, Pn, K->w2d, nk, nb, S,
-                                                                                comm_out);
-        CPPHF_LAUNCH_CHECK("scf residuals");
+        auto body = [&]() -> int {
+            if (pending_mix) CPPHF_TRY(mix_into_D(D, Pn, cfg->mixing));
+            CPPHF_TRY(build_and_occupy());
+            // the new C-DIIS residual goes to the slot after the newest entry
+            // (overwriting the oldest when the ring is full)
+            if (dm_small_supported(nb))
+                CPPHF_TRY(scf_small_residuals(F, D, Pn, K->w2d, nk, nb, S, comm_out, st));
+            else if (warp)
+                k_scf_residuals<true><<<tgrid, 32 * kWarpTeams, rsmem, st>>>(F, D, Pn, K->w2d, nk, nb, S, comm_out);
+            else
+                k_scf_residuals<false><<<tgrid, kCtaTeamThreadsDense, rsmem, st>>>(F, D, Pn, K->w2d, nk, nb, S,
+                                                                                    comm_out);
+            CPPHF_LAUNCH_CHECK("scf residuals");
+            return CPPHF_OK;
+        };
+        const int lw = low ? 1 : 0;
+        bool replayed = false;
+        if (scf_graphs && pending_mix && d_hermitian) {
+            if (!sgr.exec[0][lw] && !sgr.failed[0][lw]) {
+                cudaGraph_t g = nullptr;
+                if (cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+                    sgr.failed[0][lw] = true;
+                } else {
+                    const int rc = body();
+                    const cudaError_t e = cudaStreamEndCapture(st, &g);
+                    if (rc != CPPHF_OK || e != cudaSuccess || !g ||
+                        cudaGraphInstantiate(&sgr.exec[0][lw], g, 0) != cudaSuccess) {
+                        sgr.failed[0][lw] = true;
+                        sgr.exec[0][lw] = nullptr;
+                    }
+                    if (g) cudaGraphDestroy(g);
+                }
+                (void)cudaGetLastError();
+            }
+            if (sgr.exec[0][lw]) {
+                CPPHF_CUDA(cudaGraphLaunch(sgr.exec[0][lw], st));
+                replayed = true;
+            }
+        }
+        if (!replayed) CPPHF_TRY(body());
+        pending_mix = false;
         int nslots = 0;
         int slots[kDiisMax];
         if (acc == 1) {
@@ -960,6 +1001,8 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
             else
                 lam = 0.0;
             CPPHF_TRY(mix_into_D(D, Pn, lam));
+        } else if (scf_graphs) {
+            pending_mix = true;  // the next iteration (or the finalisation) mixes first
         } else {
             CPPHF_TRY(mix_into_D(D, Pn, cfg->mixing));
         }
@@ -978,6 +1021,7 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
         if (hist_C) hist_C[k] = c_res;
         ++k;
     }
+    if (pending_mix) CPPHF_TRY(mix_into_D(D, Pn, cfg->mixing));
     CPPHF_TRY(build_and_occupy());
     if (D_out) CPPHF_CUDA(cudaMemcpyAsync(D_out, D, fbytes, cudaMemcpyDeviceToDevice, st));
     if (F_out) CPPHF_CUDA(cudaMemcpyAsync(F_out, F, fbytes, cudaMemcpyDeviceToDevice, st));

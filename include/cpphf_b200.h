@@ -310,6 +310,13 @@ typedef struct cpphf_scf_config {
     int32_t diis_start;
     double diis_damping;
     double trust_radius;
+    /* 1: with linear mixing, no projector and a plain mesh kernel, every
+     * iteration after the first (the previous iteration's mix, the Fock build, the
+     * occupation step and the residuals) is captured once per precision as a CUDA
+     * graph and replayed; 0: every kernel is launched (for many concurrent solves
+     * from several host threads). */
+    int32_t graphs;
+    int32_t reserved1;
 } cpphf_scf_config;
 
 typedef struct cpphf_scf_result {
