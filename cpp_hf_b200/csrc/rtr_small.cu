@@ -19,111 +19,123 @@ using namespace tile;
 
 // ---------------------------------------------------------------------------
 // Direction d (mode 0: z(r); 1: z(r) + beta d; 2: d given; 3: as 1 with beta
-// and shift_z formed from the update pass's sums) and its density variation
-// dP = herm(Q M Q^H), M = [X, diag p] off the diagonal, dp on it; sums <d,d>,
-// <v,d>, <v,v> in the joint metric.  z(r) = rX / sqrt(gap^2 + lam^2) and
-// rp p(1-p)/T - shift_z.
+// and shift_z formed from the update pass's sums), one element per thread
+// (coalesced), with the sums <d,d>, <v,d>, <v,v> in the joint metric.
+// z(r) = rX / sqrt(gap^2 + lam^2) and rp p(1-p)/T - shift_z.
 // ---------------------------------------------------------------------------
 template <int NB>
-__global__ void __launch_bounds__(kThreads) k_rtr_dir_small(
-    const double2* __restrict__ rX, const double* __restrict__ rp, const double* __restrict__ eps,
-    const double* __restrict__ p, const double* __restrict__ w, const double2* __restrict__ Q,
-    const double2* __restrict__ vX, const double* __restrict__ vp, double2* dX, double* dp, double2* __restrict__ dP,
-    int64_t nk, double T_r, double lam, double beta, double shift_z, double rz_old, int mode, RtrScalars* R) {
-    using G = Geo<NB>;
-    __shared__ double2 sQ[G::TILE];
-    __shared__ double2 sM[G::TILE];
-    __shared__ double sdp[G::KT * NB];
-    __shared__ double sp[G::KT * NB];
-    __shared__ double se[G::KT * NB];
+__global__ void __launch_bounds__(256) k_rtr_dir_elem(const double2* __restrict__ rX, const double* __restrict__ rp,
+                                                      const double* __restrict__ eps, const double* __restrict__ p,
+                                                      const double* __restrict__ w, const double2* __restrict__ vX,
+                                                      const double* __restrict__ vp, double2* dX, double* dp,
+                                                      int64_t nk, double T_r, double lam, double beta, double shift_z,
+                                                      double rz_old, int mode, RtrScalars* R) {
     __shared__ double red[32 * 3];
-    const int grp = threadIdx.x / G::GS, r = threadIdx.x % G::GS;
-    const unsigned mask = group_mask<NB>(threadIdx.x & 31);
-    const double lam2 = lam * lam;
     if (mode == 3) {  // beta and shift_z from the preceding update pass (same arithmetic as the host)
         const double den = R->sums[kSumW] * (double)NB;
         shift_z = den > 0.0 ? R->sums[kSumA3] / den : 0.0;
         beta = (R->sums[kSumA1] + R->sums[kSumA2] - shift_z * R->sums[kSumA4]) / rz_old;
         mode = 1;
     }
-    const int64_t ntiles = (nk + G::KT - 1) / G::KT;
+    const double lam2 = lam * lam;
+    const int64_t nrow = nk * NB, nel = nrow * NB;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     double acc[3] = {0.0, 0.0, 0.0};
+    for (int64_t e = tid; e < nel; e += stride) {
+        double2 d;
+        if (mode == 2) {
+            d = dX[e];
+        } else {
+            const int64_t row = e / NB, k = row / NB;
+            const int j = (int)(e - row * NB);
+            const double gap = eps[row] - eps[k * NB + j];
+            const double sc = sqrt(gap * gap + lam2);
+            const double2 rv = rX[e];
+            d = mk(rv.x / sc, rv.y / sc);
+            if (mode == 1) {
+                const double2 o = dX[e];
+                d = mk(d.x + beta * o.x, d.y + beta * o.y);
+            }
+            dX[e] = d;
+        }
+        acc[0] += d.x * d.x + d.y * d.y;
+        if (vX) {
+            const double2 v = vX[e];
+            acc[1] += v.x * d.x + v.y * d.y;
+            acc[2] += v.x * v.x + v.y * v.y;
+        }
+    }
+    for (int64_t q = tid; q < nrow; q += stride) {
+        double d;
+        if (mode == 2) {
+            d = dp[q];
+        } else {
+            const double pc = occ_clip(p[q]);
+            const double z = rp[q] * pc * (1.0 - pc) / T_r - shift_z;
+            d = mode == 0 ? z : z + beta * dp[q];
+            dp[q] = d;
+        }
+        const double wk = w[q / NB];
+        acc[0] += wk * d * d;
+        if (vp) {
+            const double v = vp[q];
+            acc[1] += wk * v * d;
+            acc[2] += wk * v * v;
+        }
+    }
+    double out[3];
+    if (reduce_last_block<3>(acc, R->part, &R->counter, out, red) && threadIdx.x == 0) {
+        R->sums[kSumDD] = out[0];
+        R->sums[kSumVD] = out[1];
+        R->sums[kSumVV] = out[2];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Density variation of a direction: dP = herm(Q M Q^H) with M = [X, diag p]
+// off the diagonal (X_ij (p_j - p_i)) and dp on it (solver_rtr.hpp:61-75).
+// ---------------------------------------------------------------------------
+template <int NB>
+__global__ void __launch_bounds__(kThreads) k_rtr_dP_small(const double2* __restrict__ Q,
+                                                           const double2* __restrict__ X,
+                                                           const double* __restrict__ dp,
+                                                           const double* __restrict__ p, double2* __restrict__ dP,
+                                                           int64_t nk) {
+    using G = Geo<NB>;
+    __shared__ double2 sQ[G::TILE];
+    __shared__ double2 sM[G::TILE];
+    __shared__ double sdp[G::KT * NB];
+    __shared__ double sp[G::KT * NB];
+    const int grp = threadIdx.x / G::GS, r = threadIdx.x % G::GS;
+    const unsigned mask = group_mask<NB>(threadIdx.x & 31);
+    const int64_t ntiles = (nk + G::KT - 1) / G::KT;
     for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int64_t k0 = t * G::KT;
         const int nkt = (int)((nk - k0) < G::KT ? (nk - k0) : G::KT);
         const int n = nkt * G::NB2;
         tile_load<NB>(sQ, Q + (size_t)k0 * G::NB2, nkt);
-        double2 rv[G::PER], ov[G::PER], xv[G::PER];
-#pragma unroll
-        for (int u = 0; u < G::PER; ++u) {
-            const int e = threadIdx.x + u * kThreads;
-            const size_t g = (size_t)k0 * G::NB2 + e;
-            rv[u] = ov[u] = xv[u] = mk(0.0, 0.0);
-            if (e < n) {
-                if (mode == 2) {
-                    rv[u] = dX[g];
-                } else {
-                    rv[u] = rX[g];
-                    if (mode == 1) ov[u] = dX[g];
-                }
-                if (vX) xv[u] = vX[g];
-            }
-        }
+        tile_load<NB>(sM, X + (size_t)k0 * G::NB2, nkt);
         for (int e = threadIdx.x; e < nkt * NB; e += kThreads) {
-            const size_t q = (size_t)k0 * NB + e;
-            const double pv = p[q];
-            double d;
-            if (mode == 2) {
-                d = dp[q];
-            } else {
-                const double pc = occ_clip(pv);
-                const double z = rp[q] * pc * (1.0 - pc) / T_r - shift_z;
-                d = mode == 0 ? z : z + beta * dp[q];
-                dp[q] = d;
-                se[e] = eps[q];
-            }
-            sdp[e] = d;
-            sp[e] = pv;
-            const double wk = w[k0 + e / NB];
-            acc[0] += wk * d * d;
-            if (vp) {
-                const double v = vp[q];
-                acc[1] += wk * v * d;
-                acc[2] += wk * v * v;
-            }
-        }
-        __syncthreads();
-#pragma unroll
-        for (int u = 0; u < G::PER; ++u) {
-            const int e = threadIdx.x + u * kThreads;
-            if (e < n) {
-                const int kl = e / G::NB2, rem = e - kl * G::NB2, i = rem / NB, j = rem - i * NB;
-                double2 d = rv[u];
-                if (mode != 2) {
-                    const double gap = se[kl * NB + i] - se[kl * NB + j];
-                    const double sc = sqrt(gap * gap + lam2);
-                    d = mk(d.x / sc, d.y / sc);
-                    if (mode == 1) d = mk(d.x + beta * ov[u].x, d.y + beta * ov[u].y);
-                    dX[(size_t)k0 * G::NB2 + e] = d;
-                }
-                acc[0] += d.x * d.x + d.y * d.y;
-                acc[1] += xv[u].x * d.x + xv[u].y * d.y;
-                acc[2] += xv[u].x * xv[u].x + xv[u].y * xv[u].y;
-                sM[kl * G::MS + i * G::LD + j] =
-                    (i == j) ? mk(sdp[kl * NB + i], 0.0) : cscale(d, sp[kl * NB + j] - sp[kl * NB + i]);
-            }
+            sdp[e] = dp[(size_t)k0 * NB + e];
+            sp[e] = p[(size_t)k0 * NB + e];
         }
         __syncthreads();
         if (grp < nkt) {
             const int rr = r < NB ? r : 0;
             const double2* q = sQ + grp * G::MS;
             double2* m = sM + grp * G::MS;
+            const double* pk = sp + grp * NB;
+            const double* dk = sdp + grp * NB;
             double2 tr[NB];
 #pragma unroll
-            for (int j = 0; j < NB; ++j) {  // (Q M)_rj
+            for (int j = 0; j < NB; ++j) {  // (Q M)_rj, M formed from X on the fly
                 double2 a = mk(0.0, 0.0);
 #pragma unroll
-                for (int l = 0; l < NB; ++l) cfma(a, q[rr * G::LD + l], m[l * G::LD + j]);
+                for (int l = 0; l < NB; ++l) {
+                    const double2 mlj = (l == j) ? mk(dk[l], 0.0) : cscale(m[l * G::LD + j], pk[j] - pk[l]);
+                    cfma(a, q[rr * G::LD + l], mlj);
+                }
                 tr[j] = a;
             }
             double2 dr[NB];
@@ -134,7 +146,7 @@ __global__ void __launch_bounds__(kThreads) k_rtr_dir_small(
                 for (int l = 0; l < NB; ++l) cfmac(a, tr[l], q[j * G::LD + l]);
                 dr[j] = a;
             }
-            __syncwarp(mask);  // every row of M has been read
+            __syncwarp(mask);  // every row of X has been read
             if (r < NB) {
 #pragma unroll
                 for (int j = 0; j < NB; ++j) m[rr * G::LD + j] = dr[j];
@@ -147,12 +159,6 @@ __global__ void __launch_bounds__(kThreads) k_rtr_dir_small(
             dP[(size_t)k0 * G::NB2 + e] = mk(0.5 * (a.x + b.x), 0.5 * (a.y - b.y));
         }
         __syncthreads();
-    }
-    double out[3];
-    if (reduce_last_block<3>(acc, R->part, &R->counter, out, red) && threadIdx.x == 0) {
-        R->sums[kSumDD] = out[0];
-        R->sums[kSumVD] = out[1];
-        R->sums[kSumVV] = out[2];
     }
 }
 
@@ -407,10 +413,13 @@ int rtr_small_direction(const double2* rX, const double* rp, const double* eps, 
                         const double2* Q, const double2* vX, const double* vp, double2* dX, double* dp, double2* dP,
                         int64_t nk, int nb, double T_r, double lam, double beta, double shift_z, double rz_old,
                         int mode, RtrScalars* R, cudaStream_t st) {
-#define X(N)                                                                                             \
-    k_rtr_dir_small<N><<<tiles_grid(nk, Geo<N>::KT, kRtrMaxBlocks), kThreads, 0, st>>>(                 \
-        rX, rp, eps, p, w, Q, vX, vp, dX, dp, dP, nk, T_r, lam, beta, shift_z, rz_old, mode, R);       \
-    CPPHF_LAUNCH_CHECK("rtr direction");
+    const unsigned eg = flat_grid(nk * (int64_t)nb * nb, 256);  // one resident wave (4 x 256 threads per SM)
+#define X(N)                                                                                                   \
+    k_rtr_dir_elem<N><<<eg, 256, 0, st>>>(rX, rp, eps, p, w, vX, vp, dX, dp, nk, T_r, lam, beta, shift_z, rz_old, \
+                                          mode, R);                                                            \
+    CPPHF_LAUNCH_CHECK("rtr direction");                                                                       \
+    k_rtr_dP_small<N><<<tiles_grid(nk, Geo<N>::KT, 16 * num_sms()), kThreads, 0, st>>>(Q, dX, dp, p, dP, nk);  \
+    CPPHF_LAUNCH_CHECK("rtr density variation");
     SMALL_DISPATCH(nb, X)
 #undef X
     return CPPHF_OK;
