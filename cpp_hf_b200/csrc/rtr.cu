@@ -700,8 +700,9 @@ int solve_rtr(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* 
     // energy (+ bias), Ft = Q^H (F + S_pen) Q, eps = diag Ft, gradient G and its
     // norm, and the preconditioner scale lam_pc (solver_rtr.hpp:300-302)
     double hE[2] = {0.0, 0.0}, hg[2] = {0.0, 0.0}, hlam[2] = {0.0, 0.0};
-    double hb[4];
-    double sums[kNumSums];
+    double* const hb = host_scalars();  // pinned scalar read-back: hb[0..3], then the sums
+    double* const sums = hb + 8;
+    static_assert(8 + kNumSums <= kHostScalars, "host scalar layout");
     auto eval = [&](int s, bool with_model) -> int {
         CPPHF_TRY(finish_density());
         CPPHF_TRY(build_fock(K, P, Sig, Ft[s], nullptr, &R->energy[s], nullptr, fws, L.fock_bytes, st));

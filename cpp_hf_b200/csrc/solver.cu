@@ -293,6 +293,27 @@ bool diis_solve(std::vector<double> A, int n, std::vector<double>& x) {
 
 }  // namespace
 
+namespace {
+struct PinnedScalars {
+    double* p = nullptr;
+    ~PinnedScalars() {
+        if (p) cudaFreeHost(p);
+    }
+};
+}  // namespace
+
+double* host_scalars() {
+    thread_local PinnedScalars h;
+    thread_local double pageable[kHostScalars];
+    if (!h.p && cudaHostAlloc(reinterpret_cast<void**>(&h.p), kHostScalars * sizeof(double), cudaHostAllocDefault) !=
+                    cudaSuccess) {
+        (void)cudaGetLastError();
+        h.p = nullptr;
+        return pageable;
+    }
+    return h.p;
+}
+
 unsigned grid_for(int64_t n, int threads) {
     const int64_t want = (n + threads - 1) / threads;
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)num_sms() * 8));
@@ -526,7 +547,8 @@ int solve_dm(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* P
     CPPHF_TRY(eigh_batched(F, ew, Q, nk, nb, 0, nullptr, st));
     CPPHF_TRY(mu_solve(ew, wn, nk, nb, n_t, &S->mu, T_r, mu_it, 1, &S->mu, mws, L.mu_bytes, st));
 
-    double hbuf[4] = {0.0, 0.0, 0.0, 0.0};  // scalar read-back (pageable; each read is followed by a sync)
+    double* const hbuf = host_scalars();  // scalar read-back; each read is followed by a sync
+    for (int i = 0; i < 4; ++i) hbuf[i] = 0.0;
 
     double grad_norm = std::numeric_limits<double>::infinity();
     double E_prev = std::numeric_limits<double>::infinity();
@@ -758,7 +780,8 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
     CPPHF_CUDA(cudaMemsetAsync(S, 0, sizeof(DmScalars), st));
     CPPHF_CUDA(cudaMemcpyAsync(D, P0, fbytes, cudaMemcpyDeviceToDevice, st));
 
-    double hbuf[4] = {0.0, 0.0, 0.0, 0.0};  // scalar read-back (pageable; each read is followed by a sync)
+    double* const hbuf = host_scalars();  // scalar read-back; each read is followed by a sync
+    for (int i = 0; i < 4; ++i) hbuf[i] = 0.0;
 
     // switched precision: complex64 exchange until the density and commutator
     // residuals both fall below mixed_switch_tol; convergence is only accepted
@@ -855,7 +878,8 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
     int hcount = 0, hhead = 0;  // DIIS ring: entries held, next slot
     // Bs[a * kDiisMax + b] = <R_a, R_b>_w for ring slots a, b
     std::vector<double> Bs((size_t)kDiisMax * kDiisMax, 0.0);
-    double dbuf[kDiisMax];
+    double* const dbuf = hbuf + 8;  // DIIS overlaps of the newest residual
+    static_assert(8 + kDiisMax + 3 <= kHostScalars, "host scalar layout");
 
     // Linear mixing without a projector, trust radius or superlattice terms: the
     // mix decided at the end of an iteration is deferred to the start of the next
@@ -988,7 +1012,7 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
             CPPHF_TRY(build_fock(low ? &K32 : K, Pn, Sn, Fn, nullptr, &mu2[2], nullptr, fws, L.fock_bytes, st));
             k_oda_c1<<<rgrid, 256, 0, st>>>(F, D, Pn, K->w2d, nk, nb, S, &mu2[3]);
             CPPHF_LAUNCH_CHECK("oda slope");
-            double e2[2];
+            double* const e2 = hbuf + 8 + kDiisMax;
             CPPHF_CUDA(cudaMemcpyAsync(e2, &mu2[2], 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
             CPPHF_CUDA(cudaStreamSynchronize(st));
             const double c1 = e2[1];
@@ -1010,9 +1034,10 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
             // ---- trust-radius clip (solver_scf.hpp:410-428) ----
             k_wdiff2<<<rgrid, 256, 0, st>>>(D, Dpre, K->w2d, nk, nb2, S, &mu2[2]);
             CPPHF_LAUNCH_CHECK("trust step norm");
-            double s2 = 0.0;
-            CPPHF_CUDA(cudaMemcpyAsync(&s2, &mu2[2], sizeof(double), cudaMemcpyDeviceToHost, st));
+            double* const hs2 = hbuf + 8 + kDiisMax + 2;
+            CPPHF_CUDA(cudaMemcpyAsync(hs2, &mu2[2], sizeof(double), cudaMemcpyDeviceToHost, st));
             CPPHF_CUDA(cudaStreamSynchronize(st));
+            const double s2 = *hs2;
             const double step = std::sqrt(s2 / wsum);
             if (step > cfg->trust_radius) CPPHF_TRY(mix_into_D(Dpre, D, cfg->trust_radius / step));
         }
