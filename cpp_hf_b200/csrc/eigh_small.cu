@@ -107,12 +107,14 @@ __global__ void __launch_bounds__(kHqlThreads, 4) k_eigh_hql(const double2* __re
 #pragma unroll
             for (int i = kk + 1; i < NB; ++i) xn2 += a[i].x * a[i].x + a[i].y * a[i].y;
             const double2 x0 = a[kk + 1];
-            const double ax0 = hypot(x0.x, x0.y);
+            // entries are O(1) after the scaling, so the plain modulus cannot overflow
+            const double ax0 = sqrt(fma(x0.x, x0.x, x0.y * x0.y));
             const double xn = sqrt(xn2);
 #pragma unroll
             for (int i = 0; i < NB; ++i) ul[i] = mk(0.0, 0.0);
             if (xn > 0.0) {
-                const double2 ph = ax0 > 0.0 ? mk(x0.x / ax0, x0.y / ax0) : mk(1.0, 0.0);
+                const double iax = ax0 > 0.0 ? 1.0 / ax0 : 0.0;
+                const double2 ph = ax0 > 0.0 ? mk(x0.x * iax, x0.y * iax) : mk(1.0, 0.0);
                 al = mk(-ph.x * xn, -ph.y * xn);
                 ul[kk + 1] = mk(x0.x + ph.x * xn, x0.y + ph.y * xn);
 #pragma unroll
@@ -196,9 +198,12 @@ __global__ void __launch_bounds__(kHqlThreads, 4) k_eigh_hql(const double2* __re
     for (int i = 0; i < NB; ++i) {
         z[i] = cmul(z[i], delta);
         if (i + 1 < NB) {
-            const double m = hypot(sub[i].x, sub[i].y);
+            const double m = sqrt(fma(sub[i].x, sub[i].x, sub[i].y * sub[i].y));
             e[i] = m;
-            if (m > 0.0) delta = cmul(delta, mk(sub[i].x / m, sub[i].y / m));
+            if (m > 0.0) {
+                const double im = 1.0 / m;
+                delta = cmul(delta, mk(sub[i].x * im, sub[i].y * im));
+            }
         } else {
             e[i] = 0.0;
         }
