@@ -235,9 +235,20 @@ __global__ void __launch_bounds__(kHqlThreads, 4) k_eigh_hql(const double2* __re
                 if (j == l + 1) dl1 = d[j];
                 if (j == m) dm = d[j];
             }
-            double g = (dl1 - dl) / (2.0 * el);
-            double rr = sqrt(fma(g, g, 1.0));
-            g = dm - dl + el / (g + copysign(rr, g));
+            // Wilkinson shift: with t = d[l+1] - d[l], u = 2 e[l] and g0 = t / u,
+            // el / (g0 + sign(g0) sqrt(g0^2 + 1)) = el u / (t + sign(t) sqrt(t^2 + u^2)):
+            // one division instead of two (the tridiagonal is O(1), so t^2 + u^2
+            // can only vanish by underflow; the two-division form covers that case)
+            const double t = dl1 - dl, u2 = 2.0 * el;
+            const double den = t + copysign(sqrt(fma(t, t, u2 * u2)), t);
+            double g;
+            if (den != 0.0) {
+                g = dm - dl + el * u2 / den;
+            } else {
+                g = t / u2;
+                g = dm - dl + el / (g + copysign(sqrt(fma(g, g, 1.0)), g));
+            }
+            double rr;
             double s = 1.0, c = 1.0, p = 0.0;
             bool under = false;
 #pragma unroll
