@@ -24,7 +24,7 @@ using namespace tile;
 // z(r) = rX / sqrt(gap^2 + lam^2) and rp p(1-p)/T - shift_z.
 // ---------------------------------------------------------------------------
 template <int NB>
-__global__ void __launch_bounds__(256) k_rtr_dir_elem(const double2* __restrict__ rX, const double* __restrict__ rp,
+__global__ void __launch_bounds__(256, 4) k_rtr_dir_elem(const double2* __restrict__ rX, const double* __restrict__ rp,
                                                       const double* __restrict__ eps, const double* __restrict__ p,
                                                       const double* __restrict__ w, const double2* __restrict__ vX,
                                                       const double* __restrict__ vp, double2* dX, double* dp,
@@ -42,28 +42,51 @@ __global__ void __launch_bounds__(256) k_rtr_dir_elem(const double2* __restrict_
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     double acc[3] = {0.0, 0.0, 0.0};
-    for (int64_t e = tid; e < nel; e += stride) {
-        double2 d;
-        if (mode == 2) {
-            d = dX[e];
-        } else {
-            const int64_t row = e / NB, k = row / NB;
-            const int j = (int)(e - row * NB);
-            const double gap = eps[row] - eps[k * NB + j];
-            const double sc = sqrt(gap * gap + lam2);
-            const double2 rv = rX[e];
-            d = mk(rv.x / sc, rv.y / sc);
-            if (mode == 1) {
-                const double2 o = dX[e];
-                d = mk(d.x + beta * o.x, d.y + beta * o.y);
+    // U elements per round, their loads issued before any is used (the pass is
+    // bound by load latency); each thread still sums its elements in index order
+    constexpr int U = 2;
+    for (int64_t eb = tid; eb < nel; eb += U * stride) {
+        double2 rv[U], ov[U], xv[U];
+        double ea[U], ec[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int64_t e = eb + u * stride;
+            rv[u] = ov[u] = xv[u] = mk(0.0, 0.0);
+            ea[u] = ec[u] = 0.0;
+            if (e < nel) {
+                if (mode == 2) {
+                    ov[u] = dX[e];
+                } else {
+                    const int64_t row = e / NB, k = row / NB;
+                    const int j = (int)(e - row * NB);
+                    rv[u] = rX[e];
+                    if (mode == 1) ov[u] = dX[e];
+                    ea[u] = eps[row];
+                    ec[u] = eps[k * NB + j];
+                }
+                if (vX) xv[u] = vX[e];
             }
-            dX[e] = d;
         }
-        acc[0] += d.x * d.x + d.y * d.y;
-        if (vX) {
-            const double2 v = vX[e];
-            acc[1] += v.x * d.x + v.y * d.y;
-            acc[2] += v.x * v.x + v.y * v.y;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int64_t e = eb + u * stride;
+            if (e < nel) {
+                double2 d;
+                if (mode == 2) {
+                    d = ov[u];
+                } else {
+                    const double gap = ea[u] - ec[u];
+                    const double sc = sqrt(gap * gap + lam2);
+                    d = mk(rv[u].x / sc, rv[u].y / sc);
+                    if (mode == 1) d = mk(d.x + beta * ov[u].x, d.y + beta * ov[u].y);
+                    dX[e] = d;
+                }
+                acc[0] += d.x * d.x + d.y * d.y;
+                if (vX) {
+                    acc[1] += xv[u].x * d.x + xv[u].y * d.y;
+                    acc[2] += xv[u].x * xv[u].x + xv[u].y * xv[u].y;
+                }
+            }
         }
     }
     for (int64_t q = tid; q < nrow; q += stride) {
