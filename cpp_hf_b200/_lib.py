@@ -99,6 +99,9 @@ class Symmetry(C.Structure):
 _SIGS = {
     "cpphf_last_error": (C.c_char_p, []),
     "cpphf_version": (C.c_int, []),
+    "cpphf_device_error": (C.c_int, [C.c_int]),
+    "cpphf_set_barrier_spin_limit": (C.c_int, [C.c_longlong]),
+    "cpphf_barrier_spin_limit": (C.c_longlong, []),
     "cpphf_copy_d2h": (C.c_int, [vp, vp, sz, vp]),
     "cpphf_copy_h2d": (C.c_int, [vp, vp, sz, vp]),
     "cpphf_exchange_workspace_bytes": (sz, [i64, i64, i64, C.c_int, C.c_int]),
@@ -192,3 +195,23 @@ def check(status: int, what: str = "") -> None:
     if status == CPPHF_ERR_UNSUPPORTED:
         raise NotImplementedError(msg)
     raise NativeError(f"{what}: status {status}: {msg}")
+
+
+def check_device_error(what: str = "") -> None:
+    """Raise if a bounded device wait gave up since the last check.
+
+    Reads and clears the library's device error word (``cpphf_device_error``,
+    which synchronises the device); used by the calls that return host results.
+    """
+    v = load().cpphf_device_error(1)
+    if v == 0:
+        return
+    if v < 0:
+        check(v, what)
+    kinds = []
+    if v & 2:
+        kinds.append("a grid barrier")
+    if v & 1:
+        kinds.append("an asynchronous-copy wait")
+    raise NativeError(f"{what}: status {CPPHF_ERR_TIMEOUT}: {' and '.join(kinds) or 'a wait'} on the device gave up "
+                      "(bounded wait timeout)")

@@ -153,7 +153,11 @@ def selfenergy_fft_full(VR, P, apply_ifftshift=True, hermitian_channel_packing=F
     P_t = _to_dev(P, "c")
     VR_t = _to_dev(VR, "c")
     sigma = _exchange(VR_t, P_t, apply_ifftshift, hermitian_channel_packing)
-    return _out(sigma, as_np)
+    if as_np:
+        out = _out(sigma, True)
+        _lib.check_device_error("selfenergy_fft_full")
+        return out
+    return sigma
 
 
 def clear_fft_plan_cache():
@@ -243,8 +247,9 @@ def find_mu_bisection(bands, weights, n_e, T, maxiter=0):
     check(lib.cpphf_find_mu_bisection(_ptr(b), _ptr(w), nk, nb, float(n_e), float(T), int(maxiter),
                                       _ptr(out), _ptr(ws), ws.numel(), _stream()), "find_mu_bisection")
     mu = float(out.item())
+    _lib.check_device_error("find_mu_bisection")
     if not math.isfinite(mu):
-        raise _lib.NativeError("find_mu_bisection: device wait timed out or non-finite result")
+        raise _lib.NativeError("find_mu_bisection: non-finite result")
     return mu
 
 
@@ -413,7 +418,9 @@ def build_fock_apply(kernel_args, P, project_fn):
         elif not dproj.is_identity:
             dproj.project_(F)
             F = 0.5 * (F + F.conj().transpose(-1, -2))
-    return _out(Sigma, as_np), _out(H, as_np), _out(F, as_np), float(E.item())
+    E_host = float(E.item())
+    _lib.check_device_error("build_fock_apply")
+    return _out(Sigma, as_np), _out(H, as_np), _out(F, as_np), E_host
 
 
 # ---------------------------------------------------------------------------

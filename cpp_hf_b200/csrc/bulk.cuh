@@ -2,9 +2,10 @@
 // shared memory with mbarrier completion, plus bounded waits.
 //
 // Only global -> shared::cta copies of this GPU's own memory; no multicast.
-// Every wait is bounded: after kSpinLimit polls it records an error in
-// g_cpphf_device_error (read and cleared with cpphf_device_error()) and
-// returns false so the kernel can stop instead of hanging.
+// Every wait is bounded: after kMbarSpinLimit polls it ORs a code into the
+// library's device error word (the pointer every launch with such waits is
+// given; see wait_error_word()) and returns false so the kernel can stop
+// instead of hanging.
 #pragma once
 
 #include "common.cuh"
@@ -12,10 +13,6 @@
 #include <cuda.h>
 
 namespace cpphf {
-
-// Set by bounded waits that gave up; one copy per translation unit that
-// includes this header (read through that unit's cpphf_device_error()).
-static __device__ unsigned int g_cpphf_device_error = 0;
 
 constexpr long long kMbarSpinLimit = 2000000LL;
 
@@ -99,12 +96,12 @@ bool make_tensor_map_3d(CUtensorMap* map, const void* base, CUtensorMapDataType 
                         unsigned long long d1, unsigned long long d2, unsigned long long stride1_bytes,
                         unsigned long long stride2_bytes, unsigned b0, unsigned b1, unsigned b2);
 
-// Bounded wait for phase `parity`; false (and the device error flag set) on timeout.
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+// Bounded wait for phase `parity`; false (and kWaitErrMbar ORed into *err) on timeout.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, unsigned* err) {
     long long spins = 0;
     while (!mbar_try_wait(bar, parity)) {
         if (++spins > kMbarSpinLimit) {
-            atomicOr(&g_cpphf_device_error, 1u);
+            if (err) atomicOr(err, kWaitErrMbar);
             return false;
         }
     }

@@ -4,6 +4,7 @@
 
 #include <cudaTypedefs.h>
 
+#include <atomic>
 #include <mutex>
 #include <string>
 
@@ -24,6 +25,52 @@ int cuda_fail(cudaError_t e, const char* where) {
     g_last_error = std::string(where) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
     return CPPHF_ERR_CUDA;
 }
+
+// The device error word (one object per device: this is the only translation
+// unit that defines it; other units receive its address).
+__device__ unsigned g_wait_error = 0;
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::atomic<long long> g_barrier_spin_limit{kBarrierSpinLimit};
+}  // namespace
+
+unsigned* wait_error_word() {
+    static std::mutex mtx;
+    static unsigned* ptrs[kMaxDevices] = {nullptr};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+        (void)cudaGetLastError();
+        set_error("device error word: no usable current device");
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lock(mtx);
+    if (!ptrs[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_wait_error) != cudaSuccess) {
+            cuda_fail(cudaGetLastError(), "device error word lookup");
+            return nullptr;
+        }
+        ptrs[dev] = static_cast<unsigned*>(p);
+    }
+    return ptrs[dev];
+}
+
+int check_wait_error(cudaStream_t st, const char* where) {
+    unsigned* w = wait_error_word();
+    if (!w) return CPPHF_ERR_CUDA;
+    unsigned v = 0;
+    CPPHF_CUDA(cudaMemcpyAsync(&v, w, sizeof(v), cudaMemcpyDeviceToHost, st));
+    CPPHF_CUDA(cudaStreamSynchronize(st));
+    if (v == 0) return CPPHF_OK;
+    CPPHF_CUDA(cudaMemsetAsync(w, 0, sizeof(unsigned), st));
+    CPPHF_CUDA(cudaStreamSynchronize(st));
+    std::string what = (v & kWaitErrBarrier) ? "a grid barrier" : "";
+    if (v & kWaitErrMbar) what += what.empty() ? "an asynchronous-copy wait" : " and an asynchronous-copy wait";
+    return fail(CPPHF_ERR_TIMEOUT, std::string(where) + ": " + what + " on the device gave up (bounded wait timeout)");
+}
+
+long long barrier_spin_limit() { return g_barrier_spin_limit.load(std::memory_order_relaxed); }
 
 int num_sms() {
     int dev = 0;
@@ -64,6 +111,23 @@ extern "C" {
 const char* cpphf_last_error(void) { return cpphf::g_last_error.c_str(); }
 
 int cpphf_version(void) { return CPPHF_ABI_VERSION; }
+
+int cpphf_set_barrier_spin_limit(long long polls) {
+    cpphf::g_barrier_spin_limit.store(polls > 0 ? polls : cpphf::kBarrierSpinLimit, std::memory_order_relaxed);
+    return CPPHF_OK;
+}
+
+long long cpphf_barrier_spin_limit(void) { return cpphf::barrier_spin_limit(); }
+
+int cpphf_device_error(int clear) {
+    unsigned* w = cpphf::wait_error_word();
+    if (!w) return CPPHF_ERR_CUDA;
+    unsigned v = 0;
+    CPPHF_CUDA(cudaDeviceSynchronize());
+    CPPHF_CUDA(cudaMemcpy(&v, w, sizeof(v), cudaMemcpyDeviceToHost));
+    if (clear && v) CPPHF_CUDA(cudaMemset(w, 0, sizeof(unsigned)));
+    return (int)v;
+}
 
 }  // extern "C"
 

@@ -40,6 +40,25 @@ int cuda_fail(cudaError_t e, const char* where);
 
 int num_sms();
 
+// ---------------------------------------------------------------------------
+// Device error word.  One per device (a __device__ variable of capi.cu): a
+// bounded wait that gives up ORs a code into it, the kernel returns, and the
+// host learns of it when it next reads the word (check_wait_error(), which
+// synchronises the stream, or cpphf_device_error()).  Launches with bounded
+// waits receive its address in their arguments.
+// ---------------------------------------------------------------------------
+constexpr unsigned kWaitErrMbar = 1u;     // an mbarrier (TMA / bulk copy) wait
+constexpr unsigned kWaitErrBarrier = 2u;  // a grid barrier of a cooperative kernel
+
+// Address of the current device's error word (nullptr and the error text set
+// if it cannot be looked up).
+unsigned* wait_error_word();
+// Synchronise `st`, read the current device's error word and clear it; a set
+// word returns CPPHF_ERR_TIMEOUT with `where` in the message.
+int check_wait_error(cudaStream_t st, const char* where);
+// Grid-barrier poll limit in force (cpphf_set_barrier_spin_limit).
+long long barrier_spin_limit();
+
 // Raise a kernel's dynamic shared-memory limit to the device opt-in maximum
 // minus its static shared memory.  Attribute calls never leave a sticky error.
 template <class F>
@@ -107,6 +126,18 @@ __device__ __forceinline__ void st_l2(double2* p, double2 v) { __stcg(p, v); }
 __device__ __forceinline__ float2 ld_l2(const float2* p) { return __ldcg(p); }
 __device__ __forceinline__ void st_l2(float2* p, float2 v) { __stcg(p, v); }
 
+// Kahan-compensated per-thread accumulator (a thread's long serial chain of
+// terms); the cross-thread sums that follow are short fixed trees.
+struct Kahan {
+    double s = 0.0, c = 0.0;
+    __device__ __forceinline__ void add(double x) {
+        const double y = x - c;
+        const double t = s + y;
+        c = (t - s) - y;
+        s = t;
+    }
+};
+
 // ---------------------------------------------------------------------------
 // Warp / block reductions (fixed order -> deterministic)
 // ---------------------------------------------------------------------------
@@ -152,8 +183,11 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double (&scratch)[M])
 // ---------------------------------------------------------------------------
 // Bounded grid barrier for cooperative launches.  `sync[0]` = arrival count,
 // `sync[1]` = generation, `sync[2]` = error flag; zeroed before the launch.
-// A wait that exceeds the spin limit records CPPHF_ERR_TIMEOUT and every later
-// barrier returns at once, so no block can wait forever.
+// A wait that exceeds the poll limit sets the flag (and kWaitErrBarrier in the
+// device error word), every block waiting on the barrier sees the flag and
+// returns, and every later barrier returns at once, so no block waits forever.
+// The limit is a launch argument (default kBarrierSpinLimit, settable through
+// cpphf_set_barrier_spin_limit).
 // ---------------------------------------------------------------------------
 constexpr long long kBarrierSpinLimit = 20000000LL;  // polls (each an L2 round trip) -> seconds
 #ifndef CPPHF_POLL_SLEEP_NS
@@ -169,8 +203,19 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
 
 struct GridBarrier {
     unsigned* sync;
+    unsigned* err;
+    long long limit;
     unsigned gen;
-    __device__ void init(unsigned* s) { sync = s; gen = 0; }
+    __device__ void init(unsigned* s, long long spin_limit, unsigned* err_word) {
+        sync = s;
+        err = err_word;
+        limit = spin_limit;
+        gen = 0;
+    }
+    __device__ void give_up() {
+        atomicExch(&sync[2], 1u);
+        if (err) atomicOr(err, kWaitErrBarrier);
+    }
     // Returns false if the barrier failed (timeout seen anywhere).
     __device__ bool wait() {
         __syncthreads();
@@ -191,8 +236,8 @@ struct GridBarrier {
                     long long spins = 0;
                     while (ld_acquire_u32(&sync[1]) == gen) {
                         if (ld_acquire_u32(&sync[2]) != 0u) { ok = 0; break; }
-                        if (++spins > kBarrierSpinLimit) {
-                            atomicExch(&sync[2], 1u);
+                        if (++spins > limit) {
+                            give_up();
                             ok = 0;
                             break;
                         }
@@ -251,8 +296,12 @@ struct GridBarrier {
         } else if (threadIdx.x == 0) {
             long long spins = 0;
             while (ld_acquire_u32(&sync[1]) == gen) {
-                if (++spins > kBarrierSpinLimit) {
-                    atomicExch(&sync[2], 1u);
+                if (ld_acquire_u32(&sync[2]) != 0u) {
+                    ok_sh = 0;
+                    break;
+                }
+                if (++spins > limit) {
+                    give_up();
                     ok_sh = 0;
                     break;
                 }

@@ -21,8 +21,8 @@ int eigh_batched(const double2* M, double* w, double2* V, int64_t batch, int64_t
                  const BlockSpec* bs, cudaStream_t st);
 int make_block_spec(int64_t nb, const int64_t* sizes, int64_t n_sizes, int sort, BlockSpec& bs);
 
-// Householder + implicit QL path for 2 <= nb <= 8 (eigh_small.cu); CPPHF_EIGH_HQL=0
-// selects the Jacobi kernels instead.
+// Householder + implicit QL path for 2 <= nb <= 8 (eigh_small.cu); other nb run
+// the Jacobi kernels of eigh.cu.
 bool eigh_small_enabled(int64_t nb);
 int eigh_small(const double2* M, double* w, double2* V, int64_t batch, int64_t nb, int mode, cudaStream_t st);
 

@@ -335,13 +335,7 @@ __global__ void __launch_bounds__(kHqlThreads, 4) k_eigh_hql(const double2* __re
 
 }  // namespace
 
-bool eigh_small_enabled(int64_t nb) {
-    static const bool on = [] {
-        const char* e = std::getenv("CPPHF_EIGH_HQL");
-        return !(e && e[0] == '0');
-    }();
-    return on && nb >= 2 && nb <= 8;
-}
+bool eigh_small_enabled(int64_t nb) { return nb >= 2 && nb <= 8; }
 
 int eigh_small(const double2* M, double* w, double2* V, int64_t batch, int64_t nb, int mode, cudaStream_t st) {
     const int64_t threads = batch * (nb <= 2 ? 2 : (nb <= 4 ? 4 : 8));

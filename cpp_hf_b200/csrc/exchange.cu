@@ -354,7 +354,7 @@ __global__ void __launch_bounds__(256, 2) k_rows_fwd_p(const __grid_constant__ C
             const int ahead = t + (nst - 1) * (int)gridDim.x;
             if (ahead < ntiles) issue(ahead, (i + nst - 1) % nst);
         }
-        if (!mbar_wait(&bar[stage], (unsigned)((i / nst) & 1))) return;
+        if (!mbar_wait(&bar[stage], (unsigned)((i / nst) & 1), g.err)) return;
         unsigned char* st = smem_raw + L.stage0 + (size_t)stage * L.stage_bytes;
         const double2* in = reinterpret_cast<const double2*>(st);
         const double2* rin = reinterpret_cast<const double2*>(st + L.in_bytes);
@@ -452,7 +452,7 @@ __global__ void __launch_bounds__(kColsMaxThreads, (N1 * N2 <= 192 ? 3 : 1))
             const int ahead = t + (nst - 1) * (int)gridDim.x;
             if (ahead < ntiles) issue(ahead, (i + nst - 1) % nst);
         }
-        if (!mbar_wait(&bar[stage], (unsigned)((i / nst) & 1))) return;
+        if (!mbar_wait(&bar[stage], (unsigned)((i / nst) & 1), g.err)) return;
         unsigned char* st = smem_raw + L.stage0 + (size_t)stage * L.stage_bytes;
         Cx* S = reinterpret_cast<Cx*>(st);
         const int ky = t / nchunk, c0 = (t - ky * nchunk) * CB;
@@ -475,7 +475,7 @@ __global__ void __launch_bounds__(kColsMaxThreads, (N1 * N2 <= 192 ? 3 : 1))
             for (int n2 = 0; n2 < N2; ++n2) u[n2] = S[(a * N2 + n2) * CB + c];
             dft<N2, false>(u);
         }
-        if (!mbar_wait(barV, (unsigned)(i & 1))) return;  // this tile's VR
+        if (!mbar_wait(barV, (unsigned)(i & 1), g.err)) return;  // this tile's VR
         if (a < N1) {
 #pragma unroll
             for (int k2 = 0; k2 < N2; ++k2) {
@@ -546,7 +546,7 @@ __global__ void __launch_bounds__(256, 2) k_rows_inv_p(const __grid_constant__ C
             const int ahead = t + (nst - 1) * (int)gridDim.x;
             if (ahead < ntiles) issue(ahead, (i + nst - 1) % nst);
         }
-        if (!mbar_wait(&bar[stage], (unsigned)((i / nst) & 1))) return;
+        if (!mbar_wait(&bar[stage], (unsigned)((i / nst) & 1), g.err)) return;
         unsigned char* st = smem_raw + L.stage0 + (size_t)stage * L.stage_bytes;
         Cx* S = reinterpret_cast<Cx*>(st);
         const int kx = t / nchunk, c0 = (t - kx * nchunk) * CB;
@@ -578,375 +578,6 @@ __global__ void __launch_bounds__(256, 2) k_rows_inv_p(const __grid_constant__ C
             }
         }
         __syncthreads();
-    }
-}
-
-// ===========================================================================
-// Dataflow exchange: one persistent launch runs the three passes as a
-// software pipeline over channel chunks (square meshes with a register
-// codelet, full channel set).
-//
-// Work items are numbered in steps s = 0 .. nchunk + 2 kFlowLag - 1: step s
-// holds the n0 row lines of A(chunk s), the n1 column lines of
-// B(chunk s - kFlowLag) and the n0 row lines of C(chunk s - 2 kFlowLag).  CTAs
-// take items from a global ticket counter in increasing order, and an item
-// only waits for items with smaller tickets (B(c) for every A(c) line, C(c)
-// for every B(c) line, counted in ctl[] with release/acquire), so the launch
-// cannot deadlock whatever the residency.  The intermediate of a chunk lives
-// in T's channels of that chunk (T aliases Sigma in FP64) and stays in L2
-// between its passes; P, VR and Sigma cross DRAM once.
-//
-// Warp 0 lane 0 is the producer: it takes tickets, waits for the dependency
-// counters, and issues the TMA loads into an nst-stage ring (full/empty
-// mbarriers); warps 1.. transform.  Every wait is bounded; a producer that
-// gives up sets the device error flag and ends the consumers with a
-// sentinel item.
-// smem: tw[N] | full[kMaxPipeStages] | empty[kMaxPipeStages] | info[kMaxPipeStages] | nst stages of 2 slots
-// ===========================================================================
-constexpr int kFlowLag = 2;
-constexpr int kFlowConsumers = 128;              // consumer threads at most (4 warps)
-constexpr long long kFlowSpinLimit = 4000000LL;  // dependency polls (64 ns apart) before giving up
-
-struct FlowLayout {
-    size_t tw, full, empty, info, stage0, slot, stage_bytes, total;
-};
-
-__host__ __device__ inline FlowLayout flow_layout(int N, int CB, int nst) {
-    FlowLayout L;
-    L.tw = 0;
-    L.full = (sizeof(double2) * (size_t)N + 15) & ~(size_t)15;
-    L.empty = L.full + 8 * kMaxPipeStages;
-    L.info = L.empty + 8 * kMaxPipeStages;
-    L.stage0 = (L.info + 4 * kMaxPipeStages + 127) & ~(size_t)127;
-    L.slot = (sizeof(double2) * (size_t)N * CB + 127) & ~(size_t)127;
-    L.stage_bytes = 2 * L.slot;
-    L.total = L.stage0 + (size_t)nst * L.stage_bytes + 128;
-    return L;
-}
-
-// ticket -> (pass, chunk, line); false past the last item
-__device__ __forceinline__ bool flow_decode(int t, int nchunk, int n0, int n1, int& pass, int& chunk, int& line) {
-    int base = 0;
-    const int steps = nchunk + 2 * kFlowLag;
-    for (int s = 0; s < steps; ++s) {
-        if (s < nchunk) {
-            if (t < base + n0) {
-                pass = 0, chunk = s, line = t - base;
-                return true;
-            }
-            base += n0;
-        }
-        const int cb = s - kFlowLag;
-        if (cb >= 0 && cb < nchunk) {
-            if (t < base + n1) {
-                pass = 1, chunk = cb, line = t - base;
-                return true;
-            }
-            base += n1;
-        }
-        const int cc = s - 2 * kFlowLag;
-        if (cc >= 0 && cc < nchunk) {
-            if (t < base + n0) {
-                pass = 2, chunk = cc, line = t - base;
-                return true;
-            }
-            base += n0;
-        }
-    }
-    return false;
-}
-
-// Shared-memory twiddle load that the compiler keeps in place: the dataflow
-// kernel's twiddle indices are loop-invariant, and hoisting the loads of all
-// three passes out of the persistent loop would pin ~60 complex values in
-// registers.
-__device__ __forceinline__ double2 lds_tw(const double2* p) {
-    double2 v;
-    asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"(smem_u32(p)));
-    return v;
-}
-__device__ __forceinline__ float2 lds_tw(const float2* p) {
-    float2 v;
-    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(smem_u32(p)));
-    return v;
-}
-
-__device__ __forceinline__ void flow_bar(int nthreads) { __barrier_sync_count(1, (unsigned)nthreads); }
-
-// Consumer bodies of the dataflow kernel, one per pass.  Each is a separate
-// (non-inlined) function so that its registers are allocated on their own
-// rather than as the union of the three passes.  Every consumer thread
-// arrives on `empty` after its last read of the stage.
-
-// A: rows forward of P[kx = line, :, chunk] (- refP) -> T, then count the line
-template <class Cx, int N1, int N2>
-__device__ __forceinline__ void flow_rows_fwd(unsigned char* st, size_t slot, const Cx* tw, unsigned long long* empty,
-                                           int has_refP, Cx* T, const ExchangeGeom& g, int CB, int chunk, int line,
-                                           int c, int a, int nct, unsigned* done, bool leader) {
-    const double2* in = reinterpret_cast<const double2*>(st);
-    const double2* rin = reinterpret_cast<const double2*>(st + slot);
-    const int ch = chunk * CB + c;
-    Cx v[N1];
-    if (a < N2) {
-#pragma unroll
-        for (int n1 = 0; n1 < N1; ++n1) {
-            double2 x = in[(N2 * n1 + a) * CB + c];
-            if (has_refP) x = csub(x, rin[(N2 * n1 + a) * CB + c]);
-            v[n1] = to_c(x, Cx{});
-        }
-        dft<N1, false>(v);
-    }
-    flow_bar(nct);
-    Cx* S = reinterpret_cast<Cx*>(st);
-    if (a < N2) {
-#pragma unroll
-        for (int k1 = 0; k1 < N1; ++k1) S[(k1 * N2 + a) * CB + c] = cmul(v[k1], lds_tw(tw + a * k1));
-    }
-    flow_bar(nct);
-    Cx u[N2];
-    if (a < N1) {
-#pragma unroll
-        for (int n2 = 0; n2 < N2; ++n2) u[n2] = S[(a * N2 + n2) * CB + c];
-    }
-    mbar_arrive(empty);
-    if (a < N1) {
-        dft<N2, false>(u);
-        if (ch < g.C) {
-#pragma unroll
-            for (int k2 = 0; k2 < N2; ++k2) st_l2(T + ((size_t)line * g.n1 + (a + N1 * k2)) * g.Ct + ch, u[k2]);
-        }
-    }
-    fence_proxy_async_global();
-    flow_bar(nct);
-    if (leader) red_release_add(done, 1u);
-}
-
-// B: columns forward, * VR (or conj VR), inverse, of T[:, ky = line, chunk].
-// The product with VR is its own element-parallel step in shared memory, so no
-// thread holds a transformed line and its VR values at the same time.
-template <class Cx, int N1, int N2>
-__device__ __forceinline__ void flow_cols(unsigned char* st, size_t slot, const Cx* tw, unsigned long long* empty,
-                                          int conjv, Cx* T, const ExchangeGeom& g, int CB, int chunk, int line, int c,
-                                          int a, int nct, unsigned* done, bool leader) {
-    constexpr int N = N1 * N2;
-    Cx* S = reinterpret_cast<Cx*>(st);
-    const double2* Vt = reinterpret_cast<const double2*>(st + slot);
-    const int ch = chunk * CB + c;
-    {
-        Cx v[N1];
-        if (a < N2) {
-#pragma unroll
-            for (int n1 = 0; n1 < N1; ++n1) v[n1] = S[(N2 * n1 + a) * CB + c];
-            dft<N1, false>(v);
-        }
-        flow_bar(nct);
-        if (a < N2) {
-#pragma unroll
-            for (int k1 = 0; k1 < N1; ++k1) S[(k1 * N2 + a) * CB + c] = cmul(v[k1], lds_tw(tw + a * k1));
-        }
-    }
-    flow_bar(nct);
-    {
-        Cx u[N2];
-        if (a < N1) {
-#pragma unroll
-            for (int n2 = 0; n2 < N2; ++n2) u[n2] = S[(a * N2 + n2) * CB + c];
-            dft<N2, false>(u);
-        }
-        flow_bar(nct);
-        // u[k2] = X[kx = a + N1 k2] goes back to the slot it came from
-        if (a < N1) {
-#pragma unroll
-            for (int k2 = 0; k2 < N2; ++k2) S[(a * N2 + k2) * CB + c] = u[k2];
-        }
-    }
-    flow_bar(nct);
-    {
-        // slot q = a N2 + k2 holds kx = a + N1 k2
-        const int tid = a * CB + c;
-        for (int e = tid; e < N * CB; e += nct) {
-            const int q = e / CB, cc = e - q * CB;
-            const int qa = q / N2, qk = q - qa * N2;
-            const int kx = qa + N1 * qk;
-            double2 w = g.dv == 1 ? Vt[kx] : Vt[kx * CB + cc];
-            if (conjv) w = cconj(w);
-            S[e] = cmul(S[e], to_c(w, Cx{}));
-        }
-    }
-    flow_bar(nct);
-    {
-        Cx u[N2];
-        if (a < N1) {
-#pragma unroll
-            for (int k2 = 0; k2 < N2; ++k2) u[k2] = S[(a * N2 + k2) * CB + c];
-            dft<N2, true>(u);
-        }
-        flow_bar(nct);
-        if (a < N1) {
-#pragma unroll
-            for (int na = 0; na < N2; ++na) S[(a * N2 + na) * CB + c] = cmulc(u[na], lds_tw(tw + na * a));
-        }
-    }
-    flow_bar(nct);
-    Cx v[N1];
-    if (a < N2) {
-#pragma unroll
-        for (int k1 = 0; k1 < N1; ++k1) v[k1] = S[(k1 * N2 + a) * CB + c];
-    }
-    mbar_arrive(empty);
-    if (a < N2) {
-        dft<N1, true>(v);
-        if (ch < g.C) {
-            const int s0 = g.shift ? g.n0 / 2 : 0;
-#pragma unroll
-            for (int nbx = 0; nbx < N1; ++nbx) {
-                const int kx = a + N2 * nbx;
-                const int dx = (kx - s0 + g.n0) % g.n0;
-                st_l2(T + ((size_t)dx * g.n1 + line) * g.Ct + ch, v[nbx]);
-            }
-        }
-    }
-    fence_proxy_async_global();
-    flow_bar(nct);
-    if (leader) red_release_add(done, 1u);
-}
-
-// C: rows inverse of T[kx = line, :, chunk], scale, shift -> Sigma
-template <class Cx, int N1, int N2>
-__device__ __forceinline__ void flow_rows_inv(unsigned char* st, const Cx* tw, unsigned long long* empty,
-                                           double2* Sigma, const ExchangeGeom& g, int CB, int chunk, int line, int c,
-                                           int a, int nct, double scale) {
-    Cx* S = reinterpret_cast<Cx*>(st);
-    const int ch = chunk * CB + c;
-    {
-        Cx u[N2];
-        if (a < N1) {
-#pragma unroll
-            for (int k2 = 0; k2 < N2; ++k2) u[k2] = S[(a + N1 * k2) * CB + c];
-            dft<N2, true>(u);
-        }
-        flow_bar(nct);
-        if (a < N1) {
-#pragma unroll
-            for (int na = 0; na < N2; ++na) S[(a * N2 + na) * CB + c] = cmulc(u[na], lds_tw(tw + na * a));
-        }
-    }
-    flow_bar(nct);
-    Cx v[N1];
-    if (a < N2) {
-#pragma unroll
-        for (int k1 = 0; k1 < N1; ++k1) v[k1] = S[(k1 * N2 + a) * CB + c];
-    }
-    mbar_arrive(empty);
-    if (a < N2 && ch < g.C) {
-        dft<N1, true>(v);
-        const size_t nb2 = (size_t)g.nb * g.nb;
-        const int s1 = g.shift ? g.n1 / 2 : 0;
-#pragma unroll
-        for (int nbx = 0; nbx < N1; ++nbx) {
-            const int ky = a + N2 * nbx;
-            const int dy = (ky - s1 + g.n1) % g.n1;
-            Sigma[((size_t)line * g.n1 + dy) * nb2 + ch] = cscale(to_d(v[nbx]), scale);
-        }
-    }
-}
-
-template <class Cx, int N1, int N2>
-__global__ void __launch_bounds__(kFlowConsumers + 32, 1)
-    k_exchange_flow(const __grid_constant__ CUtensorMap mP, const __grid_constant__ CUtensorMap mR,
-                    const __grid_constant__ CUtensorMap mTr, const __grid_constant__ CUtensorMap mTc,
-                    const __grid_constant__ CUtensorMap mV, int has_refP, Cx* T, double2* Sigma, ExchangeGeom g,
-                    int CB, int nchunk, int nst, int conjv, double scale, unsigned* ctl) {
-    constexpr int N = N1 * N2;
-    extern __shared__ __align__(16) unsigned char smem_dyn[];
-    unsigned char* smem_raw = align128(smem_dyn);
-    const FlowLayout L = flow_layout(N, CB, nst);
-    Cx* tw = reinterpret_cast<Cx*>(smem_raw + L.tw);
-    unsigned long long* full = reinterpret_cast<unsigned long long*>(smem_raw + L.full);
-    unsigned long long* empty = reinterpret_cast<unsigned long long*>(smem_raw + L.empty);
-    volatile int* info = reinterpret_cast<volatile int*>(smem_raw + L.info);
-    const int nct = (int)blockDim.x - 32;  // consumer threads (whole warps)
-    build_line_twiddles(tw, N);
-    if (threadIdx.x == 0) {
-        for (int b = 0; b < nst; ++b) {
-            mbar_init(&full[b], 1);
-            mbar_init(&empty[b], (unsigned)nct);
-        }
-        fence_mbar_init();
-    }
-    __syncthreads();
-    unsigned* doneA = ctl + 1;
-    unsigned* doneB = ctl + 1 + nchunk;
-
-    if (threadIdx.x < 32) {
-        // ---------------- producer ----------------
-        if (threadIdx.x != 0) return;
-        const unsigned boxP = (unsigned)(N * CB * sizeof(double2));
-        const unsigned boxT = (unsigned)(N * CB * sizeof(Cx));
-        const unsigned boxV = (unsigned)(N * (g.dv == 1 ? 1 : CB) * sizeof(double2));
-        for (int i = 0;; ++i) {
-            const int s = i % nst;
-            if (i >= nst && !mbar_wait(&empty[s], (unsigned)(((i / nst) - 1) & 1))) return;
-            const int t = (int)atomicAdd(&ctl[0], 1u);
-            int pass = 0, chunk = 0, line = 0;
-            bool ok = flow_decode(t, nchunk, g.n0, g.n1, pass, chunk, line);
-            if (ok && pass > 0) {
-                const unsigned* cnt = pass == 1 ? &doneA[chunk] : &doneB[chunk];
-                const unsigned need = (unsigned)(pass == 1 ? g.n0 : g.n1);
-                long long spins = 0;
-                while (ld_acquire_gpu(cnt) < need) {
-                    if (++spins > kFlowSpinLimit) {
-                        atomicOr(&g_cpphf_device_error, 2u);
-                        ok = false;
-                        break;
-                    }
-                    __nanosleep(64);
-                }
-                // the intermediate was written by other CTAs' generic stores
-                fence_proxy_async_global();
-            }
-            if (!ok) {
-                info[s] = -1;
-                mbar_arrive(&full[s]);
-                return;
-            }
-            info[s] = (pass << 28) | (chunk << 16) | line;
-            unsigned char* st = smem_raw + L.stage0 + (size_t)s * L.stage_bytes;
-            const int c0 = chunk * CB;
-            fence_proxy_async_smem();
-            if (pass == 0) {
-                mbar_arrive_expect_tx(&full[s], boxP * (has_refP ? 2u : 1u));
-                tma_load_3d(st, &mP, 2 * c0, 0, line, &full[s]);
-                if (has_refP) tma_load_3d(st + L.slot, &mR, 2 * c0, 0, line, &full[s]);
-            } else if (pass == 1) {
-                mbar_arrive_expect_tx(&full[s], boxT + boxV);
-                tma_load_3d(st, &mTc, 2 * c0, line, 0, &full[s]);
-                tma_load_3d(st + L.slot, &mV, g.dv == 1 ? 0 : 2 * c0, line, 0, &full[s]);
-            } else {
-                mbar_arrive_expect_tx(&full[s], boxT);
-                tma_load_3d(st, &mTr, 2 * c0, 0, line, &full[s]);
-            }
-        }
-    }
-
-    // ---------------- consumers ----------------
-    const int ct = threadIdx.x - 32;
-    const int c = ct % CB, a = ct / CB;
-    for (int i = 0;; ++i) {
-        const int s = i % nst;
-        if (!mbar_wait(&full[s], (unsigned)((i / nst) & 1))) return;
-        const int inf = info[s];
-        if (inf < 0) return;
-        const int pass = inf >> 28, chunk = (inf >> 16) & 0xfff, line = inf & 0xffff;
-        unsigned char* st = smem_raw + L.stage0 + (size_t)s * L.stage_bytes;
-        if (pass == 0)
-            flow_rows_fwd<Cx, N1, N2>(st, L.slot, tw, &empty[s], has_refP, T, g, CB, chunk, line, c, a, nct,
-                                      &doneA[chunk], ct == 0);
-        else if (pass == 1)
-            flow_cols<Cx, N1, N2>(st, L.slot, tw, &empty[s], conjv, T, g, CB, chunk, line, c, a, nct,
-                                  &doneB[chunk], ct == 0);
-        else
-            flow_rows_inv<Cx, N1, N2>(st, tw, &empty[s], Sigma, g, CB, chunk, line, c, a, nct, scale);
     }
 }
 
@@ -1099,64 +730,16 @@ Launch plan_launch(int lanes, int C, size_t elem, int n, bool generic, int targe
 constexpr size_t kSmemMax = 227 * 1024 - 1024;
 
 // Pipelined-pass shape: threads per CTA (sets the channels per tile) and the
-// number of shared-memory stages.  CPPHF_PIPE_ROWS / CPPHF_PIPE_COLS =
-// "threads,stages" override the defaults (for tuning sweeps).
+// number of shared-memory stages.  Block shapes of 64-256 threads and 2-4
+// stages were swept on the 192x192, nb = 8 workload; 128 x 2 is the fastest
+// for both pass kinds.
 struct PipeCfg {
     int threads;
     int nst;
 };
 
-PipeCfg pipe_cfg_env(const char* name, PipeCfg dflt) {
-    const char* e = std::getenv(name);
-    if (!e) return dflt;
-    PipeCfg c = dflt;
-    if (std::sscanf(e, "%d,%d", &c.threads, &c.nst) != 2) return dflt;
-    if (c.threads < 32 || c.threads > 1024) c.threads = dflt.threads;
-    if (c.nst < 2 || c.nst > kMaxPipeStages) c.nst = dflt.nst;
-    return c;
-}
-
-PipeCfg rows_cfg() {
-    static const PipeCfg c = pipe_cfg_env("CPPHF_PIPE_ROWS", PipeCfg{128, 2});
-    return c;
-}
-
-PipeCfg cols_cfg() {
-    static const PipeCfg c = pipe_cfg_env("CPPHF_PIPE_COLS", PipeCfg{128, 2});
-    return c;
-}
-
-// CPPHF_EXCHANGE_PIPELINE=0 selects the non-pipelined kernels (for A/B timing).
-bool pipeline_enabled() {
-    static const bool on = [] {
-        const char* e = std::getenv("CPPHF_EXCHANGE_PIPELINE");
-        return !(e && e[0] == '0');
-    }();
-    return on;
-}
-
-// CPPHF_EXCHANGE_FLOW=1 selects the dataflow kernel instead of the three
-// launches (opt-in while its register use is tuned); CPPHF_FLOW_STAGES sets
-// its ring depth.
-bool flow_enabled() {
-    static const bool on = [] {
-        const char* e = std::getenv("CPPHF_EXCHANGE_FLOW");
-        return e && e[0] == '1';
-    }();
-    return on;
-}
-
-int flow_stages() {
-    static const int n = [] {
-        const char* e = std::getenv("CPPHF_FLOW_STAGES");
-        const int v = e ? std::atoi(e) : kMaxPipeStages;
-        return (v >= 2 && v <= kMaxPipeStages) ? v : kMaxPipeStages;
-    }();
-    return n;
-}
-
-// dataflow counters: ticket, done A[chunk], done B[chunk] (at most C chunks)
-size_t flow_ctl_bytes(int C) { return ((sizeof(unsigned) * (1 + 2 * (size_t)C)) + 255) & ~(size_t)255; }
+constexpr PipeCfg kRowsCfg{128, 2};
+constexpr PipeCfg kColsCfg{128, 2};
 
 template <class Cx, int N1, int N2>
 struct Spec {
@@ -1186,7 +769,7 @@ struct Spec {
         return plan_launch(N1 > N2 ? N1 : N2, g.C, sizeof(Cx), N1 * N2, false, cfg.threads);
     }
     static bool pipelined(const ExchangeGeom& g, const PipeCfg& cfg) {
-        if (g.hcp || !pipeline_enabled() || N1 * N2 > 256) return false;
+        if (g.hcp || N1 * N2 > 256) return false;
         const Launch L = pipe_launch(g, cfg);
         if (L.threads > 256) return false;  // __launch_bounds__(256)
         if (sizeof(Cx) == 8 && ((L.CB % 2) != 0 || (g.Ct % 2) != 0)) return false;
@@ -1202,7 +785,7 @@ struct Spec {
     }
     static int rows_fwd(const double2* P, const double2* refP, Cx* T, const ExchangeGeom& g, cudaStream_t st) {
         attrs();
-        const PipeCfg cfg = rows_cfg();
+        const PipeCfg cfg = kRowsCfg;
         if (pipelined(g, cfg)) {
             const Launch L = pipe_launch(g, cfg);
             const PipeLayout PL = pipe_layout(N1 * N2, L.CB, sizeof(double2), refP != nullptr, cfg.nst);
@@ -1229,7 +812,7 @@ struct Spec {
     }
     static int cols(Cx* T, const double2* VR, const ExchangeGeom& g, int vmode, cudaStream_t st) {
         attrs();
-        const PipeCfg cfg = cols_cfg();
+        const PipeCfg cfg = kColsCfg;
         if (pipelined(g, cfg) && vmode != kColsForwardOnly && pipe_launch(g, cfg).threads <= kColsMaxThreads) {
             const Launch L = pipe_launch(g, cfg);
             const ColsLayout PL = cols_layout(N1 * N2, L.CB, sizeof(Cx), cfg.nst);
@@ -1256,54 +839,9 @@ struct Spec {
         CPPHF_LAUNCH_CHECK("exchange columns convolve");
         return CPPHF_OK;
     }
-    // Dataflow launch (square mesh, no HCP, VR or conj VR column mode); returns
-    // false (nothing launched) when the shape does not qualify.
-    static bool flow(const double2* P, const double2* refP, const double2* VR, double2* Sigma, Cx* T,
-                     const ExchangeGeom& g, int vmode, unsigned* ctl, cudaStream_t st, int* status) {
-        *status = CPPHF_OK;
-        if (!ctl || g.hcp || g.n0 != g.n1 || vmode == kColsForwardOnly || !flow_enabled() || !pipeline_enabled())
-            return false;
-        const Launch Lp = plan_launch(N1 > N2 ? N1 : N2, g.C, sizeof(Cx), N1 * N2, false, kFlowConsumers);
-        if (Lp.threads > kFlowConsumers) return false;
-        if (sizeof(Cx) == 8 && ((Lp.CB % 2) != 0 || (g.Ct % 2) != 0)) return false;
-        int nst = flow_stages();
-        while (nst > 2 && flow_layout(N1 * N2, Lp.CB, nst).total > kSmemMax) --nst;
-        const FlowLayout FL = flow_layout(N1 * N2, Lp.CB, nst);
-        if (FL.total > kSmemMax) return false;
-        static std::once_flag once;
-        std::call_once(once, [] { raise_smem(k_exchange_flow<Cx, N1, N2>); });
-        CUtensorMap mP, mR, mTr, mTc, mV;
-        const int nb2 = g.nb * g.nb, N = N1 * N2;
-        bool ok = field_map(&mP, P, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, nb2, g, 2 * Lp.CB, N, 1);
-        ok = ok && field_map(&mR, refP ? refP : P, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, nb2, g, 2 * Lp.CB, N, 1);
-        ok = ok && field_map(&mTr, T, tdt(), sizeof(Cx) / 2, g.Ct, g, 2 * Lp.CB, N, 1);
-        ok = ok && field_map(&mTc, T, tdt(), sizeof(Cx) / 2, g.Ct, g, 2 * Lp.CB, 1, N);
-        if (g.dv == 1)
-            ok = ok && field_map(&mV, VR, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, 1, g, 2, 1, N);
-        else
-            ok = ok && field_map(&mV, VR, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, g.dv, g, 2 * Lp.CB, 1, N);
-        if (!ok) return false;
-        const int threads = Lp.threads + 32;
-        int per = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_exchange_flow<Cx, N1, N2>, threads, FL.total);
-        (void)cudaGetLastError();
-        if (per < 1) return false;
-        const int ntickets = Lp.nchunk * (2 * g.n0 + g.n1);
-        const int grid = std::max(1, std::min(ntickets, per * num_sms()));
-        if (cudaMemsetAsync(ctl, 0, flow_ctl_bytes(g.C), st) != cudaSuccess) {
-            *status = cuda_fail(cudaGetLastError(), "exchange flow counters");
-            return true;
-        }
-        k_exchange_flow<Cx, N1, N2><<<grid, threads, FL.total, st>>>(
-            mP, mR, mTr, mTc, mV, refP != nullptr, T, Sigma, g, Lp.CB, Lp.nchunk, nst, vmode == kColsConjVR ? 1 : 0,
-            -1.0 / ((double)g.n0 * (double)g.n1), ctl);
-        const cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) *status = cuda_fail(e, "exchange (dataflow)");
-        return true;
-    }
     static int rows_inv(const Cx* T, double2* Sigma, const ExchangeGeom& g, double scale, cudaStream_t st) {
         attrs();
-        const PipeCfg cfg = rows_cfg();
+        const PipeCfg cfg = kRowsCfg;
         if (pipelined(g, cfg)) {
             const Launch L = pipe_launch(g, cfg);
             const PipeLayout PL = pipe_layout(N1 * N2, L.CB, sizeof(Cx), false, cfg.nst);
@@ -1439,21 +977,7 @@ int pass_rows_inv(const Cx* T, double2* Sigma, const ExchangeGeom& g, double sca
 
 template <class Cx>
 int launch_exchange(const double2* P, const double2* refP, const double2* VR, double2* Sigma, Cx* T,
-                    const ExchangeGeom& g, cudaStream_t st, int vmode = kColsVR, unsigned* ctl = nullptr) {
-    if (ctl && g.n0 == g.n1) {
-        int status = CPPHF_OK;
-        bool done = false;
-        switch (g.n0) {
-#define X(N, A, B)                                                                           \
-    case N:                                                                                  \
-        if constexpr (N >= 48) done = Spec<Cx, A, B>::flow(P, refP, VR, Sigma, T, g, vmode, ctl, st, &status); \
-        break;
-            CPPHF_SPEC_SIZES(X)
-#undef X
-            default: break;
-        }
-        if (done) return status;
-    }
+                    const ExchangeGeom& g, cudaStream_t st, int vmode = kColsVR) {
     CPPHF_TRY(pass_rows_fwd<Cx>(P, refP, T, g, st));
     CPPHF_TRY(pass_cols<Cx>(T, VR, g, vmode, st));
     CPPHF_TRY(pass_rows_inv<Cx>(T, Sigma, g, -1.0 / ((double)g.n0 * (double)g.n1), st));
@@ -1475,11 +999,9 @@ size_t exchange_t_bytes(int64_t nk1, int64_t nk2, int64_t nb, int hcp, int preci
 
 }  // namespace
 
-// T (when it does not alias Sigma) followed by the dataflow counters; a
-// workspace without room for the counters runs the three-launch passes.
+// T when it does not alias Sigma (0 for the full FP64 form).
 size_t exchange_workspace_bytes(int64_t nk1, int64_t nk2, int64_t nb, int hcp, int precision) {
-    const int C = hcp ? (int)(nb * (nb + 1) / 2) : (int)(nb * nb);
-    return exchange_t_bytes(nk1, nk2, nb, hcp, precision) + flow_ctl_bytes(C);
+    return exchange_t_bytes(nk1, nk2, nb, hcp, precision);
 }
 
 int exchange(const double2* P, const double2* refP, const double2* VR, double2* Sigma, int64_t nk1, int64_t nk2,
@@ -1501,18 +1023,17 @@ int exchange(const double2* P, const double2* refP, const double2* VR, double2* 
     g.dv = dv == 1 ? 1 : (int)(nb * nb);
     g.Ct = g.C;
     g.shift = shift ? 1 : 0;
+    g.err = wait_error_word();
+    if (!g.err) return CPPHF_ERR_CUDA;
     const size_t need = exchange_t_bytes(nk1, nk2, nb, hcp, precision);
     if (need > 0 && (workspace == nullptr || workspace_bytes < need))
         return fail(CPPHF_ERR_INVALID, "exchange: workspace too small (" +
                                            std::to_string(exchange_workspace_bytes(nk1, nk2, nb, hcp, precision)) +
                                            " bytes needed)");
-    unsigned* ctl = nullptr;
-    if (workspace && workspace_bytes >= need + flow_ctl_bytes(g.C))
-        ctl = reinterpret_cast<unsigned*>(static_cast<unsigned char*>(workspace) + need);
     if (precision == 32)
-        return launch_exchange<float2>(P, refP, VR, Sigma, static_cast<float2*>(workspace), g, st, kColsVR, ctl);
+        return launch_exchange<float2>(P, refP, VR, Sigma, static_cast<float2*>(workspace), g, st, kColsVR);
     double2* T = hcp ? static_cast<double2*>(workspace) : Sigma;
-    return launch_exchange<double2>(P, refP, VR, Sigma, T, g, st, kColsVR, ctl);
+    return launch_exchange<double2>(P, refP, VR, Sigma, T, g, st, kColsVR);
 }
 
 namespace {
@@ -1556,6 +1077,7 @@ ExchangeGeom full_geom(int64_t nk1, int64_t nk2, int64_t nb, int64_t dv) {
     g.dv = dv == 1 ? 1 : (int)(nb * nb);
     g.Ct = g.C;
     g.shift = 0;
+    g.err = wait_error_word();
     return g;
 }
 
@@ -1629,19 +1151,5 @@ int cpphf_exchange(const void* P, const void* refP, const void* VR, void* Sigma,
 }
 
 int cpphf_clear_fft_plan_cache(void) { return CPPHF_OK; }
-
-// Read (and with clear != 0 reset) the device-side flag set by bounded waits
-// that gave up.  Synchronises the device.  Returns the flag (0 = none) or a
-// negative status on a CUDA error.
-int cpphf_device_error(int clear) {
-    unsigned v = 0;
-    CPPHF_CUDA(cudaDeviceSynchronize());
-    CPPHF_CUDA(cudaMemcpyFromSymbol(&v, cpphf::g_cpphf_device_error, sizeof(v)));
-    if (clear) {
-        const unsigned z = 0;
-        CPPHF_CUDA(cudaMemcpyToSymbol(cpphf::g_cpphf_device_error, &z, sizeof(z)));
-    }
-    return (int)v;
-}
 
 }  // extern "C"

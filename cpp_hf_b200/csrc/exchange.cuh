@@ -13,6 +13,7 @@ struct ExchangeGeom {
     int Ct;      // channel stride of the intermediate T
     int hcp;     // upper-triangle packing with conjugate mirror on unpack
     int shift;   // apply ifftshift on (kx, ky) to the output
+    unsigned* err = nullptr;  // device error word for bounded waits
 };
 
 size_t exchange_workspace_bytes(int64_t nk1, int64_t nk2, int64_t nb, int hcp, int precision);

@@ -9,7 +9,8 @@
 //            F = herm(h + Sigma + diag(hartree_diag)), energy partials
 //            w_k Re[h_ij P_ji + (Sigma_ij + H_ij)/2 (P - refP)_ji] (+ the
 //            mirrored term); optional dense H.
-//   energy   fixed-order sum of the block partials.
+//   energy   Kahan-compensated per-thread sums, then fixed-order block and
+//            grid trees (deterministic for a given grid).
 #include "bulk.cuh"
 #include "common.cuh"
 #include "exchange.cuh"
@@ -31,6 +32,7 @@ constexpr int kAsmThreads = 256;
 constexpr int kRedThreads = 256;
 constexpr int kMaxPartials = 2048;
 constexpr int kAsmMaxStages = 4;
+constexpr int kTileElems = 1024;  // k-blocks of at most this many elements take the bulk-pipelined assembly
 
 // rho_bar partials: grid (Gk, ceil(nb2 / CH)), CH channels per block, lanes =
 // blockDim / CH k-lanes.
@@ -131,6 +133,7 @@ struct AsmArgs {
     int64_t nk;
     int nb;
     double* part;         // energy partials [gridDim.x]
+    unsigned* err;        // device error word (bounded waits)
 };
 
 __global__ void __launch_bounds__(kAsmThreads) k_assemble(AsmArgs a) {
@@ -138,7 +141,7 @@ __global__ void __launch_bounds__(kAsmThreads) k_assemble(AsmArgs a) {
     const int nb = a.nb;
     const int npair = nb * (nb + 1) / 2;
     const int64_t total = a.nk * npair;
-    double e_acc[1] = {0.0};
+    Kahan e_k;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
          t += (int64_t)gridDim.x * blockDim.x) {
         const int64_t k = t / npair;
@@ -186,71 +189,13 @@ __global__ void __launch_bounds__(kAsmThreads) k_assemble(AsmArgs a) {
             const double2 iji = cscale(sji, 0.5);
             s += (hji.x * pij.x - hji.y * pij.y) + (iji.x * dij.x - iji.y * dij.y);
         }
-        e_acc[0] += a.w[k] * s;
+        e_k.add(a.w[k] * s);
     }
+    double e_acc[1] = {e_k.s};
     block_sum<1>(e_acc, red);
     if (threadIdx.x == 0) a.part[blockIdx.x] = e_acc[0];
 }
 
-
-// Tiled assembly: a CTA stages KT whole k-blocks (KT nb^2 contiguous elements)
-// of Sigma, h and P (and refP) in shared memory with coalesced loads, then
-// forms F = herm(h + Sigma + SC + diag(hd)) and the energy terms element by
-// element, reading transposed partners from shared memory.
-constexpr int kTileElems = 1024;
-
-__global__ void __launch_bounds__(kAsmThreads) k_assemble_tiled(AsmArgs a, int KT) {
-    extern __shared__ __align__(16) unsigned char smem_t[];
-    __shared__ double red[32];
-    const int nb = a.nb, nb2 = nb * nb;
-    const int tile = KT * nb2;
-    double2* sS = reinterpret_cast<double2*>(smem_t);
-    double2* sH = sS + tile;
-    double2* sP = sH + tile;
-    double2* sR = sP + tile;  // refP (only when present)
-    const int64_t ntiles = (a.nk + KT - 1) / KT;
-    double e_acc[1] = {0.0};
-    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const int64_t k0 = t * KT;
-        const int nkt = (int)((a.nk - k0) < (int64_t)KT ? (a.nk - k0) : (int64_t)KT);
-        const int n = nkt * nb2;
-        const size_t base = (size_t)k0 * nb2;
-        for (int e = threadIdx.x; e < n; e += blockDim.x) {
-            double2 s = a.Sigma[base + e];
-            if (a.SC) s = cadd(s, a.SC[e % nb2]);
-            sS[e] = s;
-            sH[e] = a.h[base + e];
-            sP[e] = a.P[base + e];
-            if (a.refP) sR[e] = a.refP[base + e];
-        }
-        __syncthreads();
-        for (int e = threadIdx.x; e < n; e += blockDim.x) {
-            const int kl = e / nb2, r = e - kl * nb2;
-            const int i = r / nb, j = r - i * nb;
-            const int eT = kl * nb2 + j * nb + i;
-            const double hdi = a.hd ? a.hd[i] : 0.0;
-            double2 Aij = cadd(sH[e], sS[e]);
-            double2 Aji = cadd(sH[eT], sS[eT]);
-            if (i == j) {
-                Aij.x += hdi;
-                Aji = Aij;
-            }
-            a.F[base + e] = mk(0.5 * (Aij.x + Aji.x), 0.5 * (Aij.y - Aji.y));
-            if (a.SC) a.Sigma[base + e] = sS[e];
-            if (a.Hdense) a.Hdense[base + e] = mk(i == j ? hdi : 0.0, 0.0);
-            const double2 pji = sP[eT];
-            const double2 dji = a.refP ? csub(pji, sR[eT]) : pji;
-            double2 inter = cscale(sS[e], 0.5);
-            if (i == j && a.hd) inter.x += 0.5 * hdi;
-            const double2 h = sH[e];
-            const double s = (h.x * pji.x - h.y * pji.y) + (inter.x * dji.x - inter.y * dji.y);
-            e_acc[0] += a.w[k0 + kl] * s;
-        }
-        __syncthreads();
-    }
-    block_sum<1>(e_acc, red);
-    if (threadIdx.x == 0) a.part[blockIdx.x] = e_acc[0];
-}
 
 // Pipelined assembly: persistent CTAs walk tiles of KT whole k-blocks; thread
 // 0 brings the NEXT tile's Sigma, h, P (and refP) segments into the other
@@ -287,14 +232,14 @@ __global__ void __launch_bounds__(kAsmThreads) k_assemble_bulk(AsmArgs a, int KT
         bulk_g2s(d + 2 * tile, a.P + off, bytes, &bar[s]);
         if (REF) bulk_g2s(d + 3 * tile, a.refP + off, bytes, &bar[s]);
     };
-    double e_acc[1] = {0.0};
+    Kahan e_k;
     int i = 0;
     for (int j = 0; j < nst - 1; ++j)
         if ((int64_t)blockIdx.x + (int64_t)j * gridDim.x < ntiles) issue(blockIdx.x + (int64_t)j * gridDim.x, j);
     for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
         const int s = i % nst;
         if (t + (int64_t)(nst - 1) * gridDim.x < ntiles) issue(t + (int64_t)(nst - 1) * gridDim.x, (i + nst - 1) % nst);
-        if (!mbar_wait(&bar[s], (unsigned)((i / nst) & 1))) return;
+        if (!mbar_wait(&bar[s], (unsigned)((i / nst) & 1), a.err)) return;
         const double2* sS = stg + (size_t)s * NARR * tile;
         const double2* sH = sS + tile;
         const double2* sP = sS + 2 * tile;
@@ -335,11 +280,12 @@ __global__ void __launch_bounds__(kAsmThreads) k_assemble_bulk(AsmArgs a, int KT
             if (ii == j && a.hd) inter.x += 0.5 * hdi;
             const double2 hv = sH[e];
             const double sv = (hv.x * pji.x - hv.y * pji.y) + (inter.x * dji.x - inter.y * dji.y);
-            e_acc[0] += a.w[k0 + kl] * sv;
+            e_k.add(a.w[k0 + kl] * sv);
         }
         __syncthreads();
     }
     if (energy_out) {
+        double e_acc[1] = {e_k.s};
         double out[1];
         if (reduce_last_block<1>(e_acc, a.part, counter, out, red) && threadIdx.x == 0) *energy_out = out[0];
     }
@@ -363,34 +309,14 @@ struct FockWs {
 bool sl_fock(const cpphf_kernel* K) { return K->sl && K->sl->fock_active && K->include_exchange; }
 bool sl_hart(const cpphf_kernel* K) { return K->sl && K->sl->hartree_active && K->include_hartree; }
 
-// Bulk assembly shape: complex elements per array per stage and stage count;
-// CPPHF_ASSEMBLY="elems,stages" overrides (for tuning sweeps).
+// Bulk assembly shape: complex elements per array per stage (halved with
+// refP) and stage count; 512 x 2 was the fastest of the shapes swept on the
+// 192x192, nb = 8 workload.
 struct AsmCfg {
     int elems;
     int nst;
 };
-
-AsmCfg asm_cfg() {
-    static const AsmCfg c = [] {
-        AsmCfg d{512, 2};
-        const char* e = std::getenv("CPPHF_ASSEMBLY");
-        AsmCfg v = d;
-        if (e && std::sscanf(e, "%d,%d", &v.elems, &v.nst) == 2 && v.elems >= 64 && v.elems <= 4096 && v.nst >= 2 &&
-            v.nst <= kAsmMaxStages)
-            return v;
-        return d;
-    }();
-    return c;
-}
-
-// CPPHF_ASSEMBLY_BULK=0 selects the non-pipelined assembly (for A/B timing).
-bool bulk_assembly_enabled() {
-    static const bool on = [] {
-        const char* e = std::getenv("CPPHF_ASSEMBLY_BULK");
-        return !(e && e[0] == '0');
-    }();
-    return on;
-}
+constexpr AsmCfg kAsmCfg{512, 2};
 
 FockWs fock_ws_layout(const cpphf_kernel* K) {
     FockWs L;
@@ -526,9 +452,11 @@ int build_fock(const cpphf_kernel* K, const double2* P, double2* Sigma, double2*
     a.nk = nk;
     a.nb = nb;
     a.part = part;
-    if (nb2 <= kTileElems && bulk_assembly_enabled()) {
+    a.err = wait_error_word();
+    if (!a.err) return CPPHF_ERR_CUDA;
+    if (nb2 <= kTileElems) {
         // whole k-blocks per stage: 1024 elements (3 arrays) or 512 (4 arrays with refP)
-        const AsmCfg cfg = asm_cfg();
+        const AsmCfg cfg = kAsmCfg;
         const int elems = refP ? cfg.elems / 2 : cfg.elems;
         const int KT = std::max(1, elems / nb2);
         const int64_t ntiles = (nk + KT - 1) / KT;
@@ -562,14 +490,7 @@ int build_fock(const cpphf_kernel* K, const double2* P, double2* Sigma, double2*
         CPPHF_LAUNCH_CHECK("assemble (bulk pipelined)");
         return CPPHF_OK;
     }
-    if (nb2 <= kTileElems) {
-        static std::once_flag once;
-        std::call_once(once, [] { raise_smem(k_assemble_tiled); });
-        const int KT = std::max(1, kTileElems / nb2);
-        const size_t smem = sizeof(double2) * (size_t)KT * nb2 * (refP ? 4 : 3);
-        k_assemble_tiled<<<L.Gasm, kAsmThreads, smem, st>>>(a, KT);
-        CPPHF_LAUNCH_CHECK("assemble (tiled)");
-    } else {
+    {
         k_assemble<<<L.Gasm, kAsmThreads, 0, st>>>(a);
         CPPHF_LAUNCH_CHECK("assemble");
     }

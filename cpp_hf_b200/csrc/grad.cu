@@ -33,17 +33,6 @@ struct ReduceWs {
     unsigned pad[63];
 };
 
-// Kahan-compensated per-thread accumulator; the cross-thread sum is the fixed
-// block tree of reduce_last_block.
-struct Kahan {
-    double s = 0.0, c = 0.0;
-    __device__ __forceinline__ void add(double x) {
-        const double y = x - c;
-        const double t = s + y;
-        c = (t - s) - y;
-        s = t;
-    }
-};
 
 unsigned red_grid(int64_t n) {
     const int64_t want = (n + 255) / 256;

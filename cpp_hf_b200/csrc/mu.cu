@@ -61,6 +61,8 @@ struct MuArgs {
     double* mu_out;
     double* part;     // [grid][2] min/max, [grid][kMuNV] partials, [2][kMuNV] totals
     unsigned* sync;   // [0] count [1] gen [2] error
+    unsigned* err;    // device error word (may be null)
+    long long spin_limit;  // grid-barrier poll limit
 };
 
 // Element i of a block's slice in band-major order (band = i / nk, k = i % nk):
@@ -77,7 +79,7 @@ __device__ __forceinline__ void band_major(const MuArgs& a, unsigned i, unsigned
 __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
     __shared__ double red[32 * kMuNV];  // block_sum<kMuNV> scratch (32 doubles per value)
     GridBarrier bar;
-    bar.init(a.sync);
+    bar.init(a.sync, a.spin_limit, a.err);
     const int G = gridDim.x;
     const unsigned nb = (unsigned)a.nb;
     const unsigned n = (unsigned)a.n;
@@ -414,13 +416,7 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
     if (blockIdx.x == 0 && threadIdx.x == 0) *a.mu_out = (a.mode == 0) ? 0.5 * (lo + hi) : mu;
 }
 
-// Tuning knobs (read once): CPPHF_MU_THREADS_PER_K spreads a k-point's bands
-// over more blocks; CPPHF_MU_MAXGRID caps the cooperative grid.
-int env_int(const char* name, int dflt) {
-    const char* e = std::getenv(name);
-    return e ? std::atoi(e) : dflt;
-}
-
+// Largest cooperative grid: the resident blocks of the device, at most kMuMaxGrid.
 int max_coop_grid() {
     static int g = 0;
     static std::once_flag once;
@@ -429,8 +425,6 @@ int max_coop_grid() {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_mu, kMuThreads, 0);
         if (per < 1) per = 1;
         g = std::min(kMuMaxGrid, per * num_sms());
-        const int cap = env_int("CPPHF_MU_MAXGRID", 0);
-        if (cap > 0) g = std::min(g, cap);
     });
     return g;
 }
@@ -456,7 +450,7 @@ int mu_solve(const double* eps, const double* w, int64_t nk, int64_t nb, double 
              const double* mu0, double T, int maxiter, int mode, double* mu_out, void* ws,
              size_t wsb, cudaStream_t st) {
     if (nk < 1 || nb < 1) return fail(CPPHF_ERR_INVALID, "mu: empty eigenvalue array");
-    if (nk * nb >= (int64_t)1 << 31) return fail(CPPHF_ERR_INVALID, "mu: more than 2^31 eigenvalues");
+    if (nb > (((int64_t)1 << 31) - 1) / nk) return fail(CPPHF_ERR_INVALID, "mu: more than 2^31-1 eigenvalues");
     if (!eps || !w || !mu_out) return fail(CPPHF_ERR_INVALID, "mu: null pointer");
     if (mode == 1 && !mu0) return fail(CPPHF_ERR_INVALID, "mu: null warm start");
     if (!ws || wsb < mu_workspace_bytes(nk, nb)) return fail(CPPHF_ERR_INVALID, "mu: workspace too small");
@@ -478,6 +472,9 @@ int mu_solve(const double* eps, const double* w, int64_t nk, int64_t nb, double 
     a.mode = mode;
     a.mu_out = mu_out;
     a.sync = reinterpret_cast<unsigned*>(ws);
+    a.err = wait_error_word();
+    if (!a.err) return CPPHF_ERR_CUDA;
+    a.spin_limit = barrier_spin_limit();
     a.part = reinterpret_cast<double*>(static_cast<unsigned char*>(ws) + 64);
     CPPHF_CUDA(cudaMemsetAsync(ws, 0, 64, st));
     if (grid == 1) {
@@ -527,7 +524,7 @@ static int noalloc_scratch(void** out) {
 int cpphf_find_mu_bisection_noalloc(const double* eps, const double* weights, int64_t nk, int64_t nb, double n_e,
                                     double T, int maxiter, double* mu_out, void* stream) {
     if (nk < 1 || nb < 1) return cpphf::fail(CPPHF_ERR_INVALID, "mu: empty eigenvalue array");
-    if (nk * nb > CPPHF_MU_NOALLOC_MAX_EIGENVALUES)
+    if (nb > CPPHF_MU_NOALLOC_MAX_EIGENVALUES / nk)
         return cpphf::fail(CPPHF_ERR_INVALID, "find_mu_bisection_noalloc: nk*nb exceeds the maximum of 2^31-1 eigenvalues");
     void* scratch = nullptr;
     CPPHF_TRY(noalloc_scratch(&scratch));

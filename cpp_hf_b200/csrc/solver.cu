@@ -457,15 +457,6 @@ struct IterGraphs {
     }
 };
 
-// CPPHF_SOLVE_GRAPHS=0 launches every kernel of every iteration (for A/B timing).
-bool solve_graphs_enabled() {
-    static const bool on = [] {
-        const char* e = std::getenv("CPPHF_SOLVE_GRAPHS");
-        return !(e && e[0] == '0');
-    }();
-    return on;
-}
-
 }  // namespace
 
 size_t solve_dm_workspace_bytes(const cpphf_kernel* K) { return dm_layout(K).total; }
@@ -491,7 +482,7 @@ int solve_dm(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* P
     // a replayed graph would read after they are gone.
     const bool sl_path = K->sl && (K->sl->fock_active || K->sl->hartree_active);
     const bool use_graphs = cfg->graphs != 0 && guard.capturable && (!project || cfg->project_device != 0) &&
-                            !sl_path && solve_graphs_enabled();
+                            !sl_path;
     IterGraphs graphs;
     unsigned char* W = static_cast<unsigned char*>(ws);
     auto fld = [&](size_t off) { return reinterpret_cast<double2*>(W + off); };
@@ -886,8 +877,7 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
     // one, so every iteration after the first is the same launch sequence (mix,
     // Fock build, occupations, residuals), captured once per precision.
     const bool sl_path = K->sl && (K->sl->fock_active || K->sl->hartree_active);
-    const bool scf_graphs = cfg->graphs != 0 && guard.capturable && acc == 0 && !project && !Dpre && !sl_path &&
-                            solve_graphs_enabled();
+    const bool scf_graphs = cfg->graphs != 0 && guard.capturable && acc == 0 && !project && !Dpre && !sl_path;
     IterGraphs sgr;
     bool pending_mix = false;
     while (k < max_iter && !converged) {
@@ -1109,6 +1099,14 @@ int density_from_fock(const double2* F, const double* w, int64_t nk1, int64_t nk
     return CPPHF_OK;
 }
 
+// Status of a synchronising entry point: a set device error word (a bounded
+// wait that gave up during the call) wins over the call's own status.
+int with_wait_check(int status, cudaStream_t st, const char* where) {
+    const int w = check_wait_error(st, where);
+    if (w == CPPHF_ERR_TIMEOUT || status == CPPHF_OK) return w;
+    return status;
+}
+
 }  // namespace cpphf
 
 extern "C" {
@@ -1120,9 +1118,10 @@ size_t cpphf_density_from_fock_workspace_bytes(int64_t nk, int64_t nb) {
 int cpphf_density_from_fock(const void* F, const double* w, int64_t nk1, int64_t nk2, int64_t nb, double n_e,
                             double T, double level_shift, void* P, double* eps, void* V, double* mu, void* workspace,
                             size_t workspace_bytes, void* stream) {
-    return cpphf::density_from_fock(static_cast<const double2*>(F), w, nk1, nk2, nb, n_e, T, level_shift,
-                                    static_cast<double2*>(P), eps, static_cast<double2*>(V), mu, workspace,
-                                    workspace_bytes, static_cast<cudaStream_t>(stream));
+    const int s = cpphf::density_from_fock(static_cast<const double2*>(F), w, nk1, nk2, nb, n_e, T, level_shift,
+                                           static_cast<double2*>(P), eps, static_cast<double2*>(V), mu, workspace,
+                                           workspace_bytes, static_cast<cudaStream_t>(stream));
+    return cpphf::with_wait_check(s, static_cast<cudaStream_t>(stream), "density_from_fock");
 }
 
 size_t cpphf_solve_dm_workspace_bytes(const cpphf_kernel* K) { return K ? cpphf::solve_dm_workspace_bytes(K) : 0; }
@@ -1137,10 +1136,11 @@ int cpphf_solve_dm(const cpphf_kernel* K, const cpphf_dm_config* cfg, const void
                    cpphf_project_fn project, void* project_user, void* Q_out, double* p_out, void* density_out,
                    void* fock_out, double* hist_E, double* hist_grad, cpphf_dm_result* result, void* workspace,
                    size_t workspace_bytes, void* stream) {
-    return cpphf::solve_dm(K, cfg, static_cast<const double2*>(P0), n_e, project, project_user,
-                           static_cast<double2*>(Q_out), p_out, static_cast<double2*>(density_out),
-                           static_cast<double2*>(fock_out), hist_E, hist_grad, result, workspace, workspace_bytes,
-                           static_cast<cudaStream_t>(stream));
+    const int s = cpphf::solve_dm(K, cfg, static_cast<const double2*>(P0), n_e, project, project_user,
+                                  static_cast<double2*>(Q_out), p_out, static_cast<double2*>(density_out),
+                                  static_cast<double2*>(fock_out), hist_E, hist_grad, result, workspace,
+                                  workspace_bytes, static_cast<cudaStream_t>(stream));
+    return cpphf::with_wait_check(s, static_cast<cudaStream_t>(stream), "solve_dm");
 }
 
 size_t cpphf_solve_scf_workspace_bytes(const cpphf_kernel* K) { return K ? cpphf::solve_scf_workspace_bytes(K) : 0; }
@@ -1153,9 +1153,11 @@ int cpphf_solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const vo
                     cpphf_project_fn project, void* project_user, void* density_out, void* fock_out,
                     double* hist_E, double* hist_density, double* hist_comm, cpphf_scf_result* result,
                     void* workspace, size_t workspace_bytes, void* stream) {
-    return cpphf::solve_scf(K, cfg, static_cast<const double2*>(P0), n_e, project, project_user,
-                            static_cast<double2*>(density_out), static_cast<double2*>(fock_out), hist_E, hist_density,
-                            hist_comm, result, workspace, workspace_bytes, static_cast<cudaStream_t>(stream));
+    const int s = cpphf::solve_scf(K, cfg, static_cast<const double2*>(P0), n_e, project, project_user,
+                                   static_cast<double2*>(density_out), static_cast<double2*>(fock_out), hist_E,
+                                   hist_density, hist_comm, result, workspace, workspace_bytes,
+                                   static_cast<cudaStream_t>(stream));
+    return cpphf::with_wait_check(s, static_cast<cudaStream_t>(stream), "solve_scf");
 }
 
 }  // extern "C"

@@ -37,9 +37,27 @@ extern "C" {
 const char* cpphf_last_error(void);
 int cpphf_version(void);
 
-/* Device-side flag set by bounded in-kernel waits (TMA barriers) that gave up;
- * synchronises the device, returns the flag (0 = none), clears it if clear != 0. */
+/* Device error word.  A bounded in-kernel wait that gives up (an mbarrier wait
+ * on an asynchronous copy: bit 1; a grid barrier of a cooperative kernel:
+ * bit 2) ORs its code into one word per device and the kernel returns early,
+ * leaving its outputs incomplete.  The entry points that synchronise (the
+ * solvers, cpphf_density_from_fock) read and clear the word before returning
+ * and report a set word as CPPHF_ERR_TIMEOUT.  Asynchronous entry points
+ * (cpphf_exchange, cpphf_build_fock, cpphf_find_mu_bisection, ...) return
+ * before their kernels run, so a timeout of theirs is seen by the next such
+ * read or by cpphf_device_error(), which synchronises the device, returns the
+ * word (0 = none) and clears it if clear != 0.  The mu kernels also write NaN
+ * to mu_out when their barrier gives up.  No counterpart in the reference,
+ * whose loops cannot hang (cpp_hf_native.cpp:58-70 maps its C++ exceptions). */
 int cpphf_device_error(int clear);
+
+/* Poll limit of the grid barriers in the cooperative mu kernels (each poll an
+ * L2 round trip; the default, 2e7, is seconds).  polls <= 0 restores the
+ * default.  Process-wide; read at each launch.  Small limits make a barrier
+ * give up before slower blocks arrive, which is how the timeout path is
+ * tested without hanging a GPU.  No counterpart in the reference. */
+int cpphf_set_barrier_spin_limit(long long polls);
+long long cpphf_barrier_spin_limit(void);
 
 /* Synchronous host <-> device copies on `stream` (for projector callbacks). */
 int cpphf_copy_d2h(void* dst_host, const void* src_device, size_t bytes, void* stream);
@@ -93,18 +111,20 @@ int cpphf_find_mu_bisection(const double* eps, const double* weights, int64_t nk
 /* Allocation-free variant of cpphf_find_mu_bisection.  No counterpart in the
  * reference: it exists for callers that cannot allocate device memory at call
  * time - a host plug-in whose device memory belongs to a fixed pool it may not
- * grow, a runtime that forbids cudaMalloc/cudaFree in its critical path
- * because they synchronise the device, or code issuing work from a stream
- * callback where CUDA calls that allocate are not allowed.  Same arguments and
+ * grow, or a runtime that forbids cudaMalloc/cudaFree in its critical path
+ * because they synchronise the device.  (It makes CUDA calls - it launches a
+ * kernel - so like any entry point it must not be called from a host function
+ * queued on a stream.)  Same arguments and
  * result as cpphf_find_mu_bisection minus the workspace: the scratch (grid
  * barrier words and block partials, about 74 KB) is a file-scope device array
  * that every GPU loading the library holds until the process exits.  Limit:
  * nk*nb <= CPPHF_MU_NOALLOC_MAX_EIGENVALUES; larger sizes are rejected with
  * CPPHF_ERR_INVALID.  The first call on a device looks up the array's device
  * address (with that device current) and should come before any stream
- * capture.  Calls share the array: each call clears the words that must start
- * at zero, and calls that overlap on the GPU race.  Calls no allocating
- * routine. */
+ * capture; the cached address is not valid across cudaDeviceReset() or a
+ * re-created primary context, so do not use this entry point after either.
+ * Calls share the array: each call clears the words that must start at zero,
+ * and calls that overlap on the GPU race.  Calls no allocating routine. */
 #define CPPHF_MU_NOALLOC_MAX_EIGENVALUES 2147483647LL
 int cpphf_find_mu_bisection_noalloc(const double* eps, const double* weights, int64_t nk, int64_t nb,
                                     double n_e, double T, int maxiter, double* mu_out, void* stream);

@@ -1,7 +1,8 @@
 """Pin the oracle against the reference's own tests and stored regression data.
 
-Test infrastructure.  Runs in a container where the reference checkout is
-present (default ``/root/reference``; override with ``CPPHF_REFERENCE``):
+Test infrastructure.  Runs where a checkout of the reference is present; its
+root directory is given by the ``CPPHF_REFERENCE`` environment variable
+(required, no default):
 
 1. the reference's pytest suite (``tests/``) with ``oracle.native_np`` installed
    as ``cpp_hf._native``, the trust-region Newton and deflation tests
@@ -22,7 +23,14 @@ import sys
 from pathlib import Path
 
 REPO = Path(__file__).resolve().parents[1]
-REF = Path(os.environ.get("CPPHF_REFERENCE", "/root/reference"))
+def _reference_root() -> Path:
+    root = os.environ.get("CPPHF_REFERENCE")
+    if not root:
+        raise SystemExit("set CPPHF_REFERENCE to the root of a cpp_hf checkout")
+    return Path(root)
+
+
+REF = _reference_root()
 
 # Every reference test file runs.
 DESELECT: list[str] = []

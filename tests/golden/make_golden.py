@@ -1,9 +1,9 @@
 """Generate the committed golden fixtures in ``tests/golden/`` from the reference.
 
-Run in a container that has the reference checkout (default
-``/root/reference``, override with ``CPPHF_REFERENCE``):
+Run where a checkout of the reference is present, its root directory given
+by the ``CPPHF_REFERENCE`` environment variable (required, no default):
 
-    python tests/golden/make_golden.py
+    CPPHF_REFERENCE=<reference checkout> python tests/golden/make_golden.py
 
 Writes
 
@@ -35,7 +35,14 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parents[1]
-REF = Path(os.environ.get("CPPHF_REFERENCE", "/root/reference"))
+def _reference_root() -> Path:
+    root = os.environ.get("CPPHF_REFERENCE")
+    if not root:
+        raise SystemExit("set CPPHF_REFERENCE to the root of a cpp_hf checkout")
+    return Path(root)
+
+
+REF = _reference_root()
 
 
 def _ref_cases():

@@ -59,3 +59,18 @@ def test_native_module_has_reference_names():
         a = inspect.signature(getattr(_native, name))
         b = inspect.signature(getattr(native_np, name))
         assert list(a.parameters) == list(b.parameters), name
+
+
+def test_barrier_spin_limit_setting_round_trips():
+    """Host-only setter (no device call): limit > 0 is kept, <= 0 restores the default."""
+    if not _lib.LIB_PATH.exists():
+        pytest.fail(f"{_lib.LIB_PATH} not built (run python -m cpp_hf_b200.build)")
+    lib = _lib.load()
+    default = lib.cpphf_barrier_spin_limit()
+    assert default > 1000
+    try:
+        assert lib.cpphf_set_barrier_spin_limit(5) == 0
+        assert lib.cpphf_barrier_spin_limit() == 5
+    finally:
+        lib.cpphf_set_barrier_spin_limit(0)
+    assert lib.cpphf_barrier_spin_limit() == default

@@ -1,9 +1,8 @@
 """GPU: the allocation-free chemical-potential entry point agrees with the workspace one.
 
 ``cpphf_find_mu_bisection_noalloc`` serves callers that cannot allocate device
-memory when they call in (a fixed device-memory pool they may not grow, a
-latency-critical loop where cudaMalloc/cudaFree would synchronise the device,
-work issued from a stream callback).  Its scratch is a file-scope device array
+memory when they call in (a fixed device-memory pool they may not grow, or a
+latency-critical loop where cudaMalloc/cudaFree would synchronise the device).  Its scratch is a file-scope device array
 shared by every call, so this test runs two different problems back to back
 through the C ABI and compares each result with ``cpphf_find_mu_bisection``
 (caller-provided workspace) at the tolerance the other mu tests use.  The file
