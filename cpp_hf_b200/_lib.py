@@ -48,11 +48,12 @@ class Kernel(C.Structure):
         ("nk1", i64), ("nk2", i64), ("nb", i64), ("dv", i64),
         ("include_hartree", i32), ("include_exchange", i32), ("exchange_hcp", i32),
         ("has_refP", i32), ("has_contact", i32), ("n_contact", i32),
-        ("exchange_precision", i32), ("reserved0", i32),
+        ("exchange_precision", i32), ("hermitian_packing", i32),
         ("T", f64), ("weight_sum", f64),
         ("h", vp), ("VR", vp), ("refP", vp), ("w2d", vp), ("HH", vp),
         ("contact_g", vp), ("contact_Oi", vp), ("contact_Oj", vp),
         ("sl", C.POINTER(Superlattice)),
+        ("VR_packed", vp), ("h_packed", vp),
     ]
 
 
@@ -116,6 +117,8 @@ _SIGS = {
     "cpphf_solve_mu_inloop": (C.c_int, [vp, vp, i64, i64, f64, vp, f64, C.c_int, vp, vp, sz, vp]),
     "cpphf_find_mu_bisection_noalloc": (C.c_int, [vp, vp, i64, i64, f64, f64, C.c_int, vp, vp]),
     "cpphf_build_fock_workspace_bytes": (sz, [C.POINTER(Kernel)]),
+    "cpphf_kernel_packed_bytes": (sz, [C.POINTER(Kernel)]),
+    "cpphf_kernel_pack": (C.c_int, [C.POINTER(Kernel), vp, vp, vp]),
     "cpphf_build_fock": (C.c_int, [C.POINTER(Kernel), vp, vp, vp, vp, vp, vp, vp, sz, vp]),
     "cpphf_cayley_spectral_setup": (C.c_int, [vp, vp, vp, i64, i64, vp]),
     "cpphf_cayley_unitary": (C.c_int, [vp, vp, f64, vp, i64, i64, vp]),

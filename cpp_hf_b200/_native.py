@@ -54,6 +54,15 @@ __all__ = [
 # "solve_graphs" (default True): solve_dm (and solve_scf with linear mixing)
 # replay each iteration as a captured CUDA graph; False launches every kernel
 # (better for many concurrent solves).
+# "hermitian_packing" (default True): when VR is Hermitian in the orbital pair
+# (VR_ba(R) = conj VR_ab(-R), i.e. V(q) Hermitian at every q, checked once per
+# kernel), solves transform only the nb(nb+1)/2 upper-triangle channels and
+# fuse the Fock assembly into the last FFT pass (their densities are
+# Hermitian: both solvers hermitise P0 before the first build); False keeps
+# the full nb*nb channel path.
+# "hermitian_density" (default False): build_fock_apply may assume P is
+# Hermitian and take the same packed path (the reference's exchange_hcp
+# already implies this for a scalar VR).
 DEFAULT_EXCHANGE_PRECISION = 64
 DEFAULT_MIXED_SWITCH = 1.0e-5
 
@@ -257,6 +266,23 @@ def find_mu_bisection(bands, weights, n_e, T, maxiter=0):
 # kernel view
 # ---------------------------------------------------------------------------
 
+def _vr_hermitian(VR_t):
+    """True when VR_ba(R) == conj VR_ab(-R) to 1e-12 of max|VR| (V(q) Hermitian at every q).
+
+    R -> -R is the index map j -> (-j) mod n on both mesh axes; for a scalar VR
+    (V real) the condition reads VR(R) == conj VR(-R).  Runs on the device.
+    """
+    n0, n1 = VR_t.shape[0], VR_t.shape[1]
+    i0 = (-torch.arange(n0, device=VR_t.device)) % n0
+    i1 = (-torch.arange(n1, device=VR_t.device)) % n1
+    neg = VR_t.index_select(0, i0).index_select(1, i1)
+    scale = float(VR_t.abs().max())
+    if scale == 0.0:
+        return True
+    dev = float((VR_t.transpose(-1, -2) - neg.conj()).abs().max())
+    return dev <= 1e-12 * scale
+
+
 class _DeviceKernel:
     """Device copies of a kernel_args dict + the ``cpphf_kernel`` struct."""
 
@@ -314,7 +340,42 @@ class _DeviceKernel:
         K.contact_g, K.contact_Oi, K.contact_Oj = cg.data_ptr(), cOi.data_ptr(), cOj.data_ptr()
         if self.sl is not None:
             K.sl = C.pointer(self.sl[0])
+        K.hermitian_packing = 0
         self.K = K
+        self.dv = dv1
+        self.allow_packing = bool(args.get("hermitian_packing", True)) and self.sl is None and nb <= 8
+        self._v_herm = None
+        self._packed = None
+
+    def v_hermitian(self):
+        if self._v_herm is None:
+            self._v_herm = _vr_hermitian(self._keep[1])
+        return self._v_herm
+
+    def enable_packing(self):
+        """Turn on the Hermitian-packed build when V allows it (its packed VR and
+        h are made on the device once); returns whether it is on."""
+        K = self.K
+        if not (self.allow_packing and K.include_exchange and self.v_hermitian()):
+            K.hermitian_packing = 0
+            return False
+        lib = _lib_handle()
+        if self._packed is None:
+            nbytes = lib.cpphf_kernel_packed_bytes(C.byref(K))
+            if nbytes == 0:
+                K.hermitian_packing = 0
+                return False
+            hp = _ws(nbytes)
+            vp = _ws(nbytes) if self.dv != 1 else None
+            check(lib.cpphf_kernel_pack(C.byref(K), _ptr(vp), _ptr(hp), _stream()), "kernel_pack")
+            self._packed = (vp, hp)
+            K.VR_packed = vp.data_ptr() if vp is not None else None
+            K.h_packed = hp.data_ptr()
+        K.hermitian_packing = 1
+        return True
+
+    def disable_packing(self):
+        self.K.hermitian_packing = 0
 
     def ref(self):
         return C.byref(self.K)
@@ -394,15 +455,73 @@ def _host_project(project_fn, F):
     return 0.5 * (t + t.conj().transpose(-1, -2))
 
 
+# ---------------------------------------------------------------------------
+# device copies of kernel_args kept between build_fock_apply calls
+# ---------------------------------------------------------------------------
+# A loop of build_fock_apply calls on one kernel_args dict (the reference's
+# tests, user scripts) would otherwise upload h and VR (two fields) on every
+# call.  Entries are keyed on every value of the dict: a NumPy array by its
+# identity, data pointer, shape, strides, dtype and a checksum of about 4096
+# evenly spaced elements; a torch tensor by its data pointer, shape, strides,
+# dtype and version counter (exact); any other value by its repr.  A NumPy
+# array modified in place only at elements the checksum does not sample would
+# be served stale: rebuild the dict (or call clear_kernel_cache()) after
+# editing kernel arrays in place.
+_KERNEL_CACHE_SIZE = 2
+_kernel_cache = {}
+
+
+def _value_key(v):
+    if _is_torch(v):
+        return ("t", v.data_ptr(), tuple(v.shape), tuple(v.stride()), str(v.dtype), v._version)
+    if isinstance(v, np.ndarray):
+        flat = v.reshape(-1)
+        step = max(1, flat.size // 4096)
+        return ("n", id(v), v.__array_interface__["data"][0], v.shape, v.strides, v.dtype.str,
+                hash(np.ascontiguousarray(flat[::step]).tobytes()))
+    if isinstance(v, (list, tuple)):
+        return tuple(_value_key(x) for x in v)
+    return ("v", repr(v))
+
+
+def _cached_device_kernel(kernel_args):
+    key = (torch.cuda.current_device(),) + tuple((k, _value_key(kernel_args[k])) for k in sorted(kernel_args))
+    dk = _kernel_cache.pop(key, None)
+    if dk is None:
+        dk = _DeviceKernel(kernel_args)
+    _kernel_cache[key] = dk  # most recently used last
+    while len(_kernel_cache) > _KERNEL_CACHE_SIZE:
+        _kernel_cache.pop(next(iter(_kernel_cache)))
+    return dk
+
+
+def clear_kernel_cache():
+    """Drop the device copies of kernel_args kept by build_fock_apply."""
+    _kernel_cache.clear()
+
+
+def _pinned_like(t):
+    return torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+
+
 def build_fock_apply(kernel_args, P, project_fn):
-    """cpp_hf_native.cpp:380-415 -> (Sigma, H, F, E)."""
+    """cpp_hf_native.cpp:380-415 -> (Sigma, H, F, E).
+
+    NumPy in, NumPy out: the kernel arrays' device copies are reused between
+    calls on the same kernel_args (see _cached_device_kernel), P goes up, and
+    Sigma, H and F come back into page-locked buffers that the returned arrays
+    keep alive (torch's caching host allocator reuses them once released)."""
     lib = _lib_handle()
     as_np = not _is_torch(P)
-    dk = _DeviceKernel(kernel_args)
+    dk = _cached_device_kernel(kernel_args)
     P_t = _to_dev(P, "c")
     nk1, nk2, nb = dk.shape
     if tuple(P_t.shape) != (nk1, nk2, nb, nb):
         raise ValueError("P must match h shape")
+    if kernel_args.get("hermitian_density", False) or (bool(kernel_args["exchange_hcp"]) and dk.dv == 1):
+        dk.enable_packing()
+    else:
+        dk.disable_packing()
     Sigma = torch.empty_like(P_t)
     F = torch.empty_like(P_t)
     H = torch.empty_like(P_t)
@@ -418,9 +537,19 @@ def build_fock_apply(kernel_args, P, project_fn):
         elif not dproj.is_identity:
             dproj.project_(F)
             F = 0.5 * (F + F.conj().transpose(-1, -2))
-    E_host = float(E.item())
+    if not as_np:
+        E_host = float(E.item())
+        _lib.check_device_error("build_fock_apply")
+        return Sigma, H, F, E_host
+    outs = []
+    for t in (Sigma, H, F):
+        h = _pinned_like(t)
+        h.copy_(t, non_blocking=True)
+        outs.append(h)
+    E_h = E.to("cpu", non_blocking=True)
+    _sync()
     _lib.check_device_error("build_fock_apply")
-    return _out(Sigma, as_np), _out(H, as_np), _out(F, as_np), E_host
+    return outs[0].numpy(), outs[1].numpy(), outs[2].numpy(), float(E_h[0])
 
 
 # ---------------------------------------------------------------------------
@@ -480,6 +609,7 @@ def solve_dm(kernel_args, P0, n_e, max_iter, tol_E, tol_grad, max_step, bt_shrin
     dk = _DeviceKernel(kernel_args)
     P0_t = _to_dev(P0, "c")
     nk1, nk2, nb = dk.shape
+    dk.enable_packing()  # the solver hermitizes P0 before its first build
     max_iter = int(max_iter)
     cfg = _lib.DmConfig()
     cfg.max_iter = max_iter
@@ -540,6 +670,7 @@ def solve_scf(kernel_args, P0, n_e, max_iter, density_tol, comm_tol, mixing, lev
     as_np = not _is_torch(P0)
     dk = _DeviceKernel(kernel_args)
     P0_t = _to_dev(P0, "c")
+    dk.enable_packing()  # the solver hermitizes P0 before its first build
     max_iter = int(max_iter)
     cfg = _lib.ScfConfig()
     cfg.max_iter = max_iter

@@ -24,6 +24,7 @@
 #include "fft.cuh"
 #include "fft_reg.cuh"
 #include "bulk.cuh"
+#include "exchange_pipe.cuh"
 
 #include <algorithm>
 #include <cstdio>
@@ -262,28 +263,6 @@ __global__ void __launch_bounds__(256) k_rows_inv_s(const Cx* T, double2* Sigma,
 // smem: tw[N] | mbar[kMaxPipeStages] | stage[nst] = { in tile [N][CB] (double2,
 //       or Cx for T), second tile [N][CB] double2 (refP or VR) }
 // ===========================================================================
-struct PipeLayout {
-    size_t tw, bar, stage0, stage_bytes, in_bytes, total;
-};
-
-// Offsets are relative to a 128-byte aligned base (TMA tensor copies need
-// 128-byte aligned shared-memory destinations); `total` includes the slack
-// for aligning the dynamic shared-memory base.
-constexpr int kMaxPipeStages = 4;
-constexpr int kColsMaxThreads = 128;  // launch bound of the pipelined columns pass
-
-__host__ __device__ inline PipeLayout pipe_layout(int N, int CB, size_t in_elem, bool second, int nst) {
-    PipeLayout L;
-    L.tw = 0;
-    L.bar = (sizeof(double2) * (size_t)N + 15) & ~(size_t)15;
-    L.stage0 = (L.bar + 8 * kMaxPipeStages + 127) & ~(size_t)127;
-    L.in_bytes = ((in_elem * (size_t)N * CB) + 127) & ~(size_t)127;
-    L.stage_bytes = L.in_bytes + (second ? sizeof(double2) * (size_t)N * CB : 0);
-    L.stage_bytes = (L.stage_bytes + 127) & ~(size_t)127;
-    L.total = L.stage0 + (size_t)nst * L.stage_bytes + 128;
-    return L;
-}
-
 // Columns pass: the T tiles keep the ring of nst stages, VR has one buffer that
 // is refilled for the next tile as soon as the current tile's multiply has read
 // it (VR is read once per tile, in the middle of the transform).
@@ -305,15 +284,6 @@ __host__ __device__ inline ColsLayout cols_layout(int N, int CB, size_t in_elem,
     L.vr = L.stage0 + (size_t)nst * L.stage_bytes;
     L.total = L.vr + ((sizeof(double2) * (size_t)N * CB + 127) & ~(size_t)127) + 128;
     return L;
-}
-
-// 128-byte aligned start inside a dynamic shared-memory array.  The offset is
-// taken from the 32-bit shared address and added to the array itself, so the
-// result stays a shared-memory pointer (a round trip through uintptr_t would
-// turn every access into a generic 64-bit one).
-__device__ __forceinline__ unsigned char* align128(unsigned char* p) {
-    const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(p));
-    return p + ((128u - (a & 127u)) & 127u);
 }
 
 // pass A: rows forward.  Tile t -> (kx = t / nchunk, chunk = t % nchunk).
@@ -727,7 +697,6 @@ Launch plan_launch(int lanes, int C, size_t elem, int n, bool generic, int targe
     return L;
 }
 
-constexpr size_t kSmemMax = 227 * 1024 - 1024;
 
 // Pipelined-pass shape: threads per CTA (sets the channels per tile) and the
 // number of shared-memory stages.  Block shapes of 64-256 threads and 2-4
@@ -889,30 +858,7 @@ int cap_threads(K kern, int threads) {
     return std::max(32, std::min(threads, m));
 }
 
-#define CPPHF_SPEC_SIZES(X) \
-    X(1, 1, 1)              \
-    X(2, 2, 1)              \
-    X(3, 3, 1)              \
-    X(4, 4, 1)              \
-    X(5, 5, 1)              \
-    X(6, 3, 2)              \
-    X(8, 4, 2)              \
-    X(9, 3, 3)              \
-    X(12, 4, 3)             \
-    X(16, 4, 4)             \
-    X(18, 6, 3)             \
-    X(24, 6, 4)             \
-    X(32, 8, 4)             \
-    X(36, 6, 6)             \
-    X(48, 8, 6)             \
-    X(64, 8, 8)             \
-    X(72, 9, 8)             \
-    X(96, 12, 8)            \
-    X(128, 16, 8)           \
-    X(144, 12, 12)          \
-    X(192, 16, 12)          \
-    X(256, 16, 16)          \
-    X(288, 18, 16)
+
 
 
 template <class Cx>
@@ -1002,6 +948,11 @@ size_t exchange_t_bytes(int64_t nk1, int64_t nk2, int64_t nb, int hcp, int preci
 // T when it does not alias Sigma (0 for the full FP64 form).
 size_t exchange_workspace_bytes(int64_t nk1, int64_t nk2, int64_t nb, int hcp, int precision) {
     return exchange_t_bytes(nk1, nk2, nb, hcp, precision);
+}
+
+int exchange_columns(void* T, const double2* VR, const ExchangeGeom& g, int precision, cudaStream_t st) {
+    if (precision == 32) return pass_cols<float2>(static_cast<float2*>(T), VR, g, kColsVR, st);
+    return pass_cols<double2>(static_cast<double2*>(T), VR, g, kColsVR, st);
 }
 
 int exchange(const double2* P, const double2* refP, const double2* VR, double2* Sigma, int64_t nk1, int64_t nk2,

@@ -23,4 +23,9 @@ int exchange(const double2* P, const double2* refP, const double2* VR, double2* 
              int64_t nk2, int64_t nb, int64_t dv, int hcp, int shift, int precision,
              void* workspace, size_t workspace_bytes, cudaStream_t st);
 
+// The columns pass alone on an (n0, n1, g.C) field T (complex128, or complex64
+// with precision 32): FFT along kx, times VR (g.dv = 1: one scalar per q,
+// else g.dv = g.C channels laid out like T), inverse FFT along kx, in place.
+int exchange_columns(void* T, const double2* VR, const ExchangeGeom& g, int precision, cudaStream_t st);
+
 }  // namespace cpphf

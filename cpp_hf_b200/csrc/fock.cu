@@ -30,7 +30,7 @@ namespace {
 
 constexpr int kAsmThreads = 256;
 constexpr int kRedThreads = 256;
-constexpr int kMaxPartials = 2048;
+constexpr int kMaxPartials = kFockMaxPartials;
 constexpr int kAsmMaxStages = 4;
 constexpr int kTileElems = 1024;  // k-blocks of at most this many elements take the bulk-pipelined assembly
 
@@ -301,7 +301,7 @@ __global__ void k_sum_partials(const double* __restrict__ part, int n, double* _
 }
 
 struct FockWs {
-    size_t off_part, off_counter, off_rho_part, off_rho_bar, off_sc, off_hd, off_exch, total;
+    size_t off_part, off_counter, off_rho_part, off_rho_bar, off_sc, off_hd, off_exch, off_pack, total;
     size_t off_sl, sl_bytes, off_slh, off_rho;
     int Gasm, Gk;
 };
@@ -340,6 +340,7 @@ FockWs fock_ws_layout(const cpphf_kernel* K) {
     L.off_hd = take(sizeof(double) * nb);
     const int hcp = (K->exchange_hcp && K->dv == 1) ? 1 : 0;
     L.off_exch = take(exchange_workspace_bytes(K->nk1, K->nk2, K->nb, hcp, K->exchange_precision));
+    L.off_pack = take(packed_fock_workspace_bytes(K));
     L.sl_bytes = 0;
     L.off_sl = L.off_slh = L.off_rho = o;
     if (sl_fock(K)) {
@@ -388,7 +389,7 @@ size_t build_fock_workspace_bytes(const cpphf_kernel* K) { return fock_ws_layout
 int build_fock(const cpphf_kernel* K, const double2* P, double2* Sigma, double2* F, double* hd_out,
                double* energy, double2* Hdense, void* ws, size_t wsb, cudaStream_t st) {
     CPPHF_TRY(validate_kernel(K));
-    if (!P || !Sigma || !F) return fail(CPPHF_ERR_INVALID, "build_fock: null pointer");
+    if (!P || !F) return fail(CPPHF_ERR_INVALID, "build_fock: null pointer");
     const FockWs L = fock_ws_layout(K);
     if (!ws || wsb < L.total)
         return fail(CPPHF_ERR_INVALID, "build_fock: workspace too small (" + std::to_string(L.total) + " bytes needed)");
@@ -419,6 +420,13 @@ int build_fock(const cpphf_kernel* K, const double2* P, double2* Sigma, double2*
     } else if (hd_out) {
         CPPHF_CUDA(cudaMemsetAsync(hd, 0, sizeof(double) * nb, st));
     }
+    if (packed_fock_eligible(K)) {
+        unsigned* counter = reinterpret_cast<unsigned*>(W + L.off_counter);
+        return build_fock_packed(K, P, Sigma, F, (K->include_hartree && !slh) ? hd : nullptr,
+                                 (K->has_contact || slh) ? SC : nullptr, need_pre ? rho_bar : nullptr, energy,
+                                 Hdense, part, counter, W + L.off_pack, wsb - L.off_pack, st);
+    }
+    if (!Sigma) return fail(CPPHF_ERR_INVALID, "build_fock: null Sigma");
     if (sl_fock(K)) {
         const cpphf_superlattice* sl = K->sl;
         const double2* rho = P;

@@ -561,7 +561,7 @@ int deflation(const double2* P, const double2* targets, int64_t n_defl, const do
 struct RtrLayout {
     size_t Q[2], Ft[2], G[2], P, Sig, F, vX, HvX, rX, dX, HDX, dP, Vd;
     size_t p[2], eps[2], gp, ew, lamd, vp, Hvp, rp, dp, HDp, wn;
-    size_t S, R, d2, fock_ws, mu_ws, total;
+    size_t S, R, d2, fock_ws, mu_ws, pack, total;
     size_t fock_bytes, mu_bytes;
 };
 
@@ -569,7 +569,7 @@ size_t fock_bytes_rtr(const cpphf_kernel* K) {
     // the response build runs without the reference density, the state builds with it
     cpphf_kernel Kr = *K;
     Kr.has_refP = 0;
-    return std::max(build_fock_workspace_bytes(K), build_fock_workspace_bytes(&Kr));
+    return std::max(fock_bytes_packed_kernel(K), fock_bytes_packed_kernel(&Kr));
 }
 
 RtrLayout rtr_layout(const cpphf_kernel* K, int64_t n_defl) {
@@ -617,6 +617,7 @@ RtrLayout rtr_layout(const cpphf_kernel* K, int64_t n_defl) {
     L.fock_ws = take(L.fock_bytes);
     L.mu_bytes = mu_workspace_bytes((int64_t)nk, (int64_t)nb);
     L.mu_ws = take(L.mu_bytes);
+    L.pack = take(solver_pack_bytes(K));
     L.total = take.total;
     return L;
 }
@@ -645,6 +646,9 @@ int solve_rtr(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* 
                     "solve_dm (newton): workspace too small (" + std::to_string(L.total) + " bytes needed)");
     init_rtr_attrs();
     unsigned char* W = static_cast<unsigned char*>(ws);
+    cpphf_kernel Kp;  // K with its packed VR / h (Hermitian packing), made once per solve
+    CPPHF_TRY(solver_pack(K, &Kp, W + L.pack, st));
+    K = &Kp;
     auto fld = [&](size_t off) { return reinterpret_cast<double2*>(W + off); };
     auto vec = [&](size_t off) { return reinterpret_cast<double*>(W + off); };
     double2* Q[2] = {fld(L.Q[0]), fld(L.Q[1])};
@@ -705,7 +709,7 @@ int solve_rtr(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* 
     static_assert(8 + kNumSums <= kHostScalars, "host scalar layout");
     auto eval = [&](int s, bool with_model) -> int {
         CPPHF_TRY(finish_density());
-        CPPHF_TRY(build_fock(K, P, Sig, Ft[s], nullptr, &R->energy[s], nullptr, fws, L.fock_bytes, st));
+        CPPHF_TRY(build_fock(K, P, solver_sigma(K, Sig), Ft[s], nullptr, &R->energy[s], nullptr, fws, L.fock_bytes, st));
         if (defl)
             CPPHF_TRY(deflation(P, targets, cfg->n_deflation, K->w2d, nk, nb, cfg->deflation_sigma, d_len, Ft[s],
                                 Ft[s], &R->energy[s], &R->phi, &R->pen[s], d2, R, st));
@@ -742,7 +746,7 @@ int solve_rtr(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* 
 
     // ---- initialise (Q, p) from F[P0] (solver_rtr.hpp:251-262) ----
     CPPHF_TRY(hermitize(P0, P, nk, nb, st));
-    CPPHF_TRY(build_fock(K, P, Sig, F, nullptr, nullptr, nullptr, fws, L.fock_bytes, st));
+    CPPHF_TRY(build_fock(K, P, solver_sigma(K, Sig), F, nullptr, nullptr, nullptr, fws, L.fock_bytes, st));
     CPPHF_TRY(eigh_batched(F, eps[0], Q[0], nk, nb, 0, nullptr, st));
     CPPHF_TRY(mu_solve(eps[0], wn, nk, nb, n_t, &R->mu[0], T_r, mu_it, 1, &R->mu[0], mws, L.mu_bytes, st));
     CPPHF_TRY(occupy(0, eps[0]));
@@ -777,7 +781,7 @@ int solve_rtr(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* 
         auto hvp_step = [&](int mode, double beta, double rz_old) -> int {
             CPPHF_TRY(launch_direction(rX, rp, ek, pk, K->w2d, Q[s], vX, vp, dX, dp, dP, nk, nb, T_r, lam, beta, 0.0,
                                        rz_old, mode, R, st));
-            CPPHF_TRY(build_fock(&Kr, dP, Sig, F, nullptr, nullptr, nullptr, fws, L.fock_bytes, st));
+            CPPHF_TRY(build_fock(&Kr, dP, solver_sigma(&Kr, Sig), F, nullptr, nullptr, nullptr, fws, L.fock_bytes, st));
             return launch_hvp(dX, dp, Q[s], pk, Ft[s], F, hmat, dP, pen, K->w2d, HDX, HDp, nk, nb, T_r, R, st);
         };
         auto update = [&](int mode, double a, double shift_h) -> int {
@@ -862,7 +866,7 @@ int solve_rtr(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* 
     // ---- finalize (solver_rtr.hpp:437-443) ----
     CPPHF_TRY(dm_density(Q[s], p[s], P, nk, nb, st));
     CPPHF_TRY(finish_density());
-    CPPHF_TRY(build_fock(K, P, Sig, F, nullptr, &R->efin, nullptr, fws, L.fock_bytes, st));
+    CPPHF_TRY(build_fock(K, P, solver_sigma(K, Sig), F, nullptr, &R->efin, nullptr, fws, L.fock_bytes, st));
     if (Q_out) CPPHF_CUDA(cudaMemcpyAsync(Q_out, Q[s], fbytes, cudaMemcpyDeviceToDevice, st));
     if (p_out) CPPHF_CUDA(cudaMemcpyAsync(p_out, p[s], vbytes, cudaMemcpyDeviceToDevice, st));
     if (D_out) CPPHF_CUDA(cudaMemcpyAsync(D_out, P, fbytes, cudaMemcpyDeviceToDevice, st));
@@ -924,7 +928,7 @@ int cpphf_rtr_joint_hvp(const cpphf_kernel* K, const void* X, const double* dp, 
     CPPHF_TRY(launch_direction(nullptr, nullptr, nullptr, p, K->w2d, static_cast<const double2*>(Q), nullptr,
                                nullptr, const_cast<double2*>(static_cast<const double2*>(X)),
                                const_cast<double*>(dp), dP, nk, nb, T_r, 0.0, 0.0, 0.0, 1.0, 2, R, st));
-    CPPHF_TRY(build_fock(&Kr, dP, Sig, F, nullptr, nullptr, nullptr, fws, fb, st));
+    CPPHF_TRY(build_fock(&Kr, dP, solver_sigma(&Kr, Sig), F, nullptr, nullptr, nullptr, fws, fb, st));
     CPPHF_TRY(launch_hvp(static_cast<const double2*>(X), dp, static_cast<const double2*>(Q), p,
                          static_cast<const double2*>(Ft), F, static_cast<const double2*>(K->h), dP, nullptr, K->w2d,
                          static_cast<double2*>(HX), Hp, nk, nb, T_r, R, st));

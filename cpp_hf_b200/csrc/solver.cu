@@ -356,7 +356,7 @@ struct SolverWs {
 size_t fock_bytes_any_precision(const cpphf_kernel* K) {
     cpphf_kernel K32 = *K;
     K32.exchange_precision = 32;
-    return std::max(build_fock_workspace_bytes(K), build_fock_workspace_bytes(&K32));
+    return std::max(fock_bytes_packed_kernel(K), fock_bytes_packed_kernel(&K32));
 }
 
 // Exchange precision of a switched solve: complex64 first, complex128 after.
@@ -368,7 +368,7 @@ int check_mixed(const cpphf_kernel* K, double sw) {
 }
 
 struct DmLayout {
-    size_t Q, P, Sig, F, G[2], dQ[2], Vd, p, eps, g[2], dp[2], lam, ew, wn, S, fock_ws, mu_ws, total;
+    size_t Q, P, Sig, F, G[2], dQ[2], Vd, p, eps, g[2], dp[2], lam, ew, wn, S, fock_ws, mu_ws, pack, total;
     size_t fock_bytes, mu_bytes;
 };
 
@@ -400,6 +400,7 @@ DmLayout dm_layout(const cpphf_kernel* K) {
     L.fock_ws = W.take(L.fock_bytes);
     L.mu_bytes = mu_workspace_bytes((int64_t)nk, (int64_t)nb);
     L.mu_ws = W.take(L.mu_bytes);
+    L.pack = W.take(solver_pack_bytes(K));
     L.total = W.total;
     return L;
 }
@@ -477,6 +478,9 @@ int solve_dm(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* P
         return fail(CPPHF_ERR_INVALID, "solve_dm: workspace too small (" + std::to_string(L.total) + " bytes needed)");
     const SolveStream guard(st);
     st = guard.stream();
+    cpphf_kernel Kp;  // K with its packed VR / h (Hermitian packing), made once per solve
+    CPPHF_TRY(solver_pack(K, &Kp, static_cast<unsigned char*>(ws) + L.pack, st));
+    K = &Kp;
     // Not captured: host projector callbacks (host round trips) and the superlattice
     // exchange, whose per-call channel tables are copied from host buffers that
     // a replayed graph would read after they are gone.
@@ -534,7 +538,7 @@ int solve_dm(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* P
 
     // ---- init (solver_dm.hpp:436-459) ----
     CPPHF_TRY(hermitize(P0, P, nk, nb, st));
-    CPPHF_TRY(build_fock(K, P, Sig, F, nullptr, nullptr, nullptr, fws, L.fock_bytes, st));
+    CPPHF_TRY(build_fock(K, P, solver_sigma(K, Sig), F, nullptr, nullptr, nullptr, fws, L.fock_bytes, st));
     CPPHF_TRY(eigh_batched(F, ew, Q, nk, nb, 0, nullptr, st));
     CPPHF_TRY(mu_solve(ew, wn, nk, nb, n_t, &S->mu, T_r, mu_it, 1, &S->mu, mws, L.mu_bytes, st));
 
@@ -560,7 +564,7 @@ int solve_dm(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* P
 
         // 1. density (with occupations from the last eps_work and mu) + Fock + energy
         CPPHF_TRY(density(ew));
-        CPPHF_TRY(build_fock(Kb, P, Sig, F, nullptr, &S->energy, nullptr, fws, L.fock_bytes, st));
+        CPPHF_TRY(build_fock(Kb, P, solver_sigma(Kb, Sig), F, nullptr, &S->energy, nullptr, fws, L.fock_bytes, st));
         // 2.-4. Ft = Q^H F Q, gradient, preconditioner, PR+ direction
         if (small) {
             CPPHF_TRY(dm_small_rot_grad(Q, F, p, wn, eps, G[cur], g[cur], nk, nb, T_r, cfg->denom_scale, S, st));
@@ -655,13 +659,13 @@ int solve_dm(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* P
 
     // ---- finalize (solver_dm.hpp:615-652) ----
     CPPHF_TRY(density(ew));
-    CPPHF_TRY(build_fock(K, P, Sig, F, nullptr, nullptr, nullptr, fws, L.fock_bytes, st));
+    CPPHF_TRY(build_fock(K, P, solver_sigma(K, Sig), F, nullptr, nullptr, nullptr, fws, L.fock_bytes, st));
     CPPHF_TRY(dm_rotate(Q, F, F, nullptr, nk, nb, st));
     CPPHF_TRY(eigh_batched(F, ew, Vd, nk, nb, 0, nullptr, st));
     CPPHF_TRY(dm_q_times_u(Q, Vd, nk, nb, st));
     CPPHF_TRY(mu_solve(ew, wn, nk, nb, n_t, &S->mu, T_r, mu_it, 1, &S->mu, mws, L.mu_bytes, st));
     CPPHF_TRY(density(ew));
-    CPPHF_TRY(build_fock(K, P, Sig, F, nullptr, &S->energy, nullptr, fws, L.fock_bytes, st));
+    CPPHF_TRY(build_fock(K, P, solver_sigma(K, Sig), F, nullptr, &S->energy, nullptr, fws, L.fock_bytes, st));
     if (Q_out) CPPHF_CUDA(cudaMemcpyAsync(Q_out, Q, fbytes, cudaMemcpyDeviceToDevice, st));
     if (p_out) CPPHF_CUDA(cudaMemcpyAsync(p_out, p, vbytes, cudaMemcpyDeviceToDevice, st));
     if (D_out) CPPHF_CUDA(cudaMemcpyAsync(D_out, P, fbytes, cudaMemcpyDeviceToDevice, st));
@@ -688,7 +692,7 @@ int solve_dm(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* P
 namespace {
 
 struct ScfLayout {
-    size_t D, Sig, F, Pn, V, eps, sh, occ, S, fock_ws, mu_ws, mu2, total;
+    size_t D, Sig, F, Pn, V, eps, sh, occ, S, fock_ws, mu_ws, mu2, pack, total;
     size_t fock_bytes, mu_bytes;
     size_t R, Fh, Fex, dots, Sn, Fn, Dpre;  // acceleration extras (0 when unused)
     int nhist;
@@ -728,6 +732,7 @@ ScfLayout scf_layout(const cpphf_kernel* K, const cpphf_scf_config* cfg = nullpt
         L.Fn = W.take(fld);
     }
     if (cfg && cfg->trust_radius > 0.0) L.Dpre = W.take(fld);
+    L.pack = W.take(solver_pack_bytes(K));
     L.total = W.total;
     return L;
 }
@@ -756,6 +761,9 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
         return fail(CPPHF_ERR_INVALID, "solve_scf: workspace too small (" + std::to_string(L.total) + " bytes needed)");
     const SolveStream guard(st);
     st = guard.stream();
+    cpphf_kernel Kp;  // K with its packed VR / h (Hermitian packing), made once per solve
+    CPPHF_TRY(solver_pack(K, &Kp, static_cast<unsigned char*>(ws) + L.pack, st));
+    K = &Kp;
     unsigned char* W = static_cast<unsigned char*>(ws);
     auto fld = [&](size_t off) { return reinterpret_cast<double2*>(W + off); };
     auto vec = [&](size_t off) { return reinterpret_cast<double*>(W + off); };
@@ -817,7 +825,7 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
     auto build_and_occupy = [&]() -> int {
         if (project) CPPHF_TRY(call_project(project, puser, D, K, st));
         if (project || !d_hermitian) CPPHF_TRY(hermitize(D, D, nk, nb, st));
-        CPPHF_TRY(build_fock(low ? &K32 : K, D, Sig, F, nullptr, &S->energy, nullptr, fws, L.fock_bytes, st));
+        CPPHF_TRY(build_fock(low ? &K32 : K, D, solver_sigma(low ? &K32 : K, Sig), F, nullptr, &S->energy, nullptr, fws, L.fock_bytes, st));
         if (project) {
             CPPHF_TRY(call_project(project, puser, F, K, st));
             CPPHF_TRY(hermitize(F, F, nk, nb, st));
@@ -999,7 +1007,7 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
             }
         } else if (acc == 2) {
             // ---- ODA (solver_scf.hpp:350-392): E(lambda) quadratic, one extra build ----
-            CPPHF_TRY(build_fock(low ? &K32 : K, Pn, Sn, Fn, nullptr, &mu2[2], nullptr, fws, L.fock_bytes, st));
+            CPPHF_TRY(build_fock(low ? &K32 : K, Pn, solver_sigma(low ? &K32 : K, Sn), Fn, nullptr, &mu2[2], nullptr, fws, L.fock_bytes, st));
             k_oda_c1<<<rgrid, 256, 0, st>>>(F, D, Pn, K->w2d, nk, nb, S, &mu2[3]);
             CPPHF_LAUNCH_CHECK("oda slope");
             double* const e2 = hbuf + 8 + kDiisMax;

@@ -18,8 +18,10 @@ the build runs between them, each ordered by events.  A host buffer handed to
 ``build_host_async`` must stay untouched until ``end_host_pipeline()`` (or a
 later synchronisation) returns.
 
-Each ``build`` is one call of ``cpphf_build_fock`` on the current stream
-(three exchange passes, the assembly kernel and the energy sum).
+Each ``build`` is one call of ``cpphf_build_fock`` on the current stream:
+three exchange passes and the assembly kernel (which also reduces the energy),
+or, on the Hermitian-packed path, three passes with the assembly and energy
+fused into the last.
 """
 
 from __future__ import annotations
@@ -34,10 +36,17 @@ from ._native import _DeviceKernel, _ptr, _stream, _ws
 
 
 class FockBuilder:
-    def __init__(self, kernel_args: dict, precision: int = 64):
+    """``hermitian_density=True`` declares that every density passed in is
+    Hermitian: when V(q) is Hermitian too (real symmetric layer-resolved V,
+    real scalar V) the build then transforms the nb(nb+1)/2 upper-triangle
+    channels only, with the assembly fused into the last FFT pass
+    (``packed`` tells whether that path is on)."""
+
+    def __init__(self, kernel_args: dict, precision: int = 64, hermitian_density: bool = False):
         self.lib = _lib.load()
         self.dk = _DeviceKernel(kernel_args, precision=precision)
         self.dk.K.exchange_precision = int(precision)
+        self.packed = bool(hermitian_density) and self.dk.enable_packing()
         nk1, nk2, nb = self.dk.shape
         self.shape = (nk1, nk2, nb, nb)
         dev = torch.device("cuda", torch.cuda.current_device())
@@ -51,12 +60,13 @@ class FockBuilder:
     @property
     def launches_per_build(self) -> int:
         K = self.dk.K
-        n = 2  # assembly + energy sum
+        pre = 2 if (K.include_hartree or K.has_contact) else 0
+        if self.packed:
+            return pre + 3  # rows forward, columns, rows inverse with the assembly and energy
+        n = 1  # bulk assembly with the energy
         if K.include_exchange:
             n += 3
-        if K.include_hartree or K.has_contact:
-            n += 2
-        return n
+        return n + pre
 
     def build(self, P: torch.Tensor):
         """Fock build at a device density P (complex128, C-contiguous, kernel shape)."""

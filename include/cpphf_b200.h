@@ -170,7 +170,7 @@ typedef struct cpphf_kernel {
     int32_t has_contact;
     int32_t n_contact;
     int32_t exchange_precision;
-    int32_t reserved0;
+    int32_t hermitian_packing;  /* see below */
     double T;
     double weight_sum;
     const void* h;          /* complex128 (nk1, nk2, nb, nb) */
@@ -182,7 +182,29 @@ typedef struct cpphf_kernel {
     const void* contact_Oi;   /* complex128 (n_contact, nb, nb) */
     const void* contact_Oj;   /* complex128 (n_contact, nb, nb) */
     const cpphf_superlattice* sl;  /* NULL for a plain mesh kernel */
+    const void* VR_packed;  /* complex128 packed VR (cpphf_kernel_pack) or NULL */
+    const void* h_packed;   /* complex128 packed Hermitian part of h (cpphf_kernel_pack) or NULL */
 } cpphf_kernel;
+
+/* Hermitian channel packing (hermitian_packing != 0).  The reference packs the
+ * upper triangle of P when V is a real scalar (selfenergy.hpp:119-171, flag
+ * exchange_hcp); this extends it to an orbital-resolved V(q) that is
+ * Hermitian at every q (VR_ba(R) = conj VR_ab(-R); real symmetric V such as a
+ * layer-resolved Coulomb interaction qualifies).  Setting the flag asserts
+ * that condition and that every density passed to builds and solves of this
+ * kernel is Hermitian (only its upper triangle is read, as in the reference's
+ * packed path).  Sigma is then Hermitian, the exchange transforms the
+ * nb(nb+1)/2 channels a <= b, and the Fock assembly and energy run inside the
+ * last FFT pass.  Applies for nb <= 8, VR of width 1 or nb, no superlattice
+ * terms and mesh axes of a supported length; other kernels ignore the flag.
+ * VR_packed / h_packed (cpphf_kernel_packed_bytes each) are made once per
+ * kernel by cpphf_kernel_pack; when NULL, each build packs them into its
+ * workspace (the solvers pack them once per solve).  With the flag set,
+ * cpphf_build_fock accepts Sigma == NULL (no Sigma written).  No counterpart in
+ * the reference for orbital V. */
+size_t cpphf_kernel_packed_bytes(const cpphf_kernel* K);
+/* VR_packed (may be NULL; needs dv == nb) and h_packed (may be NULL) of K. */
+int cpphf_kernel_pack(const cpphf_kernel* K, void* VR_packed, void* h_packed, void* stream);
 
 /* ------------------------------------------------------------------------
  * Fock build.  Replaces _native.build_fock_apply (cpp_hf_native.cpp:380-415 ->
@@ -190,6 +212,7 @@ typedef struct cpphf_kernel {
  * k-independent Hartree diagonal hartree_diag (nb) and the energy
  * E = sum_k w_k Re Tr[h P + (Sigma + H)(P - refP)/2] (device scalar *energy).
  * H_dense (complex128 field, may be NULL) receives the dense Hartree term.
+ * Sigma may be NULL when K's Hermitian packing applies (see cpphf_kernel).
  * ---------------------------------------------------------------------- */
 size_t cpphf_build_fock_workspace_bytes(const cpphf_kernel* K);
 int cpphf_build_fock(const cpphf_kernel* K, const void* P, void* Sigma, void* F,
