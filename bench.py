@@ -1,13 +1,17 @@
 #!/usr/bin/env python
 """Benchmark: Fock builds/s of the cpp_hf hot path on B200 (layered nb=8 model, 192x192 mesh).
 
-One step = one Fock build (``build_fock_compact``: exchange FFT convolution over
-the 64 orbital-pair channels + assembly + energy) at a fixed seeded density,
-FP64 (complex128).  Inputs are device resident for ``value``; ``e2e`` times the
-same build through the public ``FockBuilder.build_host_async`` call with the
-density copied from pinned host memory and F + E copied back every step (the
-upload of one step overlaps the download of the previous one, and the host reads
-each step's energy while the next step is in flight).
+One step = one Fock build (``build_fock_compact``: exchange FFT convolution +
+assembly + energy) at a fixed seeded Hermitian density, FP64 (complex128).  The
+layered model's V(q) is real and symmetric in the layer pair, so the build
+takes the Hermitian-packed path (36 of the 64 orbital-pair channels, the
+assembly and energy fused into the last FFT pass).  Inputs are device resident
+for ``value``; ``e2e`` times the reference-facing drop-in call
+``_native.build_fock_apply(kernel_args, P, None)`` with NumPy in and out (P
+uploaded, Sigma, H and F downloaded every step; the kernel arrays' device
+copies are reused between calls), and ``e2e_pipelined`` the repo's
+``FockBuilder.build_host_async`` stream of builds (P in, F and E out, copies
+overlapped with the builds).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl native|reference]
 
@@ -200,7 +204,7 @@ def _scf_call(native, args, P0, n_e, tol=1e-9, max_iter=1000):
                             True, False)
 
 
-def time_solves(torch, native, args_dev, P0_dev, n_e, reps):
+def time_solves(torch, native, args_dev, P0_dev, n_e, reps, n_mesh):
     """solves/s of solve (DM) and solve_scf at FP64 and switched precision, device resident."""
     stream = torch.cuda.current_stream()
     out = {}
@@ -230,6 +234,14 @@ def time_solves(torch, native, args_dev, P0_dev, n_e, reps):
         emx, dmx = results[(kind, "mixed")]
         out[f"{kind}_mixed"]["abs_dE_vs_fp64_gpu"] = abs(emx - e64)
         out[f"{kind}_mixed"]["speedup_vs_fp64"] = out[f"{kind}_mixed"]["solves_per_s"] / out[f"{kind}_fp64"]["solves_per_s"]
+        g = oracle_goldens().get(kind) if n_mesh == N_MESH else None
+        if g is not None:
+            for prec in ("fp64", "mixed"):
+                o = out[f"{kind}_{prec}"]
+                o["oracle_energy"] = g["energy"]
+                o["oracle_iterations"] = g["iterations"]
+                o["abs_dE_vs_oracle"] = abs(o["energy"] - g["energy"])
+                o["rel_dE_vs_oracle"] = abs(o["energy"] - g["energy"]) / abs(g["energy"])
     return out
 
 
@@ -283,12 +295,23 @@ def oracle_solve_estimate(args, P0_np, n_e, n_iter_gpu):
 
 
 def load_traffic():
-    """DRAM bytes per exchange from the committed ncu summary of the 192x192 nb=8 exchange."""
-    f = ROOT / "profiles" / "exchange_fp64_layered192_nb8.md"
+    """DRAM bytes per packed Fock build from the committed ncu summary of the 192x192 nb=8 build."""
+    f = ROOT / "profiles" / "fock_packed_layered192_nb8.md"
     if not f.exists():
         return None
-    m = re.search(r"^traffic_bytes_per_exchange:\s*(\d+)", f.read_text(), re.M)
-    return {"nk": [N_MESH, N_MESH], "nb": 2 * N_LAYERS, "dram_bytes_per_exchange": int(m.group(1))} if m else None
+    m = re.search(r"^traffic_bytes_per_build:\s*(\d+)", f.read_text(), re.M)
+    return {"nk": [N_MESH, N_MESH], "nb": 2 * N_LAYERS, "dram_bytes_per_build": int(m.group(1))} if m else None
+
+
+def oracle_goldens():
+    """Cached FP64 oracle solves of the 192x192 nb=8 workload (tests/golden, committed)."""
+    out = {}
+    for kind, name in (("dm", "dm_layered192.npz"), ("scf", "scf_layered192.npz")):
+        f = ROOT / "tests" / "golden" / name
+        if f.exists():
+            g = np.load(f)
+            out[kind] = {"energy": float(g["energy"]), "iterations": int(g["n_iter"])}
+    return out
 
 
 def main():
@@ -312,17 +335,21 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
         pg = dist
 
-    from cpp_hf_b200 import _lib, workloads
+    from cpp_hf_b200 import _lib, _native, workloads
     from cpp_hf_b200.fock_builder import FockBuilder
     from cpp_hf_b200._native import _ptr, _stream, _ws
 
     lib = _lib.load()
     args, _P0, _ne = workloads.layered(a.n, n_layers=N_LAYERS, seed=rank)
     P_host_np = workloads.random_hermitian_density(a.n, 2 * N_LAYERS, seed=1 + rank)
-    fb = FockBuilder(args, precision=64)
+    P_host_np = 0.5 * (P_host_np + np.conj(np.swapaxes(P_host_np, -1, -2)))  # exactly Hermitian blocks
+    fb = FockBuilder(args, precision=64, hermitian_density=True)
+    if not fb.packed:
+        raise RuntimeError("the layered workload should take the Hermitian-packed build")
     P = torch.from_numpy(P_host_np).to(dev)
     nk = a.n * a.n
     nb = 2 * N_LAYERS
+    npk = nb * (nb + 1) // 2
     field = nk * nb * nb * 16
     stream = torch.cuda.current_stream()
 
@@ -331,7 +358,7 @@ def main():
             pg.barrier()
         torch.cuda.synchronize()
 
-    # ---- device-resident Fock builds ----
+    # ---- device-resident Fock builds (Hermitian-packed, fused assembly) ----
     for _ in range(max(3, a.warmup)):
         fb.build(P)
     sampler = ClockSampler(gpu_uuid(torch, dev))
@@ -346,8 +373,9 @@ def main():
     barrier()
     t_dev = ev0.elapsed_time(ev1) / 1e3
 
-    # ---- dominant kernel: the exchange (3 FFT passes) alone, same stream ----
-    VR = fb.dk._keep[1]
+    # ---- the full 64-channel path (any V, any P), for reference ----
+    fb_full = FockBuilder(args, precision=64)
+    VR = fb_full.dk._keep[1]
     Sig = torch.empty_like(P)
     xws = _ws(lib.cpphf_exchange_workspace_bytes(a.n, a.n, nb, 0, 64))
 
@@ -355,26 +383,43 @@ def main():
         _lib.check(lib.cpphf_exchange(_ptr(P), None, _ptr(VR), _ptr(Sig), a.n, a.n, nb, nb, 0, 0, 64,
                                       _ptr(xws), xws.numel(), _stream()), "exchange")
 
-    for _ in range(5):
-        exch()
-    barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(a.steps):
-        exch()
-    e1.record(stream)
-    barrier()
-    t_ex = e0.elapsed_time(e1) / 1e3 / a.steps
+    def timed(fn, n):
+        for _ in range(5):
+            fn()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(n):
+            fn()
+        e1.record(stream)
+        barrier()
+        return e0.elapsed_time(e1) / 1e3 / n
 
-    # ---- end to end through the public API with pinned host buffers ----
-    # Pipelined: the upload of step i overlaps the download of step i-1 (two device
-    # buffer sets, copy-in / compute / copy-out streams), and the host reads step
-    # i-1's F and E while step i is in flight (two pinned result buffers).
+    t_ex = timed(exch, a.steps)
+    t_full_build = timed(lambda: fb_full.build(P), a.steps)
+    del fb_full
+
+    # ---- end to end through the drop-in call: NumPy in, NumPy out ----
+    args_np = dict(args, hermitian_density=True)
+    e2e_steps = max(3, min(a.steps, 30))
+    e2e_E = []
+    for _ in range(3):
+        e2e_E.append(_native.build_fock_apply(args_np, P_host_np, None)[3])
+    barrier()
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record(stream)
+    for _ in range(e2e_steps):
+        S_h, H_h, F_h, E_h = _native.build_fock_apply(args_np, P_host_np, None)
+        e2e_E.append(E_h)
+    g1.record(stream)
+    barrier()
+    t_e2e = g0.elapsed_time(g1) / 1e3
+
+    # ---- end to end, pipelined stream of builds through FockBuilder ----
     P_pin = torch.from_numpy(P_host_np).pin_memory()
     F_pins = [torch.empty(fb.shape, dtype=torch.complex128).pin_memory() for _ in range(2)]
     E_pins = [torch.empty(1, dtype=torch.float64).pin_memory() for _ in range(2)]
-    e2e_steps = max(3, min(a.steps, 50))
-    e2e_read = []
+    pipe_read = []
 
     def e2e_loop(n):
         fb.begin_host_pipeline()
@@ -383,21 +428,21 @@ def main():
             ev = fb.build_host_async(P_pin, F_pins[i & 1], E_pins[i & 1])
             if prev is not None:
                 prev[0].synchronize()  # the caller reads the previous step's result on the host
-                e2e_read.append(float(E_pins[prev[1]][0]))
+                pipe_read.append(float(E_pins[prev[1]][0]))
             prev = (ev, i & 1)
         fb.end_host_pipeline()
         prev[0].synchronize()
-        e2e_read.append(float(E_pins[prev[1]][0]))
+        pipe_read.append(float(E_pins[prev[1]][0]))
 
     e2e_loop(3)
     barrier()
-    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    g0.record(stream)
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
     e2e_loop(e2e_steps)
-    g1.record(stream)
+    p1.record(stream)
     barrier()
     clocks = sampler.stop()
-    t_e2e = g0.elapsed_time(g1) / 1e3
+    t_pipe = p0.elapsed_time(p1) / 1e3
 
     # ---- solves/s (DM and SCF, FP64 and switched precision), device resident ----
     solves = None
@@ -408,7 +453,7 @@ def main():
                     for k, v in args.items()}
         P0_dev = torch.from_numpy(np.ascontiguousarray(_P0)).to(dev)
         barrier()
-        solves = time_solves(torch, native, args_dev, P0_dev, _ne, a.solve_reps)
+        solves = time_solves(torch, native, args_dev, P0_dev, _ne, a.solve_reps, a.n)
         solves["newton_fp64"] = time_newton(torch, native, args_dev, P0_dev, _ne)
         barrier()
 
@@ -449,10 +494,10 @@ def main():
         }
 
     # max over ranks
-    times = torch.tensor([t_dev, t_ex, t_e2e], dtype=torch.float64, device=dev)
+    times = torch.tensor([t_dev, t_ex, t_e2e, t_pipe, t_full_build], dtype=torch.float64, device=dev)
     if pg is not None:
         pg.all_reduce(times, op=pg.ReduceOp.MAX)
-    t_dev, t_ex, t_e2e = [float(x) for x in times.cpu()]
+    t_dev, t_ex, t_e2e, t_pipe, t_full_build = [float(x) for x in times.cpu()]
 
     builds = a.steps * world
     value = builds / t_dev
@@ -465,13 +510,17 @@ def main():
             peaks = json.loads(pf.read_text())
         hbm = float(peaks.get("hbm_gbs", 6650.0))
         peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-        ex_bytes = 3 * field  # read P + read VR (dv = nb) + write Sigma
-        fock_bytes = 5 * field  # + read h + write F
-        achieved = ex_bytes / t_ex / 1e9
+        # algorithmic bytes of one packed build: the upper-triangle channels of P,
+        # of the packed VR and of the packed Hermitian part of h are read, F written
+        pk_bytes = (3 * npk + nb * nb) * 16 * nk
+        ex_bytes = 3 * field  # full exchange: read P + read VR (dv = nb) + write Sigma
+        fock_bytes_full = 5 * field  # full build: + read h + write F
+        t_build = t_dev / a.steps
+        achieved = pk_bytes / t_build / 1e9
         traffic = load_traffic()
         tr_val = None
         if traffic and traffic.get("nk") == [a.n, a.n] and traffic.get("nb") == nb:
-            tr_val = traffic.get("dram_bytes_per_exchange")
+            tr_val = traffic.get("dram_bytes_per_build")
         cb_v, cb_dt = None, None
         if world == 1 or rank == 0:
             import gc
@@ -486,33 +535,45 @@ def main():
             "n_gpus": world,
             "steps": a.steps,
             "warmup": a.warmup,
-            "ms_per_step": 1e3 * t_dev / a.steps,
+            "ms_per_step": 1e3 * t_build,
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
             "dtype": "c128",
             "data": "synthetic (seeded layered model; P random Hermitian, eigenvalues in [0,1])",
             "config": {
-                "workload": WORKLOAD, "nk": [a.n, a.n], "nb": nb, "exchange_channels": nb * nb,
+                "workload": WORKLOAD, "nk": [a.n, a.n], "nb": nb, "exchange_channels": npk,
+                "path": "Hermitian-packed build (V real symmetric, P Hermitian): 36 upper-triangle channels, "
+                        "assembly and energy fused into the last FFT pass",
                 "precision": "fp64", "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                "l2": "inputs larger than L2 (P, VR, h, Sigma, F = 5 x 37.7 MB per build)",
-                "fock_build_bytes": fock_bytes,
-                "fock_build_hbm_frac": (fock_bytes / (t_dev / a.steps) / 1e9) / hbm,
+                "l2": "inputs larger than L2 (P, packed VR, packed h, F = 101 MB per build, plus the 23.6 MB "
+                      "intermediate)",
+                "full_path": {"ms_per_build": 1e3 * t_full_build, "builds_per_s": 1.0 / t_full_build,
+                              "exchange_ms": 1e3 * t_ex, "exchange_algorithmic_bytes": ex_bytes,
+                              "exchange_frac": ex_bytes / t_ex / 1e9 / hbm,
+                              "build_bytes": fock_bytes_full,
+                              "note": "all 64 channels, separate assembly kernel (non-Hermitian V or P)"},
             },
             "roofline": {
-                "kernel": "exchange (3 FFT passes: rows fwd, columns fwd*VR*inv, rows inv)",
+                "kernel": "Hermitian-packed Fock build (3 launches: rows forward, columns * VR, rows inverse + "
+                          "assembly + energy)",
                 "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": achieved / hbm, "traffic": tr_val, "algorithmic_bytes": ex_bytes,
-                "peak_source": peak_src, "ms_per_launch": 1e3 * t_ex,
+                "frac": achieved / hbm, "traffic": tr_val, "algorithmic_bytes": pk_bytes,
+                "peak_source": peak_src, "ms_per_launch": 1e3 * t_build,
             },
             "cpu_baseline": {"value": cb_v, "unit": UNIT, "cores": host_cores(), "kind": "port",
                              "sample": f"10 oracle Fock builds on the same 192^2 nb=8 instance "
                                        f"({cb_dt:.2f} s; scipy.fft workers = host cores)"},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": field,
-                    "d2h_bytes_per_step": field + 8,
-                    "mode": "pipelined: copy-in, build and copy-out streams, two device buffer sets; "
-                            "the host reads every step's F and E",
-                    "host_energies_consistent": bool(len(set(e2e_read)) == 1 and all(map(math.isfinite, e2e_read)))},
+                    "d2h_bytes_per_step": 3 * field + 8,
+                    "mode": "reference-facing _native.build_fock_apply: NumPy P in; NumPy Sigma, H, F and E out "
+                            "(page-locked result buffers); kernel arrays' device copies reused between calls",
+                    "host_energies_consistent": bool(len(set(e2e_E)) == 1 and all(map(math.isfinite, e2e_E)))},
+            "e2e_pipelined": {"value": e2e_steps * world / t_pipe, "unit": UNIT, "h2d_bytes_per_step": field,
+                              "d2h_bytes_per_step": field + 8,
+                              "mode": "FockBuilder.build_host_async: copy-in, build and copy-out streams, two "
+                                      "device buffer sets; the host reads every step's F and E",
+                              "host_energies_consistent": bool(len(set(pipe_read)) == 1)},
             "gpu_launches": a.steps * fb.launches_per_build,
             "clocks": clocks,
         }

@@ -79,6 +79,7 @@ class ScfConfig(C.Structure):
         ("level_shift", f64), ("acceleration", i32), ("reserved", i32), ("mixed_switch_tol", f64),
         ("diis_size", i32), ("diis_start", i32), ("diis_damping", f64), ("trust_radius", f64),
         ("graphs", i32), ("reserved1", i32),
+        ("block_sizes", C.POINTER(i64)), ("n_block_sizes", i64),
     ]
 
 

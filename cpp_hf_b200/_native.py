@@ -681,6 +681,9 @@ def solve_scf(kernel_args, P0, n_e, max_iter, density_tol, comm_tol, mixing, lev
     cfg.diis_damping, cfg.trust_radius = float(diis_damping), float(trust_radius)
     cfg.mixed_switch_tol = dk.mixed_switch
     cfg.graphs = 1 if kernel_args.get("solve_graphs", True) else 0
+    bs_arr, n_bs = _sizes_arr(block_sizes if block_sizes is not None else [])
+    cfg.block_sizes = C.cast(bs_arr, C.POINTER(_lib.i64))
+    cfg.n_block_sizes = n_bs
     D = torch.empty_like(P0_t) if return_density else None
     F = torch.empty_like(P0_t) if return_fock else None
     hE = np.zeros(max(max_iter, 1))

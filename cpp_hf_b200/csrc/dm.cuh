@@ -21,7 +21,7 @@ struct DmScalars {
     int accepted;
     unsigned counter;  // last-block reduction counter (self-resetting)
     int iter;          // iterations since the start or the precision switch (CG restart count)
-    int iter_pad;
+    int slot;          // trial of its pass the accepted one was (0: ew holds it, 1: ew2)
     double pad[1];
     double part[3 * kDmMaxPartials];
 };

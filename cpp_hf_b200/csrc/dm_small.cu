@@ -194,31 +194,37 @@ __global__ void __launch_bounds__(kThreads) k_rot_grad(const double2* __restrict
     }
 }
 
-// One backtracking trial (solver_dm.hpp:577-589) by elimination.
-// Dynamic shared memory: sD (d, then U) | sF, TILE double2 each.
-// Every trial that runs writes its U(tau) and diag(U^H Ft U) (to Uout, ew), so
-// after the line search they hold the accepted trial's values and the
-// retraction reuses them.
+// Two consecutive backtracking trials (solver_dm.hpp:577-589) per pass, by
+// elimination: tau_a = tau_cur and tau_b = tau_a * shrink share the loads of d
+// and Ft and run their eliminations in lockstep.  The last block then takes
+// the reference's sequential decisions (accept tau_a on a strict decrease of
+// the frozen free energy, else try tau_b, else shrink on), so the result is
+// that of one pass per trial.  diag(U^H Ft U) goes to ew (tau_a) and ew2
+// (tau_b); S->slot records which one the accepted trial left.  `bt` is the
+// index of the pass's first trial; a pair past bt_max evaluates one trial.
+// Dynamic shared memory: sD (d, then U(tau_a)) | sF | sB (U(tau_b)), TILE double2 each.
 template <int NB>
-__global__ void __launch_bounds__(kThreads, 4) k_trial_small(const double2* __restrict__ dQ, const double2* __restrict__ Ft,
-                                                          const double* __restrict__ p, const double* __restrict__ d_p,
-                                                          const double* __restrict__ w, double* __restrict__ ew,
-                                                          double2* __restrict__ Uout, int64_t nk, double T_r,
-                                                          double shrink, int last_trial, double fallback,
-                                                          DmScalars* S) {
+__global__ void __launch_bounds__(kThreads, 3)
+    k_trial2_small(const double2* __restrict__ dQ, const double2* __restrict__ Ft, const double* __restrict__ p,
+                   const double* __restrict__ d_p, const double* __restrict__ w, double* __restrict__ ew,
+                   double* __restrict__ ew2, int64_t nk, double T_r, double shrink, int bt, int bt_max,
+                   double fallback, DmScalars* S) {
     if (S->accepted) return;  // grid-uniform
     using G = Geo<NB>;
     extern __shared__ __align__(16) double2 dyn[];
     double2* sD = dyn;
     double2* sF = dyn + G::TILE;
-    double2* sU = sD;  // U replaces d row by row once the elimination has read d
-    __shared__ double2 sPiv[G::KT * 4 * NB];
-    __shared__ double red[64];
+    double2* sB = dyn + 2 * G::TILE;
+    double2* sA = sD;  // U(tau_a) replaces d once both eliminations have read it
+    __shared__ double2 sPiv[G::KT * 8 * NB];
+    __shared__ double red[128];
     const int grp = threadIdx.x / G::GS, r = threadIdx.x % G::GS;
     const unsigned mask = group_mask<NB>(threadIdx.x & 31);
-    const double tau = S->tau_cur;
+    const double tau_a = S->tau_cur;
+    const double tau_b = tau_a * shrink;
+    const bool two = bt + 1 < bt_max;  // grid-uniform
     const int64_t ntiles = (nk + G::KT - 1) / G::KT;
-    double v[2] = {0.0, 0.0};
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
     for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int64_t k0 = t * G::KT;
         const int nkt = (int)((nk - k0) < G::KT ? (nk - k0) : G::KT);
@@ -229,80 +235,103 @@ __global__ void __launch_bounds__(kThreads, 4) k_trial_small(const double2* __re
         const int rr = r < NB ? r : 0;
         const int64_t k = k0 + grp;
         if (grp < nkt) {
-            double2 u[NB];
-            row_cayley<NB, G::LD>(sD + grp * G::MS, tau, rr, sPiv + grp * 4 * NB, u, mask);
+            double2 ua[NB], ub[NB];
+            if (two)
+                row_cayley2<NB, G::LD>(sD + grp * G::MS, tau_a, tau_b, rr, sPiv + grp * 8 * NB, ua, ub, mask);
+            else
+                row_cayley<NB, G::LD>(sD + grp * G::MS, tau_a, rr, sPiv + grp * 8 * NB, ua, mask);
             // (the elimination ends with a group barrier after its last read of d)
             if (live) {
 #pragma unroll
-                for (int j = 0; j < NB; ++j) sU[grp * G::MS + r * G::LD + j] = u[j];
+                for (int j = 0; j < NB; ++j) {
+                    sA[grp * G::MS + r * G::LD + j] = ua[j];
+                    if (two) sB[grp * G::MS + r * G::LD + j] = ub[j];
+                }
             }
         }
-        __syncthreads();
-        tile_store<NB>(Uout + (size_t)k0 * G::NB2, sU, nkt);  // coalesced
+        __syncwarp();  // a group's U rows (one warp) are complete before its diag reads them
         if (grp < nkt) {
             double2 ftj[NB];
 #pragma unroll
             for (int l = 0; l < NB; ++l) ftj[l] = sF[grp * G::MS + rr * G::LD + l];
-            const double dr = row_diag_uhfu<NB, G::GS, G::LD>(ftj, sU + grp * G::MS, r, mask, live);
+            const double da = row_diag_uhfu<NB, G::GS, G::LD>(ftj, sA + grp * G::MS, r, mask, live);
+            double db = 0.0;
+            if (two) db = row_diag_uhfu<NB, G::GS, G::LD>(ftj, sB + grp * G::MS, r, mask, live);
             if (live) {
-                ew[k * NB + r] = dr;
-                const double pv = fmin(fmax(p[k * NB + r] - tau * d_p[k * NB + r], OCC_CLIP), 1.0 - OCC_CLIP);
-                const double wk = w[k];
-                v[0] += wk * pv * dr;
-                v[1] -= wk * (pv * log(pv) + (1.0 - pv) * log1p(-pv));
+                const double wk = w[k], pk = p[k * NB + r], dpk = d_p[k * NB + r];
+                ew[k * NB + r] = da;
+                const double pa = fmin(fmax(pk - tau_a * dpk, OCC_CLIP), 1.0 - OCC_CLIP);
+                v[0] += wk * pa * da;
+                v[1] -= wk * (pa * log(pa) + (1.0 - pa) * log1p(-pa));
+                if (two) {
+                    ew2[k * NB + r] = db;
+                    const double pb = fmin(fmax(pk - tau_b * dpk, OCC_CLIP), 1.0 - OCC_CLIP);
+                    v[2] += wk * pb * db;
+                    v[3] -= wk * (pb * log(pb) + (1.0 - pb) * log1p(-pb));
+                }
             }
         }
         __syncthreads();
     }
-    double out[2];
-    if (reduce_last_block<2>(v, S->part, &S->counter, out, red) && threadIdx.x == 0) {
-        const double om = out[0] - fmax(T_r, 1.0e-14) * out[1];
-        if (om < S->omega0) {
+    double out[4];
+    if (reduce_last_block<4>(v, S->part, &S->counter, out, red) && threadIdx.x == 0) {
+        const double Tc = fmax(T_r, 1.0e-14);
+        const double om_a = out[0] - Tc * out[1];
+        if (om_a < S->omega0) {
             S->accepted = 1;
-            S->tau_final = tau;
+            S->tau_final = tau_a;
+            S->slot = 0;
         } else {
-            S->tau_cur = tau * shrink;
-            if (last_trial) S->tau_final = S->tau0 * fallback;
+            S->tau_cur = tau_a * shrink;
+            if (bt == bt_max - 1) S->tau_final = S->tau0 * fallback;
+            if (two) {
+                const double om_b = out[2] - Tc * out[3];
+                if (om_b < S->omega0) {
+                    S->accepted = 1;
+                    S->tau_final = tau_b;
+                    S->slot = 1;
+                } else {
+                    S->tau_cur = tau_b * shrink;
+                    if (bt + 1 == bt_max - 1) S->tau_final = S->tau0 * fallback;
+                }
+            }
         }
     }
 }
 
-// Retraction Q <- Q U(tau_final) and eps_work = diag(U^H Ft U).
+// Retraction Q <- Q U(tau_final), U recomputed from d by elimination, and
+// eps_work = diag(U^H Ft U): the accepted trial's (copied from ew2 when it was
+// the second of its pass) or, for the fallback step, computed here.
 // Dynamic shared memory: sD (d, then U) | sF | sQ, TILE double2 each.
 template <int NB>
 __global__ void __launch_bounds__(kThreads) k_retract_small(double2* Q, const double2* __restrict__ dQ,
                                                             const double2* __restrict__ Ft, double* __restrict__ ew,
-                                                            const double2* __restrict__ Uacc, int64_t nk,
+                                                            const double* __restrict__ ew2, int64_t nk,
                                                             const DmScalars* S) {
     using G = Geo<NB>;
     extern __shared__ __align__(16) double2 dyn[];
     double2* sD = dyn;
     double2* sF = dyn + G::TILE;
-    double2* sU = sD;  // U: the accepted trial's, or the elimination's replacing d row by row
+    double2* sU = sD;  // U replaces d row by row once the elimination has read d
     double2* sQ = dyn + 2 * G::TILE;
     __shared__ double2 sPiv[G::KT * 4 * NB];
     const int grp = threadIdx.x / G::GS, r = threadIdx.x % G::GS;
     const unsigned mask = group_mask<NB>(threadIdx.x & 31);
     const double tau = S->tau_final;
-    // an accepted trial left its U(tau) in Uacc and its diag(U^H Ft U) in ew;
-    // only the fallback step (no trial accepted) computes them here (grid-uniform)
-    const bool need_diag = S->accepted == 0;
+    const bool need_diag = S->accepted == 0;                // grid-uniform
+    const bool from_b = S->accepted != 0 && S->slot == 1;  // grid-uniform
     const int64_t ntiles = (nk + G::KT - 1) / G::KT;
     for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int64_t k0 = t * G::KT;
         const int nkt = (int)((nk - k0) < G::KT ? (nk - k0) : G::KT);
-        if (need_diag) {
-            tile_load<NB>(sD, dQ + (size_t)k0 * G::NB2, nkt);
-            tile_load<NB>(sF, Ft + (size_t)k0 * G::NB2, nkt);
-        } else {
-            tile_load<NB>(sU, Uacc + (size_t)k0 * G::NB2, nkt);
-        }
+        tile_load<NB>(sD, dQ + (size_t)k0 * G::NB2, nkt);
+        if (need_diag) tile_load<NB>(sF, Ft + (size_t)k0 * G::NB2, nkt);
         tile_load<NB>(sQ, Q + (size_t)k0 * G::NB2, nkt);
         __syncthreads();
         const bool live = grp < nkt && r < NB;
         const int rr = r < NB ? r : 0;
         const int64_t k = k0 + grp;
-        if (need_diag && grp < nkt) {
+        if (grp < nkt) {
             double2 u[NB];
             row_cayley<NB, G::LD>(sD + grp * G::MS, tau, rr, sPiv + grp * 4 * NB, u, mask);
             // (the elimination ends with a group barrier after its last read of d)
@@ -311,7 +340,7 @@ __global__ void __launch_bounds__(kThreads) k_retract_small(double2* Q, const do
                 for (int j = 0; j < NB; ++j) sU[grp * G::MS + r * G::LD + j] = u[j];
             }
         }
-        __syncthreads();
+        __syncwarp();
         if (grp < nkt) {
             if (need_diag) {
                 double2 ftj[NB];
@@ -319,6 +348,8 @@ __global__ void __launch_bounds__(kThreads) k_retract_small(double2* Q, const do
                 for (int l = 0; l < NB; ++l) ftj[l] = sF[grp * G::MS + rr * G::LD + l];
                 const double dr = row_diag_uhfu<NB, G::GS, G::LD>(ftj, sU + grp * G::MS, r, mask, live);
                 if (live) ew[k * NB + r] = dr;
+            } else if (from_b && live) {
+                ew[k * NB + r] = ew2[k * NB + r];
             }
             if (live) {
                 const double2* su = sU + grp * G::MS;
@@ -534,7 +565,7 @@ template <int NB>
 void small_attrs() {
     static std::once_flag once;
     std::call_once(once, [] {
-        raise_smem(k_trial_small<NB>);
+        raise_smem(k_trial2_small<NB>);
         raise_smem(k_retract_small<NB>);
     });
 }
@@ -609,25 +640,26 @@ int dm_small_direction(const double2* Gc, const double2* dQp, const double* g_p,
     return CPPHF_OK;
 }
 
-int dm_small_trial(const double2* dQ, const double2* Ft, const double* p, const double* d_p, const double* w,
-                   double* ew, double2* U, int64_t nk, int nb, double T_r, double shrink, int last_trial,
-                   double fallback, DmScalars* S, cudaStream_t st) {
-#define X(N)                                                                                                         \
-    small_attrs<N>();                                                                                                \
-    k_trial_small<N><<<tiles_grid(nk, Geo<N>::KT, kDmMaxPartials), kThreads, 2 * sizeof(double2) * Geo<N>::TILE,    \
-                       st>>>(dQ, Ft, p, d_p, w, ew, U, nk, T_r, shrink, last_trial, fallback, S);                    \
-    CPPHF_LAUNCH_CHECK("trial");
+int dm_small_trial2(const double2* dQ, const double2* Ft, const double* p, const double* d_p, const double* w,
+                    double* ew, double* ew2, int64_t nk, int nb, double T_r, double shrink, int bt, int bt_max,
+                    double fallback, DmScalars* S, cudaStream_t st) {
+#define X(N)                                                                                            \
+    small_attrs<N>();                                                                                   \
+    k_trial2_small<N><<<tiles_grid(nk, Geo<N>::KT, 3 * kDmMaxPartials / 4), kThreads,                   \
+                        3 * sizeof(double2) * Geo<N>::TILE, st>>>(dQ, Ft, p, d_p, w, ew, ew2, nk, T_r, shrink, \
+                                                                 bt, bt_max, fallback, S);               \
+    CPPHF_LAUNCH_CHECK("trial pair");
     SMALL_DISPATCH(nb, X)
 #undef X
     return CPPHF_OK;
 }
 
-int dm_small_retract(double2* Q, const double2* dQ, const double2* Ft, double* ew, const double2* U, int64_t nk,
+int dm_small_retract(double2* Q, const double2* dQ, const double2* Ft, double* ew, const double* ew2, int64_t nk,
                      int nb, const DmScalars* S, cudaStream_t st) {
 #define X(N)                                                                                                      \
     small_attrs<N>();                                                                                             \
     k_retract_small<N><<<tiles_grid(nk, Geo<N>::KT, 16 * num_sms()), kThreads, 3 * sizeof(double2) * Geo<N>::TILE, \
-                         st>>>(Q, dQ, Ft, ew, U, nk, S);                                                          \
+                         st>>>(Q, dQ, Ft, ew, ew2, nk, S);                                                        \
     CPPHF_LAUNCH_CHECK("retract");
     SMALL_DISPATCH(nb, X)
 #undef X

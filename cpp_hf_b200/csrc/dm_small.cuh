@@ -22,10 +22,14 @@ int dm_small_pr_beta(const double2* Gc, const double2* Gp, const double* g_p, co
 int dm_small_direction(const double2* Gc, const double2* dQp, const double* g_p, const double* dpp, const double* eps,
                        const double* p, const double* w, double2* dQ, double* d_p, int64_t nk, int nb, double T_r,
                        double max_step, DmScalars* S, cudaStream_t st);
-int dm_small_trial(const double2* dQ, const double2* Ft, const double* p, const double* d_p, const double* w,
-                   double* ew, double2* U, int64_t nk, int nb, double T_r, double shrink, int last_trial,
-                   double fallback, DmScalars* S, cudaStream_t st);
-int dm_small_retract(double2* Q, const double2* dQ, const double2* Ft, double* ew, const double2* U, int64_t nk,
+// Two consecutive line-search trials (bt, bt + 1 < bt_max) in one pass;
+// diag(U^H Ft U) of the first to ew, of the second to ew2.
+int dm_small_trial2(const double2* dQ, const double2* Ft, const double* p, const double* d_p, const double* w,
+                    double* ew, double* ew2, int64_t nk, int nb, double T_r, double shrink, int bt, int bt_max,
+                    double fallback, DmScalars* S, cudaStream_t st);
+// Q <- Q U(tau_final) (U recomputed by elimination); eps_work of the accepted
+// trial in ew (taken from ew2 when that holds it), or computed for the fallback.
+int dm_small_retract(double2* Q, const double2* dQ, const double2* Ft, double* ew, const double* ew2, int64_t nk,
                      int nb, const DmScalars* S, cudaStream_t st);
 
 }  // namespace cpphf

@@ -17,6 +17,8 @@
 #include "common.cuh"
 #include "eigh.cuh"
 
+#include <cstring>
+
 #include <algorithm>
 #include <mutex>
 #include <string>
@@ -264,6 +266,29 @@ __global__ void k_max_offblock(const double2* __restrict__ M, int64_t batch, int
     if ((threadIdx.x & 31) == 0 && m > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
 }
 
+// max |M| (out[0]) and max |M_ij| over the off-block entries (out[1]) of a
+// batch, as doubles reinterpreted for atomicMax (non-negative, so the integer
+// order is the numeric order).
+__global__ void k_block_norms(const double2* __restrict__ M, int64_t batch, int nb, BlockSpec bs,
+                              unsigned long long* out) {
+    const int64_t n = batch * (int64_t)nb * nb;
+    double all = 0.0, off = 0.0;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        const int r = (int)(e % ((int64_t)nb * nb));
+        const int i = r / nb, j = r - i * nb;
+        const double2 a = M[e];
+        const double v = hypot(a.x, a.y);
+        all = fmax(all, v);
+        if (bs.blk[i] != bs.blk[j]) off = fmax(off, v);
+    }
+    all = warp_max(all);
+    off = warp_max(off);
+    if ((threadIdx.x & 31) == 0) {
+        if (all > 0.0) atomicMax(&out[0], (unsigned long long)__double_as_longlong(all));
+        if (off > 0.0) atomicMax(&out[1], (unsigned long long)__double_as_longlong(off));
+    }
+}
+
 size_t eigh_smem(int nb, bool warp) {
     const int teams = warp ? kWarpTeamsPerCta : 1;
     const size_t mat = (size_t)nb * (nb + 1);
@@ -305,6 +330,25 @@ int eigh_batched(const double2* M, double* w, double2* V, int64_t batch, int64_t
         k_eigh<false><<<(unsigned)batch, kCtaTeamThreads, smem, st>>>(M, w, V, batch, (int)nb, mode, bs);
     }
     CPPHF_LAUNCH_CHECK("eigh");
+    return CPPHF_OK;
+}
+
+int block_structure_ok(const double2* M, int64_t batch, int64_t nb, const BlockSpec& bs, unsigned long long* dev2,
+                       cudaStream_t st, bool* ok) {
+    *ok = true;
+    if (batch <= 0) return CPPHF_OK;
+    CPPHF_CUDA(cudaMemsetAsync(dev2, 0, 2 * sizeof(unsigned long long), st));
+    const int64_t n = batch * nb * nb;
+    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)num_sms() * 8));
+    k_block_norms<<<grid, 256, 0, st>>>(M, batch, (int)nb, bs, dev2);
+    CPPHF_LAUNCH_CHECK("block structure check");
+    unsigned long long h[2] = {0ull, 0ull};
+    CPPHF_CUDA(cudaMemcpyAsync(h, dev2, sizeof(h), cudaMemcpyDeviceToHost, st));
+    CPPHF_CUDA(cudaStreamSynchronize(st));
+    double scale, off;
+    std::memcpy(&scale, &h[0], sizeof(double));
+    std::memcpy(&off, &h[1], sizeof(double));
+    *ok = off <= 1.0e-10 + 1.0e-10 * scale;
     return CPPHF_OK;
 }
 

@@ -135,6 +135,74 @@ __device__ __forceinline__ void row_cayley(const double2* d, double tau, int r, 
     __syncwarp(mask);  // the last step's readers are done before `piv` is reused
 }
 
+// Two Cayley factors U(tau_a), U(tau_b) of the same d in lockstep: one pivot
+// publication (both rows) and one group barrier per step for both
+// eliminations, so their dependent FP64 chains interleave.  Each result takes
+// the same operations row_cayley performs for its tau.  `piv` holds
+// 2 * 4 * NB values per group.
+template <int NB, int LD>
+__device__ __forceinline__ void row_cayley2(const double2* d, double tau_a, double tau_b, int r, double2* piv,
+                                            double2 (&ua)[NB], double2 (&ub)[NB], unsigned mask) {
+    double2 ma[NB], mb[NB];
+    const double ha = 0.5 * tau_a, hb = 0.5 * tau_b;
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+        const double2 dv = d[r * LD + j];
+        const double2 a = cscale(dv, ha), b = cscale(dv, hb);
+        const double one = (j == r) ? 1.0 : 0.0;
+        ma[j] = mk(one + a.x, a.y);
+        ua[j] = mk(one - a.x, -a.y);
+        mb[j] = mk(one + b.x, b.y);
+        ub[j] = mk(one - b.x, -b.y);
+    }
+#pragma unroll
+    for (int pp = 0; pp < NB; ++pp) {
+        double2* slot = piv + (pp & 1) * 4 * NB;
+        if (r == pp) {
+#pragma unroll
+            for (int j = pp; j < NB; ++j) {
+                slot[j] = ma[j];
+                slot[2 * NB + j] = mb[j];
+            }
+#pragma unroll
+            for (int j = 0; j < NB; ++j) {
+                slot[NB + j] = ua[j];
+                slot[3 * NB + j] = ub[j];
+            }
+        }
+        __syncwarp(mask);
+        const double2 pa = slot[pp], pb = slot[2 * NB + pp];
+        const double ia = 1.0 / (pa.x * pa.x + pa.y * pa.y);
+        const double ib = 1.0 / (pb.x * pb.x + pb.y * pb.y);
+        const double2 ra = mk(pa.x * ia, -pa.y * ia), rb = mk(pb.x * ib, -pb.y * ib);
+        if (r == pp) {
+#pragma unroll
+            for (int j = pp + 1; j < NB; ++j) {
+                ma[j] = cmul(ma[j], ra);
+                mb[j] = cmul(mb[j], rb);
+            }
+#pragma unroll
+            for (int j = 0; j < NB; ++j) {
+                ua[j] = cmul(ua[j], ra);
+                ub[j] = cmul(ub[j], rb);
+            }
+        } else {
+            const double2 fa = cmul(ma[pp], ra), fb = cmul(mb[pp], rb);
+#pragma unroll
+            for (int j = pp + 1; j < NB; ++j) {
+                ma[j] = csub(ma[j], cmul(fa, slot[j]));
+                mb[j] = csub(mb[j], cmul(fb, slot[2 * NB + j]));
+            }
+#pragma unroll
+            for (int j = 0; j < NB; ++j) {
+                ua[j] = csub(ua[j], cmul(fa, slot[NB + j]));
+                ub[j] = csub(ub[j], cmul(fb, slot[3 * NB + j]));
+            }
+        }
+    }
+    __syncwarp(mask);  // the last step's readers are done before `piv` is reused
+}
+
 // diag(U^H Ft U) for the group: thread j holds Ft row j (ftj); it forms
 // c_jq = conj(U_jq) (Ft U)_jq for every q from the group's padded U in shared
 // memory `su`, and the group sums c_jq over j with xor-shuffles (fixed tree).

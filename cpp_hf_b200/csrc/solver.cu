@@ -368,7 +368,7 @@ int check_mixed(const cpphf_kernel* K, double sw) {
 }
 
 struct DmLayout {
-    size_t Q, P, Sig, F, G[2], dQ[2], Vd, p, eps, g[2], dp[2], lam, ew, wn, S, fock_ws, mu_ws, pack, total;
+    size_t Q, P, Sig, F, G[2], dQ[2], Vd, p, eps, g[2], dp[2], lam, ew, wn, S, fock_ws, mu_ws, pack, blk, total;
     size_t fock_bytes, mu_bytes;
 };
 
@@ -401,6 +401,7 @@ DmLayout dm_layout(const cpphf_kernel* K) {
     L.mu_bytes = mu_workspace_bytes((int64_t)nk, (int64_t)nb);
     L.mu_ws = W.take(L.mu_bytes);
     L.pack = W.take(solver_pack_bytes(K));
+    L.blk = W.take(2 * sizeof(unsigned long long));
     L.total = W.total;
     return L;
 }
@@ -413,6 +414,38 @@ int check_block_sizes(const int64_t* sizes, int64_t n, int64_t nb) {
         tot += sizes[i];
     }
     if (tot != nb) return fail(CPPHF_ERR_INVALID, "block_sizes must sum to nb.");
+    return CPPHF_OK;
+}
+
+// solver_dm.hpp:100-115: the block path needs no projector and h, refP and the
+// active contact operators all block-diagonal in the given blocks.
+int block_problem_invariant(const cpphf_kernel* K, bool project, const BlockSpec& bs, unsigned long long* dev2,
+                            cudaStream_t st, bool* ok) {
+    *ok = false;
+    if (project) return CPPHF_OK;
+    const int64_t nk = K->nk1 * K->nk2, nb = K->nb;
+    bool good = false;
+    CPPHF_TRY(block_structure_ok(static_cast<const double2*>(K->h), nk, nb, bs, dev2, st, &good));
+    if (!good) return CPPHF_OK;
+    if (K->has_refP) {
+        CPPHF_TRY(block_structure_ok(static_cast<const double2*>(K->refP), nk, nb, bs, dev2, st, &good));
+        if (!good) return CPPHF_OK;
+    }
+    if (K->contact_g && K->n_contact > 0 && K->contact_Oi && K->contact_Oj) {
+        std::vector<double> g((size_t)K->n_contact);
+        CPPHF_CUDA(cudaMemcpyAsync(g.data(), K->contact_g, sizeof(double) * g.size(), cudaMemcpyDeviceToHost, st));
+        CPPHF_CUDA(cudaStreamSynchronize(st));
+        for (int64_t t = 0; t < K->n_contact; ++t) {
+            if (g[(size_t)t] == 0.0) continue;
+            const double2* Oi = static_cast<const double2*>(K->contact_Oi) + t * nb * nb;
+            const double2* Oj = static_cast<const double2*>(K->contact_Oj) + t * nb * nb;
+            CPPHF_TRY(block_structure_ok(Oi, 1, nb, bs, dev2, st, &good));
+            if (!good) return CPPHF_OK;
+            CPPHF_TRY(block_structure_ok(Oj, 1, nb, bs, dev2, st, &good));
+            if (!good) return CPPHF_OK;
+        }
+    }
+    *ok = true;
     return CPPHF_OK;
 }
 
@@ -495,6 +528,7 @@ int solve_dm(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* P
     double2* G[2] = {fld(L.G[0]), fld(L.G[1])};
     double2* dQ[2] = {fld(L.dQ[0]), fld(L.dQ[1])};
     double *p = vec(L.p), *eps = vec(L.eps), *lam = vec(L.lam), *ew = vec(L.ew), *wn = vec(L.wn);
+    double* ew2 = reinterpret_cast<double*>(Vd);  // second trial's eps_work (Vd is free inside the loop)
     double* g[2] = {vec(L.g[0]), vec(L.g[1])};
     double* dp[2] = {vec(L.dp[0]), vec(L.dp[1])};
     DmScalars* S = reinterpret_cast<DmScalars*>(W + L.S);
@@ -536,10 +570,22 @@ int solve_dm(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* P
         return CPPHF_OK;
     };
 
+    // block-diagonal fast path (solver_dm.hpp:403-405): block eigh, eigenvalues
+    // block by block, at the start and in the final polish; the elimination form
+    // of the Cayley factor keeps the blocks of d in every trial and retraction
+    BlockSpec bspec;
+    bool use_block = false;
+    unsigned long long* blk = reinterpret_cast<unsigned long long*>(W + L.blk);
+    if (cfg->n_block_sizes > 1) {
+        CPPHF_TRY(make_block_spec(nb, cfg->block_sizes, cfg->n_block_sizes, 0, bspec));
+        CPPHF_TRY(block_problem_invariant(K, project != nullptr, bspec, blk, st, &use_block));
+    }
+
     // ---- init (solver_dm.hpp:436-459) ----
     CPPHF_TRY(hermitize(P0, P, nk, nb, st));
     CPPHF_TRY(build_fock(K, P, solver_sigma(K, Sig), F, nullptr, nullptr, nullptr, fws, L.fock_bytes, st));
-    CPPHF_TRY(eigh_batched(F, ew, Q, nk, nb, 0, nullptr, st));
+    if (use_block) CPPHF_TRY(block_structure_ok(F, nk, nb, bspec, blk, st, &use_block));
+    CPPHF_TRY(eigh_batched(F, ew, Q, nk, nb, 0, use_block ? &bspec : nullptr, st));
     CPPHF_TRY(mu_solve(ew, wn, nk, nb, n_t, &S->mu, T_r, mu_it, 1, &S->mu, mws, L.mu_bytes, st));
 
     double* const hbuf = host_scalars();  // scalar read-back; each read is followed by a sync
@@ -581,18 +627,20 @@ int solve_dm(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* P
                                    cfg->max_step, S, st));
         }
         // 5. Cayley line search (elimination form of the spectral Cayley factor):
-        // one pass per trial; a pass after the accepted trial returns at once
-        for (int64_t bt = 0; bt < cfg->bt_max; ++bt) {
-            if (small)
-                CPPHF_TRY(dm_small_trial(dQ[cur], F, p, dp[cur], wn, ew, Vd, nk, nb, T_r, cfg->bt_shrink,
-                                         bt == cfg->bt_max - 1, fallback, S, st));
-            else
+        // small nb, two trials per pass; otherwise one pass per trial; a pass
+        // after the accepted trial returns at once
+        if (small) {
+            for (int64_t bt = 0; bt < cfg->bt_max; bt += 2)
+                CPPHF_TRY(dm_small_trial2(dQ[cur], F, p, dp[cur], wn, ew, ew2, nk, nb, T_r, cfg->bt_shrink, (int)bt,
+                                          (int)cfg->bt_max, fallback, S, st));
+        } else {
+            for (int64_t bt = 0; bt < cfg->bt_max; ++bt)
                 CPPHF_TRY(dm_trial_lu(dQ[cur], F, p, dp[cur], wn, nk, nb, T_r, cfg->bt_shrink,
                                       bt == cfg->bt_max - 1, fallback, S, st));
         }
         // 6. retraction and mu (occupations are formed by the next density step)
         if (small)
-            CPPHF_TRY(dm_small_retract(Q, dQ[cur], F, ew, Vd, nk, nb, S, st));
+            CPPHF_TRY(dm_small_retract(Q, dQ[cur], F, ew, ew2, nk, nb, S, st));
         else
             CPPHF_TRY(dm_retract_lu(Q, dQ[cur], F, ew, nk, nb, S, st));
         CPPHF_TRY(mu_solve(ew, wn, nk, nb, n_t, &S->mu, T_r, mu_it, 1, &S->mu, mws, L.mu_bytes, st));
@@ -661,7 +709,7 @@ int solve_dm(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* P
     CPPHF_TRY(density(ew));
     CPPHF_TRY(build_fock(K, P, solver_sigma(K, Sig), F, nullptr, nullptr, nullptr, fws, L.fock_bytes, st));
     CPPHF_TRY(dm_rotate(Q, F, F, nullptr, nk, nb, st));
-    CPPHF_TRY(eigh_batched(F, ew, Vd, nk, nb, 0, nullptr, st));
+    CPPHF_TRY(eigh_batched(F, ew, Vd, nk, nb, 0, use_block ? &bspec : nullptr, st));
     CPPHF_TRY(dm_q_times_u(Q, Vd, nk, nb, st));
     CPPHF_TRY(mu_solve(ew, wn, nk, nb, n_t, &S->mu, T_r, mu_it, 1, &S->mu, mws, L.mu_bytes, st));
     CPPHF_TRY(density(ew));
@@ -692,7 +740,7 @@ int solve_dm(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* P
 namespace {
 
 struct ScfLayout {
-    size_t D, Sig, F, Pn, V, eps, sh, occ, S, fock_ws, mu_ws, mu2, pack, total;
+    size_t D, Sig, F, Pn, V, eps, sh, occ, S, fock_ws, mu_ws, mu2, pack, blk, total;
     size_t fock_bytes, mu_bytes;
     size_t R, Fh, Fex, dots, Sn, Fn, Dpre;  // acceleration extras (0 when unused)
     int nhist;
@@ -733,6 +781,7 @@ ScfLayout scf_layout(const cpphf_kernel* K, const cpphf_scf_config* cfg = nullpt
     }
     if (cfg && cfg->trust_radius > 0.0) L.Dpre = W.take(fld);
     L.pack = W.take(solver_pack_bytes(K));
+    L.blk = W.take(2 * sizeof(unsigned long long));
     L.total = W.total;
     return L;
 }
@@ -789,6 +838,25 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
     K32.exchange_precision = 32;
     bool low = cfg->mixed_switch_tol > 0.0;
 
+    // block-diagonal eigh in density_from_fock (solver_scf.hpp:96-124): with more
+    // than one block summing to nb, every F that is block-diagonal to 1e-10 of
+    // its largest entry takes the block eigh (checked on each call, on the host)
+    BlockSpec sbspec;
+    bool scf_block = false;
+    unsigned long long* blk = reinterpret_cast<unsigned long long*>(W + L.blk);
+    if (cfg->block_sizes && cfg->n_block_sizes > 1) {
+        int64_t tot = 0;
+        bool pos = true;
+        for (int64_t b = 0; b < cfg->n_block_sizes; ++b) {
+            tot += cfg->block_sizes[b];
+            pos = pos && cfg->block_sizes[b] > 0;
+        }
+        if (tot == nb && pos) {
+            CPPHF_TRY(make_block_spec(nb, cfg->block_sizes, cfg->n_block_sizes, 0, sbspec));
+            scf_block = true;
+        }
+    }
+
     // the occupation mu: mu2[1] after a level shift, else mu2[0]
     double* mu_fin = (cfg->level_shift != 0.0) ? &mu2[1] : &mu2[0];
     CPPHF_CUDA(cudaMemsetAsync(mu2, 0xFF, 2 * sizeof(double), st));  // NaN: no warm start yet
@@ -798,7 +866,13 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
     bool d_hermitian = false;
     // density_from_fock (solver_scf.hpp:96-154): P_out = herm(V f V^H) from Fsrc
     auto occupy = [&](const double2* Fsrc, double2* Pout) -> int {
-        CPPHF_TRY(eigh_batched(Fsrc, eps, V, nk, nb, 0, nullptr, st));
+        const BlockSpec* bsp = nullptr;
+        if (scf_block) {
+            bool ok = false;
+            CPPHF_TRY(block_structure_ok(Fsrc, nk, nb, sbspec, blk, st, &ok));
+            if (ok) bsp = &sbspec;
+        }
+        CPPHF_TRY(eigh_batched(Fsrc, eps, V, nk, nb, 0, bsp, st));
         // the previous iteration's mu warm-starts the bisection's root (same result)
         CPPHF_TRY(mu_solve(eps, K->w2d, nk, nb, n_e, &mu2[0], K->T, 30, 0, &mu2[0], mws, L.mu_bytes, st));
         const double* e_occ = eps;
@@ -885,7 +959,8 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
     // one, so every iteration after the first is the same launch sequence (mix,
     // Fock build, occupations, residuals), captured once per precision.
     const bool sl_path = K->sl && (K->sl->fock_active || K->sl->hartree_active);
-    const bool scf_graphs = cfg->graphs != 0 && guard.capturable && acc == 0 && !project && !Dpre && !sl_path;
+    const bool scf_graphs =
+        cfg->graphs != 0 && guard.capturable && acc == 0 && !project && !Dpre && !sl_path && !scf_block;
     IterGraphs sgr;
     bool pending_mix = false;
     while (k < max_iter && !converged) {

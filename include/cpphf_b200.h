@@ -360,6 +360,13 @@ typedef struct cpphf_scf_config {
      * from several host threads). */
     int32_t graphs;
     int32_t reserved1;
+    /* block_sizes (HOST array, may be NULL): with more than one block summing to
+     * nb, each Fock matrix whose off-block entries are below 1e-10 + 1e-10 of its
+     * largest entry is diagonalised block by block (eigenvalues ordered block by
+     * block), as density_from_fock does (solver_scf.hpp:96-124).  Disables the
+     * per-iteration graph capture (the choice is made on the host). */
+    const int64_t* block_sizes;
+    int64_t n_block_sizes;
 } cpphf_scf_config;
 
 typedef struct cpphf_scf_result {
