@@ -59,6 +59,7 @@ def parse():
     ap.add_argument("--oracle-solve", type=int, default=1, help="oracle DM solve estimate on the host")
     ap.add_argument("--sweep", type=int, default=96, help="batched-sweep instances (0 = skip)")
     ap.add_argument("--sweep-streams", type=int, default=16)
+    ap.add_argument("--c64-mesh", type=int, default=0, help="nb=64 superlattice mesh (0 = skip)")
     return ap.parse_args()
 
 
@@ -272,6 +273,46 @@ def time_newton(torch, native, args_dev, P0_dev, n_e, reps=2, max_iter=60):
             "config": f"optimizer=newton, tol_grad=1e-6, max_iter={max_iter}, tr_delta0=0.5, tr_cg_max=20"}
 
 
+def time_superlattice64(torch, native, dev, n):
+    """The superlattice workload at nb = 64 (32 plane waves x 2 Dirac components,
+    triangular superlattice, w0 = 0.1, scalar V with U = 0.5, T = 0.05, filling 32
+    of 64) in its plain-mesh form (V(k - k') on every orbital pair, Hermitian
+    channel packing: 2080 channels): one Fock build and one solve() (tol_E = 1e-10),
+    device resident."""
+    from cpp_hf_b200 import superlattice as sl
+    from cpp_hf_b200.fock_builder import FockBuilder
+
+    args, P0, n_e = sl.dirac_superlattice(n, n_pw=32, seed=0, streamed=False)
+    fb = FockBuilder(args, precision=64)
+    P = torch.zeros((n, n, 64, 64), dtype=torch.complex128, device=dev)
+    P[..., :32, :32] = torch.eye(32, dtype=torch.complex128, device=dev)
+    for _ in range(2):
+        fb.build(P)
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(5):
+        fb.build(P)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_build = e0.elapsed_time(e1) / 1e3 / 5
+    del fb
+    args_dev = {k: (torch.from_numpy(v).to(dev) if isinstance(v, np.ndarray) and v.size > 64 else v)
+                for k, v in args.items()}
+    P0_dev = torch.from_numpy(P0).to(dev)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    r = _dm_call(native, args_dev, P0_dev, n_e)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3
+    return {"workload": f"Dirac superlattice, 32 plane waves x 2 (nb = 64), {n}x{n} mesh, plain-mesh form "
+                        "(scalar V on every orbital pair, 2080 packed channels)",
+            "ms_per_build": 1e3 * t_build, "solve_s": t, "iterations": int(r[6]), "converged": bool(r[7]),
+            "energy": float(r[5]), "ms_per_iteration": 1e3 * t / max(int(r[6]), 1)}
+
+
 def oracle_solve_estimate(args, P0_np, n_e, n_iter_gpu):
     """Oracle DM solve time from a bounded sample: init + 2 iterations, extrapolated to the
     iteration count of the FP64 GPU solve (the trajectories agree to ~1e-8)."""
@@ -455,6 +496,10 @@ def main():
         barrier()
         solves = time_solves(torch, native, args_dev, P0_dev, _ne, a.solve_reps, a.n)
         solves["newton_fp64"] = time_newton(torch, native, args_dev, P0_dev, _ne)
+        if a.c64_mesh > 0:
+            del args_dev, P0_dev
+            torch.cuda.empty_cache()
+            solves["superlattice_nb64"] = time_superlattice64(torch, native, dev, a.c64_mesh)
         barrier()
 
     # ---- batched sweep: concurrent streams (mixed and FP64) vs one by one in FP64 ----

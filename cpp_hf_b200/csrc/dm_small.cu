@@ -372,16 +372,16 @@ __global__ void __launch_bounds__(kThreads) k_retract_small(double2* Q, const do
     }
 }
 
-// Row kernels (PR+ beta, direction): one thread per matrix row (k, i), which
-// loads the row's NB elements of each field (independent loads, all in
-// flight at once), its eigenvalue, weight and occupation terms, so the index
-// arithmetic and the row terms are paid once per row.  The preconditioner
+// Element kernels (PR+ beta, direction): a grid-stride loop over the matrix
+// elements (coalesced), then one over the rows for the occupation terms.  At
+// most 64 registers, so four 256-thread CTAs per SM keep their loads in
+// flight (these kernels are bound by load latency).  The preconditioner
 // 1 / sqrt(gap^2 + lambda^2) is one reciprocal square root per element.
 constexpr int kThreadsE = 256;
 
 // PR+ numerator / denominator -> beta (solver_dm.hpp:513-559)
 template <int NB>
-__global__ void __launch_bounds__(kThreadsE) k_pr_beta_small(const double2* __restrict__ Gc, const double2* __restrict__ Gp,
+__global__ void __launch_bounds__(kThreadsE, 4) k_pr_beta_small(const double2* __restrict__ Gc, const double2* __restrict__ Gp,
                                                              const double* __restrict__ g_p,
                                                              const double* __restrict__ g_pp,
                                                              const double* __restrict__ eps,
@@ -431,7 +431,7 @@ __global__ void __launch_bounds__(kThreadsE) k_pr_beta_small(const double2* __re
 
 // direction + tau0 + Omega0 (solver_dm.hpp:556-573, 346-365)
 template <int NB>
-__global__ void __launch_bounds__(kThreadsE) k_direction_small(const double2* __restrict__ Gc,
+__global__ void __launch_bounds__(kThreadsE, 4) k_direction_small(const double2* __restrict__ Gc,
                                                                const double2* __restrict__ dQp,
                                                                const double* __restrict__ g_p,
                                                                const double* __restrict__ dpp,

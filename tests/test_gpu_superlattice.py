@@ -151,3 +151,19 @@ def test_dirac_superlattice_nb64_build_matches_oracle(native, oracle):
     S2, _, F2, E2 = native.build_fock_apply(a2, P, None)
     S2r, _, F2r, E2r = oracle.build_fock_apply(a2, P, None)
     assert _rel(S2, S2r) < 1e-12 and _rel(F2, F2r) < 1e-12
+
+
+def test_dirac_superlattice_nb64_plain_mesh_solve_matches_oracle(native, oracle):
+    """nb = 64 direct minimisation (the plain-mesh form: 32 plane waves x 2, scalar V,
+    Hermitian channel packing) on a 6 x 6 mesh against the oracle: the per-k nb = 64
+    kernels (Jacobi eigh, elimination Cayley factor, products) of the large-nb path."""
+    a2, P0, n_e = sl.dirac_superlattice(6, n_pw=32, seed=0, streamed=False)
+    empty = np.empty((0, 6, 6, 64, 64), np.complex128)
+    call = (a2, P0, n_e, 300, 1e-10, 0.0, 0.6, 0.5, 1e-3, 8, 10, 5, 25, 0, 0.5, 20, empty, 0.0, 1.0, [], None,
+            False, True, True)
+    got = native.solve_dm(*call)
+    ref = oracle.solve_dm(*call)
+    assert got[7] and ref[7]
+    assert got[6] == ref[6]
+    assert abs(got[5] - ref[5]) < 1e-9 * max(1.0, abs(ref[5]))
+    assert _rel(got[2], ref[2]) < 1e-8
