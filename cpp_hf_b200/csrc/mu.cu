@@ -27,6 +27,8 @@ namespace {
 constexpr int kMuThreads = 1024;
 constexpr int kMuMaxGrid = 1024;
 constexpr int64_t kMuOneBlockMax = 32768;             // eigenvalues handled by a single CTA
+constexpr int kMuCluster = 8;                         // CTAs of the cluster form (portable cluster size)
+constexpr int64_t kMuClusterMax = (int64_t)1 << 19;   // eigenvalues handled by one cluster
 constexpr int kBisectLevels = 3;                      // bisection steps per grid barrier
 constexpr int kMuNV = (1 << kBisectLevels) - 1;       // midpoints evaluated per barrier
 constexpr double kMuWide = 64.0;                      // exact multisection while the bracket exceeds 64 T
@@ -76,10 +78,67 @@ __device__ __forceinline__ void band_major(const MuArgs& a, unsigned i, unsigned
     e = a.eps[(size_t)k * nb + band];
 }
 
+// Cluster barrier: every thread of every CTA of the cluster (hardware barrier;
+// release / acquire at cluster scope orders the partials' global stores).
+__device__ __forceinline__ void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// Grid-wide synchronisation of the mu kernel.  CLUSTER = false: a cooperative
+// grid with the bounded software barrier (the last block to arrive sums the
+// partials).  CLUSTER = true: one thread-block cluster (kMuCluster CTAs) with
+// the hardware cluster barrier; every CTA sums the partials itself in the
+// same fixed order, so the partials are double-buffered by round parity (a
+// CTA may start writing round r + 1 while another still reads round r).
+template <bool CLUSTER>
+struct MuSync {
+    GridBarrier bar;
+    double* ctot;  // shared totals (cluster form)
+    __device__ void init(const MuArgs& a, double* sh) {
+        if (!CLUSTER) bar.init(a.sync, a.spin_limit, a.err);
+        ctot = sh;
+    }
+    __device__ bool all() {
+        if constexpr (CLUSTER) {
+            cluster_sync_all();
+            return true;
+        } else {
+            return bar.wait();
+        }
+    }
+    // the partials buffer of a round
+    __device__ double* partials(double* part, int round) const {
+        if constexpr (CLUSTER) return part + (size_t)(round & 1) * kMuNV * gridDim.x;
+        return part;
+    }
+    // every block's NV partials summed (fixed order); null if a wait gave up
+    template <int NV>
+    __device__ const double* reduce(const double* part, int G, double* tot) {
+        if constexpr (CLUSTER) {
+            cluster_sync_all();
+            if (threadIdx.x < NV) {
+                double s = 0.0;
+                for (int b = 0; b < G; ++b) s += __ldcg(&part[NV * b + threadIdx.x]);
+                ctot[threadIdx.x] = s;
+            }
+            __syncthreads();
+            return ctot;
+        } else {
+            return bar.wait_reduce<NV>(part, G, tot) ? tot : nullptr;
+        }
+    }
+    __device__ double load(const double* t, int j) const {
+        if constexpr (CLUSTER) return t[j];
+        return __ldcg(&t[j]);
+    }
+};
+
+template <bool CLUSTER>
 __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
     __shared__ double red[32 * kMuNV];  // block_sum<kMuNV> scratch (32 doubles per value)
-    GridBarrier bar;
-    bar.init(a.sync, a.spin_limit, a.err);
+    __shared__ double ctot_sh[kMuNV];
+    MuSync<CLUSTER> bar;
+    bar.init(a, ctot_sh);
     const int G = gridDim.x;
     const unsigned nb = (unsigned)a.nb;
     const unsigned n = (unsigned)a.n;
@@ -115,7 +174,7 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
             a.part[2 * blockIdx.x + 1] = m1;
         }
     }
-    if (!bar.wait()) {
+    if (!bar.all()) {
         if (blockIdx.x == 0 && threadIdx.x == 0) *a.mu_out = NAN;
         return;
     }
@@ -149,8 +208,8 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
     }
     const double Tfd = Tj + 1.0e-12;  // fermidirac_scalar(x, Tj) = expit(-x / (Tj + 1e-12))
     const double invTfd = 1.0 / Tfd, invTj = 1.0 / Tj;
-    double* part = a.part + 2 * G;                  // [G][kMuNV] partials of the current round
-    double* tots = part + (size_t)kMuNV * G;        // [2][kMuNV] totals, by round parity
+    double* part0 = a.part + 2 * G;                 // [G][kMuNV] partials (two such buffers in the cluster form)
+    double* tots = part0 + (size_t)kMuNV * G * (CLUSTER ? 2 : 1);  // [2][kMuNV] totals, by round parity
     __shared__ double bc_tot[kMuNV];
     int round = 0;
     if (a.mode == 0) {
@@ -212,16 +271,17 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
                 }
             }
             block_sum<kMuNV>(v, red);
+            double* part = bar.partials(part0, round);
             if (threadIdx.x == 0) {
 #pragma unroll
                 for (int j = 0; j < kMuNV; ++j) __stcg(&part[kMuNV * blockIdx.x + j], v[j]);
             }
-            double* tot = tots + (round & 1) * kMuNV;
-            if (!bar.wait_reduce<kMuNV>(part, G, tot)) {
+            const double* tot = bar.template reduce<kMuNV>(part, G, tots + (round & 1) * kMuNV);
+            if (!tot) {
                 ok = false;
                 return;
             }
-            if (threadIdx.x < kMuNV) bc_tot[threadIdx.x] = __ldcg(&tot[threadIdx.x]);
+            if (threadIdx.x < kMuNV) bc_tot[threadIdx.x] = bar.load(tot, threadIdx.x);
             __syncthreads();
             int node = 0;
             for (int l = 0; l < L; ++l) {
@@ -259,17 +319,18 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
                 }
             }
             block_sum<2>(v, red);
+            double* part = bar.partials(part0, round);
             if (threadIdx.x == 0) {
                 __stcg(&part[2 * blockIdx.x], v[0]);
                 __stcg(&part[2 * blockIdx.x + 1], v[1]);
             }
-            double* tot = tots + (round & 1) * kMuNV;
+            const double* tot = bar.template reduce<2>(part, G, tots + (round & 1) * kMuNV);
             ++round;
-            if (!bar.wait_reduce<2>(part, G, tot)) {
+            if (!tot) {
                 ok = false;
                 return;
             }
-            if (threadIdx.x < 2) bc_tot[threadIdx.x] = __ldcg(&tot[threadIdx.x]);
+            if (threadIdx.x < 2) bc_tot[threadIdx.x] = bar.load(tot, threadIdx.x);
             __syncthreads();
             N = bc_tot[0];
             Z = bc_tot[1];
@@ -378,16 +439,17 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
                 }
             }
             block_sum<2>(v, red);
+            double* part = bar.partials(part0, it);
             if (threadIdx.x == 0) {
                 __stcg(&part[2 * blockIdx.x], v[0]);
                 __stcg(&part[2 * blockIdx.x + 1], v[1]);
             }
-            double* tot = tots + (it & 1) * kMuNV;
-            if (!bar.wait_reduce<2>(part, G, tot)) {
+            const double* tot = bar.template reduce<2>(part, G, tots + (it & 1) * kMuNV);
+            if (!tot) {
                 if (blockIdx.x == 0 && threadIdx.x == 0) *a.mu_out = NAN;
                 return;
             }
-            if (threadIdx.x < 2) bc_tot[threadIdx.x] = __ldcg(&tot[threadIdx.x]);
+            if (threadIdx.x < 2) bc_tot[threadIdx.x] = bar.load(tot, threadIdx.x);
             __syncthreads();
             const double N = bc_tot[0], Z = bc_tot[1];
             __syncthreads();
@@ -422,7 +484,7 @@ int max_coop_grid() {
     static std::once_flag once;
     std::call_once(once, [] {
         int per = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_mu, kMuThreads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_mu<false>, kMuThreads, 0);
         if (per < 1) per = 1;
         g = std::min(kMuMaxGrid, per * num_sms());
     });
@@ -478,12 +540,30 @@ int mu_solve(const double* eps, const double* w, int64_t nk, int64_t nb, double 
     a.part = reinterpret_cast<double*>(static_cast<unsigned char*>(ws) + 64);
     CPPHF_CUDA(cudaMemsetAsync(ws, 0, 64, st));
     if (grid == 1) {
-        k_mu<<<1, kMuThreads, 0, st>>>(a);
+        k_mu<false><<<1, kMuThreads, 0, st>>>(a);
         CPPHF_LAUNCH_CHECK("mu (one block)");
         return CPPHF_OK;
     }
+    if (n <= kMuClusterMax) {
+        // mid-size problems: one cluster of kMuCluster CTAs, hardware cluster
+        // barriers between the rounds (no software grid barrier)
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(kMuCluster);
+        cfg.blockDim = dim3(kMuThreads);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = kMuCluster;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        CPPHF_CUDA(cudaLaunchKernelEx(&cfg, k_mu<true>, a));
+        return CPPHF_OK;
+    }
     void* args[] = {&a};
-    CPPHF_CUDA(cudaLaunchCooperativeKernel((const void*)k_mu, dim3(grid), dim3(kMuThreads), args, 0, st));
+    CPPHF_CUDA(cudaLaunchCooperativeKernel((const void*)k_mu<false>, dim3(grid), dim3(kMuThreads), args, 0, st));
     return CPPHF_OK;
 }
 

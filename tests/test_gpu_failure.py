@@ -2,9 +2,11 @@
 next call runs normally.
 
 The grid barriers of the cooperative chemical-potential kernel poll a counter
-at most ``cpphf_set_barrier_spin_limit`` times.  With a limit of one poll, the
-first blocks to reach a barrier give up before the slower ones arrive (the
-problems below need several hundred blocks), every block leaves the kernel
+at most ``cpphf_set_barrier_spin_limit`` times.  (Problems of up to 2^19
+eigenvalues run as one thread-block cluster with hardware barriers instead, so
+the cases below are larger.)  With a limit of one poll, the first blocks to
+reach a barrier give up before the slower ones arrive (the problems below need
+several hundred blocks), every block leaves the kernel
 through the barrier's error flag, and the entry point reports
 CPPHF_ERR_TIMEOUT (``RuntimeError`` in Python).  Nothing waits forever and no
 copy is in flight in that kernel, so the context stays usable: the same call
@@ -39,7 +41,7 @@ def tiny_barrier_limit():
 
 def test_find_mu_barrier_timeout_then_recovers(native, oracle, tiny_barrier_limit):
     rng = np.random.default_rng(11)
-    nk, nb, T = 36864, 8, 0.05
+    nk, nb, T = 131072, 8, 0.05
     bands = rng.normal(size=(nk, nb))
     w = np.full(nk, 1.0 / nk)
     with pytest.raises(RuntimeError, match="gave up"):
@@ -51,9 +53,9 @@ def test_find_mu_barrier_timeout_then_recovers(native, oracle, tiny_barrier_limi
 
 
 def test_solve_dm_barrier_timeout_then_recovers(native, oracle, tiny_barrier_limit):
-    # 192 x 192 Dirac mesh, nb = 2: 73 728 eigenvalues, a multi-block mu kernel
-    args, P0, n_e = workloads.dirac(192, seed=0)
-    defl = np.empty((0, 192, 192, 2, 2), np.complex128)
+    # 576 x 576 Dirac mesh, nb = 2: 663 552 eigenvalues, a multi-block cooperative mu kernel
+    args, P0, n_e = workloads.dirac(576, seed=0)
+    defl = np.empty((0, 576, 576, 2, 2), np.complex128)
     call = (args, P0, n_e, 3, 1e-10, 0.0, 0.6, 0.5, 1e-3, 8, 10, 5, 25, 0, 0.5, 20, defl, 0.0, 1.0, [], None,
             False, False, False)
     with pytest.raises(RuntimeError, match="gave up|timeout"):
