@@ -102,6 +102,9 @@ __global__ void __launch_bounds__(kThreads) k_dens_occ(const double2* __restrict
 // reductions grad_norm, lam_pc (solver_dm.hpp:130-160, 497-519).
 // Ft overwrites F.
 // ---------------------------------------------------------------------------
+// Two shared-memory stages of (Q, F) tiles: the next tile's asynchronous
+// copies are in flight while the current one is processed.
+// Dynamic shared memory: stage s = { sQ, sT } at dyn + 2 s TILE.
 template <int NB>
 __global__ void __launch_bounds__(kThreads) k_rot_grad(const double2* __restrict__ Q, double2* F,
                                                        const double* __restrict__ p, const double* __restrict__ w,
@@ -109,18 +112,30 @@ __global__ void __launch_bounds__(kThreads) k_rot_grad(const double2* __restrict
                                                        double* __restrict__ g_p, int64_t nk, double T_r,
                                                        double denom_scale, DmScalars* S) {
     using G = Geo<NB>;
-    __shared__ double2 sQ[G::TILE];  // Q, then the gradient
-    __shared__ double2 sT[G::TILE];  // F, then F Q, then Ft
+    extern __shared__ __align__(16) double2 dyn[];
     __shared__ double red[64];
     const int grp = threadIdx.x / G::GS, r = threadIdx.x % G::GS;
     const double mu = S->mu;
     const int64_t ntiles = (nk + G::KT - 1) / G::KT;
     double v[2] = {0.0, 0.0};
-    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    auto issue = [&](int64_t t, int s) {
         const int64_t k0 = t * G::KT;
         const int nkt = (int)((nk - k0) < G::KT ? (nk - k0) : G::KT);
-        tile_load<NB>(sQ, Q + (size_t)k0 * G::NB2, nkt);
-        tile_load<NB>(sT, F + (size_t)k0 * G::NB2, nkt);
+        tile_load_async<NB>(dyn + 2 * s * G::TILE, Q + (size_t)k0 * G::NB2, nkt);
+        tile_load_async<NB>(dyn + (2 * s + 1) * G::TILE, F + (size_t)k0 * G::NB2, nkt);
+    };
+    if ((int64_t)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+    cp_async_commit();
+    int it = 0;
+    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
+        const int s = it & 1;
+        if (t + (int64_t)gridDim.x < ntiles) issue(t + gridDim.x, s ^ 1);  // stage s ^ 1 was freed last iteration
+        cp_async_commit();
+        cp_async_wait_prev();
+        double2* sQ = dyn + 2 * s * G::TILE;        // Q, then the gradient
+        double2* sT = dyn + (2 * s + 1) * G::TILE;  // F, then F Q, then Ft
+        const int64_t k0 = t * G::KT;
+        const int nkt = (int)((nk - k0) < G::KT ? (nk - k0) : G::KT);
         __syncthreads();
         const bool live = grp < nkt && r < NB;
         const int64_t k = k0 + grp;
@@ -566,8 +581,19 @@ void small_attrs() {
     static std::once_flag once;
     std::call_once(once, [] {
         raise_smem(k_trial2_small<NB>);
+        raise_smem(k_rot_grad<NB>);
         raise_smem(k_retract_small<NB>);
     });
+}
+
+// CTAs of a persistent tile kernel resident on the device at once (at most
+// kDmMaxPartials, the size of the reduction partials)
+template <class K>
+int resident_ctas(K kern, size_t smem) {
+    int per = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, kThreads, smem);
+    (void)cudaGetLastError();
+    return std::max(1, std::min(kDmMaxPartials, std::max(per, 1) * num_sms()));
 }
 
 }  // namespace
@@ -608,7 +634,9 @@ int scf_small_residuals(const double2* F, const double2* D, const double2* Pn, c
 int dm_small_rot_grad(const double2* Q, double2* F, const double* p, const double* w, double* eps, double2* Gout,
                       double* g_p, int64_t nk, int nb, double T_r, double denom_scale, DmScalars* S, cudaStream_t st) {
 #define X(N)                                                                                                    \
-    k_rot_grad<N><<<tiles_grid(nk, Geo<N>::KT, kDmMaxPartials), kThreads, 0, st>>>(Q, F, p, w, eps, Gout, g_p, nk, \
+    small_attrs<N>();                                                                                           \
+    k_rot_grad<N><<<tiles_grid(nk, Geo<N>::KT, resident_ctas(k_rot_grad<N>, 4 * sizeof(double2) * Geo<N>::TILE)),   \
+                    kThreads, 4 * sizeof(double2) * Geo<N>::TILE, st>>>(Q, F, p, w, eps, Gout, g_p, nk,        \
                                                                                    T_r, denom_scale, S);        \
     CPPHF_LAUNCH_CHECK("rot_grad");
     SMALL_DISPATCH(nb, X)

@@ -61,6 +61,33 @@ __device__ __forceinline__ void tile_load(double2* s, const double2* __restrict_
     }
 }
 
+// 16-byte asynchronous global -> shared copies (cp.async, L2 only) and their
+// commit / wait: the loads of the next tile are issued before the current one
+// is processed (the wait is on this thread's own copies; it cannot hang).
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(static_cast<unsigned>(__cvta_generic_to_shared(dst))),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// every group but the most recent one has landed
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// tile_load as asynchronous copies into the padded layout (committed by the caller)
+template <int NB>
+__device__ __forceinline__ void tile_load_async(double2* s, const double2* __restrict__ g, int nkt) {
+    using G = Geo<NB>;
+    const int n = nkt * G::NB2;
+#pragma unroll
+    for (int u = 0; u < G::PER; ++u) {
+        const int e = threadIdx.x + u * kThreads;
+        if (e < n) {
+            const int kl = e / G::NB2, rem = e - kl * G::NB2, i = rem / NB, j = rem - i * NB;
+            cp_async16(&s[kl * G::MS + i * G::LD + j], g + e);
+        }
+    }
+}
+
 template <int NB>
 __device__ __forceinline__ void tile_store(double2* g, const double2* s, int nkt) {
     using G = Geo<NB>;

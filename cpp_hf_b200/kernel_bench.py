@@ -2,6 +2,7 @@
 
     python -m cpp_hf_b200.kernel_bench --op exchange --n 192 --layers 4 --reps 5
     python -m cpp_hf_b200.kernel_bench --op build --n 192 --layers 4 --reps 5
+    python -m cpp_hf_b200.kernel_bench --op build_packed --n 192 --layers 4 --reps 5
 
 Runs ``--warmup`` untimed calls then ``--reps`` timed calls of one operation on
 the seeded layered workload (device resident, current CUDA stream) and prints
@@ -24,7 +25,8 @@ from ._native import _DeviceKernel, _ptr, _stream, _ws
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--op", default="exchange",
-                    choices=["exchange", "exchange32", "exchange_hcp", "build", "eigh", "mu", "solve_dm", "solve_scf", "solve_newton",
+                    choices=["exchange", "exchange32", "exchange_hcp", "build", "build_packed", "build_packed32", "eigh",
+                             "mu", "solve_dm", "solve_scf", "solve_newton",
                              "sl_build", "sl_mesh_build", "sl_dm"])
     ap.add_argument("--pw", type=int, default=32, help="plane waves of the Dirac superlattice (sl_* ops)")
     ap.add_argument("--iters", type=int, default=10, help="solver iterations per call (solve_* ops)")
@@ -64,6 +66,18 @@ def main():
 
         def op():
             _lib.check(lib.cpphf_build_fock(C.byref(dk.K), _ptr(P), _ptr(out), _ptr(out2), None, _ptr(E), None,
+                                            _ptr(ws), ws.numel(), st), "build")
+    elif a.op in ("build_packed", "build_packed32"):
+        # Hermitian-packed build as the solvers run it (no Sigma field written)
+        if a.op == "build_packed32":
+            dk.K.exchange_precision = 32
+        if not dk.enable_packing():
+            raise SystemExit("the packed build does not apply to this kernel")
+        ws = _ws(lib.cpphf_build_fock_workspace_bytes(C.byref(dk.K)))
+        E = torch.zeros(1, dtype=torch.float64, device=dev)
+
+        def op():
+            _lib.check(lib.cpphf_build_fock(C.byref(dk.K), _ptr(P), None, _ptr(out2), None, _ptr(E), None,
                                             _ptr(ws), ws.numel(), st), "build")
     elif a.op == "eigh":
         def op():
