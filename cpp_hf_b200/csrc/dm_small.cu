@@ -43,21 +43,35 @@ __device__ __forceinline__ double expit(double x) {
 // (solver_dm.hpp:117-128 + 456-457/598-599); p written out.
 // ---------------------------------------------------------------------------
 // FROM_EW = false: the occupations are given in p (read, not written).
+// The Q tiles come through two shared-memory stages filled by cp.async (the
+// next tile's copies in flight while the current one is processed).
+// Dynamic shared memory: sQ stage 0 | sQ stage 1 | sX, TILE double2 each.
 template <int NB, bool FROM_EW>
 __global__ void __launch_bounds__(kThreads) k_dens_occ(const double2* __restrict__ Q, const double* __restrict__ ew,
                                                        const double* __restrict__ mu, double T_r, double* __restrict__ p,
                                                        double2* __restrict__ P, int64_t nk) {
     using G = Geo<NB>;
-    __shared__ double2 sQ[G::TILE];
-    __shared__ double2 sX[G::TILE];
+    extern __shared__ __align__(16) double2 dyn[];
+    double2* sX = dyn + 2 * G::TILE;
     __shared__ double sp[G::KT * NB];
     const int grp = threadIdx.x / G::GS, r = threadIdx.x % G::GS;
     const double m = FROM_EW ? *mu : 0.0;
     const int64_t ntiles = (nk + G::KT - 1) / G::KT;
-    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    auto issue = [&](int64_t t, int s) {
         const int64_t k0 = t * G::KT;
         const int nkt = (int)((nk - k0) < G::KT ? (nk - k0) : G::KT);
-        tile_load<NB>(sQ, Q + (size_t)k0 * G::NB2, nkt);
+        tile_load_async<NB>(dyn + s * G::TILE, Q + (size_t)k0 * G::NB2, nkt);
+    };
+    if ((int64_t)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+    cp_async_commit();
+    int it = 0;
+    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
+        const int s = it & 1;
+        if (t + (int64_t)gridDim.x < ntiles) issue(t + gridDim.x, s ^ 1);  // stage s ^ 1 was freed last iteration
+        cp_async_commit();
+        double2* sQ = dyn + s * G::TILE;
+        const int64_t k0 = t * G::KT;
+        const int nkt = (int)((nk - k0) < G::KT ? (nk - k0) : G::KT);
         for (int e = threadIdx.x; e < nkt * NB; e += blockDim.x) {
             if (FROM_EW) {
                 const double pv = expit((m - ew[k0 * NB + e]) / T_r);
@@ -67,6 +81,7 @@ __global__ void __launch_bounds__(kThreads) k_dens_occ(const double2* __restrict
                 sp[e] = p[k0 * NB + e];
             }
         }
+        cp_async_wait_prev();
         __syncthreads();
         if (grp < nkt && r < NB) {
             const double2* q = sQ + grp * G::MS;
@@ -577,11 +592,16 @@ __global__ void __launch_bounds__(kThreads) k_scf_residuals_small(const double2*
 }
 
 template <int NB>
+constexpr size_t kDensSmem = 3 * sizeof(double2) * Geo<NB>::TILE;  // two Q stages + the product tile
+
+template <int NB>
 void small_attrs() {
     static std::once_flag once;
     std::call_once(once, [] {
         raise_smem(k_trial2_small<NB>);
         raise_smem(k_rot_grad<NB>);
+        raise_smem(k_dens_occ<NB, true>);
+        raise_smem(k_dens_occ<NB, false>);
         raise_smem(k_retract_small<NB>);
     });
 }
@@ -603,7 +623,9 @@ bool dm_small_supported(int nb) { return nb == 2 || nb == 4 || nb == 6 || nb == 
 int dm_small_dens_occ(const double2* Q, const double* ew, const double* mu, double T_r, double* p, double2* P,
                       int64_t nk, int nb, cudaStream_t st) {
 #define X(N)                                                                                                     \
-    k_dens_occ<N, true><<<tiles_grid(nk, Geo<N>::KT, 16 * num_sms()), kThreads, 0, st>>>(Q, ew, mu, T_r, p, P, nk); \
+    small_attrs<N>();                                                                                            \
+    k_dens_occ<N, true><<<tiles_grid(nk, Geo<N>::KT, resident_ctas(k_dens_occ<N, true>, kDensSmem<N>)), kThreads,  \
+                          kDensSmem<N>, st>>>(Q, ew, mu, T_r, p, P, nk);                                        \
     CPPHF_LAUNCH_CHECK("dens_occ");
     SMALL_DISPATCH(nb, X)
 #undef X
@@ -612,7 +634,9 @@ int dm_small_dens_occ(const double2* Q, const double* ew, const double* mu, doub
 
 int dm_small_density(const double2* Q, const double* p, double2* P, int64_t nk, int nb, cudaStream_t st) {
 #define X(N)                                                                                                        \
-    k_dens_occ<N, false><<<tiles_grid(nk, Geo<N>::KT, 16 * num_sms()), kThreads, 0, st>>>(                          \
+    small_attrs<N>();                                                                                               \
+    k_dens_occ<N, false><<<tiles_grid(nk, Geo<N>::KT, resident_ctas(k_dens_occ<N, false>, kDensSmem<N>)), kThreads, \
+                           kDensSmem<N>, st>>>(                                                                      \
         Q, nullptr, nullptr, 1.0, const_cast<double*>(p), P, nk);                                                   \
     CPPHF_LAUNCH_CHECK("density");
     SMALL_DISPATCH(nb, X)

@@ -250,6 +250,9 @@ __global__ void __launch_bounds__(kPackMaxThreads, 2)
     k_rows_inv_fock_pk(const __grid_constant__ CUtensorMap mT, FusedOut o, ExchangeGeom g, PackGeom pg, int ntiles,
                        double scale, int nst) {
     constexpr int N = N1 * N2;
+    constexpr int kLanes = N1 > N2 ? N1 : N2;  // line lanes: blockDim.x = kLanes * CBp
+    constexpr int NE = N / kLanes;             // epilogue points per thread (ky = a + kLanes e)
+    constexpr int EB = 4;                      // epilogue points whose loads are issued together
     extern __shared__ __align__(16) unsigned char smem_dyn[];
     __shared__ double red[32];
     unsigned char* smem_raw = align128(smem_dyn);
@@ -258,7 +261,6 @@ __global__ void __launch_bounds__(kPackMaxThreads, 2)
     Cx* tw = reinterpret_cast<Cx*>(smem_raw + L.tw);
     unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem_raw + L.bar);
     const int c = threadIdx.x % CBp, a = threadIdx.x / CBp;
-    const int lanes = blockDim.x / CBp;
     build_line_twiddles(tw, N);
     if (threadIdx.x == 0) {
         for (int b = 0; b < nst; ++b) mbar_init(&bar[b], 1);
@@ -335,28 +337,46 @@ __global__ void __launch_bounds__(kPackMaxThreads, 2)
             add.x += hdr;
             const double mult = diag ? 1.0 : 2.0;
             const size_t slot = (size_t)q * CBp + c;
-#pragma unroll 2
-            for (int ky = a; ky < N; ky += lanes) {
-                const size_t k = (size_t)kx * g.n1 + ky;
-                const size_t base = k * nb2;
-                const double2 sg = cscale(to_d(S[ky * CBp + c]), scale);
-                const double2 hh = ld_stream(o.hp + k * pg.Ct + slot);
-                double2 f = cadd(cadd(hh, sg), add);
-                if (diag) f.y = 0.0;
-                o.F[base + rj] = f;
-                if (!diag) o.F[base + jr] = cconj(f);
-                if (o.Sigma) {
-                    o.Sigma[base + rj] = cadd(sg, sc_rj);
-                    if (!diag) o.Sigma[base + jr] = cadd(cconj(sg), sc_jr);
+            // this thread's NE points ky = a + kLanes e, in batches of EB whose
+            // loads are all issued before their first use (one memory latency
+            // per batch instead of one per point)
+#pragma unroll 1
+            for (int e0 = 0; e0 < NE; e0 += EB) {
+                double2 hh[EB], pv[EB], rv[EB];
+#pragma unroll
+                for (int e = 0; e < EB; ++e) {
+                    if (e0 + e < NE) {
+                        const size_t k = (size_t)kx * g.n1 + (a + kLanes * (e0 + e));
+                        hh[e] = ld_stream(o.hp + k * pg.Ct + slot);
+                        pv[e] = ld_stream(o.P + k * nb2 + rj);
+                        rv[e] = o.refP ? ld_stream(o.refP + k * nb2 + rj) : mk(0.0, 0.0);
+                    }
                 }
-                if (o.Hdense) {
-                    o.Hdense[base + rj] = mk(hdr, 0.0);
-                    if (!diag) o.Hdense[base + jr] = mk(0.0, 0.0);
+#pragma unroll
+                for (int e = 0; e < EB; ++e) {
+                    if (e0 + e < NE) {
+                        const int ky = a + kLanes * (e0 + e);
+                        const size_t k = (size_t)kx * g.n1 + ky;
+                        const size_t base = k * nb2;
+                        const double2 sg = cscale(to_d(S[ky * CBp + c]), scale);
+                        double2 f = cadd(cadd(hh[e], sg), add);
+                        if (diag) f.y = 0.0;
+                        o.F[base + rj] = f;
+                        if (!diag) o.F[base + jr] = cconj(f);
+                        if (o.Sigma) {
+                            o.Sigma[base + rj] = cadd(sg, sc_rj);
+                            if (!diag) o.Sigma[base + jr] = cadd(cconj(sg), sc_jr);
+                        }
+                        if (o.Hdense) {
+                            o.Hdense[base + rj] = mk(hdr, 0.0);
+                            if (!diag) o.Hdense[base + jr] = mk(0.0, 0.0);
+                        }
+                        const double2 p = pv[e];
+                        const double2 rho = csub(p, rv[e]);
+                        const double term = (hh[e].x * p.x + hh[e].y * p.y) + 0.5 * (sg.x * rho.x + sg.y * rho.y);
+                        e_k.add(o.w[k] * mult * term);
+                    }
                 }
-                const double2 p = ld_stream(o.P + base + rj);
-                const double2 rho = o.refP ? csub(p, ld_stream(o.refP + base + rj)) : p;
-                const double term = (hh.x * p.x + hh.y * p.y) + 0.5 * (sg.x * rho.x + sg.y * rho.y);
-                e_k.add(o.w[k] * mult * term);
             }
         }
         __syncthreads();
