@@ -230,15 +230,16 @@ __global__ void __launch_bounds__(kThreads) k_rot_grad(const double2* __restrict
 // the reference's sequential decisions (accept tau_a on a strict decrease of
 // the frozen free energy, else try tau_b, else shrink on), so the result is
 // that of one pass per trial.  diag(U^H Ft U) goes to ew (tau_a) and ew2
-// (tau_b); S->slot records which one the accepted trial left.  `bt` is the
-// index of the pass's first trial; a pair past bt_max evaluates one trial.
+// (tau_b), U(tau_a) to Ua and U(tau_b) to Ub; S->slot records which one the
+// accepted trial left.  `bt` is the index of the pass's first trial; a pair
+// past bt_max evaluates one trial.
 // Dynamic shared memory: sD (d, then U(tau_a)) | sF | sB (U(tau_b)), TILE double2 each.
 template <int NB>
 __global__ void __launch_bounds__(kThreads, 3)
     k_trial2_small(const double2* __restrict__ dQ, const double2* __restrict__ Ft, const double* __restrict__ p,
                    const double* __restrict__ d_p, const double* __restrict__ w, double* __restrict__ ew,
-                   double* __restrict__ ew2, int64_t nk, double T_r, double shrink, int bt, int bt_max,
-                   double fallback, DmScalars* S) {
+                   double* __restrict__ ew2, double2* __restrict__ Ua, double2* __restrict__ Ub, int64_t nk,
+                   double T_r, double shrink, int bt, int bt_max, double fallback, DmScalars* S) {
     if (S->accepted) return;  // grid-uniform
     using G = Geo<NB>;
     extern __shared__ __align__(16) double2 dyn[];
@@ -302,6 +303,10 @@ __global__ void __launch_bounds__(kThreads, 3)
             }
         }
         __syncthreads();
+        // both factors go out, so that the retraction reads the accepted one
+        tile_store<NB>(Ua + (size_t)k0 * G::NB2, sA, nkt);
+        if (two) tile_store<NB>(Ub + (size_t)k0 * G::NB2, sB, nkt);
+        __syncthreads();
     }
     double out[4];
     if (reduce_last_block<4>(v, S->part, &S->counter, out, red) && threadIdx.x == 0) {
@@ -329,14 +334,17 @@ __global__ void __launch_bounds__(kThreads, 3)
     }
 }
 
-// Retraction Q <- Q U(tau_final), U recomputed from d by elimination, and
-// eps_work = diag(U^H Ft U): the accepted trial's (copied from ew2 when it was
-// the second of its pass) or, for the fallback step, computed here.
+// Retraction Q <- Q U(tau_final) and eps_work = diag(U^H Ft U).  After an
+// accepted trial, U is the one its pass stored (Ua or Ub) and eps_work its
+// diagonal (copied from ew2 when it was the second of its pass); for the
+// fallback step both are computed here, U from d by elimination.
 // Dynamic shared memory: sD (d, then U) | sF | sQ, TILE double2 each.
 template <int NB>
 __global__ void __launch_bounds__(kThreads) k_retract_small(double2* Q, const double2* __restrict__ dQ,
                                                             const double2* __restrict__ Ft, double* __restrict__ ew,
-                                                            const double* __restrict__ ew2, int64_t nk,
+                                                            const double* __restrict__ ew2,
+                                                            const double2* __restrict__ Ua,
+                                                            const double2* __restrict__ Ub, int64_t nk,
                                                             const DmScalars* S) {
     using G = Geo<NB>;
     extern __shared__ __align__(16) double2 dyn[];
@@ -348,20 +356,25 @@ __global__ void __launch_bounds__(kThreads) k_retract_small(double2* Q, const do
     const int grp = threadIdx.x / G::GS, r = threadIdx.x % G::GS;
     const unsigned mask = group_mask<NB>(threadIdx.x & 31);
     const double tau = S->tau_final;
-    const bool need_diag = S->accepted == 0;                // grid-uniform
+    const bool need_diag = S->accepted == 0;                // grid-uniform: the fallback step
     const bool from_b = S->accepted != 0 && S->slot == 1;  // grid-uniform
+    const double2* Uacc = from_b ? Ub : Ua;
     const int64_t ntiles = (nk + G::KT - 1) / G::KT;
     for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int64_t k0 = t * G::KT;
         const int nkt = (int)((nk - k0) < G::KT ? (nk - k0) : G::KT);
-        tile_load<NB>(sD, dQ + (size_t)k0 * G::NB2, nkt);
-        if (need_diag) tile_load<NB>(sF, Ft + (size_t)k0 * G::NB2, nkt);
+        if (need_diag) {
+            tile_load<NB>(sD, dQ + (size_t)k0 * G::NB2, nkt);
+            tile_load<NB>(sF, Ft + (size_t)k0 * G::NB2, nkt);
+        } else {
+            tile_load<NB>(sU, Uacc + (size_t)k0 * G::NB2, nkt);
+        }
         tile_load<NB>(sQ, Q + (size_t)k0 * G::NB2, nkt);
         __syncthreads();
         const bool live = grp < nkt && r < NB;
         const int rr = r < NB ? r : 0;
         const int64_t k = k0 + grp;
-        if (grp < nkt) {
+        if (need_diag && grp < nkt) {
             double2 u[NB];
             row_cayley<NB, G::LD>(sD + grp * G::MS, tau, rr, sPiv + grp * 4 * NB, u, mask);
             // (the elimination ends with a group barrier after its last read of d)
@@ -408,6 +421,7 @@ __global__ void __launch_bounds__(kThreads) k_retract_small(double2* Q, const do
 // flight (these kernels are bound by load latency).  The preconditioner
 // 1 / sqrt(gap^2 + lambda^2) is one reciprocal square root per element.
 constexpr int kThreadsE = 256;
+constexpr int kUnrollE = 4;  // elements a thread has in flight in the element loops
 
 // PR+ numerator / denominator -> beta (solver_dm.hpp:513-559)
 template <int NB>
@@ -423,18 +437,30 @@ __global__ void __launch_bounds__(kThreadsE, 4) k_pr_beta_small(const double2* _
     const int64_t nrow = nk * NB, nel = nrow * NB;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    // matrix terms, one element per thread (coalesced)
-    for (int64_t e = tid; e < nel; e += stride) {
+    // matrix terms, one element per thread (coalesced), kUnrollE elements of a
+    // thread loaded before any is used
+    auto term = [&](int64_t e, double2 g, double2 gp) {
         const int64_t row = e / NB, k = row / NB;
         const int j = (int)(e - row * NB);
-        const double2 g = Gc[e], gp = Gp[e];
         const double gap = eps[row] - eps[k * NB + j];
         const double rb = rsqrt(gap * gap + lam2);
         const double2 d = mk(g.x * rb, g.y * rb);
         const double wk = w[k];
         v[0] += wk * ((g.x * d.x + g.y * d.y) - (gp.x * d.x + gp.y * d.y));
         v[1] += wk * (gp.x * gp.x + gp.y * gp.y);
+    };
+    int64_t e = tid;
+    for (; e + (kUnrollE - 1) * stride < nel; e += kUnrollE * stride) {
+        double2 g[kUnrollE], gp[kUnrollE];
+#pragma unroll
+        for (int u = 0; u < kUnrollE; ++u) {
+            g[u] = Gc[e + u * stride];
+            gp[u] = Gp[e + u * stride];
+        }
+#pragma unroll
+        for (int u = 0; u < kUnrollE; ++u) term(e + u * stride, g[u], gp[u]);
     }
+    for (; e < nel; e += stride) term(e, Gc[e], Gp[e]);
     // occupation terms, one row per thread
     for (int64_t row = tid; row < nrow; row += stride) {
         const double wk = w[row / NB];
@@ -476,18 +502,30 @@ __global__ void __launch_bounds__(kThreadsE, 4) k_direction_small(const double2*
     const int64_t nrow = nk * NB, nel = nrow * NB;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    // matrix terms, one element per thread (coalesced)
-    for (int64_t e = tid; e < nel; e += stride) {
+    // matrix terms, one element per thread (coalesced), kUnrollE elements of a
+    // thread loaded before any is used
+    auto term = [&](int64_t e, double2 g, double2 q) {
         const int64_t row = e / NB, k = row / NB;
         const int j = (int)(e - row * NB);
-        const double2 g = Gc[e];
-        const double2 q = beta != 0.0 ? dQp[e] : mk(0.0, 0.0);
         const double gap = eps[row] - eps[k * NB + j];
         const double rb = rsqrt(gap * gap + lam2);
         const double2 d = mk(g.x * rb + beta * q.x, g.y * rb + beta * q.y);
         dQ[e] = d;
         v[0] += w[k] * (d.x * d.x + d.y * d.y);
+    };
+    const bool use_prev = beta != 0.0;
+    int64_t e = tid;
+    for (; e + (kUnrollE - 1) * stride < nel; e += kUnrollE * stride) {
+        double2 g[kUnrollE], q[kUnrollE];
+#pragma unroll
+        for (int u = 0; u < kUnrollE; ++u) {
+            g[u] = Gc[e + u * stride];
+            q[u] = use_prev ? dQp[e + u * stride] : mk(0.0, 0.0);
+        }
+#pragma unroll
+        for (int u = 0; u < kUnrollE; ++u) term(e + u * stride, g[u], q[u]);
     }
+    for (; e < nel; e += stride) term(e, Gc[e], use_prev ? dQp[e] : mk(0.0, 0.0));
     // occupation terms, one row per thread
     for (int64_t row = tid; row < nrow; row += stride) {
         const double wk = w[row / NB];
@@ -509,9 +547,11 @@ __global__ void __launch_bounds__(kThreadsE, 4) k_direction_small(const double2*
     }
 }
 
+// One resident wave of the element kernels (four 256-thread CTAs per SM), or
+// fewer CTAs when the rows do not fill it.
 unsigned rows_grid(int64_t nrow) {
     const int64_t want = (nrow + kThreadsE - 1) / kThreadsE;
-    return (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, std::min<int64_t>(kDmMaxPartials, 8 * num_sms())));
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, std::min<int64_t>(kDmMaxPartials, 4 * num_sms())));
 }
 
 // ---------------------------------------------------------------------------
@@ -693,25 +733,25 @@ int dm_small_direction(const double2* Gc, const double2* dQp, const double* g_p,
 }
 
 int dm_small_trial2(const double2* dQ, const double2* Ft, const double* p, const double* d_p, const double* w,
-                    double* ew, double* ew2, int64_t nk, int nb, double T_r, double shrink, int bt, int bt_max,
-                    double fallback, DmScalars* S, cudaStream_t st) {
-#define X(N)                                                                                            \
-    small_attrs<N>();                                                                                   \
-    k_trial2_small<N><<<tiles_grid(nk, Geo<N>::KT, 3 * kDmMaxPartials / 4), kThreads,                   \
-                        3 * sizeof(double2) * Geo<N>::TILE, st>>>(dQ, Ft, p, d_p, w, ew, ew2, nk, T_r, shrink, \
-                                                                 bt, bt_max, fallback, S);               \
+                    double* ew, double* ew2, double2* Ua, double2* Ub, int64_t nk, int nb, double T_r, double shrink,
+                    int bt, int bt_max, double fallback, DmScalars* S, cudaStream_t st) {
+#define X(N)                                                                                                  \
+    small_attrs<N>();                                                                                         \
+    k_trial2_small<N><<<tiles_grid(nk, Geo<N>::KT, 3 * kDmMaxPartials / 4), kThreads,                         \
+                        3 * sizeof(double2) * Geo<N>::TILE, st>>>(dQ, Ft, p, d_p, w, ew, ew2, Ua, Ub, nk, T_r, \
+                                                                 shrink, bt, bt_max, fallback, S);             \
     CPPHF_LAUNCH_CHECK("trial pair");
     SMALL_DISPATCH(nb, X)
 #undef X
     return CPPHF_OK;
 }
 
-int dm_small_retract(double2* Q, const double2* dQ, const double2* Ft, double* ew, const double* ew2, int64_t nk,
-                     int nb, const DmScalars* S, cudaStream_t st) {
+int dm_small_retract(double2* Q, const double2* dQ, const double2* Ft, double* ew, const double* ew2,
+                     const double2* Ua, const double2* Ub, int64_t nk, int nb, const DmScalars* S, cudaStream_t st) {
 #define X(N)                                                                                                      \
     small_attrs<N>();                                                                                             \
     k_retract_small<N><<<tiles_grid(nk, Geo<N>::KT, 16 * num_sms()), kThreads, 3 * sizeof(double2) * Geo<N>::TILE, \
-                         st>>>(Q, dQ, Ft, ew, ew2, nk, S);                                                        \
+                         st>>>(Q, dQ, Ft, ew, ew2, Ua, Ub, nk, S);                                                \
     CPPHF_LAUNCH_CHECK("retract");
     SMALL_DISPATCH(nb, X)
 #undef X

@@ -23,13 +23,15 @@ int dm_small_direction(const double2* Gc, const double2* dQp, const double* g_p,
                        const double* p, const double* w, double2* dQ, double* d_p, int64_t nk, int nb, double T_r,
                        double max_step, DmScalars* S, cudaStream_t st);
 // Two consecutive line-search trials (bt, bt + 1 < bt_max) in one pass;
-// diag(U^H Ft U) of the first to ew, of the second to ew2.
+// diag(U^H Ft U) of the first to ew, of the second to ew2, the factors U to
+// Ua and Ub (full fields).
 int dm_small_trial2(const double2* dQ, const double2* Ft, const double* p, const double* d_p, const double* w,
-                    double* ew, double* ew2, int64_t nk, int nb, double T_r, double shrink, int bt, int bt_max,
-                    double fallback, DmScalars* S, cudaStream_t st);
-// Q <- Q U(tau_final) (U recomputed by elimination); eps_work of the accepted
-// trial in ew (taken from ew2 when that holds it), or computed for the fallback.
-int dm_small_retract(double2* Q, const double2* dQ, const double2* Ft, double* ew, const double* ew2, int64_t nk,
-                     int nb, const DmScalars* S, cudaStream_t st);
+                    double* ew, double* ew2, double2* Ua, double2* Ub, int64_t nk, int nb, double T_r, double shrink,
+                    int bt, int bt_max, double fallback, DmScalars* S, cudaStream_t st);
+// Q <- Q U(tau_final): U of the accepted trial read from Ua / Ub and its
+// eps_work left in ew (taken from ew2 when that holds it); for the fallback
+// step U (by elimination) and eps_work are computed here.
+int dm_small_retract(double2* Q, const double2* dQ, const double2* Ft, double* ew, const double* ew2,
+                     const double2* Ua, const double2* Ub, int64_t nk, int nb, const DmScalars* S, cudaStream_t st);
 
 }  // namespace cpphf

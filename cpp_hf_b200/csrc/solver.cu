@@ -630,9 +630,12 @@ int solve_dm(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* P
         // small nb, two trials per pass; otherwise one pass per trial; a pass
         // after the accepted trial returns at once
         if (small) {
+            // the factors U go to G[prv] and dQ[prv], which this iteration no
+            // longer reads (PR+ and the direction are done; the next iteration
+            // writes both before reading them)
             for (int64_t bt = 0; bt < cfg->bt_max; bt += 2)
-                CPPHF_TRY(dm_small_trial2(dQ[cur], F, p, dp[cur], wn, ew, ew2, nk, nb, T_r, cfg->bt_shrink, (int)bt,
-                                          (int)cfg->bt_max, fallback, S, st));
+                CPPHF_TRY(dm_small_trial2(dQ[cur], F, p, dp[cur], wn, ew, ew2, G[prv], dQ[prv], nk, nb, T_r,
+                                          cfg->bt_shrink, (int)bt, (int)cfg->bt_max, fallback, S, st));
         } else {
             for (int64_t bt = 0; bt < cfg->bt_max; ++bt)
                 CPPHF_TRY(dm_trial_lu(dQ[cur], F, p, dp[cur], wn, nk, nb, T_r, cfg->bt_shrink,
@@ -640,7 +643,7 @@ int solve_dm(const cpphf_kernel* K, const cpphf_dm_config* cfg, const double2* P
         }
         // 6. retraction and mu (occupations are formed by the next density step)
         if (small)
-            CPPHF_TRY(dm_small_retract(Q, dQ[cur], F, ew, ew2, nk, nb, S, st));
+            CPPHF_TRY(dm_small_retract(Q, dQ[cur], F, ew, ew2, G[prv], dQ[prv], nk, nb, S, st));
         else
             CPPHF_TRY(dm_retract_lu(Q, dQ[cur], F, ew, nk, nb, S, st));
         CPPHF_TRY(mu_solve(ew, wn, nk, nb, n_t, &S->mu, T_r, mu_it, 1, &S->mu, mws, L.mu_bytes, st));

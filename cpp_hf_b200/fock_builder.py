@@ -7,6 +7,7 @@ the kernel on the device instead:
 
     fb = FockBuilder(kernel_args)              # one upload
     Sigma, F, E = fb.build(P)                  # P: CUDA tensor (no copies) ...
+    F, E = fb.build_fe(P)                      # ... F and E only, as the solvers build ...
     F_host, E = fb.build_host(P_pinned)        # ... or pinned host memory
 
 A stream of builds from host memory (many densities, results read back each
@@ -75,8 +76,16 @@ class FockBuilder:
                                         _stream()), "build_fock")
         return self.Sigma, self.F, self.E
 
+    def build_fe(self, P: torch.Tensor):
+        """Fock build as the solvers run it: F and E only.  On the packed path the
+        exchange field is then never written out (the full path still needs it as
+        the assembly's input)."""
+        self._build_into(P, self.F, self.E)
+        return self.F, self.E
+
     def _build_into(self, P: torch.Tensor, F: torch.Tensor, E: torch.Tensor):
-        check(self.lib.cpphf_build_fock(C.byref(self.dk.K), _ptr(P), _ptr(self.Sigma), _ptr(F), _ptr(self.hd),
+        sig = None if self.packed else _ptr(self.Sigma)
+        check(self.lib.cpphf_build_fock(C.byref(self.dk.K), _ptr(P), sig, _ptr(F), _ptr(self.hd),
                                         _ptr(E), None, _ptr(self.ws), self.ws.numel(), _stream()), "build_fock")
 
     def begin_host_pipeline(self):
@@ -135,7 +144,7 @@ class FockBuilder:
     def build_host(self, P_host: torch.Tensor, F_host: torch.Tensor, E_host: torch.Tensor):
         """End-to-end build from host memory: H2D of P, build, D2H of F and E (async on the stream)."""
         self.P_dev.copy_(P_host, non_blocking=True)
-        self.build(self.P_dev)
+        self.build_fe(self.P_dev)
         F_host.copy_(self.F, non_blocking=True)
         E_host.copy_(self.E, non_blocking=True)
         return F_host, E_host

@@ -2,7 +2,7 @@
 next call runs normally.
 
 The grid barriers of the cooperative chemical-potential kernel poll a counter
-at most ``cpphf_set_barrier_spin_limit`` times.  (Problems of up to 2^19
+at most ``cpphf_set_barrier_spin_limit`` times.  (Problems of up to 2^16
 eigenvalues run as one thread-block cluster with hardware barriers instead, so
 the cases below are larger.)  With a limit of one poll, the first blocks to
 reach a barrier give up before the slower ones arrive (the problems below need

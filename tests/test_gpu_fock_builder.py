@@ -45,3 +45,25 @@ def test_fock_builder_host_paths_match_build_fock_apply(native, oracle):
     np.testing.assert_allclose(F_out[0].numpy(), o[2], rtol=0, atol=1e-11 * np.max(np.abs(o[2])))
     assert abs(float(E_out[0][0]) - float(o[3])) < 1e-10 * max(1.0, abs(float(o[3])))
     del rng
+
+
+def test_packed_builder_fe_matches_build_and_drop_in(native):
+    """build_fe (F and E only, no exchange field written on the packed path) gives
+    the same F and E as build() and as the drop-in call with hermitian_density."""
+    import torch
+
+    from cpp_hf_b200.fock_builder import FockBuilder
+
+    args, _P0, _ne = workloads.layered(24, seed=4)
+    P = workloads.random_hermitian_density(24, 8, seed=2)
+    P = 0.5 * (P + np.conj(np.swapaxes(P, -1, -2)))
+    fb = FockBuilder(args, hermitian_density=True)
+    assert fb.packed
+    Pd = torch.from_numpy(P).cuda()
+    _S, F0, E0 = [x.clone() for x in fb.build(Pd)]
+    F1, E1 = fb.build_fe(Pd)
+    torch.cuda.synchronize()
+    assert torch.equal(F0, F1) and float(E0) == float(E1)
+    r = native.build_fock_apply(dict(args, hermitian_density=True), P, None)
+    np.testing.assert_array_equal(F1.cpu().numpy(), r[2])
+    assert float(E1) == float(r[3])

@@ -11,11 +11,21 @@ they reconstruct; solver trajectories through their energies, densities and
 Fock matrices, with iteration counts allowed to differ by a few steps where
 the recorded run sits near a branch of the reference's control flow (the
 Newton and deflation tests drive deliberately stiff problems).
+
+Some recorded solves are not determined by the reference's arithmetic: the
+in-loop chemical-potential update (utils.hpp:79-116) moves its bracket on the
+sign of a residual that is at the rounding level once Newton has converged,
+and then bisects from the bracket's midpoint, so the trajectory changes with
+the summation order of N(mu).  ``reference_calls_sensitive.json`` (made by
+``tests/golden/make_reference_sensitivity.py``) lists the solves whose oracle
+result changes when those sums are exact, with both results; the GPU (whose
+chemical-potential sums are compensated) must then match one of the two.
 """
 
 from __future__ import annotations
 
 import gzip
+import json
 import pickle
 
 import numpy as np
@@ -27,6 +37,8 @@ pytestmark = pytest.mark.gpu
 
 _DATA = GOLDEN / "reference_calls.pkl.gz"
 CALLS = pickle.load(gzip.open(_DATA))["calls"] if _DATA.exists() else []
+_SENS = GOLDEN / "reference_calls_sensitive.json"
+SENSITIVE = json.loads(_SENS.read_text())["calls"] if _SENS.exists() else {}
 
 
 def _rel(a, b):
@@ -37,6 +49,19 @@ def _rel(a, b):
 
 def _recon(V, w):
     return (V * np.asarray(w)[..., None, :]) @ np.conj(np.swapaxes(V, -1, -2))
+
+
+def _iters_close(it, itr):
+    return abs(it - itr) <= max(2, int(0.05 * itr))
+
+
+def _check_sensitive(name, got, sens):
+    """A solve the reference's arithmetic leaves open: converged, and the GPU's
+    (iterations, energy) those of the recorded run or of the exact-sum run."""
+    it, E, conv = (got[6], got[5], got[7]) if name == "solve_dm" else (got[4], got[2], got[5])
+    assert conv
+    runs = list(zip(sens["iterations"], sens["energy"]))
+    assert any(_iters_close(it, i) and abs(E - e) < 1e-8 * max(1.0, abs(e)) for i, e in runs), (it, E, runs)
 
 
 def _check(name, got, ref):
@@ -63,7 +88,7 @@ def _check(name, got, ref):
         Q, p, D, F, mu, E, it, conv, hE, hG = got
         Qr, pr, Dr, Fr, mur, Er, itr, convr, hEr, hGr = ref
         assert conv == convr
-        assert abs(it - itr) <= max(2, int(0.05 * itr)), (it, itr)
+        assert _iters_close(it, itr), (it, itr)
         assert abs(E - Er) < 1e-8 * max(1.0, abs(Er)), (E, Er)
         if Dr is not None:
             assert _rel(D, Dr) < 1e-6
@@ -73,7 +98,7 @@ def _check(name, got, ref):
         D, F, E, mu, it, conv, hE, hD, hC = got
         Dr, Fr, Er, mur, itr, convr, hEr, hDr, hCr = ref
         assert conv == convr
-        assert abs(it - itr) <= max(2, int(0.05 * itr)), (it, itr)
+        assert _iters_close(it, itr), (it, itr)
         assert abs(E - Er) < 1e-8 * max(1.0, abs(Er)), (E, Er)
         if Dr is not None:
             assert _rel(D, Dr) < 1e-6
@@ -99,4 +124,7 @@ def test_fixture_covers_the_reference_suite():
 def test_reference_call_replays_on_gpu(native, idx):
     c = CALLS[idx]
     got = getattr(native, c["name"])(*c["args"], **c["kwargs"])
-    _check(c["name"], got, c["result"])
+    if str(idx) in SENSITIVE:
+        _check_sensitive(c["name"], got, SENSITIVE[str(idx)])
+    else:
+        _check(c["name"], got, c["result"])
