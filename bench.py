@@ -384,7 +384,8 @@ def main():
     lib = _lib.load()
     args, _P0, _ne = workloads.layered(a.n, n_layers=N_LAYERS, seed=rank)
     P_host_np = workloads.random_hermitian_density(a.n, 2 * N_LAYERS, seed=1 + rank)
-    P_host_np = 0.5 * (P_host_np + np.conj(np.swapaxes(P_host_np, -1, -2)))  # exactly Hermitian blocks
+    # exactly Hermitian blocks, C order (the sum with a transposed view is not)
+    P_host_np = np.ascontiguousarray(0.5 * (P_host_np + np.conj(np.swapaxes(P_host_np, -1, -2))))
     fb = FockBuilder(args, precision=64, hermitian_density=True)
     if not fb.packed:
         raise RuntimeError("the layered workload should take the Hermitian-packed build")

@@ -139,33 +139,6 @@ struct Kahan {
 };
 
 // ---------------------------------------------------------------------------
-// Double-double (compensated) sums.  A value is a pair (hi, lo) with
-// |lo| <= ulp(hi) / 2; dd_acc adds one double and dd_add adds another pair,
-// each with an error-free TwoSum (Knuth), so a sum of n terms carries about
-// n 2^-106 relative error instead of n 2^-53, and hi is the sum rounded once.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
-    s = a + b;
-    const double bb = s - a;
-    e = (a - (s - bb)) + (b - bb);
-}
-__device__ __forceinline__ void dd_acc(double& hi, double& lo, double x) {
-    double s, e;
-    two_sum(hi, x, s, e);
-    hi = s;
-    lo += e;
-}
-// (hi, lo) += (bhi, blo); the result does not depend on which operand is which
-// only up to the rounding of lo, so callers fix the operand order
-__device__ __forceinline__ void dd_add(double& hi, double& lo, double bhi, double blo) {
-    double s, e;
-    two_sum(hi, bhi, s, e);
-    e += lo + blo;
-    hi = s + e;
-    lo = e - (hi - s);
-}
-
-// ---------------------------------------------------------------------------
 // Warp / block reductions (fixed order -> deterministic)
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double warp_sum(double v) {
@@ -203,47 +176,6 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double (&scratch)[M])
     for (int i = 0; i < NV; ++i) {
         double s = (lane < nw) ? scratch[i * 32 + lane] : 0.0;
         v[i] = warp_sum(s);
-    }
-    __syncthreads();
-}
-
-// Compensated block sum of NV double-double values (see dd_add); the lower
-// lane's / warp's value is always the first operand, so every thread ends with
-// the same pair.  `scratch` holds at least 64*NV doubles.
-template <int NV, int M>
-__device__ __forceinline__ void block_sum_dd(double (&hi)[NV], double (&lo)[NV], double (&scratch)[M]) {
-    static_assert(M >= 64 * NV, "block_sum_dd scratch needs 64 doubles per value");
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-    auto warp_dd = [&](double& h, double& l) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const double oh = __shfl_xor_sync(0xffffffffu, h, o), ol = __shfl_xor_sync(0xffffffffu, l, o);
-            if (lane & o) {  // the partner is the lower lane: it goes first
-                double ah = oh, al = ol;
-                dd_add(ah, al, h, l);
-                h = ah;
-                l = al;
-            } else {
-                dd_add(h, l, oh, ol);
-            }
-        }
-    };
-#pragma unroll
-    for (int i = 0; i < NV; ++i) warp_dd(hi[i], lo[i]);
-    __syncthreads();
-    if (lane == 0) {
-#pragma unroll
-        for (int i = 0; i < NV; ++i) {
-            scratch[i * 64 + wid] = hi[i];
-            scratch[i * 64 + 32 + wid] = lo[i];
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < NV; ++i) {
-        hi[i] = (lane < nw) ? scratch[i * 64 + lane] : 0.0;
-        lo[i] = (lane < nw) ? scratch[i * 64 + 32 + lane] : 0.0;
-        warp_dd(hi[i], lo[i]);
     }
     __syncthreads();
 }
@@ -328,17 +260,6 @@ struct GridBarrier {
     // release/acquire atomics (no full fences).
     template <int NV = 2>
     __device__ bool wait_reduce(const double* part, int nblocks, double* tot) {
-        return wait_reduce_impl<NV, false>(part, nblocks, tot);
-    }
-    // The same with double-double partials (block b's NV high parts at
-    // part[2 NV b ..], its NV low parts after them) summed with compensation;
-    // the NV totals written are the high parts (the sums rounded once).
-    template <int NV = 2>
-    __device__ bool wait_reduce_dd(const double* part, int nblocks, double* tot) {
-        return wait_reduce_impl<NV, true>(part, nblocks, tot);
-    }
-    template <int NV, bool DD>
-    __device__ bool wait_reduce_impl(const double* part, int nblocks, double* tot) {
         __syncthreads();
         __shared__ int ok_sh, last_sh;
         if (threadIdx.x == 0) {
@@ -357,27 +278,15 @@ struct GridBarrier {
         if (last_sh) {
             // the whole block loads the partials at once (one L2 round trip for
             // up to blockDim blocks) and sums them with a fixed tree
-            __shared__ double red_wr[64 * NV];
+            __shared__ double red_wr[32 * NV];
             double sv[NV];
 #pragma unroll
             for (int v = 0; v < NV; ++v) sv[v] = 0.0;
-            if constexpr (DD) {
-                double sl[NV];
+            for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
 #pragma unroll
-                for (int v = 0; v < NV; ++v) sl[v] = 0.0;
-                for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
-#pragma unroll
-                    for (int v = 0; v < NV; ++v)
-                        dd_add(sv[v], sl[v], __ldcg(&part[2 * NV * b + v]), __ldcg(&part[2 * NV * b + NV + v]));
-                }
-                block_sum_dd<NV>(sv, sl, red_wr);
-            } else {
-                for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
-#pragma unroll
-                    for (int v = 0; v < NV; ++v) sv[v] += __ldcg(&part[NV * b + v]);
-                }
-                block_sum<NV>(sv, red_wr);
+                for (int v = 0; v < NV; ++v) sv[v] += __ldcg(&part[NV * b + v]);
             }
+            block_sum<NV>(sv, red_wr);
             if (threadIdx.x == 0) {
 #pragma unroll
                 for (int v = 0; v < NV; ++v) __stcg(&tot[v], sv[v]);

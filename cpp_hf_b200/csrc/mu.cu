@@ -14,13 +14,6 @@
 // counts instead of one per level.  Newton stops early only once its state
 // (mu, lo, hi) repeats with period 1 or 2, when the state after the remaining
 // iterations is already known.
-//
-// The sums N(mu) and dN/dmu are double-double (compensated) at every level:
-// per thread, per block and across blocks, so each is the exact sum of its
-// terms rounded once.  The reference's update rule branches on the sign of
-// N(mu) - n_e, which after convergence is at the rounding level; with the sums
-// rounded once, that sign is the one exact summation gives, independent of
-// the grid's summation order.
 #include "common.cuh"
 #include "mu.cuh"
 
@@ -117,26 +110,23 @@ struct MuSync {
     }
     // the partials buffer of a round
     __device__ double* partials(double* part, int round) const {
-        if constexpr (CLUSTER) return part + (size_t)(round & 1) * 2 * kMuNV * gridDim.x;
+        if constexpr (CLUSTER) return part + (size_t)(round & 1) * kMuNV * gridDim.x;
         return part;
     }
-    // every block's NV double-double partials (block b: NV high parts at
-    // part[2 NV b], NV low parts after them) summed with compensation in a fixed
-    // order; the totals are the rounded sums.  Null if a wait gave up.
+    // every block's NV partials summed (fixed order); null if a wait gave up
     template <int NV>
     __device__ const double* reduce(const double* part, int G, double* tot) {
         if constexpr (CLUSTER) {
             cluster_sync_all();
             if (threadIdx.x < NV) {
-                double h = 0.0, l = 0.0;
-                for (int b = 0; b < G; ++b)
-                    dd_add(h, l, __ldcg(&part[2 * NV * b + threadIdx.x]), __ldcg(&part[2 * NV * b + NV + threadIdx.x]));
-                ctot[threadIdx.x] = h;
+                double s = 0.0;
+                for (int b = 0; b < G; ++b) s += __ldcg(&part[NV * b + threadIdx.x]);
+                ctot[threadIdx.x] = s;
             }
             __syncthreads();
             return ctot;
         } else {
-            return bar.template wait_reduce_dd<NV>(part, G, tot) ? tot : nullptr;
+            return bar.wait_reduce<NV>(part, G, tot) ? tot : nullptr;
         }
     }
     __device__ double load(const double* t, int j) const {
@@ -147,7 +137,7 @@ struct MuSync {
 
 template <bool CLUSTER>
 __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
-    __shared__ double red[64 * kMuNV];  // block_sum_dd<kMuNV> scratch (64 doubles per value)
+    __shared__ double red[32 * kMuNV];  // block_sum<kMuNV> scratch (32 doubles per value)
     __shared__ double ctot_sh[kMuNV];
     MuSync<CLUSTER> bar;
     bar.init(a, ctot_sh);
@@ -220,20 +210,9 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
     }
     const double Tfd = Tj + 1.0e-12;  // fermidirac_scalar(x, Tj) = expit(-x / (Tj + 1e-12))
     const double invTfd = 1.0 / Tfd, invTj = 1.0 / Tj;
-    // [G][2 kMuNV] double-double partials (two such buffers in the cluster form)
-    double* part0 = a.part + 2 * G;
-    double* tots = part0 + (size_t)2 * kMuNV * G * (CLUSTER ? 2 : 1);  // [2][kMuNV] totals, by round parity
+    double* part0 = a.part + 2 * G;                 // [G][kMuNV] partials (two such buffers in the cluster form)
+    double* tots = part0 + (size_t)kMuNV * G * (CLUSTER ? 2 : 1);  // [2][kMuNV] totals, by round parity
     __shared__ double bc_tot[kMuNV];
-    // a block's two double-double sums into its partials slot (highs, then lows)
-    auto store_dd2 = [&](double (&h)[2], double (&l)[2], double* part) {
-        block_sum_dd<2>(h, l, red);
-        if (threadIdx.x == 0) {
-            __stcg(&part[4 * blockIdx.x], h[0]);
-            __stcg(&part[4 * blockIdx.x + 1], h[1]);
-            __stcg(&part[4 * blockIdx.x + 2], l[0]);
-            __stcg(&part[4 * blockIdx.x + 3], l[1]);
-        }
-    };
     int round = 0;
     if (a.mode == 0) {
         // Bisection (utils.hpp:49-75) in three phases.
@@ -274,9 +253,9 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
                     mid[j] = 0.0;
                 }
             }
-            double v[kMuNV], vl[kMuNV];
+            double v[kMuNV];
 #pragma unroll
-            for (int j = 0; j < kMuNV; ++j) v[j] = vl[j] = 0.0;
+            for (int j = 0; j < kMuNV; ++j) v[j] = 0.0;
             for (unsigned i = e0 + threadIdx.x; i < e1; i += blockDim.x) {
                 double wk, e;
                 band_major(a, i, nb, wk, e);
@@ -287,20 +266,17 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
                         // and below 2e-22 wk (dropped) for x <= -50
                         const double xa = (mid[j] - e) * invTfd;
                         if (xa >= kFdOne)
-                            dd_acc(v[j], vl[j], wk);
+                            v[j] += wk;
                         else if (xa > kFdZero)
-                            dd_acc(v[j], vl[j], wk * expit(-(e - mid[j]) / Tfd));
+                            v[j] += wk * expit(-(e - mid[j]) / Tfd);
                     }
                 }
             }
-            block_sum_dd<kMuNV>(v, vl, red);
+            block_sum<kMuNV>(v, red);
             double* part = bar.partials(part0, round);
             if (threadIdx.x == 0) {
 #pragma unroll
-                for (int j = 0; j < kMuNV; ++j) {
-                    __stcg(&part[2 * kMuNV * blockIdx.x + j], v[j]);
-                    __stcg(&part[2 * kMuNV * blockIdx.x + kMuNV + j], vl[j]);
-                }
+                for (int j = 0; j < kMuNV; ++j) __stcg(&part[kMuNV * blockIdx.x + j], v[j]);
             }
             const double* tot = bar.template reduce<kMuNV>(part, G, tots + (round & 1) * kMuNV);
             if (!tot) {
@@ -331,21 +307,25 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
         };
         // count N and slope Z = dN/dmu at one mu (one grid round)
         auto count_round = [&](double m, double& N, double& Z) {
-            double v[2] = {0.0, 0.0}, vl[2] = {0.0, 0.0};
+            double v[2] = {0.0, 0.0};
             for (unsigned i = e0 + threadIdx.x; i < e1; i += blockDim.x) {
                 double wk, e;
                 band_major(a, i, nb, wk, e);
                 const double xa = (m - e) * invTfd;
                 if (xa >= kFdOne) {
-                    dd_acc(v[0], vl[0], wk);
+                    v[0] += wk;
                 } else if (xa > kFdZero) {
                     const double pf = expit(-(e - m) / Tfd);
-                    dd_acc(v[0], vl[0], wk * pf);
-                    dd_acc(v[1], vl[1], wk * pf * (1.0 - pf) * invTfd);
+                    v[0] += wk * pf;
+                    v[1] += wk * pf * (1.0 - pf) * invTfd;
                 }
             }
+            block_sum<2>(v, red);
             double* part = bar.partials(part0, round);
-            store_dd2(v, vl, part);
+            if (threadIdx.x == 0) {
+                __stcg(&part[2 * blockIdx.x], v[0]);
+                __stcg(&part[2 * blockIdx.x + 1], v[1]);
+            }
             const double* tot = bar.template reduce<2>(part, G, tots + (round & 1) * kMuNV);
             ++round;
             if (!tot) {
@@ -445,7 +425,7 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
         // the full iteration count would end in.
         double mu1 = NAN, lo1 = NAN, hi1 = NAN;  // state one iteration back
         for (int it = 0; it < a.maxiter; ++it) {
-            double v[2] = {0.0, 0.0}, vl[2] = {0.0, 0.0};
+            double v[2] = {0.0, 0.0};
             for (unsigned i = e0 + threadIdx.x; i < e1; i += blockDim.x) {
                 double wk, e;
                 band_major(a, i, nb, wk, e);
@@ -453,15 +433,19 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
                 // for an argument >= 37; below -50 both terms are dropped
                 const double xa = (mu - e) * invTj;
                 if (xa >= kFdOne) {
-                    dd_acc(v[0], vl[0], wk);
+                    v[0] += wk;
                 } else if (xa > kFdZero) {
                     const double p = expit((mu - e) / Tj);
-                    dd_acc(v[0], vl[0], wk * p);
-                    dd_acc(v[1], vl[1], wk * p * (1.0 - p) / Tj);
+                    v[0] += wk * p;
+                    v[1] += wk * p * (1.0 - p) / Tj;
                 }
             }
+            block_sum<2>(v, red);
             double* part = bar.partials(part0, it);
-            store_dd2(v, vl, part);
+            if (threadIdx.x == 0) {
+                __stcg(&part[2 * blockIdx.x], v[0]);
+                __stcg(&part[2 * blockIdx.x + 1], v[1]);
+            }
             const double* tot = bar.template reduce<2>(part, G, tots + (it & 1) * kMuNV);
             if (!tot) {
                 if (blockIdx.x == 0 && threadIdx.x == 0) *a.mu_out = NAN;
@@ -517,13 +501,13 @@ int max_coop_grid() {
 // launches.  Every GPU that loads the library holds it until the process
 // exits; every call shares it.
 // ---------------------------------------------------------------------------
-constexpr size_t kMuNoAllocScratchBytes = 64 + sizeof(double) * ((2 + 2 * kMuNV) * (size_t)kMuMaxGrid + 2 * kMuNV);
+constexpr size_t kMuNoAllocScratchBytes = 64 + sizeof(double) * ((2 + kMuNV) * (size_t)kMuMaxGrid + 2 * kMuNV);
 static __device__ __align__(256) unsigned char g_mu_noalloc_scratch[kMuNoAllocScratchBytes];
 
 }  // namespace
 
 size_t mu_workspace_bytes(int64_t, int64_t) {
-    return 64 + sizeof(double) * ((2 + 2 * kMuNV) * (size_t)kMuMaxGrid + 2 * kMuNV);
+    return 64 + sizeof(double) * ((2 + kMuNV) * (size_t)kMuMaxGrid + 2 * kMuNV);
 }
 
 int mu_solve(const double* eps, const double* w, int64_t nk, int64_t nb, double target,

@@ -69,8 +69,14 @@ class FockBuilder:
             n += 3
         return n + pre
 
+    def _check_density(self, P: torch.Tensor):
+        if not (isinstance(P, torch.Tensor) and P.is_cuda and P.dtype == torch.complex128
+                and tuple(P.shape) == self.shape and P.is_contiguous()):
+            raise ValueError(f"P must be a C-contiguous complex128 CUDA tensor of shape {self.shape}")
+
     def build(self, P: torch.Tensor):
         """Fock build at a device density P (complex128, C-contiguous, kernel shape)."""
+        self._check_density(P)
         check(self.lib.cpphf_build_fock(C.byref(self.dk.K), _ptr(P), _ptr(self.Sigma), _ptr(self.F),
                                         _ptr(self.hd), _ptr(self.E), None, _ptr(self.ws), self.ws.numel(),
                                         _stream()), "build_fock")
@@ -80,6 +86,7 @@ class FockBuilder:
         """Fock build as the solvers run it: F and E only.  On the packed path the
         exchange field is then never written out (the full path still needs it as
         the assembly's input)."""
+        self._check_density(P)
         self._build_into(P, self.F, self.E)
         return self.F, self.E
 
@@ -108,6 +115,8 @@ class FockBuilder:
         stream, D2H of F and E on the copy-out stream (see the module docstring).
         Returns the CUDA event after which F_host and E_host hold the result."""
         pp = self._pipe
+        if not (P_host.is_contiguous() and tuple(P_host.shape) == self.shape):
+            raise ValueError(f"P_host must be a C-contiguous tensor of shape {self.shape}")
         b = pp["i"] & 1
         pp["i"] += 1
         cur = torch.cuda.current_stream()

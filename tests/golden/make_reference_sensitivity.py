@@ -15,9 +15,11 @@ This script re-runs every recorded ``solve_dm`` / ``solve_scf`` call of
 ``reference_calls.pkl.gz`` through the oracle with the chemical-potential
 sums taken exactly (``math.fsum``) instead of NumPy's pairwise order, and
 writes ``reference_calls_sensitive.json``: the calls whose iteration count or
-energy changes, with both results.  The GPU replay compares those calls at
-the spread the reference's arithmetic itself leaves (see
-``tests/test_gpu_reference_calls.py``).
+energy changes, with both results and the amplitude of the runs' own energy
+oscillation after their first two iterations (a run that stops on the plateau
+test during an oscillation can stop anywhere within it).  The
+GPU replay compares those calls at the spread the reference's arithmetic itself
+leaves (see ``tests/test_gpu_reference_calls.py``).
 
     python tests/golden/make_reference_sensitivity.py
 """
@@ -75,24 +77,42 @@ def mu_inloop_exact(eps, w_norm, n_target_norm, mu0, T, maxiter=25):
     return mu
 
 
-def rerun_exact(call):
-    """The call through the oracle with exact chemical-potential sums: (iterations, energy)."""
+def _summary(name, r):
+    """(iterations, final energy, energy history) of a solver result tuple."""
+    if name == "solve_dm":
+        return int(r[6]), float(r[5]), np.asarray(r[8], dtype=np.float64)
+    return int(r[4]), float(r[2]), np.asarray(r[6], dtype=np.float64)
+
+
+def rerun_exact_full(call):
+    """The call through the oracle with exact chemical-potential sums."""
     orig = native_np._solve_mu_inloop
     native_np._solve_mu_inloop = mu_inloop_exact
     try:
         r = getattr(native_np, call["name"])(*call["args"], **call["kwargs"])
     finally:
         native_np._solve_mu_inloop = orig
-    if call["name"] == "solve_dm":
-        return int(r[6]), float(r[5])
-    return int(r[4]), float(r[2])
+    return _summary(call["name"], r)
+
+
+def rerun_exact(call):
+    """(iterations, energy) of the call through the oracle with exact chemical-potential sums."""
+    return rerun_exact_full(call)[:2]
 
 
 def recorded(call):
-    r = call["result"]
-    if call["name"] == "solve_dm":
-        return int(r[6]), float(r[5])
-    return int(r[4]), float(r[2])
+    """(iterations, energy) the recorded run returned."""
+    return _summary(call["name"], call["result"])[:2]
+
+
+def late_amplitude(e_final, *histories):
+    """The largest distance from the final energy that the runs' energies reach
+    after their first two iterations (the initial descent): how far the
+    reference's own trajectory oscillates on the input."""
+    late = [h[2:] for h in histories if len(h) > 2]
+    if not late:
+        return 0.0
+    return float(np.max(np.abs(np.concatenate(late) - e_final)))
 
 
 def main() -> int:
@@ -101,11 +121,14 @@ def main() -> int:
     for i, c in enumerate(calls):
         if c["name"] not in ("solve_dm", "solve_scf"):
             continue
-        it0, e0 = recorded(c)
-        it1, e1 = rerun_exact(c)
+        it0, e0, h0 = _summary(c["name"], c["result"])
+        it1, e1, h1 = rerun_exact_full(c)
         if it1 != it0 or abs(e1 - e0) > 1e-12 * max(1.0, abs(e0)):
-            out[str(i)] = {"name": c["name"], "test": c["test"], "iterations": [it0, it1], "energy": [e0, e1]}
-            print(f"{i:3d} {c['name']} {c['test']}: iterations {it0} -> {it1}, energy {e0!r} -> {e1!r}", flush=True)
+            amp = late_amplitude(e0, h0, h1)
+            out[str(i)] = {"name": c["name"], "test": c["test"], "iterations": [it0, it1], "energy": [e0, e1],
+                           "late_amplitude": amp}
+            print(f"{i:3d} {c['name']} {c['test']}: iterations {it0} -> {it1}, energy {e0!r} -> {e1!r}, "
+                  f"late oscillation {amp:.3e}", flush=True)
     (HERE / "reference_calls_sensitive.json").write_text(json.dumps(
         {"doc": "recorded solver calls whose oracle result changes when the chemical-potential sums are exact "
                 "(make_reference_sensitivity.py)", "calls": out}, indent=1) + "\n")

@@ -56,7 +56,7 @@ def test_packed_builder_fe_matches_build_and_drop_in(native):
 
     args, _P0, _ne = workloads.layered(24, seed=4)
     P = workloads.random_hermitian_density(24, 8, seed=2)
-    P = 0.5 * (P + np.conj(np.swapaxes(P, -1, -2)))
+    P = np.ascontiguousarray(0.5 * (P + np.conj(np.swapaxes(P, -1, -2))))
     fb = FockBuilder(args, hermitian_density=True)
     assert fb.packed
     Pd = torch.from_numpy(P).cuda()
@@ -67,3 +67,5 @@ def test_packed_builder_fe_matches_build_and_drop_in(native):
     r = native.build_fock_apply(dict(args, hermitian_density=True), P, None)
     np.testing.assert_array_equal(F1.cpu().numpy(), r[2])
     assert float(E1) == float(r[3])
+    with pytest.raises(ValueError):
+        fb.build_fe(Pd.transpose(-1, -2))  # not C-contiguous
