@@ -60,7 +60,7 @@ def parse():
     ap.add_argument("--oracle-solve", type=int, default=1, help="oracle DM solve estimate on the host")
     ap.add_argument("--sweep", type=int, default=96, help="batched-sweep instances (0 = skip)")
     ap.add_argument("--sweep-streams", type=int, default=16)
-    ap.add_argument("--c64-mesh", type=int, default=0, help="nb=64 superlattice mesh (0 = skip)")
+    ap.add_argument("--c64-mesh", type=int, default=144, help="nb=64 superlattice mesh (0 = skip)")
     return ap.parse_args()
 
 

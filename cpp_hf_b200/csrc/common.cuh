@@ -252,66 +252,6 @@ struct GridBarrier {
         __syncthreads();
         return ok_sh != 0;
     }
-
-    // Barrier whose last arriving block first sums the (NV x nblocks) partials
-    // `part` (block b's values at part[NV b .. NV b + NV)) with all its threads in
-    // a fixed order and writes the NV totals to `tot`, so the released
-    // blocks read NV numbers instead of all partials.  Ordering uses
-    // release/acquire atomics (no full fences).
-    template <int NV = 2>
-    __device__ bool wait_reduce(const double* part, int nblocks, double* tot) {
-        __syncthreads();
-        __shared__ int ok_sh, last_sh;
-        if (threadIdx.x == 0) {
-            ok_sh = 1;
-            last_sh = 0;
-            if (ld_acquire_u32(&sync[2]) != 0u) {
-                ok_sh = 0;
-            } else {
-                unsigned arrived;
-                asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(arrived) : "l"(&sync[0]) : "memory");
-                last_sh = (arrived == (unsigned)nblocks - 1) ? 1 : 0;
-            }
-        }
-        __syncthreads();
-        if (!ok_sh) return false;
-        if (last_sh) {
-            // the whole block loads the partials at once (one L2 round trip for
-            // up to blockDim blocks) and sums them with a fixed tree
-            __shared__ double red_wr[32 * NV];
-            double sv[NV];
-#pragma unroll
-            for (int v = 0; v < NV; ++v) sv[v] = 0.0;
-            for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
-#pragma unroll
-                for (int v = 0; v < NV; ++v) sv[v] += __ldcg(&part[NV * b + v]);
-            }
-            block_sum<NV>(sv, red_wr);
-            if (threadIdx.x == 0) {
-#pragma unroll
-                for (int v = 0; v < NV; ++v) __stcg(&tot[v], sv[v]);
-                sync[0] = 0u;
-                asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(&sync[1]) : "memory");
-            }
-        } else if (threadIdx.x == 0) {
-            long long spins = 0;
-            while (ld_acquire_u32(&sync[1]) == gen) {
-                if (ld_acquire_u32(&sync[2]) != 0u) {
-                    ok_sh = 0;
-                    break;
-                }
-                if (++spins > limit) {
-                    give_up();
-                    ok_sh = 0;
-                    break;
-                }
-                if (kPollSleepNs) __nanosleep(kPollSleepNs);
-            }
-        }
-        if (threadIdx.x == 0) gen += 1;
-        __syncthreads();
-        return ok_sh != 0;
-    }
 };
 
 }  // namespace cpphf

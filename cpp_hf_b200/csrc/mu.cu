@@ -63,7 +63,7 @@ struct MuArgs {
     int maxiter;
     int mode;  // 0 bisection (utils.hpp:49-75), 1 in-loop newton (utils.hpp:79-116)
     double* mu_out;
-    double* part;     // [grid][2] min/max, [grid][kMuNV] partials, [2][kMuNV] totals
+    double* part;     // [grid][2] min/max, then two [grid][kMuNV] partials buffers (by round parity)
     unsigned* sync;   // [0] count [1] gen [2] error
     unsigned* err;    // device error word (may be null)
     long long spin_limit;  // grid-barrier poll limit
@@ -87,18 +87,21 @@ __device__ __forceinline__ void cluster_sync_all() {
 }
 
 // Grid-wide synchronisation of the mu kernel.  CLUSTER = false: a cooperative
-// grid with the bounded software barrier (the last block to arrive sums the
-// partials).  CLUSTER = true: one thread-block cluster (kMuCluster CTAs) with
-// the hardware cluster barrier; every CTA sums the partials itself in the
-// same fixed order, so the partials are double-buffered by round parity (a
-// CTA may start writing round r + 1 while another still reads round r).
+// grid with the bounded software barrier; CLUSTER = true: one thread-block
+// cluster (kMuCluster CTAs) with the hardware cluster barrier.  In both, every
+// block sums all blocks' partials itself in the same fixed order after the
+// barrier (a few KB from L2; no block waits for a last arriver's reduction), so
+// the partials are double-buffered by round parity (a block may start writing
+// round r + 1 while another still reads round r).
 template <bool CLUSTER>
 struct MuSync {
     GridBarrier bar;
-    double* ctot;  // shared totals (cluster form)
-    __device__ void init(const MuArgs& a, double* sh) {
+    double* ctot;  // shared totals
+    double (*red)[32 * kMuNV];  // the kernel's block_sum scratch
+    __device__ void init(const MuArgs& a, double* sh, double (*scratch)[32 * kMuNV]) {
         if (!CLUSTER) bar.init(a.sync, a.spin_limit, a.err);
         ctot = sh;
+        red = scratch;
     }
     __device__ bool all() {
         if constexpr (CLUSTER) {
@@ -110,29 +113,34 @@ struct MuSync {
     }
     // the partials buffer of a round
     __device__ double* partials(double* part, int round) const {
-        if constexpr (CLUSTER) return part + (size_t)(round & 1) * kMuNV * gridDim.x;
-        return part;
+        return part + (size_t)(round & 1) * kMuNV * gridDim.x;
     }
     // every block's NV partials summed (fixed order); null if a wait gave up
     template <int NV>
-    __device__ const double* reduce(const double* part, int G, double* tot) {
+    __device__ const double* reduce(const double* part, int G) {
         if constexpr (CLUSTER) {
             cluster_sync_all();
-            if (threadIdx.x < NV) {
-                double s = 0.0;
-                for (int b = 0; b < G; ++b) s += __ldcg(&part[NV * b + threadIdx.x]);
-                ctot[threadIdx.x] = s;
-            }
-            __syncthreads();
-            return ctot;
         } else {
-            return bar.wait_reduce<NV>(part, G, tot) ? tot : nullptr;
+            if (!bar.wait()) return nullptr;
         }
+        // all threads load the partials at once (one L2 round trip), then the
+        // block's fixed tree: every block forms the same totals
+        double v[NV];
+#pragma unroll
+        for (int j = 0; j < NV; ++j) v[j] = 0.0;
+        for (int b = threadIdx.x; b < G; b += blockDim.x) {
+#pragma unroll
+            for (int j = 0; j < NV; ++j) v[j] += __ldcg(&part[NV * b + j]);
+        }
+        block_sum<NV>(v, *red);
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int j = 0; j < NV; ++j) ctot[j] = v[j];
+        }
+        __syncthreads();
+        return ctot;
     }
-    __device__ double load(const double* t, int j) const {
-        if constexpr (CLUSTER) return t[j];
-        return __ldcg(&t[j]);
-    }
+    __device__ double load(const double* t, int j) const { return t[j]; }
 };
 
 template <bool CLUSTER>
@@ -140,7 +148,7 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
     __shared__ double red[32 * kMuNV];  // block_sum<kMuNV> scratch (32 doubles per value)
     __shared__ double ctot_sh[kMuNV];
     MuSync<CLUSTER> bar;
-    bar.init(a, ctot_sh);
+    bar.init(a, ctot_sh, &red);
     const int G = gridDim.x;
     const unsigned nb = (unsigned)a.nb;
     const unsigned n = (unsigned)a.n;
@@ -210,8 +218,7 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
     }
     const double Tfd = Tj + 1.0e-12;  // fermidirac_scalar(x, Tj) = expit(-x / (Tj + 1e-12))
     const double invTfd = 1.0 / Tfd, invTj = 1.0 / Tj;
-    double* part0 = a.part + 2 * G;                 // [G][kMuNV] partials (two such buffers in the cluster form)
-    double* tots = part0 + (size_t)kMuNV * G * (CLUSTER ? 2 : 1);  // [2][kMuNV] totals, by round parity
+    double* part0 = a.part + 2 * G;  // two [G][kMuNV] partials buffers, by round parity
     __shared__ double bc_tot[kMuNV];
     int round = 0;
     if (a.mode == 0) {
@@ -278,7 +285,7 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
 #pragma unroll
                 for (int j = 0; j < kMuNV; ++j) __stcg(&part[kMuNV * blockIdx.x + j], v[j]);
             }
-            const double* tot = bar.template reduce<kMuNV>(part, G, tots + (round & 1) * kMuNV);
+            const double* tot = bar.template reduce<kMuNV>(part, G);
             if (!tot) {
                 ok = false;
                 return;
@@ -326,7 +333,7 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
                 __stcg(&part[2 * blockIdx.x], v[0]);
                 __stcg(&part[2 * blockIdx.x + 1], v[1]);
             }
-            const double* tot = bar.template reduce<2>(part, G, tots + (round & 1) * kMuNV);
+            const double* tot = bar.template reduce<2>(part, G);
             ++round;
             if (!tot) {
                 ok = false;
@@ -446,7 +453,7 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
                 __stcg(&part[2 * blockIdx.x], v[0]);
                 __stcg(&part[2 * blockIdx.x + 1], v[1]);
             }
-            const double* tot = bar.template reduce<2>(part, G, tots + (it & 1) * kMuNV);
+            const double* tot = bar.template reduce<2>(part, G);
             if (!tot) {
                 if (blockIdx.x == 0 && threadIdx.x == 0) *a.mu_out = NAN;
                 return;
@@ -501,13 +508,13 @@ int max_coop_grid() {
 // launches.  Every GPU that loads the library holds it until the process
 // exits; every call shares it.
 // ---------------------------------------------------------------------------
-constexpr size_t kMuNoAllocScratchBytes = 64 + sizeof(double) * ((2 + kMuNV) * (size_t)kMuMaxGrid + 2 * kMuNV);
+constexpr size_t kMuNoAllocScratchBytes = 64 + sizeof(double) * ((2 + 2 * kMuNV) * (size_t)kMuMaxGrid + 2 * kMuNV);
 static __device__ __align__(256) unsigned char g_mu_noalloc_scratch[kMuNoAllocScratchBytes];
 
 }  // namespace
 
 size_t mu_workspace_bytes(int64_t, int64_t) {
-    return 64 + sizeof(double) * ((2 + kMuNV) * (size_t)kMuMaxGrid + 2 * kMuNV);
+    return 64 + sizeof(double) * ((2 + 2 * kMuNV) * (size_t)kMuMaxGrid + 2 * kMuNV);
 }
 
 int mu_solve(const double* eps, const double* w, int64_t nk, int64_t nb, double target,
