@@ -3,8 +3,8 @@
 //
 // Every block owns a contiguous slice of the (nk*nb) eigenvalues.  Per round
 // a block reduces its slice (fixed tree) into partials, the grid meets at a
-// bounded barrier whose last block sums the partials in block order, and every
-// block replays the reference's scalar update rule itself, so the whole grid
+// bounded barrier, every block sums all blocks' partials with the same fixed
+// tree and replays the reference's scalar update rule itself, so the whole grid
 // agrees on (lo, hi, mu).  The results are those of the reference's fixed
 // iteration counts (30 bisection steps by default, mu_maxiter Newton steps).
 // Bisection runs its first levels as exact multisection rounds, then finds
@@ -26,6 +26,7 @@ namespace {
 
 constexpr int kMuThreads = 1024;
 constexpr int kMuMaxGrid = 1024;
+constexpr int kMuCache = 2;                           // eigenvalues a thread keeps in registers across rounds
 constexpr int64_t kMuOneBlockMax = 32768;             // eigenvalues handled by a single CTA
 constexpr int kMuCluster = 8;                         // CTAs of the cluster form (portable cluster size)
 // eigenvalues handled by one cluster: up to 8 per thread and round; beyond
@@ -155,6 +156,32 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
     const unsigned per = (n + G - 1) / G;  // (k, band) elements per block
     const unsigned e0 = blockIdx.x * per;
     const unsigned e1 = min(n, e0 + per);
+    // The thread's eigenvalues and weights (band-major), loaded once: with at
+    // most kMuCache of them per thread (the cooperative grid at the sizes the
+    // solvers run) they stay in registers for every round; otherwise every
+    // round reloads them.  Same elements, same order either way.
+    const bool cached = (per + blockDim.x - 1) / blockDim.x <= (unsigned)kMuCache;  // grid-uniform
+    double cw[kMuCache], ce[kMuCache];
+#pragma unroll
+    for (int u = 0; u < kMuCache; ++u) {
+        const unsigned i = e0 + threadIdx.x + u * blockDim.x;
+        cw[u] = 0.0;
+        ce[u] = 0.0;
+        if (cached && i < e1) band_major(a, i, nb, cw[u], ce[u]);
+    }
+    auto for_each_elem = [&](auto&& f) {
+        if (cached) {
+#pragma unroll
+            for (int u = 0; u < kMuCache; ++u)
+                if (e0 + threadIdx.x + u * blockDim.x < e1) f(cw[u], ce[u]);
+        } else {
+            for (unsigned i = e0 + threadIdx.x; i < e1; i += blockDim.x) {
+                double wk, e;
+                band_major(a, i, nb, wk, e);
+                f(wk, e);
+            }
+        }
+    };
 
     // 1. global min / max of eps
     double lmin = INFINITY, lmax = -INFINITY;
@@ -263,9 +290,7 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
             double v[kMuNV];
 #pragma unroll
             for (int j = 0; j < kMuNV; ++j) v[j] = 0.0;
-            for (unsigned i = e0 + threadIdx.x; i < e1; i += blockDim.x) {
-                double wk, e;
-                band_major(a, i, nb, wk, e);
+            for_each_elem([&](double wk, double e) {
 #pragma unroll
                 for (int j = 0; j < kMuNV; ++j) {
                     if (j < nodes) {
@@ -278,7 +303,7 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
                             v[j] += wk * expit(-(e - mid[j]) / Tfd);
                     }
                 }
-            }
+            });
             block_sum<kMuNV>(v, red);
             double* part = bar.partials(part0, round);
             if (threadIdx.x == 0) {
@@ -315,9 +340,7 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
         // count N and slope Z = dN/dmu at one mu (one grid round)
         auto count_round = [&](double m, double& N, double& Z) {
             double v[2] = {0.0, 0.0};
-            for (unsigned i = e0 + threadIdx.x; i < e1; i += blockDim.x) {
-                double wk, e;
-                band_major(a, i, nb, wk, e);
+            for_each_elem([&](double wk, double e) {
                 const double xa = (m - e) * invTfd;
                 if (xa >= kFdOne) {
                     v[0] += wk;
@@ -326,7 +349,7 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
                     v[0] += wk * pf;
                     v[1] += wk * pf * (1.0 - pf) * invTfd;
                 }
-            }
+            });
             block_sum<2>(v, red);
             double* part = bar.partials(part0, round);
             if (threadIdx.x == 0) {
@@ -433,9 +456,7 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
         double mu1 = NAN, lo1 = NAN, hi1 = NAN;  // state one iteration back
         for (int it = 0; it < a.maxiter; ++it) {
             double v[2] = {0.0, 0.0};
-            for (unsigned i = e0 + threadIdx.x; i < e1; i += blockDim.x) {
-                double wk, e;
-                band_major(a, i, nb, wk, e);
+            for_each_elem([&](double wk, double e) {
                 // p = expit((mu - e) / Tj) is exactly 1 (and p (1 - p) exactly 0)
                 // for an argument >= 37; below -50 both terms are dropped
                 const double xa = (mu - e) * invTj;
@@ -446,7 +467,7 @@ __global__ void __launch_bounds__(kMuThreads) k_mu(MuArgs a) {
                     v[0] += wk * p;
                     v[1] += wk * p * (1.0 - p) / Tj;
                 }
-            }
+            });
             block_sum<2>(v, red);
             double* part = bar.partials(part0, it);
             if (threadIdx.x == 0) {
