@@ -338,7 +338,8 @@ __global__ void __launch_bounds__(kThreads, 3)
 // accepted trial, U is the one its pass stored (Ua or Ub) and eps_work its
 // diagonal (copied from ew2 when it was the second of its pass); for the
 // fallback step both are computed here, U from d by elimination.
-// Dynamic shared memory: sD (d, then U) | sF | sQ, TILE double2 each.
+// Dynamic shared memory: four tiles (two (U, Q) stages for an accepted trial;
+// d, Ft and Q for the fallback step).
 template <int NB>
 __global__ void __launch_bounds__(kThreads) k_retract_small(double2* Q, const double2* __restrict__ dQ,
                                                             const double2* __restrict__ Ft, double* __restrict__ ew,
@@ -360,6 +361,51 @@ __global__ void __launch_bounds__(kThreads) k_retract_small(double2* Q, const do
     const bool from_b = S->accepted != 0 && S->slot == 1;  // grid-uniform
     const double2* Uacc = from_b ? Ub : Ua;
     const int64_t ntiles = (nk + G::KT - 1) / G::KT;
+    if (!need_diag) {
+        // accepted trial: Q <- Q U with U read back, two shared-memory stages of
+        // (U, Q) tiles filled by cp.async (the next tile's copies in flight
+        // while the current one is multiplied)
+        auto issue = [&](int64_t t, int st) {
+            const int64_t k0 = t * G::KT;
+            const int nkt = (int)((nk - k0) < G::KT ? (nk - k0) : G::KT);
+            tile_load_async<NB>(dyn + 2 * st * G::TILE, Uacc + (size_t)k0 * G::NB2, nkt);
+            tile_load_async<NB>(dyn + (2 * st + 1) * G::TILE, Q + (size_t)k0 * G::NB2, nkt);
+        };
+        if ((int64_t)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+        cp_async_commit();
+        int it = 0;
+        for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
+            const int st = it & 1;
+            if (t + (int64_t)gridDim.x < ntiles) issue(t + gridDim.x, st ^ 1);  // freed last iteration
+            cp_async_commit();
+            cp_async_wait_prev();
+            __syncthreads();
+            const double2* su = dyn + 2 * st * G::TILE + grp * G::MS;
+            double2* sq = dyn + (2 * st + 1) * G::TILE;
+            const int64_t k0 = t * G::KT;
+            const int nkt = (int)((nk - k0) < G::KT ? (nk - k0) : G::KT);
+            if (grp < nkt && r < NB) {
+                const int64_t k = k0 + grp;
+                if (from_b) ew[k * NB + r] = ew2[k * NB + r];
+                double2* qrow = sq + grp * G::MS + r * G::LD;
+                double2 qr[NB];
+#pragma unroll
+                for (int l = 0; l < NB; ++l) qr[l] = qrow[l];
+#pragma unroll
+                for (int j = 0; j < NB; ++j) {
+                    double2 acc = mk(0.0, 0.0);
+#pragma unroll
+                    for (int l = 0; l < NB; ++l) cfma(acc, qr[l], su[l * G::LD + j]);
+                    qrow[j] = acc;  // only this thread reads or writes this row
+                }
+            }
+            __syncthreads();
+            tile_store<NB>(Q + (size_t)k0 * G::NB2, sq, nkt);
+            __syncthreads();
+        }
+        return;
+    }
+    // fallback step: U(tau_final) by elimination and its eps_work
     for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int64_t k0 = t * G::KT;
         const int nkt = (int)((nk - k0) < G::KT ? (nk - k0) : G::KT);
@@ -437,30 +483,34 @@ __global__ void __launch_bounds__(kThreadsE, 4) k_pr_beta_small(const double2* _
     const int64_t nrow = nk * NB, nel = nrow * NB;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    // matrix terms, one element per thread (coalesced), kUnrollE elements of a
-    // thread loaded before any is used
-    auto term = [&](int64_t e, double2 g, double2 gp) {
+    // matrix terms, one element per thread (coalesced): kUnrollE elements of a
+    // thread have all their loads (G, G_prev, both eigenvalues, the weight)
+    // issued before any is used, so a batch costs one memory latency
+    struct Ld {
+        double2 g, gp;
+        double er, ej, wk;
+    };
+    auto load = [&](int64_t e) {
         const int64_t row = e / NB, k = row / NB;
         const int j = (int)(e - row * NB);
-        const double gap = eps[row] - eps[k * NB + j];
+        return Ld{Gc[e], Gp[e], eps[row], eps[k * NB + j], w[k]};
+    };
+    auto term = [&](const Ld& x) {
+        const double gap = x.er - x.ej;
         const double rb = rsqrt(gap * gap + lam2);
-        const double2 d = mk(g.x * rb, g.y * rb);
-        const double wk = w[k];
-        v[0] += wk * ((g.x * d.x + g.y * d.y) - (gp.x * d.x + gp.y * d.y));
-        v[1] += wk * (gp.x * gp.x + gp.y * gp.y);
+        const double2 d = mk(x.g.x * rb, x.g.y * rb);
+        v[0] += x.wk * ((x.g.x * d.x + x.g.y * d.y) - (x.gp.x * d.x + x.gp.y * d.y));
+        v[1] += x.wk * (x.gp.x * x.gp.x + x.gp.y * x.gp.y);
     };
     int64_t e = tid;
     for (; e + (kUnrollE - 1) * stride < nel; e += kUnrollE * stride) {
-        double2 g[kUnrollE], gp[kUnrollE];
+        Ld x[kUnrollE];
 #pragma unroll
-        for (int u = 0; u < kUnrollE; ++u) {
-            g[u] = Gc[e + u * stride];
-            gp[u] = Gp[e + u * stride];
-        }
+        for (int u = 0; u < kUnrollE; ++u) x[u] = load(e + u * stride);
 #pragma unroll
-        for (int u = 0; u < kUnrollE; ++u) term(e + u * stride, g[u], gp[u]);
+        for (int u = 0; u < kUnrollE; ++u) term(x[u]);
     }
-    for (; e < nel; e += stride) term(e, Gc[e], Gp[e]);
+    for (; e < nel; e += stride) term(load(e));
     // occupation terms, one row per thread
     for (int64_t row = tid; row < nrow; row += stride) {
         const double wk = w[row / NB];
@@ -502,30 +552,35 @@ __global__ void __launch_bounds__(kThreadsE, 4) k_direction_small(const double2*
     const int64_t nrow = nk * NB, nel = nrow * NB;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    // matrix terms, one element per thread (coalesced), kUnrollE elements of a
-    // thread loaded before any is used
-    auto term = [&](int64_t e, double2 g, double2 q) {
+    // matrix terms, one element per thread (coalesced): kUnrollE elements of a
+    // thread have all their loads (G, the previous direction, both
+    // eigenvalues, the weight) issued before any is used
+    const bool use_prev = beta != 0.0;
+    struct Ld {
+        double2 g, q;
+        double er, ej, wk;
+    };
+    auto load = [&](int64_t e) {
         const int64_t row = e / NB, k = row / NB;
         const int j = (int)(e - row * NB);
-        const double gap = eps[row] - eps[k * NB + j];
-        const double rb = rsqrt(gap * gap + lam2);
-        const double2 d = mk(g.x * rb + beta * q.x, g.y * rb + beta * q.y);
-        dQ[e] = d;
-        v[0] += w[k] * (d.x * d.x + d.y * d.y);
+        return Ld{Gc[e], use_prev ? dQp[e] : mk(0.0, 0.0), eps[row], eps[k * NB + j], w[k]};
     };
-    const bool use_prev = beta != 0.0;
+    auto term = [&](int64_t e, const Ld& x) {
+        const double gap = x.er - x.ej;
+        const double rb = rsqrt(gap * gap + lam2);
+        const double2 d = mk(x.g.x * rb + beta * x.q.x, x.g.y * rb + beta * x.q.y);
+        dQ[e] = d;
+        v[0] += x.wk * (d.x * d.x + d.y * d.y);
+    };
     int64_t e = tid;
     for (; e + (kUnrollE - 1) * stride < nel; e += kUnrollE * stride) {
-        double2 g[kUnrollE], q[kUnrollE];
+        Ld x[kUnrollE];
 #pragma unroll
-        for (int u = 0; u < kUnrollE; ++u) {
-            g[u] = Gc[e + u * stride];
-            q[u] = use_prev ? dQp[e + u * stride] : mk(0.0, 0.0);
-        }
+        for (int u = 0; u < kUnrollE; ++u) x[u] = load(e + u * stride);
 #pragma unroll
-        for (int u = 0; u < kUnrollE; ++u) term(e + u * stride, g[u], q[u]);
+        for (int u = 0; u < kUnrollE; ++u) term(e + u * stride, x[u]);
     }
-    for (; e < nel; e += stride) term(e, Gc[e], use_prev ? dQp[e] : mk(0.0, 0.0));
+    for (; e < nel; e += stride) term(e, load(e));
     // occupation terms, one row per thread
     for (int64_t row = tid; row < nrow; row += stride) {
         const double wk = w[row / NB];
@@ -750,8 +805,8 @@ int dm_small_retract(double2* Q, const double2* dQ, const double2* Ft, double* e
                      const double2* Ua, const double2* Ub, int64_t nk, int nb, const DmScalars* S, cudaStream_t st) {
 #define X(N)                                                                                                      \
     small_attrs<N>();                                                                                             \
-    k_retract_small<N><<<tiles_grid(nk, Geo<N>::KT, 16 * num_sms()), kThreads, 3 * sizeof(double2) * Geo<N>::TILE, \
-                         st>>>(Q, dQ, Ft, ew, ew2, Ua, Ub, nk, S);                                                \
+    k_retract_small<N><<<tiles_grid(nk, Geo<N>::KT, resident_ctas(k_retract_small<N>, 4 * sizeof(double2) * Geo<N>::TILE)), \
+                         kThreads, 4 * sizeof(double2) * Geo<N>::TILE, st>>>(Q, dQ, Ft, ew, ew2, Ua, Ub, nk, S);        \
     CPPHF_LAUNCH_CHECK("retract");
     SMALL_DISPATCH(nb, X)
 #undef X
