@@ -621,24 +621,38 @@ __global__ void __launch_bounds__(kThreads) k_scf_residuals_small(const double2*
                                                                   const double* __restrict__ w, int64_t nk,
                                                                   DmScalars* S, double2* __restrict__ comm_out) {
     using G = Geo<NB>;
-    __shared__ double2 sF[G::TILE];
-    __shared__ double2 sD[G::TILE];
+    extern __shared__ __align__(16) double2 dyn[];
     __shared__ double red[64];
     const int grp = threadIdx.x / G::GS, r = threadIdx.x % G::GS;
     const int64_t ntiles = (nk + G::KT - 1) / G::KT;
     double v[2] = {0.0, 0.0};
-    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    // two shared-memory stages of (F, D) tiles filled by cp.async: the next
+    // tile's copies are in flight while the current one is reduced
+    auto issue = [&](int64_t t, int st) {
+        const int64_t k0 = t * G::KT;
+        const int nkt = (int)((nk - k0) < G::KT ? (nk - k0) : G::KT);
+        tile_load_async<NB>(dyn + 2 * st * G::TILE, F + (size_t)k0 * G::NB2, nkt);
+        tile_load_async<NB>(dyn + (2 * st + 1) * G::TILE, D + (size_t)k0 * G::NB2, nkt);
+    };
+    if ((int64_t)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+    cp_async_commit();
+    int it = 0;
+    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
+        const int st = it & 1;
+        if (t + (int64_t)gridDim.x < ntiles) issue(t + gridDim.x, st ^ 1);  // freed last iteration
+        cp_async_commit();
+        double2* sF = dyn + 2 * st * G::TILE;
+        const double2* sD = dyn + (2 * st + 1) * G::TILE;
         const int64_t k0 = t * G::KT;
         const int nkt = (int)((nk - k0) < G::KT ? (nk - k0) : G::KT);
         const int n = nkt * G::NB2;
-        tile_load<NB>(sF, F + (size_t)k0 * G::NB2, nkt);
-        tile_load<NB>(sD, D + (size_t)k0 * G::NB2, nkt);
-        double2 pv[G::PER];
+        double2 pv[G::PER];  // loaded while the stage's copies land
 #pragma unroll
         for (int u = 0; u < G::PER; ++u) {
             const int e = threadIdx.x + u * kThreads;
             pv[u] = e < n ? Pn[(size_t)k0 * G::NB2 + e] : mk(0.0, 0.0);
         }
+        cp_async_wait_prev();
         __syncthreads();
 #pragma unroll
         for (int u = 0; u < G::PER; ++u) {
@@ -698,6 +712,7 @@ void small_attrs() {
         raise_smem(k_dens_occ<NB, true>);
         raise_smem(k_dens_occ<NB, false>);
         raise_smem(k_retract_small<NB>);
+        raise_smem(k_scf_residuals_small<NB>);
     });
 }
 
@@ -742,7 +757,9 @@ int dm_small_density(const double2* Q, const double* p, double2* P, int64_t nk, 
 int scf_small_residuals(const double2* F, const double2* D, const double2* Pn, const double* w, int64_t nk, int nb,
                         DmScalars* S, double2* comm_out, cudaStream_t st) {
 #define X(N)                                                                                                      \
-    k_scf_residuals_small<N><<<tiles_grid(nk, Geo<N>::KT, kDmMaxPartials), kThreads, 0, st>>>(F, D, Pn, w, nk, S, \
+    small_attrs<N>();                                                                                              \
+    k_scf_residuals_small<N><<<tiles_grid(nk, Geo<N>::KT, resident_ctas(k_scf_residuals_small<N>, 4 * sizeof(double2) * Geo<N>::TILE)), \
+                               kThreads, 4 * sizeof(double2) * Geo<N>::TILE, st>>>(F, D, Pn, w, nk, S,          \
                                                                                              comm_out);            \
     CPPHF_LAUNCH_CHECK("scf residuals");
     SMALL_DISPATCH(nb, X)
