@@ -252,7 +252,7 @@ __global__ void __launch_bounds__(kPackMaxThreads, 2)
     constexpr int N = N1 * N2;
     constexpr int kLanes = N1 > N2 ? N1 : N2;  // line lanes: blockDim.x = kLanes * CBp
     constexpr int NE = N / kLanes;             // epilogue points per thread (ky = a + kLanes e)
-    constexpr int EB = 4;                      // epilogue points whose loads are issued together
+    constexpr int EB = 2;                      // epilogue points whose loads are issued together (4 and 6: more spills, slower)
     extern __shared__ __align__(16) unsigned char smem_dyn[];
     __shared__ double red[32];
     unsigned char* smem_raw = align128(smem_dyn);
