@@ -45,14 +45,15 @@ __device__ __forceinline__ double expit(double x) {
 // FROM_EW = false: the occupations are given in p (read, not written).
 // The Q tiles come through two shared-memory stages filled by cp.async (the
 // next tile's copies in flight while the current one is processed).
-// Dynamic shared memory: sQ stage 0 | sQ stage 1 | sX, TILE double2 each.
+// Dynamic shared memory: sQ stage 0 | sQ stage 1, TILE double2 each; the
+// product X = Q diag(p) Q^H of a tile replaces its Q stage once every row of Q
+// has been read.
 template <int NB, bool FROM_EW>
 __global__ void __launch_bounds__(kThreads) k_dens_occ(const double2* __restrict__ Q, const double* __restrict__ ew,
                                                        const double* __restrict__ mu, double T_r, double* __restrict__ p,
                                                        double2* __restrict__ P, int64_t nk) {
     using G = Geo<NB>;
     extern __shared__ __align__(16) double2 dyn[];
-    double2* sX = dyn + 2 * G::TILE;
     __shared__ double sp[G::KT * NB];
     const int grp = threadIdx.x / G::GS, r = threadIdx.x % G::GS;
     const double m = FROM_EW ? *mu : 0.0;
@@ -83,7 +84,9 @@ __global__ void __launch_bounds__(kThreads) k_dens_occ(const double2* __restrict
         }
         cp_async_wait_prev();
         __syncthreads();
-        if (grp < nkt && r < NB) {
+        const bool live = grp < nkt && r < NB;
+        double2 xr[NB];
+        if (live) {
             const double2* q = sQ + grp * G::MS;
             const double* pk = sp + grp * NB;
             double2 qr[NB];
@@ -94,8 +97,14 @@ __global__ void __launch_bounds__(kThreads) k_dens_occ(const double2* __restrict
                 double2 acc = mk(0.0, 0.0);
 #pragma unroll
                 for (int l = 0; l < NB; ++l) cfmac(acc, qr[l], q[j * G::LD + l]);
-                sX[grp * G::MS + r * G::LD + j] = acc;
+                xr[j] = acc;
             }
+        }
+        __syncthreads();  // every row of Q is read: X takes the stage's place
+        double2* sX = sQ;
+        if (live) {
+#pragma unroll
+            for (int j = 0; j < NB; ++j) sX[grp * G::MS + r * G::LD + j] = xr[j];
         }
         __syncthreads();
         const int n = nkt * G::NB2;
@@ -701,7 +710,7 @@ __global__ void __launch_bounds__(kThreads) k_scf_residuals_small(const double2*
 }
 
 template <int NB>
-constexpr size_t kDensSmem = 3 * sizeof(double2) * Geo<NB>::TILE;  // two Q stages + the product tile
+constexpr size_t kDensSmem = 2 * sizeof(double2) * Geo<NB>::TILE;  // two Q stages (X replaces its Q)
 
 template <int NB>
 void small_attrs() {
