@@ -164,9 +164,12 @@ __device__ __forceinline__ void row_cayley(const double2* d, double tau, int r, 
 
 // Two Cayley factors U(tau_a), U(tau_b) of the same d in lockstep: one pivot
 // publication (both rows) and one group barrier per step for both
-// eliminations, so their dependent FP64 chains interleave.  Each result takes
-// the same operations row_cayley performs for its tau.  `piv` holds
-// 2 * 4 * NB values per group.
+// eliminations, so their dependent FP64 chains interleave.  With M = I + tau d/2,
+// U = M^{-1} (I - tau d/2) = 2 M^{-1} - I: the elimination runs on [M | I],
+// whose right-hand block has filled in only columns 0..pp when pivot pp is
+// eliminated, so each step updates pp + 1 right-hand columns instead of nb.
+// M = I + (skew-Hermitian) is well conditioned and the elimination needs no
+// pivoting.  `piv` holds 2 * 4 * NB values per group.
 template <int NB, int LD>
 __device__ __forceinline__ void row_cayley2(const double2* d, double tau_a, double tau_b, int r, double2* piv,
                                             double2 (&ua)[NB], double2 (&ub)[NB], unsigned mask) {
@@ -178,9 +181,9 @@ __device__ __forceinline__ void row_cayley2(const double2* d, double tau_a, doub
         const double2 a = cscale(dv, ha), b = cscale(dv, hb);
         const double one = (j == r) ? 1.0 : 0.0;
         ma[j] = mk(one + a.x, a.y);
-        ua[j] = mk(one - a.x, -a.y);
         mb[j] = mk(one + b.x, b.y);
-        ub[j] = mk(one - b.x, -b.y);
+        ua[j] = mk(one, 0.0);  // right-hand block: row r of I, then of M^{-1}
+        ub[j] = mk(one, 0.0);
     }
 #pragma unroll
     for (int pp = 0; pp < NB; ++pp) {
@@ -192,7 +195,7 @@ __device__ __forceinline__ void row_cayley2(const double2* d, double tau_a, doub
                 slot[2 * NB + j] = mb[j];
             }
 #pragma unroll
-            for (int j = 0; j < NB; ++j) {
+            for (int j = 0; j <= pp; ++j) {
                 slot[NB + j] = ua[j];
                 slot[3 * NB + j] = ub[j];
             }
@@ -209,7 +212,7 @@ __device__ __forceinline__ void row_cayley2(const double2* d, double tau_a, doub
                 mb[j] = cmul(mb[j], rb);
             }
 #pragma unroll
-            for (int j = 0; j < NB; ++j) {
+            for (int j = 0; j <= pp; ++j) {
                 ua[j] = cmul(ua[j], ra);
                 ub[j] = cmul(ub[j], rb);
             }
@@ -221,11 +224,17 @@ __device__ __forceinline__ void row_cayley2(const double2* d, double tau_a, doub
                 mb[j] = csub(mb[j], cmul(fb, slot[2 * NB + j]));
             }
 #pragma unroll
-            for (int j = 0; j < NB; ++j) {
+            for (int j = 0; j <= pp; ++j) {
                 ua[j] = csub(ua[j], cmul(fa, slot[NB + j]));
                 ub[j] = csub(ub[j], cmul(fb, slot[3 * NB + j]));
             }
         }
+    }
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {  // U = 2 M^{-1} - I
+        const double one = (j == r) ? 1.0 : 0.0;
+        ua[j] = mk(2.0 * ua[j].x - one, 2.0 * ua[j].y);
+        ub[j] = mk(2.0 * ub[j].x - one, 2.0 * ub[j].y);
     }
     __syncwarp(mask);  // the last step's readers are done before `piv` is reused
 }
