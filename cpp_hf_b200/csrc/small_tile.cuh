@@ -113,13 +113,15 @@ __device__ __forceinline__ unsigned group_mask(int lane) {
 // ---------------------------------------------------------------------------
 // Cayley unitary U(tau) = (I + tau d/2)^{-1} (I - tau d/2) of one k-point by
 // Gauss-Jordan elimination, one row per thread (row r of the result in u[]).
-// At step pp the owner of row pp publishes its unscaled row through the
-// group's shared slot `piv` (two slots, used alternately, so one group barrier
-// per step suffices); every thread then forms the reciprocal pivot itself:
-// the owner scales its row, the others subtract (f / pivot) times the
-// published row, touching only the columns right of the pivot in the left
-// block (the ones left of it are already zero).  The rows end normalised, so
-// u[] is row r of U.  `piv` holds 2 * 2 * NB values per group.
+// At step pp the owner of row pp publishes its row through the group's shared
+// slot `piv` (two slots, used alternately, so one group barrier per step
+// suffices); every thread then forms the reciprocal pivot itself, and the
+// others subtract (f / pivot) times the published row, touching only the
+// columns right of the pivot in the left block (the ones left of it are
+// already zero).  The pivot rows are not normalised during the elimination:
+// the owner's update is the same instruction stream with f = 0, so a group
+// never diverges, and every row is divided by its own pivot (kept from its
+// step) at the end.  `piv` holds 2 * 2 * NB values per group.
 // ---------------------------------------------------------------------------
 template <int NB, int LD>
 __device__ __forceinline__ void row_cayley(const double2* d, double tau, int r, double2* piv, double2 (&u)[NB],
@@ -133,6 +135,7 @@ __device__ __forceinline__ void row_cayley(const double2* d, double tau, int r, 
         mrow[j] = mk(one + a.x, a.y);
         u[j] = mk(one - a.x, -a.y);
     }
+    double2 rs = mk(1.0, 0.0);  // reciprocal of this row's pivot
 #pragma unroll
     for (int pp = 0; pp < NB; ++pp) {
         double2* slot = piv + (pp & 1) * 2 * NB;
@@ -146,19 +149,16 @@ __device__ __forceinline__ void row_cayley(const double2* d, double tau, int r, 
         const double2 pv = slot[pp];
         const double inv = 1.0 / (pv.x * pv.x + pv.y * pv.y);
         const double2 rp = mk(pv.x * inv, -pv.y * inv);
-        if (r == pp) {
+        const bool own = r == pp;
+        if (own) rs = rp;
+        const double2 f = own ? mk(0.0, 0.0) : cmul(mrow[pp], rp);
 #pragma unroll
-            for (int j = pp + 1; j < NB; ++j) mrow[j] = cmul(mrow[j], rp);
+        for (int j = pp + 1; j < NB; ++j) mrow[j] = csub(mrow[j], cmul(f, slot[j]));
 #pragma unroll
-            for (int j = 0; j < NB; ++j) u[j] = cmul(u[j], rp);
-        } else {
-            const double2 f = cmul(mrow[pp], rp);
-#pragma unroll
-            for (int j = pp + 1; j < NB; ++j) mrow[j] = csub(mrow[j], cmul(f, slot[j]));
-#pragma unroll
-            for (int j = 0; j < NB; ++j) u[j] = csub(u[j], cmul(f, slot[NB + j]));
-        }
+        for (int j = 0; j < NB; ++j) u[j] = csub(u[j], cmul(f, slot[NB + j]));
     }
+#pragma unroll
+    for (int j = 0; j < NB; ++j) u[j] = cmul(u[j], rs);
     __syncwarp(mask);  // the last step's readers are done before `piv` is reused
 }
 
@@ -168,6 +168,8 @@ __device__ __forceinline__ void row_cayley(const double2* d, double tau, int r, 
 // U = M^{-1} (I - tau d/2) = 2 M^{-1} - I: the elimination runs on [M | I],
 // whose right-hand block has filled in only columns 0..pp when pivot pp is
 // eliminated, so each step updates pp + 1 right-hand columns instead of nb.
+// As in row_cayley the pivot rows stay unnormalised (no divergence in the
+// group) and each row is divided by its pivot at the end.
 // M = I + (skew-Hermitian) is well conditioned and the elimination needs no
 // pivoting.  `piv` holds 2 * 4 * NB values per group.
 template <int NB, int LD>
@@ -182,9 +184,10 @@ __device__ __forceinline__ void row_cayley2(const double2* d, double tau_a, doub
         const double one = (j == r) ? 1.0 : 0.0;
         ma[j] = mk(one + a.x, a.y);
         mb[j] = mk(one + b.x, b.y);
-        ua[j] = mk(one, 0.0);  // right-hand block: row r of I, then of M^{-1}
+        ua[j] = mk(one, 0.0);  // right-hand block: row r of I, then of M^{-1} times the pivot
         ub[j] = mk(one, 0.0);
     }
+    double2 rsa = mk(1.0, 0.0), rsb = mk(1.0, 0.0);  // reciprocals of this row's pivots
 #pragma unroll
     for (int pp = 0; pp < NB; ++pp) {
         double2* slot = piv + (pp & 1) * 4 * NB;
@@ -205,36 +208,33 @@ __device__ __forceinline__ void row_cayley2(const double2* d, double tau_a, doub
         const double ia = 1.0 / (pa.x * pa.x + pa.y * pa.y);
         const double ib = 1.0 / (pb.x * pb.x + pb.y * pb.y);
         const double2 ra = mk(pa.x * ia, -pa.y * ia), rb = mk(pb.x * ib, -pb.y * ib);
-        if (r == pp) {
+        const bool own = r == pp;
+        if (own) {
+            rsa = ra;
+            rsb = rb;
+        }
+        const double2 fa = own ? mk(0.0, 0.0) : cmul(ma[pp], ra);
+        const double2 fb = own ? mk(0.0, 0.0) : cmul(mb[pp], rb);
 #pragma unroll
-            for (int j = pp + 1; j < NB; ++j) {
-                ma[j] = cmul(ma[j], ra);
-                mb[j] = cmul(mb[j], rb);
-            }
+        for (int j = pp + 1; j < NB; ++j) {
+            ma[j] = csub(ma[j], cmul(fa, slot[j]));
+            mb[j] = csub(mb[j], cmul(fb, slot[2 * NB + j]));
+        }
 #pragma unroll
-            for (int j = 0; j <= pp; ++j) {
-                ua[j] = cmul(ua[j], ra);
-                ub[j] = cmul(ub[j], rb);
-            }
-        } else {
-            const double2 fa = cmul(ma[pp], ra), fb = cmul(mb[pp], rb);
-#pragma unroll
-            for (int j = pp + 1; j < NB; ++j) {
-                ma[j] = csub(ma[j], cmul(fa, slot[j]));
-                mb[j] = csub(mb[j], cmul(fb, slot[2 * NB + j]));
-            }
-#pragma unroll
-            for (int j = 0; j <= pp; ++j) {
-                ua[j] = csub(ua[j], cmul(fa, slot[NB + j]));
-                ub[j] = csub(ub[j], cmul(fb, slot[3 * NB + j]));
-            }
+        for (int j = 0; j <= pp; ++j) {
+            ua[j] = csub(ua[j], cmul(fa, slot[NB + j]));
+            ub[j] = csub(ub[j], cmul(fb, slot[3 * NB + j]));
         }
     }
+    // U = 2 M^{-1} - I, row r of M^{-1} being the right-hand row over its pivot
+    rsa = mk(2.0 * rsa.x, 2.0 * rsa.y);
+    rsb = mk(2.0 * rsb.x, 2.0 * rsb.y);
 #pragma unroll
-    for (int j = 0; j < NB; ++j) {  // U = 2 M^{-1} - I
+    for (int j = 0; j < NB; ++j) {
         const double one = (j == r) ? 1.0 : 0.0;
-        ua[j] = mk(2.0 * ua[j].x - one, 2.0 * ua[j].y);
-        ub[j] = mk(2.0 * ub[j].x - one, 2.0 * ub[j].y);
+        const double2 a = cmul(ua[j], rsa), b = cmul(ub[j], rsb);
+        ua[j] = mk(a.x - one, a.y);
+        ub[j] = mk(b.x - one, b.y);
     }
     __syncwarp(mask);  // the last step's readers are done before `piv` is reused
 }
