@@ -275,28 +275,24 @@ __global__ void __launch_bounds__(kThreads, 3)
         const int rr = r < NB ? r : 0;
         const int64_t k = k0 + grp;
         if (grp < nkt) {
+            // thread r: column r of U(tau_a) and U(tau_b) (transposed eliminations)
             double2 ua[NB], ub[NB];
-            if (two)
-                row_cayley2<NB, G::LD>(sD + grp * G::MS, tau_a, tau_b, rr, sPiv + grp * 8 * NB, ua, ub, mask);
-            else
-                row_cayley<NB, G::LD>(sD + grp * G::MS, tau_a, rr, sPiv + grp * 8 * NB, ua, mask);
+            double da, db;
+            if (two) {
+                row_cayley2<NB, G::LD, true>(sD + grp * G::MS, tau_a, tau_b, rr, sPiv + grp * 8 * NB, ua, ub, mask);
+                col_diag_uhfu<NB, G::LD, true>(sF + grp * G::MS, ua, ub, da, db);
+            } else {
+                row_cayley<NB, G::LD, true>(sD + grp * G::MS, tau_a, rr, sPiv + grp * 8 * NB, ua, mask);
+                col_diag_uhfu<NB, G::LD, false>(sF + grp * G::MS, ua, ub, da, db);
+            }
             // (the elimination ends with a group barrier after its last read of d)
             if (live) {
 #pragma unroll
                 for (int j = 0; j < NB; ++j) {
-                    sA[grp * G::MS + r * G::LD + j] = ua[j];
-                    if (two) sB[grp * G::MS + r * G::LD + j] = ub[j];
+                    sA[grp * G::MS + j * G::LD + r] = ua[j];
+                    if (two) sB[grp * G::MS + j * G::LD + r] = ub[j];
                 }
             }
-        }
-        __syncwarp();  // a group's U rows (one warp) are complete before its diag reads them
-        if (grp < nkt) {
-            double2 ftj[NB];
-#pragma unroll
-            for (int l = 0; l < NB; ++l) ftj[l] = sF[grp * G::MS + rr * G::LD + l];
-            const double da = row_diag_uhfu<NB, G::GS, G::LD>(ftj, sA + grp * G::MS, r, mask, live);
-            double db = 0.0;
-            if (two) db = row_diag_uhfu<NB, G::GS, G::LD>(ftj, sB + grp * G::MS, r, mask, live);
             if (live) {
                 const double wk = w[k], pk = p[k * NB + r], dpk = d_p[k * NB + r];
                 ew[k * NB + r] = da;

@@ -211,7 +211,9 @@ __global__ void __launch_bounds__(kHqlThreads, 4) k_eigh_hql(const double2* __re
 
     // ---- 3. implicit QL ----
     constexpr double kEps = 2.220446049250313e-16;
-#pragma unroll 1
+    // l unrolled: the sweeps for eigenvalue l address d, e and z at
+    // compile-time offsets and issue only the rotations of rows l..NB-2
+#pragma unroll
     for (int l = 0; l < NB; ++l) {
         int iter = 0;
         while (true) {

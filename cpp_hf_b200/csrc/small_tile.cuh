@@ -122,15 +122,18 @@ __device__ __forceinline__ unsigned group_mask(int lane) {
 // the owner's update is the same instruction stream with f = 0, so a group
 // never diverges, and every row is divided by its own pivot (kept from its
 // step) at the end.  `piv` holds 2 * 2 * NB values per group.
+// With TR the elimination runs on the transposed system (thread r reads
+// column r of d): U^T = (M^T)^{-1} N^T with M, N = I +- tau d/2 commuting,
+// and M^T = I + (skew-Hermitian) as well, so u[] is column r of U.
 // ---------------------------------------------------------------------------
-template <int NB, int LD>
+template <int NB, int LD, bool TR = false>
 __device__ __forceinline__ void row_cayley(const double2* d, double tau, int r, double2* piv, double2 (&u)[NB],
                                            unsigned mask) {
     double2 mrow[NB];
     const double h = 0.5 * tau;
 #pragma unroll
     for (int j = 0; j < NB; ++j) {
-        const double2 a = cscale(d[r * LD + j], h);
+        const double2 a = cscale(TR ? d[j * LD + r] : d[r * LD + j], h);
         const double one = (j == r) ? 1.0 : 0.0;
         mrow[j] = mk(one + a.x, a.y);
         u[j] = mk(one - a.x, -a.y);
@@ -169,17 +172,18 @@ __device__ __forceinline__ void row_cayley(const double2* d, double tau, int r, 
 // whose right-hand block has filled in only columns 0..pp when pivot pp is
 // eliminated, so each step updates pp + 1 right-hand columns instead of nb.
 // As in row_cayley the pivot rows stay unnormalised (no divergence in the
-// group) and each row is divided by its pivot at the end.
+// group) and each row is divided by its pivot at the end; with TR the results
+// are columns of U (U^T = 2 (M^T)^{-1} - I).
 // M = I + (skew-Hermitian) is well conditioned and the elimination needs no
 // pivoting.  `piv` holds 2 * 4 * NB values per group.
-template <int NB, int LD>
+template <int NB, int LD, bool TR = false>
 __device__ __forceinline__ void row_cayley2(const double2* d, double tau_a, double tau_b, int r, double2* piv,
                                             double2 (&ua)[NB], double2 (&ub)[NB], unsigned mask) {
     double2 ma[NB], mb[NB];
     const double ha = 0.5 * tau_a, hb = 0.5 * tau_b;
 #pragma unroll
     for (int j = 0; j < NB; ++j) {
-        const double2 dv = d[r * LD + j];
+        const double2 dv = TR ? d[j * LD + r] : d[r * LD + j];
         const double2 a = cscale(dv, ha), b = cscale(dv, hb);
         const double one = (j == r) ? 1.0 : 0.0;
         ma[j] = mk(one + a.x, a.y);
@@ -237,6 +241,29 @@ __device__ __forceinline__ void row_cayley2(const double2* d, double tau_a, doub
         ub[j] = mk(b.x - one, b.y);
     }
     __syncwarp(mask);  // the last step's readers are done before `piv` is reused
+}
+
+// diag(U^H Ft U) of one or two factors when thread r holds column r of each
+// (ua, ub): diag_r = sum_j Re[conj(U_jr) (Ft U)_jr], Ft read row by row from
+// the group's padded tile `sf` (one read serves both factors; no shuffles).
+template <int NB, int LD, bool TWO>
+__device__ __forceinline__ void col_diag_uhfu(const double2* sf, const double2 (&ua)[NB], const double2 (&ub)[NB],
+                                              double& da, double& db) {
+    double sa = 0.0, sb = 0.0;
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+        double2 ya = mk(0.0, 0.0), yb = mk(0.0, 0.0);
+#pragma unroll
+        for (int l = 0; l < NB; ++l) {
+            const double2 f = sf[j * LD + l];
+            cfma(ya, f, ua[l]);
+            if (TWO) cfma(yb, f, ub[l]);
+        }
+        sa += ua[j].x * ya.x + ua[j].y * ya.y;
+        if (TWO) sb += ub[j].x * yb.x + ub[j].y * yb.y;
+    }
+    da = sa;
+    db = sb;
 }
 
 // diag(U^H Ft U) for the group: thread j holds Ft row j (ftj); it forms

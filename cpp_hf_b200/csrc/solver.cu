@@ -54,8 +54,6 @@ __global__ void k_hermitize(const double2* src, double2* dst, int64_t nk, int nb
     }
 }
 
-__global__ void k_set_scalar(double* p, double v) { *p = v; }
-
 // level-shifted SCF occupations (solver_scf.hpp:127-141):
 // shifted = eps + ls (1 - f(eps - mu_raw)); output occ = f(shifted - mu) later.
 __device__ __forceinline__ double expit_d(double x) {
