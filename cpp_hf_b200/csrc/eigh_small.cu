@@ -50,13 +50,14 @@ __device__ __forceinline__ double2 shfl2(double2 v, int src, unsigned mask) {
     return mk(__shfl_sync(mask, v.x, src), __shfl_sync(mask, v.y, src));
 }
 
-// three CTAs per SM (<= 168 registers): with the QL loop over l unrolled, four
-// CTAs (128 registers) spill and run 4 % slower.  Splitting the kernel after
-// the reduction (a QL kernel at 96 registers and five CTAs per SM, the
-// tridiagonal and Z handed over through V) was slower still: the QL is bound by
-// its instruction count more than by latency.
+// four CTAs per SM (<= 128 registers, a few spilled): on the Fock matrices of
+// an SCF solve (192 x 192, nb = 8) 194 us per call against 220 us at three CTAs
+// without spills (on random Hermitian matrices three CTAs are 4 % faster).
+// Splitting the kernel after the reduction (a QL kernel at 96 registers and
+// five CTAs per SM, the tridiagonal and Z handed over through V) was slower:
+// the QL is bound by its instruction count more than by latency.
 template <int NB>
-__global__ void __launch_bounds__(kHqlThreads, 3) k_eigh_hql(const double2* __restrict__ M, double* __restrict__ w,
+__global__ void __launch_bounds__(kHqlThreads, 4) k_eigh_hql(const double2* __restrict__ M, double* __restrict__ w,
                                                           double2* __restrict__ Vout, int64_t batch, int mode) {
     constexpr int GS = HqlGeo<NB>::GS;
     const int lane = threadIdx.x & 31;
