@@ -26,6 +26,16 @@ struct DmScalars {
     double part[3 * kDmMaxPartials];
 };
 
+// One element of the SCF linear mix D + mixing (P_new - D) (solver_scf.hpp:395-401),
+// shared by the mix kernel and the residual pass that fuses it, so both round alike;
+// the Hermitian part of the mix m is then (m_ij + conj m_ji) / 2 per element.
+__device__ __forceinline__ double2 scf_mix_elem(double2 d, double2 pn, double mixing) {
+    return cadd(d, cscale(csub(pn, d), mixing));
+}
+__device__ __forceinline__ double2 scf_mix_herm(double2 mij, double2 mji) {
+    return mk(0.5 * (mij.x + mji.x), 0.5 * (mij.y - mji.y));
+}
+
 int dm_check_nb(int64_t nb);
 int dm_density(const double2* Q, const double* p, double2* P, int64_t nk, int nb, cudaStream_t st);
 int dm_rotate(const double2* U, const double2* M, double2* Out, double* eps, int64_t nk, int nb, cudaStream_t st);

@@ -617,14 +617,17 @@ unsigned rows_grid(int64_t nrow) {
 // ---------------------------------------------------------------------------
 // SCF residuals (solver_scf.hpp:64-75, 224-242): sum_k w_k |Pn - D|_F^2 and
 // sum_k w_k |F D - D F|_F^2 into S->grad_norm and S->lam_pc; the commutator
-// itself goes to comm_out when given (the C-DIIS residual).
+// itself goes to comm_out when given (the C-DIIS residual).  With mix_out the
+// pass also writes the linear mix herm(D + mixing (Pn - D)) (solver_scf.hpp:
+// 395-401) from the tiles it holds; mix_out may be D (each tile is read into
+// shared memory before it is written back).
 // ---------------------------------------------------------------------------
 template <int NB>
-__global__ void __launch_bounds__(kThreads) k_scf_residuals_small(const double2* __restrict__ F,
-                                                                  const double2* __restrict__ D,
+__global__ void __launch_bounds__(kThreads, 3) k_scf_residuals_small(const double2* __restrict__ F, const double2* D,
                                                                   const double2* __restrict__ Pn,
                                                                   const double* __restrict__ w, int64_t nk,
-                                                                  DmScalars* S, double2* __restrict__ comm_out) {
+                                                                  DmScalars* S, double2* __restrict__ comm_out,
+                                                                  double2* mix_out, double mixing) {
     using G = Geo<NB>;
     extern __shared__ __align__(16) double2 dyn[];
     __shared__ double red[64];
@@ -696,6 +699,32 @@ __global__ void __launch_bounds__(kThreads) k_scf_residuals_small(const double2*
             __syncthreads();
             tile_store<NB>(comm_out + (size_t)k0 * G::NB2, sF, nkt);
         }
+        if (mix_out) {  // grid-uniform
+            __syncthreads();  // every read of F (or of the commutator tile) is done
+            double2* sM = sF;  // the elementwise mix m = D + mixing (Pn - D)
+#pragma unroll
+            for (int u = 0; u < G::PER; ++u) {
+                const int e = threadIdx.x + u * kThreads;
+                if (e < n) {
+                    const int kl = e / G::NB2, rem = e - kl * G::NB2, i = rem / NB, j = rem - i * NB;
+                    const int o = kl * G::MS + i * G::LD + j;
+                    sM[o] = scf_mix_elem(sD[o], pv[u], mixing);
+                }
+            }
+            __syncthreads();
+            double2* sH = dyn + (2 * st + 1) * G::TILE;  // D's stage takes the Hermitian part
+#pragma unroll
+            for (int u = 0; u < G::PER; ++u) {
+                const int e = threadIdx.x + u * kThreads;
+                if (e < n) {
+                    const int kl = e / G::NB2, rem = e - kl * G::NB2, i = rem / NB, j = rem - i * NB;
+                    sH[kl * G::MS + i * G::LD + j] =
+                        scf_mix_herm(sM[kl * G::MS + i * G::LD + j], sM[kl * G::MS + j * G::LD + i]);
+                }
+            }
+            __syncthreads();
+            tile_store<NB>(mix_out + (size_t)k0 * G::NB2, sH, nkt);
+        }
         __syncthreads();
     }
     double out[2];
@@ -760,12 +789,13 @@ int dm_small_density(const double2* Q, const double* p, double2* P, int64_t nk, 
 }
 
 int scf_small_residuals(const double2* F, const double2* D, const double2* Pn, const double* w, int64_t nk, int nb,
-                        DmScalars* S, double2* comm_out, cudaStream_t st) {
+                        DmScalars* S, double2* comm_out, double2* mix_out, double mixing, cudaStream_t st) {
 #define X(N)                                                                                                      \
     small_attrs<N>();                                                                                              \
     k_scf_residuals_small<N><<<tiles_grid(nk, Geo<N>::KT, resident_ctas(k_scf_residuals_small<N>, 4 * sizeof(double2) * Geo<N>::TILE)), \
                                kThreads, 4 * sizeof(double2) * Geo<N>::TILE, st>>>(F, D, Pn, w, nk, S,          \
-                                                                                             comm_out);            \
+                                                                                             comm_out, mix_out,    \
+                                                                                             mixing);              \
     CPPHF_LAUNCH_CHECK("scf residuals");
     SMALL_DISPATCH(nb, X)
 #undef X

@@ -7,9 +7,10 @@
 namespace cpphf {
 
 bool dm_small_supported(int nb);
-// SCF density and commutator residuals (S->grad_norm, S->lam_pc), commutator to comm_out if given
+// SCF density and commutator residuals (S->grad_norm, S->lam_pc), commutator to comm_out if given;
+// with mix_out (which may be D itself) also the linear mix herm(D + mixing (Pn - D))
 int scf_small_residuals(const double2* F, const double2* D, const double2* Pn, const double* w, int64_t nk, int nb,
-                        DmScalars* S, double2* comm_out, cudaStream_t st);
+                        DmScalars* S, double2* comm_out, double2* mix_out, double mixing, cudaStream_t st);
 // P = herm(Q diag(p) Q^H) from given occupations p
 int dm_small_density(const double2* Q, const double* p, double2* P, int64_t nk, int nb, cudaStream_t st);
 int dm_small_dens_occ(const double2* Q, const double* ew, const double* mu, double T_r, double* p, double2* P,

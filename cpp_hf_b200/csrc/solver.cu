@@ -136,9 +136,9 @@ __global__ void k_scf_mix(const double2* D, const double2* Pn, double mixing, do
         const int j = i + r;
         const size_t ij = (size_t)k * nb * nb + (size_t)i * nb + j, ji = (size_t)k * nb * nb + (size_t)j * nb + i;
         const double2 dij = D[ij], dji = D[ji];
-        const double2 a = cadd(dij, cscale(csub(Pn[ij], dij), mixing));
-        const double2 b = cadd(dji, cscale(csub(Pn[ji], dji), mixing));
-        const double2 h = mk(0.5 * (a.x + b.x), 0.5 * (a.y - b.y));
+        const double2 a = scf_mix_elem(dij, Pn[ij], mixing);
+        const double2 b = scf_mix_elem(dji, Pn[ji], mixing);
+        const double2 h = scf_mix_herm(a, b);
         out[ij] = h;
         out[ji] = cconj(h);
     }
@@ -962,6 +962,10 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
     const bool sl_path = K->sl && (K->sl->fock_active || K->sl->hartree_active);
     const bool scf_graphs =
         cfg->graphs != 0 && guard.capturable && acc == 0 && !project && !Dpre && !sl_path && !scf_block;
+    // On that path with nb <= 8 the residual pass also writes the mix into D (the
+    // residuals need the unmixed D only in the same pass; a converged iteration
+    // overwrites D with P_new), so no separate mix runs.
+    const bool fuse_mix = scf_graphs && dm_small_supported(nb);
     IterGraphs sgr;
     bool pending_mix = false;
     while (k < max_iter && !converged) {
@@ -972,7 +976,8 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
             // the new C-DIIS residual goes to the slot after the newest entry
             // (overwriting the oldest when the ring is full)
             if (dm_small_supported(nb))
-                CPPHF_TRY(scf_small_residuals(F, D, Pn, K->w2d, nk, nb, S, comm_out, st));
+                CPPHF_TRY(scf_small_residuals(F, D, Pn, K->w2d, nk, nb, S, comm_out, fuse_mix ? D : nullptr,
+                                              cfg->mixing, st));
             else if (warp)
                 k_scf_residuals<true><<<tgrid, 32 * kWarpTeams, rsmem, st>>>(F, D, Pn, K->w2d, nk, nb, S, comm_out);
             else
@@ -983,7 +988,7 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
         };
         const int lw = low ? 1 : 0;
         bool replayed = false;
-        if (scf_graphs && pending_mix && d_hermitian) {
+        if (scf_graphs && (pending_mix || fuse_mix) && d_hermitian) {
             if (!sgr.exec[0][lw] && !sgr.failed[0][lw]) {
                 cudaGraph_t g = nullptr;
                 if (cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
@@ -1100,7 +1105,9 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
                 lam = 0.0;
             CPPHF_TRY(mix_into_D(D, Pn, lam));
         } else if (scf_graphs) {
-            pending_mix = true;  // the next iteration (or the finalisation) mixes first
+            // the next iteration (or the finalisation) mixes first, unless the
+            // residual pass has mixed D already
+            if (!fuse_mix) pending_mix = true;
         } else {
             CPPHF_TRY(mix_into_D(D, Pn, cfg->mixing));
         }
