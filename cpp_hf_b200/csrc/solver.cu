@@ -886,11 +886,17 @@ int solve_scf(const cpphf_kernel* K, const cpphf_scf_config* cfg, const double2*
         // unchanged copy of eps and returns mu_raw itself
         if (cfg->level_shift != 0.0)
             CPPHF_TRY(mu_solve(e_occ, K->w2d, nk, nb, n_e, mu_fin, K->T, 30, 0, mu_fin, mws, L.mu_bytes, st));
-        k_fermi<<<grid_for(nk * nb, 256), 256, 0, st>>>(e_occ, mu_fin, K->T, occ, nk * nb);
-        CPPHF_LAUNCH_CHECK("fermi");
-        // dm_density writes (X + X^H) / 2, exactly Hermitian: only a projector needs
-        // the hermitisation again
-        CPPHF_TRY(dm_density(V, occ, Pout, nk, nb, st));
+        // the density pass writes (X + X^H) / 2, exactly Hermitian: only a projector
+        // needs the hermitisation again
+        if (dm_small_supported(nb)) {
+            // occupations expit((mu - e) / (T + 1e-12)) formed inside the density pass:
+            // the same value as k_fermi's expit(-(e - mu) / (T + 1e-12)), one launch less
+            CPPHF_TRY(dm_small_dens_occ(V, e_occ, mu_fin, K->T + 1.0e-12, occ, Pout, nk, nb, st));
+        } else {
+            k_fermi<<<grid_for(nk * nb, 256), 256, 0, st>>>(e_occ, mu_fin, K->T, occ, nk * nb);
+            CPPHF_LAUNCH_CHECK("fermi");
+            CPPHF_TRY(dm_density(V, occ, Pout, nk, nb, st));
+        }
         if (project) {
             CPPHF_TRY(call_project(project, puser, Pout, K, st));
             CPPHF_TRY(hermitize(Pout, Pout, nk, nb, st));
