@@ -242,7 +242,14 @@ __global__ void __launch_bounds__(kThreads) k_rot_grad(const double2* __restrict
 // (tau_b), U(tau_a) to Ua and U(tau_b) to Ub; S->slot records which one the
 // accepted trial left.  `bt` is the index of the pass's first trial; a pair
 // past bt_max evaluates one trial.
-// Dynamic shared memory: sD (d, then U(tau_a)) | sF | sB (U(tau_b)), TILE double2 each.
+// Dynamic shared memory: sD | sF, one d tile and one Ft tile, refilled by
+// cp.async as soon as they are consumed: each thread copies its column of d
+// into registers before the eliminations, so the next tile's d streams in
+// during the eliminations and the diagonal, and the next Ft (needed only after
+// the next tile's eliminations) streams in once the diagonal has read this
+// one.  Each thread holds a column of U after the transposed eliminations and
+// stores it directly: for a fixed row j the group's eight columns are one
+// contiguous 128-byte run of U.
 template <int NB>
 __global__ void __launch_bounds__(kThreads, 3)
     k_trial2_small(const double2* __restrict__ dQ, const double2* __restrict__ Ft, const double* __restrict__ p,
@@ -254,8 +261,6 @@ __global__ void __launch_bounds__(kThreads, 3)
     extern __shared__ __align__(16) double2 dyn[];
     double2* sD = dyn;
     double2* sF = dyn + G::TILE;
-    double2* sB = dyn + 2 * G::TILE;
-    double2* sA = sD;  // U(tau_a) replaces d once both eliminations have read it
     __shared__ double2 sPiv[G::KT * 8 * NB];
     __shared__ double red[128];
     const int grp = threadIdx.x / G::GS, r = threadIdx.x % G::GS;
@@ -264,55 +269,67 @@ __global__ void __launch_bounds__(kThreads, 3)
     const double tau_b = tau_a * shrink;
     const bool two = bt + 1 < bt_max;  // grid-uniform
     const int64_t ntiles = (nk + G::KT - 1) / G::KT;
+    auto tile_k = [&](int64_t t) { return (int)((nk - t * G::KT) < G::KT ? (nk - t * G::KT) : G::KT); };
+    if ((int64_t)blockIdx.x < ntiles) {
+        tile_load_async<NB>(sD, dQ + (size_t)blockIdx.x * G::KT * G::NB2, tile_k(blockIdx.x));
+        tile_load_async<NB>(sF, Ft + (size_t)blockIdx.x * G::KT * G::NB2, tile_k(blockIdx.x));
+    }
+    cp_async_commit();
     double v[4] = {0.0, 0.0, 0.0, 0.0};
     for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int64_t k0 = t * G::KT;
-        const int nkt = (int)((nk - k0) < G::KT ? (nk - k0) : G::KT);
-        tile_load<NB>(sD, dQ + (size_t)k0 * G::NB2, nkt);
-        tile_load<NB>(sF, Ft + (size_t)k0 * G::NB2, nkt);
-        __syncthreads();
+        const int nkt = tile_k(t);
+        const int64_t tn = t + gridDim.x;  // this block's next tile
+        cp_async_wait_all();
+        __syncthreads();  // this tile's d and Ft have landed
         const bool live = grp < nkt && r < NB;
         const int rr = r < NB ? r : 0;
         const int64_t k = k0 + grp;
+        double2 dv[NB];  // column rr of d (transposed eliminations)
+#pragma unroll
+        for (int j = 0; j < NB; ++j) dv[j] = sD[grp * G::MS + j * G::LD + rr];
+        __syncthreads();  // every column of d is in registers: the next d may land
+        if (tn < ntiles) tile_load_async<NB>(sD, dQ + (size_t)tn * G::KT * G::NB2, tile_k(tn));
+        cp_async_commit();
+        double2 ua[NB], ub[NB];
+        double da = 0.0, db = 0.0;
         if (grp < nkt) {
-            // thread r: column r of U(tau_a) and U(tau_b) (transposed eliminations)
-            double2 ua[NB], ub[NB];
-            double da, db;
+            // thread r: column r of U(tau_a) and U(tau_b)
             if (two) {
-                row_cayley2<NB, G::LD, true>(sD + grp * G::MS, tau_a, tau_b, rr, sPiv + grp * 8 * NB, ua, ub, mask);
+                row_cayley2_reg<NB>(dv, tau_a, tau_b, rr, sPiv + grp * 8 * NB, ua, ub, mask);
                 col_diag_uhfu<NB, G::LD, true>(sF + grp * G::MS, ua, ub, da, db);
             } else {
-                row_cayley<NB, G::LD, true>(sD + grp * G::MS, tau_a, rr, sPiv + grp * 8 * NB, ua, mask);
+                row_cayley_reg<NB>(dv, tau_a, rr, sPiv + grp * 8 * NB, ua, mask);
                 col_diag_uhfu<NB, G::LD, false>(sF + grp * G::MS, ua, ub, da, db);
             }
-            // (the elimination ends with a group barrier after its last read of d)
-            if (live) {
+        }
+        __syncthreads();  // every read of Ft is done: the next Ft may land
+        if (tn < ntiles) tile_load_async<NB>(sF, Ft + (size_t)tn * G::KT * G::NB2, tile_k(tn));
+        cp_async_commit();
+        if (live) {
+            // both factors go out, so that the retraction reads the accepted one
+            double2* ga = Ua + (size_t)k * G::NB2 + r;
 #pragma unroll
-                for (int j = 0; j < NB; ++j) {
-                    sA[grp * G::MS + j * G::LD + r] = ua[j];
-                    if (two) sB[grp * G::MS + j * G::LD + r] = ub[j];
-                }
+            for (int j = 0; j < NB; ++j) ga[j * NB] = ua[j];
+            if (two) {
+                double2* gb = Ub + (size_t)k * G::NB2 + r;
+#pragma unroll
+                for (int j = 0; j < NB; ++j) gb[j * NB] = ub[j];
             }
-            if (live) {
-                const double wk = w[k], pk = p[k * NB + r], dpk = d_p[k * NB + r];
-                ew[k * NB + r] = da;
-                const double pa = fmin(fmax(pk - tau_a * dpk, OCC_CLIP), 1.0 - OCC_CLIP);
-                v[0] += wk * pa * da;
-                v[1] -= wk * (pa * log(pa) + (1.0 - pa) * log1p(-pa));
-                if (two) {
-                    ew2[k * NB + r] = db;
-                    const double pb = fmin(fmax(pk - tau_b * dpk, OCC_CLIP), 1.0 - OCC_CLIP);
-                    v[2] += wk * pb * db;
-                    v[3] -= wk * (pb * log(pb) + (1.0 - pb) * log1p(-pb));
-                }
+            const double wk = w[k], pk = p[k * NB + r], dpk = d_p[k * NB + r];
+            ew[k * NB + r] = da;
+            const double pa = fmin(fmax(pk - tau_a * dpk, OCC_CLIP), 1.0 - OCC_CLIP);
+            v[0] += wk * pa * da;
+            v[1] -= wk * (pa * log(pa) + (1.0 - pa) * log1p(-pa));
+            if (two) {
+                ew2[k * NB + r] = db;
+                const double pb = fmin(fmax(pk - tau_b * dpk, OCC_CLIP), 1.0 - OCC_CLIP);
+                v[2] += wk * pb * db;
+                v[3] -= wk * (pb * log(pb) + (1.0 - pb) * log1p(-pb));
             }
         }
-        __syncthreads();
-        // both factors go out, so that the retraction reads the accepted one
-        tile_store<NB>(Ua + (size_t)k0 * G::NB2, sA, nkt);
-        if (two) tile_store<NB>(Ub + (size_t)k0 * G::NB2, sB, nkt);
-        __syncthreads();
     }
+    cp_async_wait_all();
     double out[4];
     if (reduce_last_block<4>(v, S->part, &S->counter, out, red) && threadIdx.x == 0) {
         const double Tc = fmax(T_r, 1.0e-14);
@@ -844,9 +861,11 @@ int dm_small_trial2(const double2* dQ, const double2* Ft, const double* p, const
                     int bt, int bt_max, double fallback, DmScalars* S, cudaStream_t st) {
 #define X(N)                                                                                                  \
     small_attrs<N>();                                                                                         \
-    k_trial2_small<N><<<tiles_grid(nk, Geo<N>::KT, 3 * kDmMaxPartials / 4), kThreads,                         \
-                        3 * sizeof(double2) * Geo<N>::TILE, st>>>(dQ, Ft, p, d_p, w, ew, ew2, Ua, Ub, nk, T_r, \
-                                                                 shrink, bt, bt_max, fallback, S);             \
+    k_trial2_small<N><<<tiles_grid(nk, Geo<N>::KT,                                                            \
+                                   std::min(3 * kDmMaxPartials / 4,                                           \
+                                            (int)resident_ctas(k_trial2_small<N>, 2 * sizeof(double2) * Geo<N>::TILE))), \
+                        kThreads, 2 * sizeof(double2) * Geo<N>::TILE, st>>>(dQ, Ft, p, d_p, w, ew, ew2, Ua, Ub, nk, \
+                                                                           T_r, shrink, bt, bt_max, fallback, S); \
     CPPHF_LAUNCH_CHECK("trial pair");
     SMALL_DISPATCH(nb, X)
 #undef X

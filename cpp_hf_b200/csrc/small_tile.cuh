@@ -72,6 +72,7 @@ __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 // every group but the most recent one has landed
 __device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 // tile_load as asynchronous copies into the padded layout (committed by the caller)
 template <int NB>
@@ -126,14 +127,15 @@ __device__ __forceinline__ unsigned group_mask(int lane) {
 // column r of d): U^T = (M^T)^{-1} N^T with M, N = I +- tau d/2 commuting,
 // and M^T = I + (skew-Hermitian) as well, so u[] is column r of U.
 // ---------------------------------------------------------------------------
-template <int NB, int LD, bool TR = false>
-__device__ __forceinline__ void row_cayley(const double2* d, double tau, int r, double2* piv, double2 (&u)[NB],
-                                           unsigned mask) {
+// (row_cayley_reg takes this thread's row of d, or column with TR, in registers)
+template <int NB>
+__device__ __forceinline__ void row_cayley_reg(const double2 (&dv)[NB], double tau, int r, double2* piv,
+                                               double2 (&u)[NB], unsigned mask) {
     double2 mrow[NB];
     const double h = 0.5 * tau;
 #pragma unroll
     for (int j = 0; j < NB; ++j) {
-        const double2 a = cscale(TR ? d[j * LD + r] : d[r * LD + j], h);
+        const double2 a = cscale(dv[j], h);
         const double one = (j == r) ? 1.0 : 0.0;
         mrow[j] = mk(one + a.x, a.y);
         u[j] = mk(one - a.x, -a.y);
@@ -165,6 +167,15 @@ __device__ __forceinline__ void row_cayley(const double2* d, double tau, int r, 
     __syncwarp(mask);  // the last step's readers are done before `piv` is reused
 }
 
+template <int NB, int LD, bool TR = false>
+__device__ __forceinline__ void row_cayley(const double2* d, double tau, int r, double2* piv, double2 (&u)[NB],
+                                           unsigned mask) {
+    double2 dv[NB];
+#pragma unroll
+    for (int j = 0; j < NB; ++j) dv[j] = TR ? d[j * LD + r] : d[r * LD + j];
+    row_cayley_reg<NB>(dv, tau, r, piv, u, mask);
+}
+
 // Two Cayley factors U(tau_a), U(tau_b) of the same d in lockstep: one pivot
 // publication (both rows) and one group barrier per step for both
 // eliminations, so their dependent FP64 chains interleave.  With M = I + tau d/2,
@@ -176,15 +187,14 @@ __device__ __forceinline__ void row_cayley(const double2* d, double tau, int r, 
 // are columns of U (U^T = 2 (M^T)^{-1} - I).
 // M = I + (skew-Hermitian) is well conditioned and the elimination needs no
 // pivoting.  `piv` holds 2 * 4 * NB values per group.
-template <int NB, int LD, bool TR = false>
-__device__ __forceinline__ void row_cayley2(const double2* d, double tau_a, double tau_b, int r, double2* piv,
-                                            double2 (&ua)[NB], double2 (&ub)[NB], unsigned mask) {
+template <int NB>
+__device__ __forceinline__ void row_cayley2_reg(const double2 (&dv)[NB], double tau_a, double tau_b, int r,
+                                                double2* piv, double2 (&ua)[NB], double2 (&ub)[NB], unsigned mask) {
     double2 ma[NB], mb[NB];
     const double ha = 0.5 * tau_a, hb = 0.5 * tau_b;
 #pragma unroll
     for (int j = 0; j < NB; ++j) {
-        const double2 dv = TR ? d[j * LD + r] : d[r * LD + j];
-        const double2 a = cscale(dv, ha), b = cscale(dv, hb);
+        const double2 a = cscale(dv[j], ha), b = cscale(dv[j], hb);
         const double one = (j == r) ? 1.0 : 0.0;
         ma[j] = mk(one + a.x, a.y);
         mb[j] = mk(one + b.x, b.y);
@@ -241,6 +251,15 @@ __device__ __forceinline__ void row_cayley2(const double2* d, double tau_a, doub
         ub[j] = mk(b.x - one, b.y);
     }
     __syncwarp(mask);  // the last step's readers are done before `piv` is reused
+}
+
+template <int NB, int LD, bool TR = false>
+__device__ __forceinline__ void row_cayley2(const double2* d, double tau_a, double tau_b, int r, double2* piv,
+                                            double2 (&ua)[NB], double2 (&ub)[NB], unsigned mask) {
+    double2 dv[NB];
+#pragma unroll
+    for (int j = 0; j < NB; ++j) dv[j] = TR ? d[j * LD + r] : d[r * LD + j];
+    row_cayley2_reg<NB>(dv, tau_a, tau_b, r, piv, ua, ub, mask);
 }
 
 // diag(U^H Ft U) of one or two factors when thread r holds column r of each
