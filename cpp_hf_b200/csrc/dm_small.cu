@@ -127,7 +127,12 @@ __global__ void __launch_bounds__(kThreads) k_dens_occ(const double2* __restrict
 // Ft overwrites F.
 // ---------------------------------------------------------------------------
 // Two shared-memory stages of (Q, F) tiles: the next tile's asynchronous
-// copies are in flight while the current one is processed.
+// copies are in flight while the current one is processed.  Thread r forms
+// column r of T = F Q and then column r of Ft = Q^H T from registers (the same
+// products and summation order as row by row), so T never goes through shared
+// memory; Ft's column replaces F's in the stage for the transposed reads of the
+// gradient, and Ft and G go from registers straight to global memory (a
+// group's eight columns of one row are one 128-byte run).
 // Dynamic shared memory: stage s = { sQ, sT } at dyn + 2 s TILE.
 template <int NB>
 __global__ void __launch_bounds__(kThreads) k_rot_grad(const double2* __restrict__ Q, double2* F,
@@ -156,62 +161,68 @@ __global__ void __launch_bounds__(kThreads) k_rot_grad(const double2* __restrict
         if (t + (int64_t)gridDim.x < ntiles) issue(t + gridDim.x, s ^ 1);  // stage s ^ 1 was freed last iteration
         cp_async_commit();
         cp_async_wait_prev();
-        double2* sQ = dyn + 2 * s * G::TILE;        // Q, then the gradient
-        double2* sT = dyn + (2 * s + 1) * G::TILE;  // F, then F Q, then Ft
+        const double2* sQ = dyn + 2 * s * G::TILE;  // Q
+        double2* sT = dyn + (2 * s + 1) * G::TILE;  // F, then Ft by columns
         const int64_t k0 = t * G::KT;
         const int nkt = (int)((nk - k0) < G::KT ? (nk - k0) : G::KT);
         __syncthreads();
         const bool live = grp < nkt && r < NB;
         const int64_t k = k0 + grp;
         double2* tt = sT + grp * G::MS;
-        double2* q = sQ + grp * G::MS;
-        if (live) {  // row r of F Q replaces row r of F (only this thread touches that row)
-            double2 fr[NB];
+        const double2* q = sQ + grp * G::MS;
+        const int rr = r < NB ? r : 0;
+        double2 ftc[NB];  // column rr of Ft
+        if (grp < nkt) {
+            double2 tc[NB];  // column rr of T = F Q: T_ir = sum_l F_il Q_lr
+            {
+                double2 qc[NB];
 #pragma unroll
-            for (int l = 0; l < NB; ++l) fr[l] = tt[r * G::LD + l];
+                for (int l = 0; l < NB; ++l) qc[l] = q[l * G::LD + rr];
 #pragma unroll
-            for (int j = 0; j < NB; ++j) {
+                for (int i = 0; i < NB; ++i) {
+                    double2 acc = mk(0.0, 0.0);
+#pragma unroll
+                    for (int l = 0; l < NB; ++l) cfma(acc, tt[i * G::LD + l], qc[l]);
+                    tc[i] = acc;
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < NB; ++j) {  // Ft_jr = sum_i conj(Q_ij) T_ir
                 double2 acc = mk(0.0, 0.0);
 #pragma unroll
-                for (int l = 0; l < NB; ++l) cfma(acc, fr[l], q[l * G::LD + j]);
-                tt[r * G::LD + j] = acc;
+                for (int i = 0; i < NB; ++i) cfma(acc, cconj(q[i * G::LD + j]), tc[i]);
+                ftc[j] = acc;
             }
         }
-        __syncthreads();
-        double2 ftr[NB];
-        if (live) {  // Ft = Q^H T (row r): Ft_rj = sum_l conj(Q_lr) T_lj
-#pragma unroll
-            for (int j = 0; j < NB; ++j) {
-                double2 acc = mk(0.0, 0.0);
-#pragma unroll
-                for (int l = 0; l < NB; ++l) cfma(acc, cconj(q[l * G::LD + r]), tt[l * G::LD + j]);
-                ftr[j] = acc;
-            }
-        }
-        __syncthreads();  // all reads of Q and of F Q are done
+        __syncthreads();  // every read of F is done: Ft's columns take its place
         if (live) {
 #pragma unroll
-            for (int j = 0; j < NB; ++j) tt[r * G::LD + j] = ftr[j];
+            for (int j = 0; j < NB; ++j) tt[j * G::LD + r] = ftc[j];
         }
         __syncthreads();
         if (live) {
             const double pr = p[k * NB + r];
-            double er = ftr[0].x;
+            double er = ftc[0].x;
 #pragma unroll
             for (int j = 1; j < NB; ++j)
-                if (j == r) er = ftr[j].x;
+                if (j == r) er = ftc[j].x;
             eps[k * NB + r] = er;
+            double2* gf = F + (size_t)k * G::NB2 + r;     // column r of Ft over F
+            double2* gg = Gout + (size_t)k * G::NB2 + r;  // column r of G
             double gsq = 0.0;
 #pragma unroll
             for (int j = 0; j < NB; ++j) {
+                // g_jr = [(p_r - p_j) Ft_jr - conj((p_j - p_r) Ft_rj)] / 2, the
+                // transpose partner of row r's element (its modulus is the same)
                 double2 gv = mk(0.0, 0.0);
                 if (j != r) {
                     const double pj = p[k * NB + j];
-                    const double2 aij = cscale(ftr[j], pj - pr);
-                    const double2 aji = cscale(tt[j * G::LD + r], pr - pj);
+                    const double2 aij = cscale(ftc[j], pr - pj);
+                    const double2 aji = cscale(tt[r * G::LD + j], pj - pr);
                     gv = mk(0.5 * (aij.x - aji.x), 0.5 * (aij.y + aji.y));
                 }
-                q[r * G::LD + j] = gv;  // the gradient row takes Q's place
+                gf[j * NB] = ftc[j];
+                gg[j * NB] = gv;
                 gsq += gv.x * gv.x + gv.y * gv.y;
             }
             v[0] += w[k] * gsq;
@@ -219,10 +230,7 @@ __global__ void __launch_bounds__(kThreads) k_rot_grad(const double2* __restrict
             g_p[k * NB + r] = er + T_r * (log(pv) - log1p(-pv)) - mu;
             v[1] += er * er;
         }
-        __syncthreads();
-        tile_store<NB>(F + (size_t)k0 * G::NB2, sT, nkt);
-        tile_store<NB>(Gout + (size_t)k0 * G::NB2, sQ, nkt);
-        __syncthreads();
+        __syncthreads();  // the stage is free for the copies issued next iteration
     }
     double out[2];
     if (reduce_last_block<2>(v, S->part, &S->counter, out, red) && threadIdx.x == 0) {
