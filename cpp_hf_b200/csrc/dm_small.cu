@@ -394,7 +394,9 @@ __global__ void __launch_bounds__(kThreads) k_retract_small(double2* Q, const do
     if (!need_diag) {
         // accepted trial: Q <- Q U with U read back, two shared-memory stages of
         // (U, Q) tiles filled by cp.async (the next tile's copies in flight
-        // while the current one is multiplied)
+        // while the current one is multiplied); thread r forms column r of Q U
+        // (the same products in the same order as row by row) and stores it
+        // directly (a group's eight columns of one row are one 128-byte run)
         auto issue = [&](int64_t t, int st) {
             const int64_t k0 = t * G::KT;
             const int nkt = (int)((nk - k0) < G::KT ? (nk - k0) : G::KT);
@@ -411,27 +413,25 @@ __global__ void __launch_bounds__(kThreads) k_retract_small(double2* Q, const do
             cp_async_wait_prev();
             __syncthreads();
             const double2* su = dyn + 2 * st * G::TILE + grp * G::MS;
-            double2* sq = dyn + (2 * st + 1) * G::TILE;
+            const double2* sq = dyn + (2 * st + 1) * G::TILE + grp * G::MS;
             const int64_t k0 = t * G::KT;
             const int nkt = (int)((nk - k0) < G::KT ? (nk - k0) : G::KT);
             if (grp < nkt && r < NB) {
                 const int64_t k = k0 + grp;
                 if (from_b) ew[k * NB + r] = ew2[k * NB + r];
-                double2* qrow = sq + grp * G::MS + r * G::LD;
-                double2 qr[NB];
+                double2 uc[NB];  // column r of U
 #pragma unroll
-                for (int l = 0; l < NB; ++l) qr[l] = qrow[l];
+                for (int l = 0; l < NB; ++l) uc[l] = su[l * G::LD + r];
+                double2* gq = Q + (size_t)k * G::NB2 + r;
 #pragma unroll
-                for (int j = 0; j < NB; ++j) {
+                for (int j = 0; j < NB; ++j) {  // (Q U)_jr
                     double2 acc = mk(0.0, 0.0);
 #pragma unroll
-                    for (int l = 0; l < NB; ++l) cfma(acc, qr[l], su[l * G::LD + j]);
-                    qrow[j] = acc;  // only this thread reads or writes this row
+                    for (int l = 0; l < NB; ++l) cfma(acc, sq[j * G::LD + l], uc[l]);
+                    gq[j * NB] = acc;
                 }
             }
-            __syncthreads();
-            tile_store<NB>(Q + (size_t)k0 * G::NB2, sq, nkt);
-            __syncthreads();
+            __syncthreads();  // the stage is free for the copies issued next iteration
         }
         return;
     }
